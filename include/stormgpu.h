@@ -1,0 +1,197 @@
+/*
+ * stormgpu.h -- C ABI of the B200 mapping library (libstormgpu.so).
+ *
+ * The reference mapper (SToRM) has no plugin API: its hot path is the static function
+ * process_read() in run.c, driven by the per-reference, per-strand OpenMP read loops of
+ * reads_against_references() (run.c:764-1109), with the SIMD filter reached through three
+ * function pointers (run.c:15-221):
+ *
+ *     void     (*init)(unsigned match, unsigned mismatch, unsigned gapopen,
+ *                      unsigned gapext, unsigned threshold, unsigned readlength);
+ *     unsigned (*align)(unsigned char *genome, int *pos_genome, unsigned char *read);
+ *     void     (*clean)(void);
+ *
+ * This header replaces that seam: the host driver hands the library the packed reference
+ * and the packed, tag-sorted reads, and gets back for every read the MAP_DETAIL_SIZE (4)
+ * best alignments in the exact semantics of HitInfoType (hit_map.h:17-40), from which it
+ * formats the SAM output.  All integer, all bit-exact with the reference's CPU build.
+ *
+ * Conventions: plain pointers and sizes, no exceptions, every function returns 0 on
+ * success or a negative STORMGPU_E* code; stormgpu_last_error() gives a message.  A
+ * context owns its device memory; one context per thread (calls on a context are not
+ * thread-safe, except stormgpu_submit/stormgpu_poll which the serving loop serialises).
+ *
+ * Codes are 2-bit, packed four per byte, first code in the low bits (codes.h:129-130):
+ * nucleotides A,C,G,T = 0..3, colours 0..3.  Quality levels are 2-bit (0..3), packed the
+ * same way (read_quality.h:129-133).
+ */
+#ifndef STORMGPU_H
+#define STORMGPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define STORMGPU_MAP_DETAIL   4        /* MAP_DETAIL_SIZE, util.h:30 */
+#define STORMGPU_MIN_SCORE    (-16383) /* MIN_SCORE, alignment.h:48 */
+#define STORMGPU_UNMAPPED     (-1)     /* UNMAPPED, hit_map.h:9 */
+#define STORMGPU_MAX_SEEDS    16
+#define STORMGPU_MAX_SPAN     64
+#define STORMGPU_MAX_READ_LEN 1024
+#define STORMGPU_MAX_INDELS   64
+
+/* error codes */
+#define STORMGPU_OK        0
+#define STORMGPU_EINVAL  (-1)   /* bad argument (mirrors RETURN_INPUT_ERR, load_data.h:8) */
+#define STORMGPU_ENOMEM  (-2)   /* device or host allocation failed (RETURN_MEM_ERR) */
+#define STORMGPU_ECUDA   (-3)   /* a CUDA call failed, or no usable GPU */
+#define STORMGPU_ESTATE  (-4)   /* call out of order (e.g. map before build_index) */
+#define STORMGPU_ETIMEOUT (-5)  /* a bounded device wait ran out */
+
+/* Mapping parameters: the reference's command-line options, same signs and defaults
+ * (alignment.h:24-28, alignment.h:51-52, index.h:16, main.c:302-313). */
+typedef struct stormgpu_params {
+  int32_t colour;            /* 0: storm-nucleotide, 1: storm-color */
+  int32_t match;             /* -m, > 0            (default  5) */
+  int32_t mismatch;          /* -x, <= 0           (default -4) */
+  int32_t gap_open;          /* -d, <= 0           (default -9) */
+  int32_t gap_extend;        /* -e, <= 0           (default -4) */
+  int32_t allowed_indels;    /* -i, >= 0           (default  3) */
+  int32_t min_score;         /* -t                 (default 115) */
+  int32_t min_score_filter;  /* -z                 (default 100) */
+  int32_t stdev_distance;    /* -l; <= 0 disables the repeat filter (default 100) */
+  int32_t senses;            /* bit 0: forward, bit 1: reverse complement (default 3) */
+  int32_t device;            /* CUDA device ordinal */
+} stormgpu_params;
+
+/* One alignment of a read, the fields of HitInfoType (hit_map.h:17-40).  An empty slot has
+ * ref_id = ref_start = UNMAPPED and score = MIN_SCORE, as hit_map__update initialises it. */
+typedef struct stormgpu_hit {
+  int32_t score;
+  int32_t ref_id;
+  int32_t ref_start;
+  int32_t ref_end;
+  int16_t read_start;
+  int16_t read_end;
+  int32_t sense;             /* +1 forward, -1 reverse complement, 0 empty */
+  int32_t tb_len;            /* traceback length in 4-bit operations */
+} stormgpu_hit;
+
+/* A batch of reads, tag-sorted by the caller (reads_data.c:59-67).  Read r has lengths[r]
+ * codes at codes + r*code_stride and quality levels at levels + r*level_stride (levels may
+ * be NULL: every level is then 3, alignment.c:157-160). */
+typedef struct stormgpu_reads {
+  int64_t        n;
+  const uint8_t *codes;
+  int64_t        code_stride;
+  const uint8_t *levels;
+  int64_t        level_stride;
+  const int16_t *lengths;
+  const uint8_t *first_levels; /* colour space only: level of the primer colour (first_qual,
+                                  reads_data.h:27), which read__reverse moves to the end of
+                                  the reversed read (read_quality.c:238); NULL: level 3 */
+} stormgpu_reads;
+
+/* Per-read results.  hits[r*4 + k] is the rank-k alignment; traceback operations of that
+ * slot are packed two per byte (high nibble first, alignment.h:81-83) at
+ * tb + (r*4 + k)*tb_stride, already in start-to-end order (hit_map.c:137-141).
+ * mapped[r] != 0 iff the read reached hit_map__update at least once (hit_map.c:53-74). */
+typedef struct stormgpu_results {
+  stormgpu_hit *hits;        /* n * 4 */
+  uint8_t      *tb;          /* n * 4 * tb_stride */
+  int64_t       tb_stride;   /* >= (max read length + allowed_indels + 1) / 2 */
+  uint8_t      *mapped;      /* n */
+} stormgpu_results;
+
+typedef struct stormgpu_ctx stormgpu_ctx;
+
+/* Library and device --------------------------------------------------------------------- */
+const char *stormgpu_version(void);
+const char *stormgpu_last_error(void);
+/* 1 if a CUDA device is usable, 0 otherwise (never aborts). */
+int stormgpu_device_available(void);
+
+/* Context: parameters and the seed family.  `seeds` is the reference's -s syntax
+ * ("#-##;1101:0 3", seed.c:25-135); an invalid list gives STORMGPU_EINVAL.
+ * Replaces: the set-up half of reads_against_references (run.c:790-858). */
+int  stormgpu_open(const stormgpu_params *params, const char *seeds, stormgpu_ctx **out);
+void stormgpu_close(stormgpu_ctx *ctx);
+
+/* Reference sequences, in file order.  `codes` holds n_codes packed codes; `mask` holds the
+ * packed per-code masked flag (non-ACGT input, reference_data.c:115-126); masked regions are
+ * [starts[k], ends[k]) in ascending order (reference_data.c:121-177).
+ * Replaces: load_reference_db's output (reference_data.c:195-252). */
+int stormgpu_add_reference(stormgpu_ctx *ctx, const uint8_t *codes, const uint8_t *mask,
+                           int64_t n_codes, const int32_t *region_starts,
+                           const int32_t *region_ends, int32_t n_regions);
+
+/* Build the device-resident spaced-seed index of every reference sequence for every seed.
+ * Replaces: index__build_reference (index.c:19-195), called per sequence per seed
+ * (run.c:876-884). */
+int stormgpu_build_index(stormgpu_ctx *ctx);
+
+/* Map a batch: every read against every sequence, forward then reverse, the top-4 table
+ * updated in the reference's order (sequence, strand, diagonal).  Host buffers in and out.
+ * Replaces: the read loops of run.c:865-994 around process_read (run.c:555-747) and
+ * hit_map__update (hit_map.c:50-144). */
+int stormgpu_map(stormgpu_ctx *ctx, const stormgpu_reads *reads, stormgpu_results *out);
+
+/* Device-resident variant for callers that already hold the reads in GPU memory:
+ * every pointer in `reads` and `out` is a device pointer.  `stream` is a cudaStream_t
+ * (NULL: the context's stream).  Asynchronous; stormgpu_sync() waits. */
+int stormgpu_map_device(stormgpu_ctx *ctx, const stormgpu_reads *reads,
+                        stormgpu_results *out, void *stream);
+int stormgpu_sync(stormgpu_ctx *ctx);
+
+/* Statistics of the last stormgpu_map* call. */
+typedef struct stormgpu_stats {
+  int64_t candidates;        /* diagonals produced by the hit gather */
+  int64_t filter_passed;     /* diagonals passing the banded SW filter */
+  int64_t aligned;           /* full alignments computed */
+  int64_t seed_lookups;      /* (seed, read position) key lookups */
+  int64_t hit_positions;     /* index positions read by the hit gather */
+  int64_t filter_cells;      /* algorithmic filter cells: L * (2*min(i,15)+1) per diagonal */
+  int64_t align_cells;       /* L * (2*i+1) per full alignment */
+  int64_t kernels;           /* kernel launches */
+  double  ms_index, ms_gather, ms_filter, ms_align, ms_replay, ms_total;
+} stormgpu_stats;
+int stormgpu_get_stats(stormgpu_ctx *ctx, stormgpu_stats *out);
+
+/* Unit-level entry points (host buffers), one kernel each, used by the parity tests.
+ * ------------------------------------------------------------------------------------- */
+
+/* Banded SW filter (alignment_simd.c:2282-3404, semantics shared by every ISA): for each
+ * i < n, pass[i] = 1 iff the saturating-u8 local band score of the read against the genome
+ * window starting at code pos[i] exceeds min(threshold, 254).  W = 2,4,8,16 cells per hit.
+ * `genome` points at code 0 of a packed sequence that is readable (zero) for `pad` codes
+ * before and after its n_codes codes.  match..gapext are the absolute values that
+ * run.c:839 passes to the init function. */
+int stormgpu_sw_filter(int W, int read_len, uint32_t match, uint32_t mismatch,
+                       uint32_t gapopen, uint32_t gapext, uint32_t threshold,
+                       const uint8_t *genome, int64_t n_codes, int64_t pad,
+                       const int32_t *pos, int64_t n, const uint8_t *read, uint8_t *pass);
+
+/* Full banded alignment + traceback of one read against n windows (alignment.c:488-734).
+ * Window k starts at code win[k] of `genome`/`mask` (same padding rule as above).  Outputs
+ * per window: score (MIN_SCORE-free: the unaborted best score), abort bound (the smallest
+ * max_on_line + best_possible over rows 1..L-1; the reference aborts iff bound < threshold),
+ * best_i, best_j, best_i0, best_j0, traceback length and the traceback operations in the
+ * reference's end-to-start order, packed two per byte at tb + k*tb_stride. */
+int stormgpu_align(const stormgpu_params *params, const uint8_t *read, const uint8_t *levels,
+                   int read_len, const uint8_t *genome, const uint8_t *mask, int64_t n_codes,
+                   int64_t pad, const int32_t *win, int64_t n, int32_t *score, int32_t *bound,
+                   int16_t *best, int32_t *tb_len, uint8_t *tb, int64_t tb_stride);
+
+/* CSR index of one sequence for one seed (index.c:19-195): first[4^w + 1] offsets and
+ * map[first[4^w]] positions, ascending within each key. */
+int stormgpu_index_one(const char *seed, int32_t stdev_distance, const uint8_t *codes,
+                       int64_t n_codes, int64_t pad, const int32_t *region_starts,
+                       const int32_t *region_ends, int32_t n_regions, int32_t *first,
+                       int32_t *map, int64_t map_capacity, int64_t *map_len);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* STORMGPU_H */

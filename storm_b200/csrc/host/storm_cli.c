@@ -1,0 +1,268 @@
+/*
+ * storm_cli.c -- command line of storm-nucleotide / storm-color.
+ *
+ * Same getopt string, defaults, checks and exit codes as the reference front end
+ * (main.c:174-463); the driver steps of reads_against_references (run.c:764-1109): parse the
+ * seeds, load and tag-sort the reads, load the reference, map, write the SAM and the
+ * unmapped FASTQ.  Extension: reads of different lengths are accepted in one file; they are
+ * mapped in one batch and reported grouped by length (ascending), each group in tag order,
+ * i.e. exactly the concatenation of per-length runs of the reference.
+ */
+#include "storm_cli.h"
+
+#include <getopt.h>
+#include <stdarg.h>
+#include <stdlib.h>
+#include <string.h>
+#include <time.h>
+#include <unistd.h>
+
+#define DEFAULT_SEEDS_NUC "####--#-#--##--####;#####--###-#-###;###-##-#######"
+#define DEFAULT_SEEDS_COL "####----##--##-####;####-###--#----####;####-####-####"
+#define DEFAULT_SEED_FILE_NUC "seeds/solexa_lossy-3-12.in"
+#define DEFAULT_SEED_FILE_COL "seeds/solid_lossy-3-12.in"
+
+static int verbosity = 1;
+
+static void msg(int level, const char *fmt, ...) {
+  if (level > verbosity) return;
+  va_list ap;
+  va_start(ap, fmt);
+  vfprintf(stderr, fmt, ap);
+  va_end(ap);
+  fflush(stderr);
+}
+
+static void err(const char *fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  fprintf(stderr, "\033[31;1m");
+  vfprintf(stderr, fmt, ap);
+  fprintf(stderr, "\033[0m\n");
+  va_end(ap);
+  fflush(stderr);
+}
+
+/* seed.c:140-179: one seed per line, '%' lines ignored, trailing blanks removed, ';' added */
+static char *seeds_from_file(const char *path) {
+  FILE *f = fopen(path, "r");
+  if (!f) return NULL;
+  size_t cap = 1024, n = 0;
+  char *s = calloc(cap, 1);
+  char line[65536];
+  while (fgets(line, sizeof(line), f)) {
+    if (line[0] == '%') continue;
+    size_t l = strlen(line);
+    while (l > 0 && (line[l - 1] == '\n' || line[l - 1] == '\r' || line[l - 1] == ' ' || line[l - 1] == '\t')) line[--l] = 0;
+    if (n + l + 2 > cap) { cap = (n + l + 2) * 2; s = realloc(s, cap); }
+    memcpy(s + n, line, l);
+    n += l;
+    s[n] = 0;
+    if (n == 0 || s[n - 1] != ';') { s[n++] = ';'; s[n] = 0; }
+  }
+  fclose(f);
+  return s;
+}
+
+static void usage(const char *prog, const char *seeds) {
+  fprintf(stderr,
+          "\nSToRM (B200 build)\n\nUSAGE: %s parameters\n\n"
+          "Mandatory:\n  -g <genome_file>  reference (.fasta/.multifasta)\n"
+          "  -r <reads_file>   reads (.fastq)\n\n"
+          "Optional:\n  -s <seed list>  default: %s\n  -S <seed file>\n  -l <number>  repeat filter (stdev distance, <=0 disables)\n"
+          "  -j  ignore lowercase   -F forward only   -R reverse only\n"
+          "  -o <sam file>   -O <unmapped fastq>   -M <1..4>   -A\n"
+          "  -m <match> -x <mismatch> -d <gap open> -e <gap extend> -i <indels>\n"
+          "  -t <min score> -z <filter min score> -u <uniqueness> -b <quality base>\n"
+          "  -v <verbosity>  -h\n", prog, seeds);
+}
+
+int storm_cli_main(int argc, char **argv, int colour, const storm_mapper *mapper) {
+  const char *optstring = "g:r:q:s:S:a:b:f:p:m:x:d:e:t:z:T:i:v:o:O:l:u:M:N:jFRhcPHUGA";
+  char *genome_file = NULL, *reads_file = NULL, *qual_file = NULL;
+  char *single_read = NULL, *single_ref = NULL;
+  int match = 5, mismatch = -4, gap_open = -9, gap_extend = -4;
+  int allowed_indels = 3, simd_diags = 3, min_score = 115, min_score_filter = 100;
+  int quality_base = 33, map_unordered = 0, print_all = 0, uniqueness = 0, uniq_thr = 0;
+  int stdev = 100, ignore_lower = 0, senses = 3;
+  FILE *output = stdout, *unmapped = NULL;
+  char *seeds = seeds_from_file(colour ? DEFAULT_SEED_FILE_COL : DEFAULT_SEED_FILE_NUC);
+  if (!seeds) seeds = colour ? DEFAULT_SEEDS_COL : DEFAULT_SEEDS_NUC;
+  int opt;
+#define INTARG(v) do { if (sscanf(optarg, "%d", &(v)) != 1) { err("Mandatory numeric parameter missing for option %c.", opt); exit(1); } } while (0)
+#define FATAL_VALUE(v, what) do { err("Invalid value %d for option %c. Expected: %s.", v, opt, what); exit(1); } while (0)
+#define STRARG(t) do { if (strlen(optarg) == 2 && optarg[0] == '-' && optarg[1] != ':' && strchr(optstring, optarg[1])) { err("Mandatory parameter missing for option %c.", opt); exit(1); } t = optarg; } while (0)
+  while ((opt = getopt(argc, argv, optstring)) != -1) {
+    switch (opt) {
+    case 'g':
+      if (genome_file) { err("Genome file previously set with \"%s\".\nUnable to set it again.\n", genome_file); exit(1); }
+      STRARG(genome_file);
+      break;
+    case 'r':
+      if (reads_file) { err("Read file previously set with \"%s\".\nUnable to set it again.\n", reads_file); exit(1); }
+      STRARG(reads_file);
+      break;
+    case 'q':
+      if (qual_file) { err("Quality file previously set with \"%s\".\nUnable to set it again.\n", qual_file); exit(1); }
+      STRARG(qual_file);
+      break;
+    case 'S': {
+      char *t = seeds_from_file(optarg);
+      if (!t) { err("Unable to read seeds input file %s.", optarg); exit(1); }
+      seeds = t;
+      break;
+    }
+    case 's': seeds = optarg; break;
+    case 'm': INTARG(match); if (match <= 0) FATAL_VALUE(match, "a strictly positive integer"); break;
+    case 'x': INTARG(mismatch); if (mismatch > 0) FATAL_VALUE(mismatch, "a negative value or zero"); break;
+    case 'd': INTARG(gap_open); if (gap_open > 0) FATAL_VALUE(gap_open, "a negative value or zero"); break;
+    case 'e': INTARG(gap_extend); if (gap_extend > 0) FATAL_VALUE(gap_extend, "a negative value or zero"); break;
+    case 't': INTARG(min_score); break;
+    case 'z': INTARG(min_score_filter); break;
+    case 'b': INTARG(quality_base); break;
+    case 'i':
+      INTARG(allowed_indels);
+      if (allowed_indels < 0) FATAL_VALUE(allowed_indels, "a positive value or zero");
+      if (allowed_indels >= 16) {
+        msg(1, "SToRM may not handle more than 15 indels in SIMD (local alignment) filter (16 diagonals).\n"
+               "However final alignment does support this -i <%d> value...\n", allowed_indels);
+        simd_diags = 15;
+      } else simd_diags = allowed_indels;
+      break;
+    case 'a': single_read = optarg; break;
+    case 'p': break;
+    case 'f': single_ref = optarg; break;
+    case 'o':
+      if (!strcmp(optarg, "NULL") || !strcmp(optarg, "null")) output = NULL;
+      else if (!(output = fopen(optarg, "w"))) { err("Could not open or create output file %s.\n", optarg); exit(1); }
+      break;
+    case 'O':
+      if (!strcmp(optarg, "NULL") || !strcmp(optarg, "null")) unmapped = NULL;
+      else if (!(unmapped = fopen(optarg, "w"))) { err("Could not open or create FASTQ output file %s.\n", optarg); exit(1); }
+      break;
+    case 'F': senses = 1; break;
+    case 'R': senses = 2; break;
+    case 'h': usage(argv[0], seeds); return 0;
+    case 'G': break;
+    case 'M':
+      INTARG(map_unordered);
+      if (map_unordered <= 0) FATAL_VALUE(map_unordered, "a strictly positive integer");
+      if (map_unordered > STORMGPU_MAP_DETAIL) FATAL_VALUE(map_unordered, "a value smaller than MAP_DETAIL_SIZE (4)");
+      break;
+    case 'A':
+      if (!map_unordered) {
+        err("The -A (output all reads in SAM) parameter is not available with the Ordered Mapping\n"
+            "because not all mappable reads are already displayed in this mode.\n"
+            "Please use the Unordered Mapping (-M <number>) before using -A.\n");
+        exit(1);
+      }
+      print_all = 1;
+      break;
+    case 'v':
+      INTARG(verbosity);
+      if (verbosity < 0 || verbosity > 3) verbosity = 1;
+      break;
+    case 'P': case 'U': break;
+    case 'H': { int w; INTARG(w); break; }
+    case 'N': { int nt; INTARG(nt); if (nt <= 0) FATAL_VALUE(nt, "a strictly positive integer"); break; }
+    case 'l':
+      INTARG(stdev);
+      if (stdev <= 0) stdev = 0;
+      break;
+    case 'j': ignore_lower = 1; break;
+    case 'u':
+      uniqueness = 1;
+      INTARG(uniq_thr);
+      if (uniq_thr <= 0) FATAL_VALUE(uniq_thr, "a positive integer");
+      break;
+    default:
+      exit(1);
+    }
+  }
+  (void)simd_diags;
+  int delta_m = match - mismatch;
+  if (single_read && single_ref) {
+    err("The two-sequence alignment mode (-a/-f) is not part of this build.");
+    exit(1);
+  }
+  if (!reads_file || !genome_file) {
+    err("\nNot enough mandatory parameters provided.\n");
+    usage(argv[0], seeds);
+    return 0;
+  }
+  if (!map_unordered) {
+    err("The per-position (ordered) mapping without -M is not part of this build; use -M <1..4>.");
+    exit(1);
+  }
+  if (min_score < STORMGPU_MIN_SCORE) {
+    err("-t below %d is not supported.", STORMGPU_MIN_SCORE);
+    exit(1);
+  }
+  time_t t0 = time(NULL);
+  stormgpu_params p;
+  memset(&p, 0, sizeof(p));
+  p.colour = colour;
+  p.match = match; p.mismatch = mismatch; p.gap_open = gap_open; p.gap_extend = gap_extend;
+  p.allowed_indels = allowed_indels; p.min_score = min_score; p.min_score_filter = min_score_filter;
+  p.stdev_distance = stdev; p.senses = senses; p.device = 0;
+  if (allowed_indels > STORMGPU_MAX_INDELS) { err("-i above %d is not supported.", STORMGPU_MAX_INDELS); exit(1); }
+
+  msg(1, "Loading reads database...\n");
+  sh_reads reads;
+  if (sh_load_reads(reads_file, qual_file, colour, quality_base, 1, &reads) != 0) {
+    err("%s", sh_last_error());
+    err("Reads could not be loaded. Exiting.");
+    exit(-1);
+  }
+  msg(1, "Loaded %ld reads (read length %d..%d).\n", (long)reads.n, reads.min_len, reads.max_len);
+  sh_sort_reads(&reads);
+  msg(1, "Loading reference database...\n");
+  sh_refs refs;
+  if (sh_load_reference(genome_file, colour, ignore_lower, &refs) != 0) {
+    err("%s", sh_last_error());
+    err("Reference could not be loaded. Exiting.");
+    exit(-1);
+  }
+  msg(1, "Loaded %d reference sequence%s.\n", refs.n, refs.n == 1 ? "" : "s");
+
+  stormgpu_results res;
+  res.tb_stride = ((reads.max_len + allowed_indels + 1) / 2 + 7) & ~7;
+  res.hits = calloc((size_t)(reads.n ? reads.n : 1) * 4, sizeof(stormgpu_hit));
+  res.tb = calloc((size_t)(reads.n ? reads.n : 1) * 4, (size_t)res.tb_stride);
+  res.mapped = calloc((size_t)(reads.n ? reads.n : 1), 1);
+  char emsg[512] = {0};
+  int rc = mapper->map(mapper->user, &p, seeds, &refs, &reads, &res, emsg, sizeof(emsg));
+  if (rc == STORMGPU_EINVAL && strstr(emsg, "seed")) {
+    err("The seed pattern is invalid: \"%s\".\nExpected: {0,1}+ or {-,#}+ with at least one '1'/'#' (seed separator ';').", seeds);
+    exit(-1);
+  }
+  if (rc != 0) {
+    err("Mapping failed (%s): %s", mapper->name, emsg);
+    exit(2);
+  }
+  int64_t mapped = 0;
+  for (int64_t r = 0; r < reads.n; ++r) mapped += res.mapped[r] != 0;
+  msg(1, "\nAligned %ld of %ld reads (%5.2f%%) in %ld seconds.\n", (long)mapped, (long)reads.n,
+      reads.n ? mapped * 100.0 / reads.n : 0.0, (long)(time(NULL) - t0));
+
+  sh_sam_opts so;
+  memset(&so, 0, sizeof(so));
+  so.colour = colour; so.max_rank = map_unordered; so.print_all = print_all;
+  so.uniqueness = uniqueness; so.uniqueness_threshold = uniq_thr; so.min_score = min_score;
+  so.delta_m = delta_m; so.quality_base = quality_base; so.argc = argc; so.argv = argv;
+  if (output) {
+    static char obuf[1 << 22];
+    setvbuf(output, obuf, _IOFBF, sizeof(obuf));
+    sh_write_sam(output, &so, &refs, &reads, &res, 0, reads.n, 1);
+    fflush(output);
+  } else {
+    err("No file name provided for SAM output.");
+  }
+  if (unmapped) sh_write_unmapped_fastq(unmapped, &so, &reads, &res);
+  if (output && output != stdout) fclose(output);
+  if (unmapped) fclose(unmapped);
+  free(res.hits); free(res.tb); free(res.mapped);
+  sh_free_reads(&reads);
+  sh_free_reference(&refs);
+  return 0;
+}

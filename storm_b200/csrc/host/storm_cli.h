@@ -1,0 +1,29 @@
+/*
+ * storm_cli.h -- the storm-nucleotide / storm-color command line (main.c:174-463 and the
+ * driver reads_against_references, run.c:764-1109), parameterised by the mapper that fills
+ * the per-read results, so that the same front end drives the CUDA library.
+ */
+#ifndef STORM_CLI_H
+#define STORM_CLI_H
+
+#include "storm_host.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct storm_mapper {
+  const char *name;
+  /* fill `out` (already allocated for reads->n reads) for all reads against all sequences;
+   * return 0 or a negative error code (message through `err`). */
+  int (*map)(void *user, const stormgpu_params *p, const char *seeds, const sh_refs *refs,
+             const sh_reads *reads, stormgpu_results *out, char *err, int errlen);
+  void *user;
+} storm_mapper;
+
+int storm_cli_main(int argc, char **argv, int colour, const storm_mapper *mapper);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

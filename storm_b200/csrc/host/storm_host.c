@@ -1,0 +1,687 @@
+/*
+ * storm_host.c -- input loading, read ordering, SAM / FASTQ output (see storm_host.h).
+ */
+#include "storm_host.h"
+
+#include <ctype.h>
+#include <math.h>
+#include <stdarg.h>
+#include <stdlib.h>
+#include <string.h>
+
+static char g_err[512];
+const char *sh_last_error(void) { return g_err; }
+static int fail(int code, const char *fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_err, sizeof(g_err), fmt, ap);
+  va_end(ap);
+  return code;
+}
+
+/* Quality levels (read_quality.h:83-91, read_quality.c:189-195) */
+static const int LEVEL_UB[4] = {2, 7, 10, 93};
+static inline int quality_level(int q) {
+  int i = 0;
+  while (i < 3 && LEVEL_UB[i] < q) ++i;
+  return i;
+}
+
+static inline void put2(uint8_t *p, int64_t i, int v) {
+  p[i >> 2] = (uint8_t)(p[i >> 2] | ((v & 3) << ((i & 3) << 1)));
+}
+static inline int get2(const uint8_t *p, int64_t i) { return (p[i >> 2] >> ((i & 3) << 1)) & 3; }
+
+/* whole file in memory, NUL-terminated */
+static char *slurp(const char *path, size_t *len) {
+  FILE *f = fopen(path, "rb");
+  if (!f) return NULL;
+  size_t cap = 1 << 20, n = 0;
+  char *buf = malloc(cap + 1);
+  for (;;) {
+    if (n == cap) { cap *= 2; buf = realloc(buf, cap + 1); }
+    size_t got = fread(buf + n, 1, cap - n, f);
+    if (!got) break;
+    n += got;
+  }
+  fclose(f);
+  buf[n] = 0;
+  *len = n;
+  return buf;
+}
+
+/* ---------------------------------------------------------------------------- reference */
+
+/* reference_data.c:14-190: one FASTA chunk per '>' header; whitespace skipped; letters
+ * upper-cased unless -j; non-ACGT letters are masked and coded rand()&3 (nucleotide) or as
+ * the previous base (colour); colour space stores the XOR of consecutive bases and keeps
+ * the first base apart; masked regions are the maximal runs of masked codes. */
+int sh_load_reference(const char *path, int colour, int ignore_lowercase, sh_refs *out) {
+  memset(out, 0, sizeof(*out));
+  size_t len;
+  char *buf = slurp(path, &len);
+  if (!buf) return fail(STORMGPU_EINVAL, "Failed to read input file %s (reference sequence).", path);
+  /* count chunks: lines starting with '>' (reference_data.c:210-220) */
+  int nseq = 0;
+  for (size_t i = 0; i < len; ++i)
+    if ((i == 0 || buf[i - 1] == '\n') && buf[i] == '>') nseq++;
+  int headerless = nseq == 0;
+  if (headerless) nseq = 1;
+  out->names = calloc((size_t)nseq, sizeof(char *));
+  out->sizes = calloc((size_t)nseq, sizeof(int64_t));
+  out->codes = calloc((size_t)nseq, sizeof(uint8_t *));
+  out->masks = calloc((size_t)nseq, sizeof(uint8_t *));
+  out->alloc_codes = calloc((size_t)nseq, sizeof(uint8_t *));
+  out->alloc_masks = calloc((size_t)nseq, sizeof(uint8_t *));
+  out->rs = calloc((size_t)nseq, sizeof(int32_t *));
+  out->re = calloc((size_t)nseq, sizeof(int32_t *));
+  out->nreg = calloc((size_t)nseq, sizeof(int32_t));
+  out->first_base = calloc((size_t)nseq, 1);
+  size_t p = 0;
+  int s;
+  for (s = 0; s < nseq; ++s) {
+    if (p >= len) break;
+    /* header line */
+    if (buf[p] == '>') {
+      size_t e = p;
+      while (e < len && buf[e] != '\n') e++;
+      size_t nl = strcspn(buf + p + 1, " \r\n");
+      if (nl > e - p - 1) nl = e - p - 1;
+      if (nl == 0) { free(buf); return fail(STORMGPU_EINVAL, "Empty fasta header line in the reference sequence."); }
+      out->names[s] = malloc(nl + 1);
+      memcpy(out->names[s], buf + p + 1, nl);
+      out->names[s][nl] = 0;
+      if (out->names[s][0] == '=' || out->names[s][0] == '*') out->names[s][0] = '-';
+      p = (e < len) ? e + 1 : e;
+    }
+    /* measure */
+    size_t q = p;
+    int64_t size = 0;
+    while (q < len) {
+      int c = ignore_lowercase ? (unsigned char)buf[q] : toupper((unsigned char)buf[q]);
+      if (c == '>') break;
+      q++;
+      if (isspace(c)) continue;
+      size++;
+    }
+    if (size == 0) break; /* reference_data.c:67-70, load_reference_db:241-246 */
+    int64_t nbytes = (size + 3) / 4 + 1;
+    int64_t tot = nbytes + 2 * SH_PAD_BYTES;
+    uint8_t *ca = calloc((size_t)tot, 1), *ma = calloc((size_t)tot, 1);
+    memset(ma, 0x55, SH_PAD_BYTES);
+    uint8_t *cd = ca + SH_PAD_BYTES, *mk = ma + SH_PAD_BYTES;
+    int64_t i = 0, mstart = -1;
+    int32_t rcap = 16, nr = 0;
+    int32_t *rs = malloc(sizeof(int32_t) * (size_t)rcap), *re = malloc(sizeof(int32_t) * (size_t)rcap);
+    int code_prev = 0, have_first = 0;
+    while (p < len) {
+      int c = ignore_lowercase ? (unsigned char)buf[p] : toupper((unsigned char)buf[p]);
+      if (c == '>') break;
+      p++;
+      if (isspace(c)) continue;
+      int code;
+      if (!(c == 'A' || c == 'C' || c == 'G' || c == 'T')) {
+        code = colour ? code_prev : (rand() & 3);
+        if (mstart == -1) mstart = i;
+        put2(mk, i, 1);
+      } else {
+        code = (c == 'A') ? 0 : (c == 'C') ? 1 : (c == 'G') ? 2 : 3;
+        if (mstart != -1) {
+          if (nr == rcap) { rcap *= 2; rs = realloc(rs, sizeof(int32_t) * (size_t)rcap); re = realloc(re, sizeof(int32_t) * (size_t)rcap); }
+          rs[nr] = (int32_t)mstart; re[nr] = (int32_t)i; nr++;
+          mstart = -1;
+        }
+      }
+      if (!colour) {
+        put2(cd, i, code);
+        i++;
+      } else if (!have_first) {
+        have_first = 1;
+        code_prev = code;
+        out->first_base[s] = (uint8_t)code;
+      } else {
+        put2(cd, i, code_prev ^ code);
+        i++;
+        code_prev = code;
+      }
+    }
+    if (mstart != -1) {
+      if (nr == rcap) { rcap *= 2; rs = realloc(rs, sizeof(int32_t) * (size_t)rcap); re = realloc(re, sizeof(int32_t) * (size_t)rcap); }
+      rs[nr] = (int32_t)mstart; re[nr] = (int32_t)i; nr++;
+    }
+    out->sizes[s] = i;
+    /* mask the rest of the last byte and everything after (reference_data.c:183-188) */
+    for (int64_t k = i; k & 3; ++k) put2(mk, k, 1);
+    memset(mk + ((i + 3) >> 2), 0x55, (size_t)(tot - SH_PAD_BYTES - ((i + 3) >> 2)));
+    out->alloc_codes[s] = ca; out->alloc_masks[s] = ma;
+    out->codes[s] = cd; out->masks[s] = mk;
+    out->rs[s] = rs; out->re[s] = re; out->nreg[s] = nr;
+    if (headerless && s == 0 && out->names[s] == NULL) {
+      fprintf(stderr, "No fasta header line in the reference sequence.\n");
+    }
+    if (i == 0) { s++; break; }
+  }
+  out->n = s;
+  free(buf);
+  if (out->n <= 0) return fail(STORMGPU_EINVAL, "Reference could not be loaded.");
+  return 0;
+}
+
+void sh_free_reference(sh_refs *r) {
+  for (int s = 0; s < r->n; ++s) {
+    free(r->names ? r->names[s] : NULL);
+    free(r->alloc_codes[s]); free(r->alloc_masks[s]);
+    free(r->rs[s]); free(r->re[s]);
+  }
+  free(r->names); free(r->sizes); free(r->codes); free(r->masks); free(r->alloc_codes);
+  free(r->alloc_masks); free(r->rs); free(r->re); free(r->nreg); free(r->first_base);
+  memset(r, 0, sizeof(*r));
+}
+
+/* ---------------------------------------------------------------------------- reads */
+
+typedef struct growbuf { char *p; size_t n, cap; } growbuf;
+static void gb_put(growbuf *g, const void *src, size_t n) {
+  if (g->n + n > g->cap) {
+    g->cap = (g->n + n) * 2 + 4096;
+    g->p = realloc(g->p, g->cap);
+  }
+  memcpy(g->p + g->n, src, n);
+  g->n += n;
+}
+
+typedef struct rawread {
+  size_t name_off, seq_off, qual_off;
+  int name_len, seq_len, qual_len;
+  int has_qual;
+} rawread;
+
+/* reads_data.c:538-564: printable common prefix of the first and last read names */
+static char *common_name(const char *a, const char *b) {
+  int l = 0, t = 0;
+  while (a[l] && b[l] && a[l] == b[l]) {
+    char c = a[l];
+    if ((t == 0 && ((c >= '!' && c <= ')') || (c >= '+' && c <= '<') || (c >= '>' && c <= '~'))) ||
+        (t > 0 && c >= '!' && c <= '~'))
+      t = l + 1;
+    l++;
+  }
+  if (t <= 0) return NULL;
+  char *s = malloc((size_t)t + 1);
+  memcpy(s, a, (size_t)t);
+  s[t] = 0;
+  return s;
+}
+
+static int next_line(const char *buf, size_t len, size_t *pos, const char **line, size_t *ll) {
+  if (*pos >= len) return 0;
+  size_t s = *pos, e = s;
+  while (e < len && buf[e] != '\n') e++;
+  *line = buf + s;
+  *ll = e - s;  /* without '\n' */
+  *pos = (e < len) ? e + 1 : e;
+  return 1;
+}
+
+/* name of a header line: after the marker, up to the first char outside '!'..'~' or '@',
+ * at most 255 chars (reads_data.c:466-478) */
+static int header_name_len(const char *line, size_t ll) {
+  int n = 1;
+  while ((size_t)n < ll && (signed char)line[n] > ' ' && (signed char)line[n] <= '~' && line[n] != '@') {
+    n++;
+    if (n >= 256) break;
+  }
+  return n - 1;
+}
+
+static int fill_reads(sh_reads *out, const char *buf, rawread *rr, int64_t n, int colour,
+                      int quality_base, int allow_mixed, int any_qual) {
+  int minl = 1 << 30, maxl = 0;
+  for (int64_t i = 0; i < n; ++i) {
+    int L = rr[i].seq_len - (colour ? 2 : 0);
+    if (L <= 0) return fail(STORMGPU_EINVAL, "Reads file seams corrupt: the read #%ld length is %d.", (long)i + 1, L);
+    if (L > STORMGPU_MAX_READ_LEN) return fail(STORMGPU_EINVAL, "Read #%ld is longer than %d.", (long)i + 1, STORMGPU_MAX_READ_LEN);
+    if (L < minl) minl = L;
+    if (L > maxl) maxl = L;
+  }
+  if (!allow_mixed && n && minl != maxl)
+    return fail(STORMGPU_EINVAL, "The reads do not all have the same length (%d..%d). All the reads must be of equal length for the parallel processing.", minl, maxl);
+  out->n = n;
+  out->colour = colour;
+  out->min_len = n ? minl : 0;
+  out->max_len = n ? maxl : 0;
+  out->has_quality = any_qual;
+  out->code_stride = ((maxl + 3) / 4 + 7) & ~7;
+  out->level_stride = out->code_stride;
+  out->codes = calloc((size_t)(n ? n : 1), (size_t)out->code_stride);
+  out->levels = any_qual ? calloc((size_t)(n ? n : 1), (size_t)out->level_stride) : NULL;
+  out->lengths = calloc((size_t)(n ? n : 1), sizeof(int16_t));
+  out->tags = calloc((size_t)(n ? n : 1), sizeof(uint64_t));
+  out->names = calloc((size_t)(n ? n : 1), sizeof(char *));
+  out->first_base = calloc((size_t)(n ? n : 1), 1);
+  out->first_level = calloc((size_t)(n ? n : 1), 1);
+  out->file_index = calloc((size_t)(n ? n : 1), sizeof(int64_t));
+  short *qv = calloc((size_t)maxl + 2, sizeof(short));
+  for (int64_t i = 0; i < n; ++i) {
+    const rawread *r = &rr[i];
+    out->file_index[i] = i;
+    out->names[i] = malloc((size_t)r->name_len + 1);
+    memcpy(out->names[i], buf + r->name_off, (size_t)r->name_len);
+    out->names[i][r->name_len] = 0;
+    const char *sq = buf + r->seq_off;
+    int L = r->seq_len - (colour ? 2 : 0);
+    out->lengths[i] = (int16_t)L;
+    uint8_t *cd = out->codes + i * out->code_stride;
+    if (!colour) {
+      for (int k = 0; k < L; ++k) {
+        char c = sq[k];
+        put2(cd, k, c == 'A' ? 0 : c == 'C' ? 1 : c == 'G' ? 2 : c == 'T' ? 3 : 0);
+      }
+    } else {
+      /* reads_data.c:488-491: real first base = TRANSFORM(primer, first colour) */
+      int c0 = sq[0];
+      int b = ((c0 & 0x4) >> 1) | (((c0 & 0x4) >> 2) ^ ((c0 & 0x2) >> 1));
+      out->first_base[i] = (uint8_t)((b ^ (sq[1] & 3)) & 3);
+      for (int k = 0; k < L; ++k) put2(cd, k, sq[k + 2] & 3);
+    }
+    /* tag: maximum of the rolling 64-bit window, codes remapped to a,t,g,c order */
+    uint64_t tag = 0, ct = 0;
+    for (int k = 0; k < L; ++k) {
+      ct = (ct << 2) | (uint64_t)((((unsigned)get2(cd, k) + 1) & 3) ^ 1);
+      if (ct > tag) tag = ct;
+    }
+    out->tags[i] = tag;
+    if (any_qual && r->has_qual) {
+      const char *ql = buf + r->qual_off;
+      int qlen = r->qual_len;
+      memset(qv, 0, sizeof(short) * ((size_t)maxl + 2));
+      if (colour) {
+        int v = (int)(signed char)(qlen > 0 ? ql[0] : '\n') - quality_base;
+        if (v < 0) return fail(STORMGPU_EINVAL, "Quality level char induces a negative value (read #%ld).", (long)i + 1);
+        out->first_level[i] = (uint8_t)quality_level(v > 93 ? 93 : v);
+      }
+      int lim = L < qlen ? L : qlen;
+      for (int k = colour ? 1 : 0; k < lim; ++k) {
+        int v = (int)(signed char)ql[k] - quality_base;
+        if (v < 0) return fail(STORMGPU_EINVAL, "Quality level char \"%c\" induces a negative value (read #%ld).", ql[k], (long)i + 1);
+        qv[k] = (short)(v > 93 ? 93 : v);
+      }
+      uint8_t *lv = out->levels + i * out->level_stride;
+      /* colour: level of colour k is the quality of file colour k+1 (compress shift 1); the
+       * last one reads one past the parsed qualities, which is 0 (read_quality.c:31-41) */
+      for (int k = 0; k < L; ++k) put2(lv, k, quality_level(colour ? (k + 1 < L ? qv[k + 1] : 0) : qv[k]));
+    }
+  }
+  free(qv);
+  return 0;
+}
+
+static int load_fastq(const char *path, int colour, int quality_base, int allow_mixed, sh_reads *out) {
+  size_t len;
+  char *buf = slurp(path, &len);
+  if (!buf) return fail(STORMGPU_EINVAL, "Failed to read input file %s (read sequences).", path);
+  size_t pos = 0;
+  const char *line;
+  size_t ll;
+  char *title = NULL;
+  /* leading comments (reads_data.c:374-392) */
+  size_t rec_start = 0;
+  int lineno = 0;
+  while (1) {
+    rec_start = pos;
+    if (!next_line(buf, len, &pos, &line, &ll)) { free(buf); return fail(STORMGPU_EINVAL, "Failed to read input file %s (read sequences) first line.", path); }
+    if (ll >= 9 && !title && strncmp(line, "# Title: ", 9) == 0) {
+      size_t nl = strcspn(line + 9, "\r\n");
+      if (nl > ll - 9) nl = ll - 9;
+      title = malloc(nl + 1);
+      memcpy(title, line + 9, nl);
+      title[nl] = 0;
+    }
+    if (ll > 0 && line[0] == '#') { lineno++; continue; }
+    break;
+  }
+  pos = rec_start;
+  int64_t cap = 1 << 16, n = 0;
+  rawread *rr = malloc(sizeof(rawread) * (size_t)cap);
+  int any_qual = 0;
+  int state = 0; /* 0 header, 1 seq, 2 plus, 3 qual */
+  while (next_line(buf, len, &pos, &line, &ll)) {
+    size_t l2 = ll;
+    while (l2 > 0 && (line[l2 - 1] == '\r' || line[l2 - 1] == '\n')) l2--;
+    if (state == 0) {
+      if (ll == 0 || line[0] != '@') { free(rr); free(buf); free(title); return fail(STORMGPU_EINVAL, "Reads file seams corrupt at line %d.", lineno + 1); }
+      if (n == cap) { cap *= 2; rr = realloc(rr, sizeof(rawread) * (size_t)cap); }
+      rr[n].name_off = (size_t)(line - buf) + 1;
+      rr[n].name_len = header_name_len(line, l2);
+      rr[n].has_qual = 0;
+      rr[n].qual_len = 0;
+      state = 1;
+    } else if (state == 1) {
+      if (ll == 0) { free(rr); free(buf); free(title); return fail(STORMGPU_EINVAL, "Reads file seams corrupt at line %d.", lineno + 1); }
+      rr[n].seq_off = (size_t)(line - buf);
+      rr[n].seq_len = (int)strcspn(line, "\r\n");
+      if ((size_t)rr[n].seq_len > ll) rr[n].seq_len = (int)ll;
+      n++;
+      state = 2;
+    } else if (state == 2) {
+      if (ll == 0 || line[0] != '+') { free(rr); free(buf); free(title); return fail(STORMGPU_EINVAL, "Reads file seams corrupt at line %d.", lineno + 1); }
+      state = 3;
+    } else {
+      rr[n - 1].qual_off = (size_t)(line - buf);
+      rr[n - 1].qual_len = (int)l2;
+      rr[n - 1].has_qual = 1;
+      any_qual = 1;
+      state = 0;
+    }
+    lineno++;
+  }
+  if (n == 0) { free(rr); free(buf); free(title); return fail(STORMGPU_EINVAL, "Reads could not be loaded."); }
+  memset(out, 0, sizeof(*out));
+  int rc = fill_reads(out, buf, rr, n, colour, quality_base, allow_mixed, any_qual);
+  if (rc == 0) {
+    if (title) out->db_name = title;
+    else out->db_name = common_name(out->names[0], out->names[n - 1]);
+  } else free(title);
+  free(rr);
+  free(buf);
+  return rc;
+}
+
+int sh_load_reads(const char *path, const char *qual_path, int colour, int quality_base,
+                  int allow_mixed, sh_reads *out) {
+  const char *dot = strrchr(path, '.');
+  if (dot && (!strcmp(dot, ".fastq") || !strcmp(dot, ".fq") || !strcmp(dot, ".fastq2") || !strcmp(dot, ".fq2")))
+    return load_fastq(path, colour, quality_base, allow_mixed, out);
+  (void)qual_path;
+  return fail(STORMGPU_EINVAL, "Reads file %s: only FASTQ input (.fastq/.fq) is supported by this build.", path);
+}
+
+void sh_free_reads(sh_reads *r) {
+  for (int64_t i = 0; i < r->n; ++i) free(r->names[i]);
+  free(r->names); free(r->codes); free(r->levels); free(r->lengths); free(r->tags);
+  free(r->first_base); free(r->first_level); free(r->file_index); free(r->db_name);
+  memset(r, 0, sizeof(*r));
+}
+
+/* ---------------------------------------------------------------------------- ordering */
+
+typedef struct sortkey { int16_t len; uint64_t tag; int64_t idx; } sortkey;
+static int cmp_sortkey(const void *a, const void *b) {
+  const sortkey *x = a, *y = b;
+  if (x->len != y->len) return x->len < y->len ? -1 : 1;
+  if (x->tag != y->tag) return x->tag < y->tag ? -1 : 1;
+  return (x->idx > y->idx) - (x->idx < y->idx);
+}
+
+void sh_sort_reads(sh_reads *r) {
+  int64_t n = r->n;
+  sortkey *k = malloc(sizeof(sortkey) * (size_t)(n ? n : 1));
+  for (int64_t i = 0; i < n; ++i) { k[i].len = r->lengths[i]; k[i].tag = r->tags[i]; k[i].idx = i; }
+  qsort(k, (size_t)n, sizeof(sortkey), cmp_sortkey);
+  uint8_t *codes = malloc((size_t)(n ? n : 1) * (size_t)r->code_stride);
+  uint8_t *levels = r->levels ? malloc((size_t)(n ? n : 1) * (size_t)r->level_stride) : NULL;
+  int16_t *lengths = malloc(sizeof(int16_t) * (size_t)(n ? n : 1));
+  uint64_t *tags = malloc(sizeof(uint64_t) * (size_t)(n ? n : 1));
+  char **names = malloc(sizeof(char *) * (size_t)(n ? n : 1));
+  uint8_t *fb = malloc((size_t)(n ? n : 1)), *fl = malloc((size_t)(n ? n : 1));
+  int64_t *fi = malloc(sizeof(int64_t) * (size_t)(n ? n : 1));
+  for (int64_t i = 0; i < n; ++i) {
+    int64_t s = k[i].idx;
+    memcpy(codes + i * r->code_stride, r->codes + s * r->code_stride, (size_t)r->code_stride);
+    if (levels) memcpy(levels + i * r->level_stride, r->levels + s * r->level_stride, (size_t)r->level_stride);
+    lengths[i] = r->lengths[s]; tags[i] = r->tags[s]; names[i] = r->names[s];
+    fb[i] = r->first_base[s]; fl[i] = r->first_level[s]; fi[i] = r->file_index[s];
+  }
+  free(r->codes); free(r->levels); free(r->lengths); free(r->tags); free(r->names);
+  free(r->first_base); free(r->first_level); free(r->file_index);
+  r->codes = codes; r->levels = levels; r->lengths = lengths; r->tags = tags; r->names = names;
+  r->first_base = fb; r->first_level = fl; r->file_index = fi;
+  free(k);
+}
+
+void sh_reads_view(const sh_reads *r, stormgpu_reads *v) {
+  v->n = r->n;
+  v->codes = r->codes;
+  v->code_stride = r->code_stride;
+  v->levels = r->levels;
+  v->level_stride = r->level_stride;
+  v->lengths = r->lengths;
+  v->first_levels = r->colour ? r->first_level : NULL;
+}
+
+/* ---------------------------------------------------------------------------- SAM */
+
+static inline int tb_get(const uint8_t *t, int i) { return (t[i >> 1] >> ((i & 1) ? 0 : 4)) & 0xF; }
+
+/* alignment.c:749-887 */
+int sh_traceback_to_cigar(const uint8_t *tb, int tb_len, const uint8_t *ref, int64_t ref_start,
+                          int colour, int ref_start_symbol, char *cigar, char *seq) {
+  int edit = 0, span = colour ? 1 : 0, prev = 0x3, slen = 0;
+  int64_t ri = 0;
+  int ref_hist = 0, read_hist = 0;
+  char *cp = cigar;
+  *cp = 0;
+  uint8_t sq[2 * STORMGPU_MAX_READ_LEN + 8];
+  if (colour) sq[slen++] = 0;
+  for (int i = 0; i < tb_len; ++i) {
+    int cell = tb_get(tb, i);
+    int type;
+    if ((cell & 0xC) == 0x4) type = 0x4;
+    else if (colour && (cell & 0xC) == 0x8) type = 0x8;
+    else if ((cell & 0xC) == 0xC) type = 0xC;
+    else type = cell;
+    int code = cell & 3;
+    switch (type) {
+    case 0x3:
+      edit--;
+      if (!colour) code = get2(ref, ref_start + ri);
+      /* fall through */
+    case 0x4:
+      edit++;
+      if (colour) {
+        ref_hist ^= get2(ref, ref_start + ri);
+        code = ref_hist ^ read_hist;
+      }
+      sq[slen++] = (uint8_t)code;
+      if (colour) read_hist ^= code;
+      ri++;
+      break;
+    case 0x8:
+      if (colour) {
+        edit++;
+        sq[slen++] = (uint8_t)code;
+        read_hist ^= code;
+        ref_hist ^= get2(ref, ref_start + ri);
+        ri++;
+      }
+      break;
+    case 0xC:
+      edit++;
+      sq[slen++] = (uint8_t)code;
+      if (colour) read_hist ^= code;
+      break;
+    case 0x1:
+      edit++;
+      if (colour) ref_hist ^= get2(ref, ref_start + ri);
+      ri++;
+      break;
+    default:
+      break;
+    }
+    int crt = (type == 0x1 || type == 0xC) ? type : 0x3;
+    if (crt == prev) span++;
+    else {
+      if (span) cp += sprintf(cp, "%d%c", span, prev == 0x3 ? 'M' : prev == 0xC ? 'I' : prev == 0x1 ? 'D' : '?');
+      span = 1;
+      prev = crt;
+    }
+  }
+  if (span) sprintf(cp, "%d%c", span, prev == 0x3 ? 'M' : prev == 0xC ? 'I' : prev == 0x1 ? 'D' : '?');
+  static const char B[4] = {'A', 'C', 'G', 'T'};
+  if (!colour) {
+    for (int u = 0; u < slen; ++u) seq[u] = B[sq[u] & 3];
+  } else {
+    int c = ref_start_symbol;
+    for (int u = 0; u < slen; ++u) { c = (c ^ sq[u]) & 3; seq[u] = B[c]; }
+  }
+  seq[slen] = 0;
+  return edit;
+}
+
+/* hit_map.c:384-403 */
+int sh_mapq(int rank, int score0, int score1, int score_rank, int min_score, int delta_m) {
+  double n;
+  if (rank == 0) {
+    int s2 = score1 > min_score ? score1 : min_score;
+    n = (double)(score0 - s2) / (double)delta_m;
+  } else {
+    n = (double)(score_rank - score0) / (double)delta_m;
+  }
+  int mapq = (int)(-4.343 * (n * log(.3)));
+  mapq = (int)(mapq - 4.343 * log(.3));
+  if (mapq < 0) mapq = 0;
+  if (mapq > 254) mapq = 254;
+  return mapq;
+}
+
+/* base of sequence s at position pos in colour space, from its first base and colours */
+static int ref_symbol_at(const sh_refs *refs, int s, int64_t pos) {
+  int b = refs->first_base[s];
+  for (int64_t p = 0; p < pos && p < refs->sizes[s]; ++p) b ^= get2(refs->codes[s], p);
+  return b & 3;
+}
+
+typedef struct colour_cursor { int seq; int64_t pos; int base; } colour_cursor;
+
+int sh_write_sam(FILE *f, const sh_sam_opts *o, const sh_refs *refs, const sh_reads *reads,
+                 const stormgpu_results *res, int64_t first, int64_t count, int header) {
+  const int colour = o->colour;
+  if (header) {
+    fprintf(f, "@HD\tVN:1.4\tSO:unsorted\n");
+    for (int s = 0; s < refs->n; ++s)
+      fprintf(f, "@SQ\tSN:%s\tLN:%ld\n", refs->names[s] ? refs->names[s] : "*",
+              (long)(refs->sizes[s] + (colour ? 1 : 0)));
+    const char *rg = reads->db_name ? reads->db_name : "*";
+    fprintf(f, "@RG\tID:%s\tSM:%s\n", rg, rg);
+    fprintf(f, "@PG\tID:%s\tVN:%s\tCL:\"", "SToRM", "0.0101");
+    for (int i = 0; i < o->argc; ++i) fprintf(f, "%s ", o->argv[i]);
+    fprintf(f, "\"\n");
+  }
+  /* colour space: prefix bases per sequence, computed lazily from a checkpoint table */
+  int64_t **chk = NULL;
+  const int64_t STEP = 4096;
+  if (colour) {
+    chk = calloc((size_t)refs->n, sizeof(int64_t *));
+    for (int s = 0; s < refs->n; ++s) {
+      int64_t nck = refs->sizes[s] / STEP + 2;
+      chk[s] = malloc(sizeof(int64_t) * (size_t)nck);
+      int b = refs->first_base[s];
+      for (int64_t p = 0, k = 0; k < nck; ++k) {
+        chk[s][k] = b;
+        for (int64_t e = (k + 1) * STEP; p < e && p < refs->sizes[s]; ++p) b ^= get2(refs->codes[s], p);
+      }
+    }
+  }
+  char cigar[4 * STORMGPU_MAX_READ_LEN + 64], seq[2 * STORMGPU_MAX_READ_LEN + 8];
+  static const char B[4] = {'A', 'C', 'G', 'T'};
+  char *qbuf = malloc((size_t)reads->max_len + 8);
+  for (int64_t r = first; r < first + count; ++r) {
+    const stormgpu_hit *h = &res->hits[r * 4];
+    int L = reads->lengths[r];
+    if (res->mapped[r]) {
+      int M = o->max_rank;
+#define REPORTABLE(k) ((k) < M && h[k].ref_start != -1 && \
+   ((o->uniqueness == 0) || (((k) + 1 < M) && ((h[k].score - h[(k) + 1].score) >= o->uniqueness_threshold)) || ((k) + 1 == M)))
+      int nrep = 0;
+      for (int k = 0; REPORTABLE(k); ++k) nrep++;
+      for (int k = 0; REPORTABLE(k); ++k) {
+        int rev = (h[k].sense & 2) != 0;  /* sense is +1/-1; -1 & ALIGNMENT_SENSE_REVERSE */
+        int flag = (rev ? 0x10 : 0) | (k ? 0x100 : 0);
+        int ref_id = h[k].ref_id;
+        int64_t ref_start = h[k].ref_start;
+        int mapq = sh_mapq(k, h[0].score, h[1].score, h[k].score, o->min_score, o->delta_m);
+        int sym = 0;
+        if (colour) {
+          if (ref_start >= 0) {
+            int64_t ck = ref_start / STEP;
+            int b = (int)chk[ref_id][ck];
+            for (int64_t p = ck * STEP; p < ref_start && p < refs->sizes[ref_id]; ++p) b ^= get2(refs->codes[ref_id], p);
+            sym = b & 3;
+          } else sym = ref_symbol_at(refs, ref_id, 0);
+        }
+        int ed = sh_traceback_to_cigar(res->tb + (size_t)(r * 4 + k) * (size_t)res->tb_stride, h[k].tb_len,
+                                       refs->codes[ref_id], ref_start, colour, sym, cigar, seq);
+        fprintf(f, "%s\t%d\t%s\t%ld\t%d\t%s\t*\t0\t0\t%s\t", reads->names[r], flag,
+                refs->names[ref_id] ? refs->names[ref_id] : "*", (long)(ref_start + 1), mapq, cigar, seq);
+        if (reads->levels) {
+          const uint8_t *lv = reads->levels + r * reads->level_stride;
+          int qi = 0;
+          if (rev) {
+            for (int q = L - 1; q >= 0; --q) { int c = o->quality_base + LEVEL_UB[get2(lv, q)]; qbuf[qi++] = (char)(c < 126 ? c : 126); }
+            if (colour) { int c = o->quality_base + LEVEL_UB[reads->first_level[r]]; qbuf[qi++] = (char)(c < 126 ? c : 126); }
+          } else {
+            if (colour) { int c = o->quality_base + LEVEL_UB[reads->first_level[r]]; qbuf[qi++] = (char)(c < 126 ? c : 126); }
+            for (int q = 0; q < L; ++q) { int c = o->quality_base + LEVEL_UB[get2(lv, q)]; qbuf[qi++] = (char)(c < 126 ? c : 126); }
+          }
+          fwrite(qbuf, 1, (size_t)qi, f);
+        } else {
+          fputc('*', f);
+        }
+        fprintf(f, "\tAS:i:%d\tNM:i:%d\tNH:i:%d\n", h[k].score, ed, nrep);
+      }
+#undef REPORTABLE
+    } else if (o->print_all) {
+      if (colour) {
+        fprintf(f, "%s\t4\t*\t0\t255\t*\t*\t0\t0\t*\t*\n", reads->names[r]);
+      } else {
+        fprintf(f, "%s\t4\t*\t0\t255\t*\t*\t0\t0\t", reads->names[r]);
+        const uint8_t *cd = reads->codes + r * reads->code_stride;
+        for (int q = 0; q < L; ++q) qbuf[q] = B[get2(cd, q)];
+        fwrite(qbuf, 1, (size_t)L, f);
+        fputc('\t', f);
+        if (reads->levels) {
+          const uint8_t *lv = reads->levels + r * reads->level_stride;
+          for (int q = 0; q < L; ++q) { int c = o->quality_base + LEVEL_UB[get2(lv, q)]; qbuf[q] = (char)(c < 126 ? c : 126); }
+          fwrite(qbuf, 1, (size_t)L, f);
+        } else fputc('*', f);
+        fputc('\n', f);
+      }
+    }
+  }
+  free(qbuf);
+  if (chk) {
+    for (int s = 0; s < refs->n; ++s) free(chk[s]);
+    free(chk);
+  }
+  return 0;
+}
+
+/* hit_map.c:514-579 */
+int sh_write_unmapped_fastq(FILE *f, const sh_sam_opts *o, const sh_reads *reads,
+                            const stormgpu_results *res) {
+  static const char B[4] = {'A', 'C', 'G', 'T'}, CL[4] = {'0', '1', '2', '3'};
+  for (int64_t r = 0; r < reads->n; ++r) {
+    if (res->mapped[r]) continue;
+    int L = reads->lengths[r];
+    fprintf(f, "@%s\n", reads->names[r]);
+    const uint8_t *cd = reads->codes + r * reads->code_stride;
+    if (!o->colour) {
+      for (int k = 0; k < L; ++k) fputc(B[get2(cd, k)], f);
+    } else {
+      fputc(B[reads->first_base[r] & 3], f);
+      for (int k = 0; k < L; ++k) fputc(CL[get2(cd, k)], f);
+    }
+    fprintf(f, "\n+%s\n", reads->names[r]);
+    if (reads->levels) {
+      const uint8_t *lv = reads->levels + r * reads->level_stride;
+      if (o->colour) { int c = o->quality_base + LEVEL_UB[reads->first_level[r]]; fputc(c < 126 ? c : 126, f); }
+      for (int q = 0; q < L; ++q) { int c = o->quality_base + LEVEL_UB[get2(lv, q)]; fputc(c < 126 ? c : 126, f); }
+    } else {
+      int c = o->quality_base + 93;
+      if (o->colour) fputc(c < 126 ? c : 126, f);
+      for (int q = 0; q < L; ++q) fputc(c < 126 ? c : 126, f);
+    }
+    fputc('\n', f);
+  }
+  return 0;
+}

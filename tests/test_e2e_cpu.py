@@ -1,0 +1,151 @@
+"""End-to-end parity on the CPU: the reference binary (oracle/_ref, built from its sources)
+against the product's front end (loader, tag sort, SAM and FASTQ writers) driven by the
+oracle mapper (oracle/storm-oracle-*), on small seeded inputs over the option surface.
+
+The reference is run with MALLOC_PERTURB_=255 (every malloc returns zeroed memory): in colour
+space its SAM writer ORs bits into an uninitialised buffer (hit_map.c:243-251) and the
+quality loader reads one past the parsed qualities (read_quality.c:38), so without it the
+reference's own output changes from run to run.  The @PG line (argv echo) is compared with
+the binary name normalised."""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+import ffi
+from storm_b200 import synth
+
+pytestmark = pytest.mark.skipif(not ffi.ref_available(), reason="oracle/_ref not built")
+
+ORACLE_BIN = {0: os.path.join(ffi.ORACLE_DIR, "storm-oracle-nucleotide"),
+              1: os.path.join(ffi.ORACLE_DIR, "storm-oracle-color")}
+REF_BIN = {0: os.path.join(ffi.REF_DIR, "storm-nucleotide"), 1: os.path.join(ffi.REF_DIR, "storm-color")}
+
+
+def _build():
+    subprocess.run(["make", "-s", "-C", ffi.ORACLE_DIR, "storm-oracle-nucleotide",
+                    "storm-oracle-color"], check=True)
+
+
+def run_pair(tmp, colour, args, ref="ref.fa", reads="reads.fq", outputs=("out.sam", "un.fq")):
+    _build()
+    res = {}
+    for name, exe in (("ref", REF_BIN[colour]), ("new", ORACLE_BIN[colour])):
+        cmd = [exe, "-g", ref, "-r", reads, "-o", name + "_" + outputs[0], "-v", "0"] + list(args)
+        if "-O" not in args and outputs[1]:
+            cmd += ["-O", name + "_" + outputs[1]]
+        env = dict(os.environ, MALLOC_PERTURB_="255")
+        p = subprocess.run(cmd, cwd=tmp, env=env, capture_output=True, timeout=600)
+        res[name] = p
+    for name in ("ref", "new"):
+        assert res[name].returncode == res["ref"].returncode, (name, res[name].stderr[-2000:])
+    if res["ref"].returncode != 0:
+        return None
+    out = {}
+    for name in ("ref", "new"):
+        with open(os.path.join(tmp, name + "_" + outputs[0]), "rb") as f:
+            lines = f.read().split(b"\n")
+        out[name] = [l for l in lines if not l.startswith(b"@PG")]
+        pg = [l for l in lines if l.startswith(b"@PG")]
+        assert len(pg) == 1
+        out[name + "_pg"] = pg[0].split(b"-g", 1)[1].replace(name.encode() + b"_", b"X_")
+    assert out["ref"] == out["new"], _first_diff(out["ref"], out["new"])
+    assert out["ref_pg"] == out["new_pg"]
+    if outputs[1]:
+        a = open(os.path.join(tmp, "ref_" + outputs[1]), "rb").read()
+        b = open(os.path.join(tmp, "new_" + outputs[1]), "rb").read()
+        assert a == b
+    return out["ref"]
+
+
+def _first_diff(a, b):
+    for i, (x, y) in enumerate(zip(a, b)):
+        if x != y:
+            return "line %d:\nref %r\nnew %r" % (i, x, y)
+    return "lengths %d vs %d" % (len(a), len(b))
+
+
+def _mapped(lines):
+    return sum(1 for l in lines if l and not l.startswith(b"@"))
+
+
+@pytest.fixture(scope="module")
+def nuc_data(tmp_path_factory):
+    d = tmp_path_factory.mktemp("nuc")
+    synth.generate(0, 0.05, str(d / "ref.fa"), str(d / "reads.fq"))
+    return str(d)
+
+
+@pytest.mark.parametrize("args", [
+    ["-M", "1", "-z", "100", "-t", "100", "-i", "3", "-b", "33"],
+    ["-M", "4", "-A", "-z", "90", "-t", "95"],
+    ["-M", "2", "-F"],
+    ["-M", "3", "-R", "-u", "5"],
+    ["-M", "4", "-i", "0", "-z", "60", "-t", "60"],
+    ["-M", "1", "-i", "1"],
+    ["-M", "4", "-i", "7", "-z", "80"],
+    ["-M", "4", "-i", "15", "-z", "80"],
+    ["-M", "4", "-i", "20", "-z", "70", "-t", "90"],
+    ["-M", "4", "-l", "3"],
+    ["-M", "4", "-l", "0", "-s", "#####-##-###;####--##-####"],
+    ["-M", "4", "-s", "###-##-#######:0 5 10 20 30"],
+    ["-M", "1", "-m", "3", "-x", "-2", "-d", "-5", "-e", "-1", "-t", "60", "-z", "60"],
+    ["-M", "1", "-b", "30"],
+])
+def test_nucleotide_options(nuc_data, args):
+    lines = run_pair(nuc_data, 0, args)
+    assert _mapped(lines) > 0
+
+
+def test_bad_quality_base_fails_like_reference(nuc_data):
+    """Quality characters below -b are an input error (read_quality.c:197-208): exit -1."""
+    assert run_pair(nuc_data, 0, ["-M", "1", "-b", "48"]) is None
+
+
+@pytest.fixture(scope="module")
+def col_data(tmp_path_factory):
+    d = tmp_path_factory.mktemp("col")
+    synth.generate(1, 0.004, str(d / "ref.fa"), str(d / "reads.fq"))
+    return str(d)
+
+
+@pytest.mark.parametrize("args", [
+    ["-M", "1", "-z", "105", "-t", "120", "-i", "7", "-s",
+     "####-##-#-####;###-#--##-##--###;####-#---#----#--####"],
+    ["-M", "4", "-A", "-i", "3"],
+    ["-M", "2", "-i", "10", "-z", "90", "-t", "100"],
+])
+def test_colour_options(col_data, args):
+    lines = run_pair(col_data, 1, args)
+    assert _mapped(lines) > 0
+
+
+def test_masked_multi_sequence(tmp_path):
+    """N runs in the reference (masked regions, rand()&3 codes), several sequences, an N at the
+    very start and end, lowercase letters, and N / lowercase bases inside reads."""
+    rng = np.random.default_rng(5)
+    genome = synth.make_genome([30000, 12000, 5000], 9)
+    text = []
+    for name, seq in genome:
+        s = bytearray(synth.BASES[seq].tobytes())
+        for _ in range(6):
+            a = int(rng.integers(0, len(s) - 50))
+            s[a:a + int(rng.integers(1, 40))] = b"N" * len(s[a:a + int(rng.integers(1, 40))])
+        s[0:3] = b"NNN"
+        s[-2:] = b"NN"
+        low = int(rng.integers(0, len(s) - 100))
+        s[low:low + 60] = s[low:low + 60].lower()
+        text.append(b">" + name.encode() + b" some description\n" +
+                    b"\n".join(bytes(s[i:i + 70]) for i in range(0, len(s), 70)) + b"\n")
+    (tmp_path / "ref.fa").write_bytes(b"".join(text))
+    seqs, quals = synth.simulate_nucleotide_reads(genome, 3000, 50, 8)
+    synth.write_fastq(str(tmp_path / "reads.fq"), seqs, quals)
+    raw = bytearray((tmp_path / "reads.fq").read_bytes())
+    lines = raw.split(b"\n")
+    for k in range(1, len(lines), 40):
+        if k % 4 == 1 and len(lines[k]) > 10:
+            lines[k] = lines[k][:5] + b"N" + lines[k][6:8].lower() + lines[k][8:]
+    (tmp_path / "reads.fq").write_bytes(b"\n".join(lines))
+    run_pair(str(tmp_path), 0, ["-M", "4", "-A", "-z", "90", "-t", "95"])
+    run_pair(str(tmp_path), 0, ["-M", "4", "-j", "-z", "90", "-t", "95"])
