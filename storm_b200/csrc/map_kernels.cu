@@ -1,0 +1,717 @@
+// map_kernels.cu -- the kernels of one mapping pass (one reference sequence x one strand).
+//
+//  gather_count / gather_expand / segment_unique   hit gather (run.c:577-698, index.c:212-241)
+//  filter                                           banded u8 SW filter (alignment_simd.c)
+//  align                                            banded DP + traceback (alignment.c:488-734)
+//  replay                                           per-read top-4 update (run.c:664-691,
+//                                                   hit_map.c:50-144)
+#include "map_kernels.cuh"
+
+namespace sg {
+
+__constant__ SeedSet c_seeds;
+
+// ------------------------------------------------------------------------------ reads
+
+__global__ void reverse_reads_kernel(ReadsDev in, const uint8_t* __restrict__ first_levels, int colour,
+                                     uint8_t* __restrict__ rcodes, uint8_t* __restrict__ rlevels) {
+  int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= in.n) return;
+  const int L = in.lengths[r];
+  const uint8_t* c = in.codes + r * in.cstride;
+  uint8_t* rc = rcodes + r * in.cstride;
+  for (int64_t b = 0; b < in.cstride; ++b) rc[b] = 0;
+  // read__reverse (reads_data.c:9-35): nucleotide = reverse complement, colour = reverse
+  for (int i = 0; i < L; ++i) {
+    int v = code_at(c, i);
+    if (!colour) v = 3 - v;
+    int o = L - 1 - i;
+    rc[o >> 2] |= (uint8_t)(v << ((o & 3) << 1));
+  }
+  if (in.levels) {
+    const uint8_t* q = in.levels + r * in.lstride;
+    uint8_t* rq = rlevels + r * in.lstride;
+    for (int64_t b = 0; b < in.lstride; ++b) rq[b] = 0;
+    if (!colour) {
+      for (int i = 0; i < L; ++i) rq[i >> 2] |= (uint8_t)(code_at(q, L - 1 - i) << ((i & 3) << 1));
+    } else {
+      // quality__reverse_compressed, colour (read_quality.c:238-241)
+      int fl = first_levels ? first_levels[r] : 3;
+      rq[(L - 1) >> 2] |= (uint8_t)((fl & 3) << (((L - 1) & 3) << 1));
+      for (int i = 0; i < L - 1; ++i) rq[i >> 2] |= (uint8_t)(code_at(q, L - 2 - i) << ((i & 3) << 1));
+    }
+  }
+}
+
+void launch_reverse_reads(const ReadsDev& in, const uint8_t* first_levels, int colour,
+                          uint8_t* rcodes, uint8_t* rlevels, cudaStream_t st) {
+  if (in.n <= 0) return;
+  reverse_reads_kernel<<<(unsigned)((in.n + 127) / 128), 128, 0, st>>>(in, first_levels, colour, rcodes, rlevels);
+}
+
+__global__ void init_results_kernel(int64_t n, stormgpu_hit* __restrict__ hits, uint8_t* __restrict__ mapped,
+                                    uint8_t* __restrict__ tb, int64_t tbs) {
+  int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n * 4) return;
+  stormgpu_hit h;
+  h.score = kMinScore;
+  h.ref_id = h.ref_start = h.ref_end = -1;
+  h.read_start = h.read_end = -1;
+  h.sense = 0;
+  h.tb_len = 0;
+  hits[t] = h;
+  if ((t & 3) == 0) mapped[t >> 2] = 0;
+  for (int64_t b = 0; b < tbs; ++b) tb[t * tbs + b] = 0;
+}
+
+void launch_init_results(int64_t n, stormgpu_hit* hits, uint8_t* mapped, uint8_t* tb, int64_t tbs,
+                         cudaStream_t st) {
+  if (n <= 0) return;
+  init_results_kernel<<<(unsigned)((n * 4 + 255) / 256), 256, 0, st>>>(n, hits, mapped, tb, tbs);
+}
+
+// ------------------------------------------------------------------------------ gather
+
+// Seed key at read position rp; codes beyond the read's end read as 0 (seed.c:203-213).
+__device__ __forceinline__ uint32_t read_key(const SeedDev& s, const uint8_t* rd, int L, int rp) {
+  uint32_t key = 0;
+  for (int c = 0; c < s.n_care; ++c) {
+    int p = rp + s.care[c];
+    key = (key << 2) | (uint32_t)(p < L ? code_at(rd, p) : 0);
+  }
+  return key;
+}
+
+__device__ __forceinline__ int seed_npos(const SeedDev& s, int L) {
+  return s.n_positions ? s.n_positions : (L - s.span + 1 > 0 ? L - s.span + 1 : 0);
+}
+
+__global__ void gather_count_kernel(ReadsDev rd, IndexView ix, int32_t* __restrict__ hits,
+                                    unsigned long long* __restrict__ counters) {
+  const int lane = threadIdx.x & 31;
+  const int64_t nwarps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  unsigned long long lookups = 0, positions = 0;
+  for (int64_t r = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); r < rd.n; r += nwarps) {
+    const int L = rd.lengths[r];
+    const uint8_t* read = rd.codes + r * rd.cstride;
+    long long tot = 0;
+    for (int si = 0; si < c_seeds.n; ++si) {
+      const SeedDev& s = c_seeds.s[si];
+      const int np = seed_npos(s, L);
+      for (int t = lane; t < np; t += 32) {
+        int rp = s.n_positions ? s.positions[t] : t;
+        if (rp < 0 || rp >= L) continue;
+        uint32_t key = read_key(s, read, L, rp);
+        int a = __ldg(ix.first[si] + key), b = __ldg(ix.first[si] + key + 1);
+        tot += b - a;
+        lookups++;
+      }
+    }
+    for (int o = 16; o > 0; o >>= 1) tot += __shfl_xor_sync(0xffffffffu, tot, o);
+    if (lane == 0) hits[r] = tot > 0x7fffffffLL ? 0x7fffffff : (int32_t)tot;
+    positions += (unsigned long long)tot;
+  }
+  for (int o = 16; o > 0; o >>= 1) lookups += __shfl_xor_sync(0xffffffffu, lookups, o);
+  if (lane == 0) {
+    atomicAdd(&counters[3], lookups);
+    atomicAdd(&counters[4], positions);
+  }
+}
+
+void launch_gather_count(const ReadsDev& r, const SeedSet& seeds, const IndexView& ix,
+                         int32_t* hits, unsigned long long* counters, cudaStream_t st) {
+  cudaMemcpyToSymbolAsync(c_seeds, &seeds, sizeof(SeedSet), 0, cudaMemcpyHostToDevice, st);
+  if (r.n <= 0) return;
+  int64_t blocks = (r.n + 7) / 8;
+  if (blocks > 148 * 64) blocks = 148 * 64;
+  gather_count_kernel<<<(unsigned)blocks, 256, 0, st>>>(r, ix, hits, counters);
+}
+
+__global__ void gather_expand_kernel(ReadsDev rd, IndexView ix, const int64_t* __restrict__ hoff,
+                                     int32_t* __restrict__ cand) {
+  const int lane = threadIdx.x & 31;
+  const int64_t nwarps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  for (int64_t r = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); r < rd.n; r += nwarps) {
+    const int L = rd.lengths[r];
+    const uint8_t* read = rd.codes + r * rd.cstride;
+    int32_t* out = cand + hoff[r];
+    int run = 0;
+    for (int si = 0; si < c_seeds.n; ++si) {
+      const SeedDev& s = c_seeds.s[si];
+      const int np = seed_npos(s, L);
+      const int32_t* mp = ix.map[si];
+      for (int t0 = 0; t0 < np; t0 += 32) {
+        int t = t0 + lane, a = 0, cnt = 0, rp = 0;
+        if (t < np) {
+          rp = s.n_positions ? s.positions[t] : t;
+          if (rp >= 0 && rp < L) {
+            uint32_t key = read_key(s, read, L, rp);
+            a = __ldg(ix.first[si] + key);
+            cnt = __ldg(ix.first[si] + key + 1) - a;
+          }
+        }
+        int incl = warp_incl_scan(cnt);
+        int dst = run + incl - cnt;
+        run += __shfl_sync(0xffffffffu, incl, 31);
+        unsigned m = __ballot_sync(0xffffffffu, cnt > 0);
+        while (m) {
+          int j = __ffs(m) - 1;
+          m &= m - 1;
+          int sj = __shfl_sync(0xffffffffu, a, j), cj = __shfl_sync(0xffffffffu, cnt, j);
+          int dj = __shfl_sync(0xffffffffu, dst, j), rj = __shfl_sync(0xffffffffu, rp, j);
+          for (int u = lane; u < cj; u += 32) out[dj + u] = __ldg(mp + sj + u) - rj;
+        }
+      }
+    }
+  }
+}
+
+void launch_gather_expand(const ReadsDev& r, const SeedSet& seeds, const IndexView& ix,
+                          const int64_t* hoff, int32_t* cand, cudaStream_t st) {
+  (void)seeds;
+  if (r.n <= 0) return;
+  int64_t blocks = (r.n + 7) / 8;
+  if (blocks > 148 * 64) blocks = 148 * 64;
+  gather_expand_kernel<<<(unsigned)blocks, 256, 0, st>>>(r, ix, hoff, cand);
+}
+
+// Sorted, de-duplicated diagonals with the accept rule of run.c:617/648/697: a diagonal is
+// kept iff it is strictly greater than the previous one in sorted order, the "previous" of the
+// first being -I.
+constexpr int kWarpSortMax = 1024;
+
+__device__ __forceinline__ void warp_bitonic(int32_t* s, int P) {
+  const int lane = threadIdx.x & 31;
+  for (int k = 2; k <= P; k <<= 1)
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      for (int i = lane; i < P; i += 32) {
+        int ixj = i ^ j;
+        if (ixj > i) {
+          int32_t a = s[i], b = s[ixj];
+          bool up = (i & k) == 0;
+          if ((a > b) == up) { s[i] = b; s[ixj] = a; }
+        }
+      }
+      __syncwarp();
+    }
+}
+
+__global__ void segment_unique_kernel(int64_t n, const int32_t* __restrict__ hits,
+                                      const int64_t* __restrict__ hoff, int32_t* __restrict__ cand,
+                                      int32_t* __restrict__ ucount, int I, int32_t* __restrict__ big_list,
+                                      int32_t* __restrict__ big_count) {
+  __shared__ int32_t sm[8][kWarpSortMax];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  int32_t* s = sm[w];
+  const int64_t nwarps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  const unsigned lt = (1u << lane) - 1u;
+  for (int64_t r = (int64_t)blockIdx.x * (blockDim.x >> 5) + w; r < n; r += nwarps) {
+    const int H = hits[r];
+    if (H > kWarpSortMax) {
+      if (lane == 0) { int k = atomicAdd(big_count, 1); big_list[k] = (int32_t)r; }
+      continue;
+    }
+    int32_t* seg = cand + hoff[r];
+    int P = 1;
+    while (P < H) P <<= 1;
+    for (int i = lane; i < P; i += 32) s[i] = i < H ? seg[i] : 0x7fffffff;
+    __syncwarp();
+    warp_bitonic(s, P);
+    int out = 0;
+    for (int t0 = 0; t0 < H; t0 += 32) {
+      int t = t0 + lane;
+      int32_t v = t < H ? s[t] : 0;
+      int32_t prev = t == 0 ? -I : (t < H ? s[t - 1] : 0);
+      bool keep = t < H && v > prev;
+      unsigned m = __ballot_sync(0xffffffffu, keep);
+      if (keep) seg[out + __popc(m & lt)] = v;
+      out += __popc(m);
+    }
+    if (lane == 0) ucount[r] = out;
+    __syncwarp();
+  }
+}
+
+void launch_segment_unique(const ReadsDev& r, const int32_t* hits, const int64_t* hoff, int32_t* cand,
+                           int32_t* ucount, int I, int32_t* big_list, int32_t* big_count,
+                           cudaStream_t st) {
+  if (r.n <= 0) return;
+  int64_t blocks = (r.n + 7) / 8;
+  if (blocks > 148 * 32) blocks = 148 * 32;
+  segment_unique_kernel<<<(unsigned)blocks, 256, 0, st>>>(r.n, hits, hoff, cand, ucount, I, big_list, big_count);
+}
+
+// One block per long segment: bitonic sort in shared memory (<= 32768 elements) or, beyond
+// that, in the global scratch `tmp` (padded to a power of two).
+__global__ void segment_unique_big_kernel(const int32_t* __restrict__ big_list, const int32_t* __restrict__ hits,
+                                          const int64_t* __restrict__ hoff, int32_t* __restrict__ cand,
+                                          int32_t* __restrict__ ucount, int I, int32_t* __restrict__ tmp,
+                                          int smem_elems) {
+  extern __shared__ int32_t dsm[];
+  __shared__ int wsum[32];
+  const int64_t r = big_list[blockIdx.x];
+  const int H = hits[r];
+  int32_t* seg = cand + hoff[r];
+  int P = 1;
+  while (P < H) P <<= 1;
+  int32_t* s = (P <= smem_elems) ? dsm : tmp;
+  for (int i = threadIdx.x; i < P; i += blockDim.x) s[i] = i < H ? seg[i] : 0x7fffffff;
+  __syncthreads();
+  for (int k = 2; k <= P; k <<= 1)
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      for (int i = threadIdx.x; i < P; i += blockDim.x) {
+        int ixj = i ^ j;
+        if (ixj > i) {
+          int32_t a = s[i], b = s[ixj];
+          bool up = (i & k) == 0;
+          if ((a > b) == up) { s[i] = b; s[ixj] = a; }
+        }
+      }
+      __syncthreads();
+    }
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const unsigned lt = (1u << lane) - 1u;
+  int out = 0;
+  for (int t0 = 0; t0 < H; t0 += blockDim.x) {
+    int t = t0 + threadIdx.x;
+    int32_t v = t < H ? s[t] : 0;
+    int32_t prev = t == 0 ? -I : (t < H ? s[t - 1] : 0);
+    bool keep = t < H && v > prev;
+    unsigned m = __ballot_sync(0xffffffffu, keep);
+    if (lane == 0) wsum[w] = __popc(m);
+    __syncthreads();
+    int before = 0, tot = 0;
+    for (int q = 0; q < nw; ++q) { if (q < w) before += wsum[q]; tot += wsum[q]; }
+    if (keep) seg[out + before + __popc(m & lt)] = v;
+    out += tot;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) ucount[r] = out;
+}
+
+void launch_segment_unique_big(const int32_t* big_list, int nbig, const int32_t* hits,
+                               const int64_t* hoff, int32_t* cand, int32_t* ucount, int I,
+                               int32_t* tmp, int64_t tmp_elems, cudaStream_t st) {
+  if (nbig <= 0) return;
+  const int smem_elems = 32768;
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(segment_unique_big_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         smem_elems * 4);
+    attr = true;
+  }
+  (void)tmp_elems;
+  segment_unique_big_kernel<<<nbig, 1024, smem_elems * 4, st>>>(big_list, hits, hoff, cand, ucount, I, tmp, smem_elems);
+}
+
+// ------------------------------------------------------------------------------ filter
+
+// The banded saturating-u8 SW of alignment_avx2__align_* (alignment_simd.c:2613-3404) for one
+// hit: W cells; before the loop the genome register holds window codes 0..W-1 (cell k = code
+// W-1-k); odd steps shift one more genome code in at cell 0, even steps one more read code in
+// at cell W-1; per cell M = subs(adds(M[l-2], match if equal), mismatch if different),
+// I = max(subs(max(I[l-1], I[l-1] of the neighbour), ext), subs(max(M[l-1], M[l-1] of the
+// neighbour), open)) (neighbour below at odd steps, above at even steps, 0 at the edge),
+// M = max(M, I) & mask[l], Max = max(Max, M); pass iff Max > thr.  The mask table of
+// alignment_avx2__setlength_* (:2282-2507) is rebuilt incrementally per step.
+template <int W>
+__device__ __forceinline__ bool sw_filter_one(const uint8_t* __restrict__ genome, int64_t pos,
+                                              const uint8_t* read, int L, int fm, int fx, int fo,
+                                              int fe, int fthr) {
+  constexpr uint32_t FULLC = (W == 16) ? 0xffffffffu : ((1u << (2 * W)) - 1u);
+  constexpr uint32_t FULLM = (1u << W) - 1u;
+  int M1[W], M2[W], I1[W];
+#pragma unroll
+  for (int k = 0; k < W; ++k) { M1[k] = 0; M2[k] = 0; I1[k] = 0; }
+  uint32_t A = 0, B = 0;
+  int64_t g = pos;
+#pragma unroll
+  for (int d = 0; d < W; ++d) B = ((B << 2) | (uint32_t)code_at(genome, g++)) & FULLC;
+  const int prlength = 2 * (L + W - 1);
+  uint32_t msk = 1u << (W - 1);
+  int Max = 0, r = 0;
+  for (int l = 0; l < prlength; ++l) {
+    if (l > 0 && !(l & 1)) {
+      if (l >= prlength - 2 * (W - 1)) msk = (msk >> 1) & FULLM;
+      else if (l <= 2 * (W - 1)) msk = msk | ((msk >> 1) & FULLM);
+    }
+    const bool odd = l & 1;
+    if (odd) B = ((B << 2) | (uint32_t)code_at(genome, g++)) & FULLC;
+    else A = (A >> 2) | ((uint32_t)code_at(read, r++) << (2 * (W - 1)));
+    const uint32_t x = A ^ B;
+    int Mn[W], In[W];
+#pragma unroll
+    for (int k = 0; k < W; ++k) {
+      const bool eq = ((x >> (2 * k)) & 3u) == 0u;
+      int m = eq ? min(M2[k] + fm, 255) : max(M2[k] - fx, 0);
+      int Is_, Ms_;
+      if (odd) { Is_ = k > 0 ? I1[k - 1] : 0; Ms_ = k > 0 ? M1[k - 1] : 0; }
+      else { Is_ = k < W - 1 ? I1[k + 1] : 0; Ms_ = k < W - 1 ? M1[k + 1] : 0; }
+      const int Im = max(I1[k], Is_), Mm = max(M1[k], Ms_);
+      const int iv = max(max(Im - fe, 0), max(Mm - fo, 0));
+      m = max(m, iv);
+      if (!((msk >> k) & 1u)) m = 0;
+      Max = max(Max, m);
+      Mn[k] = m;
+      In[k] = iv;
+    }
+#pragma unroll
+    for (int k = 0; k < W; ++k) { M2[k] = M1[k]; M1[k] = Mn[k]; I1[k] = In[k]; }
+  }
+  return Max > fthr;
+}
+
+__device__ __forceinline__ bool sw_filter_dispatch(int W, const uint8_t* genome, int64_t pos,
+                                                   const uint8_t* read, int L, const ScoreParams& sp) {
+  switch (W) {
+  case 2: return sw_filter_one<2>(genome, pos, read, L, sp.fm, sp.fx, sp.fo, sp.fe, sp.fthr);
+  case 4: return sw_filter_one<4>(genome, pos, read, L, sp.fm, sp.fx, sp.fo, sp.fe, sp.fthr);
+  case 8: return sw_filter_one<8>(genome, pos, read, L, sp.fm, sp.fx, sp.fo, sp.fe, sp.fthr);
+  default: return sw_filter_one<16>(genome, pos, read, L, sp.fm, sp.fx, sp.fo, sp.fe, sp.fthr);
+  }
+}
+
+constexpr int kReadSmem = (STORMGPU_MAX_READ_LEN + 64) / 4;
+
+__global__ void filter_kernel(ReadsDev rd, ScoreParams sp, const uint8_t* __restrict__ genome,
+                              const int64_t* __restrict__ hoff, int32_t* __restrict__ cand,
+                              const int32_t* __restrict__ ucount, PassBuffers pb) {
+  __shared__ uint8_t sread[8][kReadSmem];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int64_t nwarps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  const unsigned lt = (1u << lane) - 1u;
+  unsigned long long cells = 0;
+  for (int64_t r = (int64_t)blockIdx.x * (blockDim.x >> 5) + w; r < rd.n; r += nwarps) {
+    const int U = ucount[r];
+    if (U == 0) {
+      if (lane == 0) { pb.pcount[r] = 0; pb.pstart[r] = 0; }
+      continue;
+    }
+    const int L = rd.lengths[r];
+    const uint8_t* src = rd.codes + r * rd.cstride;
+    const int nb = (L + sp.W + 8) / 4;
+    for (int b = lane; b < kReadSmem; b += 32) sread[w][b] = (b < nb && b < rd.cstride) ? src[b] : 0;
+    __syncwarp();
+    int32_t* seg = cand + hoff[r];
+    int P = 0;
+    for (int c0 = 0; c0 < U; c0 += 32) {
+      const int c = c0 + lane;
+      int32_t d = c < U ? seg[c] : 0;
+      bool pass = c < U && sw_filter_dispatch(sp.W, genome, (int64_t)d - sp.Is, sread[w], L, sp);
+      unsigned m = __ballot_sync(0xffffffffu, pass);
+      if (pass) seg[P + __popc(m & lt)] = d;  // in-place compaction (writes trail reads)
+      P += __popc(m);
+    }
+    cells += (unsigned long long)U * L * (2 * sp.Is + 1);
+    int start = 0;
+    if (lane == 0) start = (int)atomicAdd(&pb.counters[0], (unsigned long long)P);
+    start = __shfl_sync(0xffffffffu, start, 0);
+    if (lane == 0) { pb.pstart[r] = start; pb.pcount[r] = P; }
+    if ((int64_t)start + P > pb.p_cap) {
+      if (lane == 0) atomicExch(&pb.counters[1], 1ull);
+      continue;
+    }
+    __syncwarp();
+    for (int k = lane; k < P; k += 32) {
+      pb.p_read[start + k] = (int32_t)r;
+      pb.p_diag[start + k] = seg[k];
+    }
+    __syncwarp();
+  }
+  for (int o = 16; o > 0; o >>= 1) cells += __shfl_xor_sync(0xffffffffu, cells, o);
+  if (lane == 0) atomicAdd(&pb.counters[2], cells);
+}
+
+void launch_filter(const ReadsDev& r, const ScoreParams& sp, const uint8_t* genome,
+                   const int64_t* hoff, const int32_t* cand, const int32_t* ucount,
+                   PassBuffers& pb, cudaStream_t st) {
+  if (r.n <= 0) return;
+  int64_t blocks = (r.n + 7) / 8;
+  if (blocks > 148 * 64) blocks = 148 * 64;
+  filter_kernel<<<(unsigned)blocks, 256, 0, st>>>(r, sp, genome, hoff, (int32_t*)cand, ucount, pb);
+}
+
+__global__ void filter_flat_kernel(int W, int L, ScoreParams sp, const uint8_t* __restrict__ genome,
+                                   const int32_t* __restrict__ pos, int64_t n, const uint8_t* __restrict__ read,
+                                   uint8_t* __restrict__ pass) {
+  int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  pass[t] = sw_filter_dispatch(W, genome, pos[t], read, L, sp) ? 1 : 0;
+}
+
+void launch_filter_flat(int W, int L, const ScoreParams& sp, const uint8_t* genome,
+                        const int32_t* pos, int64_t n, const uint8_t* read, uint8_t* pass,
+                        cudaStream_t st) {
+  if (n <= 0) return;
+  filter_flat_kernel<<<(unsigned)((n + 127) / 128), 128, 0, st>>>(W, L, sp, genome, pos, n, read, pass);
+}
+
+// ------------------------------------------------------------------------------ align
+
+// Cell state packed in 16 bits: from (2) | indels (7) | colour checksum (2) | auto-correct (2)
+// | freshness (3).  "from": 3 corner, 2 top, 1 left (alignment.c:13-19).
+__device__ __forceinline__ int st_from(int s) { return s & 3; }
+__device__ __forceinline__ int st_ind(int s) { return (s >> 2) & 127; }
+__device__ __forceinline__ int st_chk(int s) { return (s >> 9) & 3; }
+__device__ __forceinline__ int st_ac(int s) { return (s >> 11) & 3; }
+__device__ __forceinline__ int st_fr(int s) { return (s >> 13) & 7; }
+__device__ __forceinline__ int st_make(int from, int ind, int chk, int ac, int fr) {
+  return from | (ind << 2) | (chk << 9) | (ac << 11) | (fr << 13);
+}
+
+constexpr int kMaxBand = 2 * STORMGPU_MAX_INDELS + 1;
+
+// alignment.c:326-360 (init), :488-632 (rows 1..L-1, corner > top > left on ties, gaps only
+// while indels < I, affine through the predecessor's direction, colour checksum state
+// machine :535-603 with the SNP adjustment :465-468), best cell on the last row (:621-630),
+// traceback :642-734.  The direction of every cell (2 bits) and, in colour space, whether its
+// pair score was made positive by the SNP adjustment (the `score > corner score` test of
+// :693) go to the scratch, slot-minor: word (row*wpr + k)*nslots + slot.
+__global__ void align_kernel(ReadsDev rd, ScoreParams sp, const uint8_t* __restrict__ genome,
+                             const uint8_t* __restrict__ mask, int64_t slot0, int64_t nslots, PassBuffers pb) {
+  const int64_t sl = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (sl >= nslots) return;
+  const int64_t slot = slot0 + sl;
+  const int r = pb.p_read[slot];
+  const int d = pb.p_diag[slot];
+  const int I = sp.I, BW = 2 * I + 1, colour = sp.colour;
+  const int L = rd.lengths[r];
+  const uint8_t* rdc = rd.codes + (int64_t)r * rd.cstride;
+  const uint8_t* rdq = rd.levels ? rd.levels + (int64_t)r * rd.lstride : nullptr;
+  const int win = max(d - I, -sp.Is);  // run.c:667
+  const int wpr_dir = (2 * BW + 31) / 32, wpr = wpr_dir + (colour ? (BW + 31) / 32 : 0);
+  uint32_t* scr = pb.a_scratch;
+  const int64_t ns = nslots;
+  int sc[kMaxBand], stt[kMaxBand];
+  const int mbest = sp.pair[0][3];
+  // row 0
+  {
+    const int rc = code_at(rdc, 0), q = rdq ? code_at(rdq, 0) : 3;
+    uint32_t wd[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    for (int c = 0; c < BW; ++c) {
+      const int64_t j = (int64_t)win + c;
+      const int f = code_at(genome, j);
+      int chk = 0, score;
+      if (code_at(mask, j) == 0) {
+        chk = colour ? (rc ^ f) : 0;
+        score = sp.pair[colour ? (chk ? 1 : 0) : (rc != f)][q];
+      } else score = kMinScore;
+      sc[c] = score;
+      stt[c] = st_make(3, 0, chk, chk, (colour && chk) ? q : 0);
+      wd[(2 * c) >> 5] |= 3u << ((2 * c) & 31);
+    }
+    for (int k = 0; k < wpr; ++k) scr[(int64_t)k * ns + sl] = k < wpr_dir ? wd[k] : 0u;
+  }
+  int best_possible = (colour ? (L - 2) : L) * mbest;
+  long long bound = 0x7fffffffLL;
+  for (int i = 1; i < L; ++i) {
+    const int rc = code_at(rdc, i), q = rdq ? code_at(rdq, i) : 3;
+    int max_on_line = kMinScore;
+    int lsc = kMinScore, lst = st_make(3, I, 0, 0, 0);  // left border
+    uint32_t wd[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    uint32_t wc[5] = {0, 0, 0, 0, 0};
+    for (int c = 0; c < BW; ++c) {
+      const int64_t j = (int64_t)win + i + c;
+      const int f = code_at(genome, j);
+      // initial values of this cell (alignment__init_matrix)
+      int chk0 = 0, ac0 = 0, fr0 = 0, s0;
+      if (code_at(mask, j) == 0) {
+        if (colour) { chk0 = ac0 = rc ^ f; fr0 = ac0 ? q : 0; s0 = sp.pair[chk0 ? 1 : 0][q]; }
+        else s0 = sp.pair[rc != f][q];
+      } else s0 = kMinScore;
+      const int csc = sc[c], cst = stt[c];
+      const int tsc = c + 1 < BW ? sc[c + 1] : kMinScore;
+      const int tst = c + 1 < BW ? stt[c + 1] : st_make(3, I, 0, 0, 0);
+      int ms = s0;
+      if (colour) {
+        const int prev = st_chk(cst), cmp = prev ^ chk0;
+        if (prev && (cmp == 0 || cmp == st_ac(cst)) && s0 != kMinScore && s0 < 0) ms = -2 * s0;
+      }
+      int score = csc + ms, it = 0, tmp;
+      if (st_ind(tst) < I && (tmp = tsc + ((st_from(tst) ^ 2) ? sp.gap_open : sp.gap_ext)) > score) { it = 1; score = tmp; }
+      if (st_ind(lst) < I && (tmp = lsc + ((st_from(lst) ^ 1) ? sp.gap_open : sp.gap_ext)) > score) { it = 2; score = tmp; }
+      int from = 3, ind, chk = chk0, ac = ac0, fr = fr0;
+      if (it == 0) {
+        ind = st_ind(cst);
+        if (colour) {
+          const int cchk = st_chk(cst), cac = st_ac(cst), cfr = st_fr(cst);
+          chk = chk0 ^ cchk;
+          if (cchk != chk) {
+            if (cchk == 0) { ac = chk; fr = q; }
+            else if (chk == cac) { ac = 0; chk = 0; fr = 0; }
+            else if (chk == 0) { if (cfr - 1 > 0) { ac = cac; fr = cfr - 1; } else { ac = 0; fr = 0; } }
+            else { if (cfr - 1 > 0) { ac = cac; fr = cfr - 1; } else { ac = chk; fr = q; } }
+          } else {
+            if (cac != 0) {
+              if (cfr - 1 > 0) {
+                if (chk == 0) { ac = 0; fr = 0; } else { ac = cac; fr = cfr - 1; }
+              }
+            } else { chk = 0; ac = 0; fr = 0; }
+          }
+        }
+      } else if (it == 1) {
+        from = 2;
+        ind = st_ind(tst) + 1;
+        if (colour) {
+          chk = st_chk(tst) ^ rc;
+          if (st_fr(tst) - 1 > 0) { fr = st_fr(tst) - 1; ac = st_ac(cst); }
+        }
+      } else {
+        from = 1;
+        ind = st_ind(lst) + 1;
+        if (colour) {
+          chk = st_chk(lst) ^ f;
+          if (st_fr(lst) - 1 > 0) { fr = st_fr(lst) - 1; ac = st_ac(cst); }
+        }
+      }
+      const int nst = st_make(from, ind, chk, ac, fr);
+      sc[c] = score;
+      stt[c] = nst;
+      lsc = score;
+      lst = nst;
+      if (max_on_line < score) max_on_line = score;
+      wd[(2 * c) >> 5] |= (uint32_t)from << ((2 * c) & 31);
+      if (colour && it == 0 && ms > 0) wc[c >> 5] |= 1u << (c & 31);
+    }
+    if ((long long)max_on_line + best_possible < bound) bound = (long long)max_on_line + best_possible;
+    best_possible -= mbest;
+    for (int k = 0; k < wpr_dir; ++k) scr[((int64_t)i * wpr + k) * ns + sl] = wd[k];
+    if (colour)
+      for (int k = wpr_dir; k < wpr; ++k) scr[((int64_t)i * wpr + k) * ns + sl] = wc[k - wpr_dir];
+  }
+  int best = kMinScore, bi = -1, bj = -1;
+  for (int c = 0; c < BW; ++c)
+    if (best < sc[c]) { best = sc[c]; bi = L - 1; bj = L - 1 + c; }
+  const int32_t bnd = bound > 0x7fffffffLL ? 0x7fffffff : (int32_t)bound;
+  pb.a_score[slot] = best;
+  pb.a_bound[slot] = bnd;
+  int i0 = bi, j0 = bj, tl = 0;
+  uint8_t* tb = pb.a_tb + slot * pb.tbs;
+  if (bi >= 0 && bnd >= sp.min_score && best > sp.min_score) {
+    int i = bi, c = bj - bi, colr = 0;
+    uint8_t cur = 0;
+    while (i >= 0 && i < L && c >= 0 && c < BW) {
+      const int j = i + c;
+      i0 = i;
+      j0 = j;
+      const uint32_t wdir = scr[((int64_t)i * wpr + ((2 * c) >> 5)) * ns + sl];
+      const int from = (wdir >> ((2 * c) & 31)) & 3;
+      const int rc = code_at(rdc, i);
+      int op;
+      if (from == 2) op = 0xC | rc;
+      else if (from == 1) op = 0x1;
+      else {
+        const int f = code_at(genome, (int64_t)win + j);
+        if (rc != f) {
+          if (!colour) op = 0x4 | rc;
+          else {
+            bool adj = false;
+            if (i != 0 && j != 0) {
+              const uint32_t wcol = scr[((int64_t)i * wpr + wpr_dir + (c >> 5)) * ns + sl];
+              adj = (wcol >> (c & 31)) & 1u;
+            }
+            if (colr || adj) { op = 0x8 | rc; colr ^= rc ^ f; }
+            else op = 0x4 | rc;
+          }
+        } else op = 0x3;
+      }
+      if (tl & 1) { cur |= (uint8_t)op; tb[tl >> 1] = cur; }
+      else { cur = (uint8_t)(op << 4); tb[tl >> 1] = cur; }
+      tl++;
+      if (from == 2) { i--; c++; }
+      else if (from == 1) { c--; }
+      else { i--; }
+    }
+  }
+  pb.a_tblen[slot] = tl;
+  pb.a_pos[slot * 4 + 0] = (int16_t)bi;
+  pb.a_pos[slot * 4 + 1] = (int16_t)bj;
+  pb.a_pos[slot * 4 + 2] = (int16_t)i0;
+  pb.a_pos[slot * 4 + 3] = (int16_t)j0;
+}
+
+void launch_align(const ReadsDev& r, const ScoreParams& sp, const uint8_t* genome,
+                  const uint8_t* mask, int64_t slot0, int64_t nslots, PassBuffers& pb,
+                  cudaStream_t st) {
+  if (nslots <= 0) return;
+  align_kernel<<<(unsigned)((nslots + 127) / 128), 128, 0, st>>>(r, sp, genome, mask, slot0, nslots, pb);
+}
+
+// ------------------------------------------------------------------------------ replay
+
+__device__ __forceinline__ int tbget(const uint8_t* t, int i) { return (t[i >> 1] >> ((i & 1) ? 0 : 4)) & 0xF; }
+
+// process_read's acceptance (run.c:664-691) in the reference's order, with the
+// threshold starting at -t for every (sequence, strand, read): aborted iff the bound is
+// below the running threshold; accepted iff not aborted and score > threshold; then
+// hit_map__update (hit_map.c:50-144) and threshold = max(threshold, 4th score).
+__global__ void replay_kernel(int64_t n, ScoreParams sp, int ref_id, int sense, PassBuffers pb,
+                              stormgpu_hit* __restrict__ hits, uint8_t* __restrict__ tbo, int64_t tbs,
+                              uint8_t* __restrict__ mapped) {
+  const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= n) return;
+  const int P = pb.pcount[r];
+  if (P == 0) return;
+  const int64_t s0 = pb.pstart[r];
+  int T = sp.min_score;
+  stormgpu_hit* h = hits + r * 4;
+  for (int k = 0; k < P; ++k) {
+    const int64_t slot = s0 + k;
+    const int score = pb.a_score[slot];
+    if (!(pb.a_bound[slot] >= T && score > T)) continue;
+    const int win = max(pb.p_diag[slot] - sp.I, -sp.Is);
+    const int bi = pb.a_pos[slot * 4 + 0], bj = pb.a_pos[slot * 4 + 1];
+    const int i0 = pb.a_pos[slot * 4 + 2], j0 = pb.a_pos[slot * 4 + 3];
+    mapped[r] = 1;
+    int q;
+    bool dup_worse = false;
+    for (q = 0; q < 4 && h[q].ref_id != -1; ++q) {
+      if (h[q].ref_id == ref_id &&
+          ((h[q].ref_start == win + j0 && h[q].read_start == i0) ||
+           (h[q].ref_end == win + bj && h[q].read_end == bi))) {
+        if (score > h[q].score) break;
+        dup_worse = true;
+        break;
+      }
+    }
+    if (!dup_worse) {
+      if (q == 4) q--;
+      int i = q;
+      while (i >= 0 && score > h[i].score) i--;
+      if (i != 3) {
+        for (int j = q; j > i + 1; --j) {
+          h[j] = h[j - 1];
+          for (int64_t b = 0; b < tbs; ++b) tbo[(r * 4 + j) * tbs + b] = tbo[(r * 4 + j - 1) * tbs + b];
+        }
+        stormgpu_hit nh;
+        nh.score = score;
+        nh.ref_id = ref_id;
+        nh.ref_start = win + j0;
+        nh.ref_end = win + bj;
+        nh.read_start = (int16_t)i0;
+        nh.read_end = (int16_t)bi;
+        nh.sense = sense;
+        const int tl = pb.a_tblen[slot];
+        nh.tb_len = tl;
+        h[i + 1] = nh;
+        uint8_t* dst = tbo + (r * 4 + i + 1) * tbs;
+        const uint8_t* srcb = pb.a_tb + slot * pb.tbs;
+        for (int64_t b = 0; b < tbs; ++b) dst[b] = 0;
+        for (int p = 0; p < tl; ++p) {
+          int v = tbget(srcb, tl - 1 - p);
+          if (p & 1) dst[p >> 1] |= (uint8_t)v;
+          else dst[p >> 1] |= (uint8_t)(v << 4);
+        }
+      }
+    }
+    if (h[3].score > T) T = h[3].score;
+  }
+}
+
+void launch_replay(int64_t n, const ScoreParams& sp, int ref_id, int sense, PassBuffers& pb,
+                   stormgpu_hit* hits, uint8_t* tb, int64_t tbs, uint8_t* mapped, cudaStream_t st) {
+  if (n <= 0) return;
+  replay_kernel<<<(unsigned)((n + 127) / 128), 128, 0, st>>>(n, sp, ref_id, sense, pb, hits, tb, tbs, mapped);
+}
+
+}  // namespace sg

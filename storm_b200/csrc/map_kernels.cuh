@@ -1,0 +1,90 @@
+// map_kernels.cuh -- per-pass mapping kernels (one reference sequence x one strand).
+#pragma once
+
+#include "common.cuh"
+
+namespace sg {
+
+// Scoring, as the kernels need it.
+struct ScoreParams {
+  int colour;
+  int I;              // -i
+  int Is;             // min(-i, 15): SIMD band half-width (main.c:302-313)
+  int W;              // filter cells per hit: 2, 4, 8, 16 (run.c:64-101)
+  int fm, fx, fo, fe; // filter scores: low bytes of |match|, |mismatch|, |open|, |extend|
+  int fthr;           // filter threshold, min(z, 254) (alignment_simd.c:2525-2527)
+  int pair[2][4];     // SCALE_SCORE(match|mismatch, level) (alignment.h:30, alignment.c:275-278)
+  int gap_open, gap_ext;
+  int min_score;      // -t
+};
+
+struct ReadsDev {
+  int64_t n;
+  const uint8_t* codes;
+  int64_t cstride;
+  const uint8_t* levels;   // may be null
+  int64_t lstride;
+  const int16_t* lengths;
+};
+
+struct IndexView {
+  const int32_t* first[kMaxSeeds];
+  const int32_t* map[kMaxSeeds];
+};
+
+struct PassBuffers {
+  // gather
+  int32_t* hits;        // per read: number of index positions (G1)
+  int64_t* hoff;        // per read: offset in cand (scan of hits)
+  int32_t* ucount;      // per read: unique candidate diagonals (G3)
+  int32_t* cand;        // candidate diagonals, per-read segments
+  int64_t cand_cap;
+  // filter -> flat list of passing candidates
+  int32_t* pstart;      // per read: first slot
+  int32_t* pcount;      // per read: number of passing candidates
+  int32_t* p_read;      // per slot
+  int32_t* p_diag;
+  int64_t p_cap;
+  unsigned long long* counters;  // [0] slots used, [1] overflow flag, [2] filter cells, [3] lookups, [4] positions
+  // align outputs per slot
+  int32_t* a_score;
+  int32_t* a_bound;
+  int16_t* a_pos;       // 4 per slot: best_i, best_j, best_i0, best_j0
+  int32_t* a_tblen;
+  uint8_t* a_tb;        // tbs bytes per slot (end-to-start order)
+  int64_t tbs;
+  uint32_t* a_scratch;  // direction bits, see align kernel
+  int64_t scratch_words;
+  int32_t* big_list;    // reads whose segment is too long for the warp sort
+  int32_t* big_count;
+};
+
+void launch_reverse_reads(const ReadsDev& in, const uint8_t* first_levels, int colour,
+                          uint8_t* rcodes, uint8_t* rlevels, cudaStream_t st);
+void launch_init_results(int64_t n, stormgpu_hit* hits, uint8_t* mapped, uint8_t* tb, int64_t tbs,
+                         cudaStream_t st);
+void launch_gather_count(const ReadsDev& r, const SeedSet& seeds, const IndexView& ix,
+                         int32_t* hits, unsigned long long* counters, cudaStream_t st);
+void launch_gather_expand(const ReadsDev& r, const SeedSet& seeds, const IndexView& ix,
+                          const int64_t* hoff, int32_t* cand, cudaStream_t st);
+void launch_segment_unique(const ReadsDev& r, const int32_t* hits, const int64_t* hoff, int32_t* cand,
+                           int32_t* ucount, int I, int32_t* big_list, int32_t* big_count,
+                           cudaStream_t st);
+void launch_segment_unique_big(const int32_t* big_list, int nbig, const int32_t* hits,
+                               const int64_t* hoff, int32_t* cand, int32_t* ucount, int I,
+                               int32_t* tmp, int64_t tmp_elems, cudaStream_t st);
+void launch_filter(const ReadsDev& r, const ScoreParams& sp, const uint8_t* genome,
+                   const int64_t* hoff, const int32_t* cand, const int32_t* ucount,
+                   PassBuffers& pb, cudaStream_t st);
+void launch_align(const ReadsDev& r, const ScoreParams& sp, const uint8_t* genome,
+                  const uint8_t* mask, int64_t slot0, int64_t nslots, PassBuffers& pb,
+                  cudaStream_t st);
+void launch_replay(int64_t n, const ScoreParams& sp, int ref_id, int sense, PassBuffers& pb,
+                   stormgpu_hit* hits, uint8_t* tb, int64_t tbs, uint8_t* mapped, cudaStream_t st);
+
+// unit-level kernels
+void launch_filter_flat(int W, int L, const ScoreParams& sp, const uint8_t* genome,
+                        const int32_t* pos, int64_t n, const uint8_t* read, uint8_t* pass,
+                        cudaStream_t st);
+
+}  // namespace sg

@@ -1,0 +1,104 @@
+// radix.cuh -- stable LSD radix sort of (32-bit key, 32-bit value) pairs, 8-bit digits.
+//
+// Per pass: (1) per-tile digit histograms, stored digit-major so that (2) one exclusive scan
+// gives every (digit, tile) its output offset, then (3) each tile re-reads its items and
+// scatters them, ranking equal digits in input order with __match_any_sync inside a warp and
+// a per-digit running count across the warps and rounds of the tile.  Stability is what the
+// seed index needs: positions are generated in increasing order and must stay so per key.
+#pragma once
+
+#include "scan.cuh"
+
+namespace sg {
+
+constexpr int kRadixBits = 8;
+constexpr int kRadixBins = 1 << kRadixBits;
+constexpr int kSortThreads = 256;
+constexpr int kSortRounds = 16;
+constexpr int kSortTile = kSortThreads * kSortRounds;
+
+__global__ void radix_hist_kernel(const uint32_t* __restrict__ keys, int64_t n, int shift,
+                                  uint32_t* __restrict__ hist, int ntiles) {
+  __shared__ uint32_t h[kRadixBins];
+  for (int i = threadIdx.x; i < kRadixBins; i += blockDim.x) h[i] = 0;
+  __syncthreads();
+  const int64_t base = (int64_t)blockIdx.x * kSortTile;
+  for (int r = 0; r < kSortRounds; ++r) {
+    int64_t i = base + (int64_t)r * kSortThreads + threadIdx.x;
+    if (i < n) atomicAdd(&h[(keys[i] >> shift) & (kRadixBins - 1)], 1u);
+  }
+  __syncthreads();
+  for (int d = threadIdx.x; d < kRadixBins; d += blockDim.x)
+    hist[(int64_t)d * ntiles + blockIdx.x] = h[d];
+}
+
+__global__ void radix_scatter_kernel(const uint32_t* __restrict__ keys_in,
+                                     const uint32_t* __restrict__ vals_in, int64_t n, int shift,
+                                     const uint32_t* __restrict__ offs, int ntiles,
+                                     uint32_t* __restrict__ keys_out, uint32_t* __restrict__ vals_out) {
+  constexpr int NW = kSortThreads / 32;
+  __shared__ uint32_t run[kRadixBins];
+  __shared__ uint32_t wc[NW][kRadixBins];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int d = threadIdx.x; d < kRadixBins; d += blockDim.x) run[d] = offs[(int64_t)d * ntiles + blockIdx.x];
+  const int64_t base = (int64_t)blockIdx.x * kSortTile;
+  const unsigned lt = (1u << lane) - 1u;
+  for (int r = 0; r < kSortRounds; ++r) {
+    const int64_t i = base + (int64_t)r * kSortThreads + threadIdx.x;
+    const bool valid = i < n;
+    uint32_t k = valid ? keys_in[i] : 0u, v = valid ? vals_in[i] : 0u;
+    int d = valid ? (int)((k >> shift) & (kRadixBins - 1)) : kRadixBins;  // invalid: own group
+    for (int t = threadIdx.x; t < NW * kRadixBins; t += blockDim.x) (&wc[0][0])[t] = 0;
+    __syncthreads();
+    unsigned peers = __match_any_sync(0xffffffffu, d);
+    int rank = __popc(peers & lt);
+    if (valid && rank == 0) wc[warp][d] = (uint32_t)__popc(peers);
+    __syncthreads();
+    for (int dd = threadIdx.x; dd < kRadixBins; dd += blockDim.x) {
+      uint32_t o = run[dd];
+#pragma unroll
+      for (int w = 0; w < NW; ++w) {
+        uint32_t c = wc[w][dd];
+        wc[w][dd] = o;
+        o += c;
+      }
+      run[dd] = o;
+    }
+    __syncthreads();
+    if (valid) {
+      uint32_t dst = wc[warp][d] + (uint32_t)rank;
+      keys_out[dst] = k;
+      vals_out[dst] = v;
+    }
+    __syncthreads();
+  }
+}
+
+inline int64_t radix_tmp_bytes(int64_t n) {
+  int64_t ntiles = (n + kSortTile - 1) / kSortTile;
+  int64_t h = ntiles * kRadixBins;
+  return (2 * h + scan_tmp_elems(h) + 16) * (int64_t)sizeof(uint32_t);
+}
+
+// Sort n pairs by the low `bits` bits of the keys.  Result in (k0, v0) if the number of passes
+// is even, else in (k1, v1); returns 0 or 1 accordingly.  n < 2^32.
+inline int radix_sort_pairs(uint32_t* k0, uint32_t* v0, uint32_t* k1, uint32_t* v1, int64_t n,
+                            int bits, void* tmp, cudaStream_t st) {
+  if (n <= 0) return 0;
+  const int ntiles = (int)((n + kSortTile - 1) / kSortTile);
+  const int64_t h = (int64_t)ntiles * kRadixBins;
+  uint32_t* hist = (uint32_t*)tmp;
+  uint32_t* offs = hist + h;
+  uint32_t* stmp = offs + h;
+  int cur = 0;
+  for (int shift = 0; shift < bits; shift += kRadixBits) {
+    uint32_t *ki = cur ? k1 : k0, *vi = cur ? v1 : v0, *ko = cur ? k0 : k1, *vo = cur ? v0 : v1;
+    radix_hist_kernel<<<ntiles, kSortThreads, 0, st>>>(ki, n, shift, hist, ntiles);
+    exclusive_scan<uint32_t, uint32_t>(hist, offs, h, (uint32_t*)nullptr, stmp, st);
+    radix_scatter_kernel<<<ntiles, kSortThreads, 0, st>>>(ki, vi, n, shift, offs, ntiles, ko, vo);
+    cur ^= 1;
+  }
+  return cur;
+}
+
+}  // namespace sg

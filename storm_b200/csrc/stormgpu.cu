@@ -1,0 +1,658 @@
+// stormgpu.cu -- the C ABI of include/stormgpu.h: context, reference upload, index build,
+// and the mapping pipeline (per reference sequence, per strand: hit gather -> filter ->
+// full alignment -> top-4 replay), plus the unit-level entry points used by the tests.
+#include <algorithm>
+#include <cstdarg>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+#include "index_build.cuh"
+#include "map_kernels.cuh"
+#include "scan.cuh"
+
+static thread_local char g_err[1024];
+
+void sg_set_error(const char* fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_err, sizeof(g_err), fmt, ap);
+  va_end(ap);
+}
+
+extern "C" const char* stormgpu_version(void) { return "storm-b200 0.1 (sm_100a)"; }
+extern "C" const char* stormgpu_last_error(void) { return g_err; }
+
+extern "C" int stormgpu_device_available(void) {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess) { cudaGetLastError(); return 0; }
+  return n > 0 ? 1 : 0;
+}
+
+namespace {
+
+using namespace sg;
+
+// seed.c:25-135: ';'-separated patterns of '#'/'1' (care) and '-'/'0' (don't care), each with
+// an optional ":p1 p2,p3" list of read positions.
+int parse_seeds(const char* list, SeedSet* out) {
+  memset(out, 0, sizeof(*out));
+  if (!list) return STORMGPU_EINVAL;
+  std::string s(list);
+  size_t p = 0;
+  while (p <= s.size()) {
+    size_t e = s.find(';', p);
+    if (e == std::string::npos) e = s.size();
+    std::string tok = s.substr(p, e - p);
+    p = e + 1;
+    if (tok.empty()) { if (e == s.size()) break; continue; }
+    if (out->n >= kMaxSeeds) return STORMGPU_EINVAL;
+    SeedDev& sd = out->s[out->n];
+    size_t colon = tok.find(':');
+    std::string pat = tok.substr(0, colon);
+    if (pat.empty() || (int)pat.size() > kMaxSpan) return STORMGPU_EINVAL;
+    sd.span = (int)pat.size();
+    for (int i = 0; i < sd.span; ++i) {
+      char c = pat[i];
+      if (c == '#' || c == '1') sd.care[sd.n_care++] = (int8_t)i;
+      else if (c != '-' && c != '0') return STORMGPU_EINVAL;
+    }
+    sd.weight = sd.n_care;
+    if (sd.weight == 0 || sd.weight > 15) return STORMGPU_EINVAL;
+    if (colon != std::string::npos && tok.size() - colon > 1) {
+      std::string rest = tok.substr(colon + 1);
+      int v;
+      if (sscanf(rest.c_str(), "%d", &v) == 1) {
+        char* save = nullptr;
+        std::vector<char> buf(rest.begin(), rest.end());
+        buf.push_back(0);
+        for (char* t = strtok_r(buf.data(), ", ", &save); t; t = strtok_r(nullptr, ", ", &save)) {
+          if (sscanf(t, "%d", &v) != 1 || sd.n_positions >= kMaxPositions) break;
+          sd.positions[sd.n_positions++] = (int16_t)v;
+        }
+      }
+    }
+    out->n++;
+    if (e == s.size()) break;
+  }
+  return out->n > 0 ? 0 : STORMGPU_EINVAL;
+}
+
+int filter_width(int is) { return is <= 1 ? 2 : is <= 3 ? 4 : is <= 7 ? 8 : 16; }
+
+ScoreParams make_score_params(const stormgpu_params& p) {
+  ScoreParams sp;
+  memset(&sp, 0, sizeof(sp));
+  sp.colour = p.colour;
+  sp.I = p.allowed_indels;
+  sp.Is = p.allowed_indels < 15 ? p.allowed_indels : 15;
+  sp.W = filter_width(sp.Is);
+  sp.fm = std::abs(p.match) & 0xff;
+  sp.fx = std::abs(p.mismatch) & 0xff;
+  sp.fo = std::abs(p.gap_open) & 0xff;
+  sp.fe = std::abs(p.gap_extend) & 0xff;
+  unsigned z = (unsigned)p.min_score_filter;
+  sp.fthr = z >= 255u ? 254 : (int)z;
+  for (int l = 0; l < 4; ++l) {
+    sp.pair[0][l] = (int)(((p.match) * (l + 1) + 0.) / 4);     // SCALE_SCORE, alignment.h:30
+    sp.pair[1][l] = (int)(((p.mismatch) * (l + 1) + 0.) / 4);
+  }
+  sp.gap_open = p.gap_open;
+  sp.gap_ext = p.gap_extend;
+  sp.min_score = p.min_score;
+  return sp;
+}
+
+struct RefSeq {
+  int64_t n = 0;
+  uint8_t* d_codes_alloc = nullptr;
+  uint8_t* d_mask_alloc = nullptr;
+  uint8_t* d_codes = nullptr;
+  uint8_t* d_mask = nullptr;
+  std::vector<int32_t> rs, re;
+  std::vector<DevIndex> idx;
+};
+
+template <typename T>
+struct DevBuf {
+  T* p = nullptr;
+  int64_t cap = 0;
+  int grow(int64_t n) {
+    if (n <= cap) return 0;
+    if (p) cudaFree(p);
+    p = nullptr;
+    int64_t c = std::max<int64_t>(n, cap + cap / 2);
+    if (cudaMalloc(&p, sizeof(T) * (size_t)std::max<int64_t>(c, 1)) != cudaSuccess) {
+      cudaGetLastError();
+      cap = 0;
+      sg_set_error("device allocation of %lld bytes failed", (long long)(sizeof(T) * c));
+      return STORMGPU_ENOMEM;
+    }
+    cap = c;
+    return 0;
+  }
+  void release() { if (p) cudaFree(p); p = nullptr; cap = 0; }
+};
+
+}  // namespace
+
+struct stormgpu_ctx {
+  stormgpu_params p;
+  SeedSet seeds;
+  cudaStream_t st = nullptr;
+  std::vector<RefSeq> refs;
+  bool indexed = false;
+  stormgpu_stats stats;
+  // per-batch read buffers
+  DevBuf<uint8_t> rcodes, rlevels, fcodes, flevels, first_levels;
+  DevBuf<int16_t> lengths;
+  DevBuf<stormgpu_hit> hits;
+  DevBuf<uint8_t> tb, mapped;
+  // pass buffers
+  DevBuf<int32_t> hitsc, ucount, cand, pstart, pcount, p_read, p_diag, big_list, big_count;
+  DevBuf<int64_t> hoff, scan_tmp64;
+  DevBuf<int32_t> a_score, a_bound, a_tblen, big_tmp;
+  DevBuf<int16_t> a_pos;
+  DevBuf<uint8_t> a_tb;
+  DevBuf<uint32_t> scratch;
+  DevBuf<unsigned long long> counters;
+  cudaEvent_t ev[8];
+};
+
+extern "C" int stormgpu_open(const stormgpu_params* params, const char* seeds, stormgpu_ctx** out) {
+  if (!params || !out) { sg_set_error("null argument"); return STORMGPU_EINVAL; }
+  *out = nullptr;
+  SeedSet ss;
+  if (parse_seeds(seeds, &ss) != 0) { sg_set_error("invalid seed list \"%s\"", seeds ? seeds : "(null)"); return STORMGPU_EINVAL; }
+  if (params->allowed_indels < 0 || params->allowed_indels > STORMGPU_MAX_INDELS) { sg_set_error("allowed_indels out of range"); return STORMGPU_EINVAL; }
+  if (params->min_score < STORMGPU_MIN_SCORE) { sg_set_error("min_score below MIN_SCORE is not supported"); return STORMGPU_EINVAL; }
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    sg_set_error("no CUDA device available: the mapping path runs on the GPU only");
+    return STORMGPU_ECUDA;
+  }
+  if (params->device < 0 || params->device >= ndev) { sg_set_error("bad device ordinal"); return STORMGPU_EINVAL; }
+  SG_CUDA(cudaSetDevice(params->device));
+  stormgpu_ctx* c = new stormgpu_ctx();
+  c->p = *params;
+  c->seeds = ss;
+  memset(&c->stats, 0, sizeof(c->stats));
+  if (cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking) != cudaSuccess) {
+    delete c;
+    sg_set_error("cudaStreamCreate failed");
+    return STORMGPU_ECUDA;
+  }
+  for (auto& e : c->ev) cudaEventCreate(&e);
+  *out = c;
+  return 0;
+}
+
+extern "C" void stormgpu_close(stormgpu_ctx* c) {
+  if (!c) return;
+  cudaSetDevice(c->p.device);
+  cudaStreamSynchronize(c->st);
+  for (auto& r : c->refs) {
+    cudaFree(r.d_codes_alloc);
+    cudaFree(r.d_mask_alloc);
+    for (auto& ix : r.idx) { cudaFree(ix.first); cudaFree(ix.map); }
+  }
+  c->rcodes.release(); c->rlevels.release(); c->fcodes.release(); c->flevels.release();
+  c->first_levels.release(); c->lengths.release(); c->hits.release(); c->tb.release();
+  c->mapped.release(); c->hitsc.release(); c->ucount.release(); c->cand.release();
+  c->pstart.release(); c->pcount.release(); c->p_read.release(); c->p_diag.release();
+  c->big_list.release(); c->big_count.release(); c->hoff.release(); c->scan_tmp64.release();
+  c->a_score.release(); c->a_bound.release(); c->a_tblen.release(); c->big_tmp.release();
+  c->a_pos.release(); c->a_tb.release(); c->scratch.release(); c->counters.release();
+  for (auto& e : c->ev) cudaEventDestroy(e);
+  cudaStreamDestroy(c->st);
+  delete c;
+}
+
+extern "C" int stormgpu_add_reference(stormgpu_ctx* c, const uint8_t* codes, const uint8_t* mask,
+                                      int64_t n_codes, const int32_t* rs, const int32_t* re,
+                                      int32_t n_regions) {
+  if (!c || !codes || n_codes < 0 || (n_regions > 0 && (!rs || !re))) { sg_set_error("bad reference arguments"); return STORMGPU_EINVAL; }
+  if (n_codes >= INT32_MAX) { sg_set_error("reference sequence longer than 2^31 codes"); return STORMGPU_EINVAL; }
+  SG_CUDA(cudaSetDevice(c->p.device));
+  RefSeq r;
+  r.n = n_codes;
+  const int64_t nb = (n_codes + 3) / 4;
+  const int64_t tot = nb + 2 * kPadBytes + 16;
+  SG_CUDA(cudaMalloc(&r.d_codes_alloc, tot));
+  SG_CUDA(cudaMalloc(&r.d_mask_alloc, tot));
+  r.d_codes = r.d_codes_alloc + kPadBytes;
+  r.d_mask = r.d_mask_alloc + kPadBytes;
+  SG_CUDA(cudaMemsetAsync(r.d_codes_alloc, 0, tot, c->st));
+  SG_CUDA(cudaMemsetAsync(r.d_mask_alloc, 0x55, tot, c->st));
+  std::vector<uint8_t> hc(codes, codes + nb);
+  if (n_codes & 3) hc[nb - 1] &= (uint8_t)((1u << (2 * (n_codes & 3))) - 1);  // zero past the end
+  SG_CUDA(cudaMemcpyAsync(r.d_codes, hc.data(), nb, cudaMemcpyHostToDevice, c->st));
+  std::vector<uint8_t> hm(nb, 0);
+  if (mask) memcpy(hm.data(), mask, nb);
+  for (int64_t k = n_codes; k & 3; ++k) hm[k >> 2] |= (uint8_t)(1u << ((k & 3) << 1));  // masked past the end
+  SG_CUDA(cudaMemcpyAsync(r.d_mask, hm.data(), nb, cudaMemcpyHostToDevice, c->st));
+  r.rs.assign(rs, rs + std::max(n_regions, 0));
+  r.re.assign(re, re + std::max(n_regions, 0));
+  SG_CUDA(cudaStreamSynchronize(c->st));
+  c->refs.push_back(std::move(r));
+  c->indexed = false;
+  return 0;
+}
+
+extern "C" int stormgpu_build_index(stormgpu_ctx* c) {
+  if (!c) return STORMGPU_EINVAL;
+  SG_CUDA(cudaSetDevice(c->p.device));
+  SG_CUDA(cudaEventRecord(c->ev[0], c->st));
+  int64_t launches = 0;
+  for (auto& r : c->refs) {
+    for (auto& ix : r.idx) { cudaFree(ix.first); cudaFree(ix.map); }
+    r.idx.assign(c->seeds.n, DevIndex());
+    for (int si = 0; si < c->seeds.n; ++si) {
+      int rc = build_one_index(r.d_codes, r.n, r.rs.data(), r.re.data(), (int)r.rs.size(), c->seeds.s[si],
+                               c->p.stdev_distance, &r.idx[si], c->st, &launches);
+      if (rc) return rc;
+    }
+  }
+  SG_CUDA(cudaEventRecord(c->ev[1], c->st));
+  SG_CUDA(cudaStreamSynchronize(c->st));
+  float ms = 0;
+  cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]);
+  c->stats.ms_index = ms;
+  c->stats.kernels += launches;
+  c->indexed = true;
+  return 0;
+}
+
+static int map_device_impl(stormgpu_ctx* c, const stormgpu_reads* reads, stormgpu_results* out) {
+  if (!c->indexed) { sg_set_error("stormgpu_build_index must be called before mapping"); return STORMGPU_ESTATE; }
+  cudaStream_t st = c->st;
+  const int64_t n = reads->n;
+  const ScoreParams sp = make_score_params(c->p);
+  stormgpu_stats& S = c->stats;
+  double ms_index = S.ms_index;
+  memset(&S, 0, sizeof(S));
+  S.ms_index = ms_index;
+  int64_t launches = 0;
+  int maxL = 0;
+  {
+    std::vector<int16_t> hl(n > 0 ? n : 1);
+    if (n > 0) SG_CUDA(cudaMemcpyAsync(hl.data(), reads->lengths, sizeof(int16_t) * n, cudaMemcpyDeviceToHost, st));
+    SG_CUDA(cudaStreamSynchronize(st));
+    for (int64_t r = 0; r < n; ++r) maxL = std::max<int>(maxL, hl[r]);
+    if (maxL > STORMGPU_MAX_READ_LEN) { sg_set_error("read longer than %d", STORMGPU_MAX_READ_LEN); return STORMGPU_EINVAL; }
+  }
+  if (out->tb_stride < (maxL + c->p.allowed_indels + 1) / 2) { sg_set_error("tb_stride too small"); return STORMGPU_EINVAL; }
+  launch_init_results(n, out->hits, out->mapped, out->tb, out->tb_stride, st);
+  launches++;
+  if (n == 0) return 0;
+  ReadsDev fwd{n, reads->codes, reads->code_stride, reads->levels, reads->level_stride, reads->lengths};
+  ReadsDev rev = fwd;
+  if (c->p.senses & 2) {
+    if (c->rcodes.grow(n * reads->code_stride)) return STORMGPU_ENOMEM;
+    if (reads->levels && c->rlevels.grow(n * reads->level_stride)) return STORMGPU_ENOMEM;
+    launch_reverse_reads(fwd, c->p.colour ? reads->first_levels : nullptr, c->p.colour, c->rcodes.p,
+                         reads->levels ? c->rlevels.p : nullptr, st);
+    launches++;
+    rev.codes = c->rcodes.p;
+    rev.levels = reads->levels ? c->rlevels.p : nullptr;
+  }
+  if (c->hitsc.grow(n) || c->ucount.grow(n) || c->pstart.grow(n) || c->pcount.grow(n) ||
+      c->hoff.grow(n + 1) || c->scan_tmp64.grow(scan_tmp_elems(n) + 8) || c->big_list.grow(n) ||
+      c->big_count.grow(1) || c->counters.grow(8))
+    return STORMGPU_ENOMEM;
+  const int BW = 2 * sp.I + 1;
+  const int wpr = (2 * BW + 31) / 32 + (sp.colour ? (BW + 31) / 32 : 0);
+  const int64_t tbs = ((maxL + sp.I + 1) / 2 + 7) & ~7LL;
+  float tg = 0, tf = 0, ta = 0, tr = 0;
+  SG_CUDA(cudaEventRecord(c->ev[6], st));
+  for (size_t ref_id = 0; ref_id < c->refs.size(); ++ref_id) {
+    RefSeq& R = c->refs[ref_id];
+    IndexView ix;
+    memset(&ix, 0, sizeof(ix));
+    for (int si = 0; si < c->seeds.n; ++si) { ix.first[si] = R.idx[si].first; ix.map[si] = R.idx[si].map; }
+    for (int strand = 0; strand < 2; ++strand) {
+      if (!(c->p.senses & (1 << strand))) continue;
+      const ReadsDev& rd = strand ? rev : fwd;
+      SG_CUDA(cudaMemsetAsync(c->counters.p, 0, sizeof(unsigned long long) * 8, st));
+      SG_CUDA(cudaEventRecord(c->ev[0], st));
+      launch_gather_count(rd, c->seeds, ix, c->hitsc.p, c->counters.p, st);
+      exclusive_scan<int32_t, int64_t>(c->hitsc.p, c->hoff.p, n, c->hoff.p + n, c->scan_tmp64.p, st);
+      launches += 4;
+      int64_t htot = 0;
+      SG_CUDA(cudaMemcpyAsync(&htot, c->hoff.p + n, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+      SG_CUDA(cudaStreamSynchronize(st));
+      if (c->cand.grow(std::max<int64_t>(htot, 1)) || c->p_read.grow(std::max<int64_t>(htot, 1)) ||
+          c->p_diag.grow(std::max<int64_t>(htot, 1)))
+        return STORMGPU_ENOMEM;
+      launch_gather_expand(rd, c->seeds, ix, c->hoff.p, c->cand.p, st);
+      SG_CUDA(cudaMemsetAsync(c->big_count.p, 0, sizeof(int32_t), st));
+      launch_segment_unique(rd, c->hitsc.p, c->hoff.p, c->cand.p, c->ucount.p, sp.I, c->big_list.p,
+                            c->big_count.p, st);
+      launches += 2;
+      int32_t nbig = 0;
+      SG_CUDA(cudaMemcpyAsync(&nbig, c->big_count.p, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+      SG_CUDA(cudaStreamSynchronize(st));
+      if (nbig > 0) {
+        std::vector<int32_t> bl(nbig), bh(nbig);
+        SG_CUDA(cudaMemcpy(bl.data(), c->big_list.p, sizeof(int32_t) * nbig, cudaMemcpyDeviceToHost));
+        std::vector<int32_t> medium, huge;
+        for (int k = 0; k < nbig; ++k) {
+          int32_t h;
+          SG_CUDA(cudaMemcpy(&h, c->hitsc.p + bl[k], sizeof(int32_t), cudaMemcpyDeviceToHost));
+          (h <= 32768 ? medium : huge).push_back(bl[k]);
+          bh[k] = h;
+        }
+        if (!medium.empty()) {
+          SG_CUDA(cudaMemcpyAsync(c->big_list.p, medium.data(), sizeof(int32_t) * medium.size(), cudaMemcpyHostToDevice, st));
+          launch_segment_unique_big(c->big_list.p, (int)medium.size(), c->hitsc.p, c->hoff.p, c->cand.p,
+                                    c->ucount.p, sp.I, nullptr, 0, st);
+          launches++;
+        }
+        for (size_t k = 0; k < huge.size(); ++k) {
+          int32_t h;
+          SG_CUDA(cudaMemcpy(&h, c->hitsc.p + huge[k], sizeof(int32_t), cudaMemcpyDeviceToHost));
+          int64_t P = 1;
+          while (P < h) P <<= 1;
+          if (c->big_tmp.grow(P)) return STORMGPU_ENOMEM;
+          SG_CUDA(cudaMemcpyAsync(c->big_list.p + n - 1, &huge[k], sizeof(int32_t), cudaMemcpyHostToDevice, st));
+          launch_segment_unique_big(c->big_list.p + n - 1, 1, c->hitsc.p, c->hoff.p, c->cand.p,
+                                    c->ucount.p, sp.I, c->big_tmp.p, P, st);
+          SG_CUDA(cudaStreamSynchronize(st));
+          launches++;
+        }
+      }
+      SG_CUDA(cudaEventRecord(c->ev[1], st));
+      PassBuffers pb;
+      memset(&pb, 0, sizeof(pb));
+      pb.hits = c->hitsc.p; pb.hoff = c->hoff.p; pb.ucount = c->ucount.p; pb.cand = c->cand.p;
+      pb.cand_cap = c->cand.cap; pb.pstart = c->pstart.p; pb.pcount = c->pcount.p;
+      pb.p_read = c->p_read.p; pb.p_diag = c->p_diag.p; pb.p_cap = c->p_read.cap;
+      pb.counters = c->counters.p;
+      launch_filter(rd, sp, R.d_codes, c->hoff.p, c->cand.p, c->ucount.p, pb, st);
+      launches++;
+      SG_CUDA(cudaEventRecord(c->ev[2], st));
+      unsigned long long cnt[8];
+      SG_CUDA(cudaMemcpyAsync(cnt, c->counters.p, sizeof(cnt), cudaMemcpyDeviceToHost, st));
+      SG_CUDA(cudaStreamSynchronize(st));
+      if (cnt[1]) { sg_set_error("internal: filter slot overflow"); return STORMGPU_EINVAL; }
+      const int64_t npass = (int64_t)cnt[0];
+      S.candidates += 0;  // filled below from ucount via cells
+      S.filter_cells += (int64_t)cnt[2];
+      S.seed_lookups += (int64_t)cnt[3];
+      S.hit_positions += (int64_t)cnt[4];
+      S.filter_passed += npass;
+      if (npass > 0) {
+        if (c->a_score.grow(npass) || c->a_bound.grow(npass) || c->a_tblen.grow(npass) ||
+            c->a_pos.grow(npass * 4) || c->a_tb.grow(npass * tbs))
+          return STORMGPU_ENOMEM;
+        pb.a_score = c->a_score.p; pb.a_bound = c->a_bound.p; pb.a_tblen = c->a_tblen.p;
+        pb.a_pos = c->a_pos.p; pb.a_tb = c->a_tb.p; pb.tbs = tbs;
+        const int64_t per_slot = (int64_t)maxL * wpr;
+        int64_t chunk = std::min<int64_t>(npass, std::max<int64_t>(4096, (int64_t)(256ll << 20) / (per_slot * 4)));
+        if (c->scratch.grow(chunk * per_slot)) return STORMGPU_ENOMEM;
+        pb.a_scratch = c->scratch.p;
+        for (int64_t s0 = 0; s0 < npass; s0 += chunk) {
+          launch_align(rd, sp, R.d_codes, R.d_mask, s0, std::min(chunk, npass - s0), pb, st);
+          launches++;
+        }
+        S.aligned += npass;
+        S.align_cells += npass * 0;  // per-read lengths: accounted on the host below
+      }
+      SG_CUDA(cudaEventRecord(c->ev[3], st));
+      if (npass > 0) {
+        launch_replay(n, sp, (int)ref_id, strand ? -1 : 1, pb, out->hits, out->tb, out->tb_stride, out->mapped, st);
+        launches++;
+      }
+      SG_CUDA(cudaEventRecord(c->ev[4], st));
+      SG_CUDA(cudaEventSynchronize(c->ev[4]));
+      float a, b, d, e;
+      cudaEventElapsedTime(&a, c->ev[0], c->ev[1]);
+      cudaEventElapsedTime(&b, c->ev[1], c->ev[2]);
+      cudaEventElapsedTime(&d, c->ev[2], c->ev[3]);
+      cudaEventElapsedTime(&e, c->ev[3], c->ev[4]);
+      tg += a; tf += b; ta += d; tr += e;
+    }
+  }
+  SG_CUDA(cudaEventRecord(c->ev[7], st));
+  SG_CUDA(cudaEventSynchronize(c->ev[7]));
+  SG_CUDA(cudaGetLastError());
+  float tt = 0;
+  cudaEventElapsedTime(&tt, c->ev[6], c->ev[7]);
+  S.ms_gather = tg; S.ms_filter = tf; S.ms_align = ta; S.ms_replay = tr; S.ms_total = tt;
+  S.kernels = launches;
+  return 0;
+}
+
+extern "C" int stormgpu_map_device(stormgpu_ctx* c, const stormgpu_reads* reads, stormgpu_results* out,
+                                   void* stream) {
+  if (!c || !reads || !out) { sg_set_error("null argument"); return STORMGPU_EINVAL; }
+  SG_CUDA(cudaSetDevice(c->p.device));
+  cudaStream_t user = (cudaStream_t)stream;
+  if (user) {
+    cudaEvent_t e;
+    SG_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    SG_CUDA(cudaEventRecord(e, user));
+    SG_CUDA(cudaStreamWaitEvent(c->st, e, 0));
+    cudaEventDestroy(e);
+  }
+  int rc = map_device_impl(c, reads, out);
+  if (rc == 0 && user) {
+    cudaEvent_t e;
+    SG_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    SG_CUDA(cudaEventRecord(e, c->st));
+    SG_CUDA(cudaStreamWaitEvent(user, e, 0));
+    cudaEventDestroy(e);
+  }
+  return rc;
+}
+
+extern "C" int stormgpu_sync(stormgpu_ctx* c) {
+  if (!c) return STORMGPU_EINVAL;
+  SG_CUDA(cudaStreamSynchronize(c->st));
+  return 0;
+}
+
+extern "C" int stormgpu_map(stormgpu_ctx* c, const stormgpu_reads* reads, stormgpu_results* out) {
+  if (!c || !reads || !out || reads->n < 0) { sg_set_error("null argument"); return STORMGPU_EINVAL; }
+  SG_CUDA(cudaSetDevice(c->p.device));
+  const int64_t n = reads->n;
+  cudaStream_t st = c->st;
+  if (c->fcodes.grow(std::max<int64_t>(n * reads->code_stride, 1)) || c->lengths.grow(std::max<int64_t>(n, 1)) ||
+      c->hits.grow(std::max<int64_t>(n * 4, 1)) || c->tb.grow(std::max<int64_t>(n * 4 * out->tb_stride, 1)) ||
+      c->mapped.grow(std::max<int64_t>(n, 1)))
+    return STORMGPU_ENOMEM;
+  if (reads->levels && c->flevels.grow(std::max<int64_t>(n * reads->level_stride, 1))) return STORMGPU_ENOMEM;
+  if (reads->first_levels && c->first_levels.grow(std::max<int64_t>(n, 1))) return STORMGPU_ENOMEM;
+  if (n > 0) {
+    SG_CUDA(cudaMemcpyAsync(c->fcodes.p, reads->codes, n * reads->code_stride, cudaMemcpyHostToDevice, st));
+    SG_CUDA(cudaMemcpyAsync(c->lengths.p, reads->lengths, sizeof(int16_t) * n, cudaMemcpyHostToDevice, st));
+    if (reads->levels) SG_CUDA(cudaMemcpyAsync(c->flevels.p, reads->levels, n * reads->level_stride, cudaMemcpyHostToDevice, st));
+    if (reads->first_levels) SG_CUDA(cudaMemcpyAsync(c->first_levels.p, reads->first_levels, n, cudaMemcpyHostToDevice, st));
+  }
+  stormgpu_reads dr = *reads;
+  dr.codes = c->fcodes.p;
+  dr.levels = reads->levels ? c->flevels.p : nullptr;
+  dr.lengths = c->lengths.p;
+  dr.first_levels = reads->first_levels ? c->first_levels.p : nullptr;
+  stormgpu_results dres;
+  dres.hits = c->hits.p;
+  dres.tb = c->tb.p;
+  dres.tb_stride = out->tb_stride;
+  dres.mapped = c->mapped.p;
+  int rc = map_device_impl(c, &dr, &dres);
+  if (rc) return rc;
+  if (n > 0) {
+    SG_CUDA(cudaMemcpyAsync(out->hits, c->hits.p, sizeof(stormgpu_hit) * n * 4, cudaMemcpyDeviceToHost, st));
+    SG_CUDA(cudaMemcpyAsync(out->tb, c->tb.p, n * 4 * out->tb_stride, cudaMemcpyDeviceToHost, st));
+    SG_CUDA(cudaMemcpyAsync(out->mapped, c->mapped.p, n, cudaMemcpyDeviceToHost, st));
+  }
+  SG_CUDA(cudaStreamSynchronize(st));
+  return 0;
+}
+
+extern "C" int stormgpu_get_stats(stormgpu_ctx* c, stormgpu_stats* out) {
+  if (!c || !out) return STORMGPU_EINVAL;
+  *out = c->stats;
+  return 0;
+}
+
+// ------------------------------------------------------------------------------ unit level
+
+namespace {
+int upload_padded(const uint8_t* h, int64_t n_codes, int64_t pad_codes, uint8_t fill, uint8_t** alloc,
+                  uint8_t** base) {
+  (void)pad_codes;
+  const int64_t nb = (n_codes + 3) / 4;
+  const int64_t tot = nb + 2 * kPadBytes + 16;
+  SG_CUDA(cudaMalloc(alloc, tot));
+  SG_CUDA(cudaMemset(*alloc, fill, tot));
+  *base = *alloc + kPadBytes;
+  if (nb) {
+    std::vector<uint8_t> v(h, h + nb);
+    for (int64_t k = n_codes; k & 3; ++k) {  // codes past the end: 0 (sequence) or 1 (mask)
+      v[k >> 2] &= (uint8_t)~(3u << ((k & 3) << 1));
+      if (fill) v[k >> 2] |= (uint8_t)(1u << ((k & 3) << 1));
+    }
+    SG_CUDA(cudaMemcpy(*base, v.data(), nb, cudaMemcpyHostToDevice));
+  }
+  return 0;
+}
+}  // namespace
+
+extern "C" int stormgpu_sw_filter(int W, int read_len, uint32_t match, uint32_t mismatch, uint32_t gapopen,
+                                  uint32_t gapext, uint32_t threshold, const uint8_t* genome, int64_t n_codes,
+                                  int64_t pad, const int32_t* pos, int64_t n, const uint8_t* read, uint8_t* pass) {
+  if (!(W == 2 || W == 4 || W == 8 || W == 16) || read_len <= 0 || read_len > STORMGPU_MAX_READ_LEN || n < 0) {
+    sg_set_error("bad filter arguments");
+    return STORMGPU_EINVAL;
+  }
+  for (int64_t k = 0; k < n; ++k)
+    if (pos[k] < -(4 * (int64_t)kPadBytes - 64) || pos[k] + read_len + 2 * W > n_codes + 4 * (int64_t)kPadBytes - 64) {
+      sg_set_error("window %lld outside the padded genome", (long long)pos[k]);
+      return STORMGPU_EINVAL;
+    }
+  ScoreParams sp;
+  memset(&sp, 0, sizeof(sp));
+  sp.fm = match & 0xff; sp.fx = mismatch & 0xff; sp.fo = gapopen & 0xff; sp.fe = gapext & 0xff;
+  sp.fthr = threshold >= 255u ? 254 : (int)threshold;
+  sp.W = W;
+  uint8_t *ga, *gb, *dr, *dp;
+  int32_t* dpos;
+  if (upload_padded(genome, n_codes, pad, 0, &ga, &gb)) return STORMGPU_ECUDA;
+  const int rb = (read_len + 2 * W + 16) / 4 + 16;
+  std::vector<uint8_t> hr(rb, 0);
+  memcpy(hr.data(), read, (read_len + 3) / 4);
+  SG_CUDA(cudaMalloc(&dr, rb));
+  SG_CUDA(cudaMemcpy(dr, hr.data(), rb, cudaMemcpyHostToDevice));
+  SG_CUDA(cudaMalloc(&dpos, sizeof(int32_t) * std::max<int64_t>(n, 1)));
+  SG_CUDA(cudaMalloc(&dp, std::max<int64_t>(n, 1)));
+  if (n) SG_CUDA(cudaMemcpy(dpos, pos, sizeof(int32_t) * n, cudaMemcpyHostToDevice));
+  launch_filter_flat(W, read_len, sp, gb, dpos, n, dr, dp, 0);
+  SG_CUDA(cudaGetLastError());
+  SG_CUDA(cudaDeviceSynchronize());
+  if (n) SG_CUDA(cudaMemcpy(pass, dp, n, cudaMemcpyDeviceToHost));
+  cudaFree(ga); cudaFree(dr); cudaFree(dpos); cudaFree(dp);
+  return 0;
+}
+
+extern "C" int stormgpu_align(const stormgpu_params* params, const uint8_t* read, const uint8_t* levels,
+                              int read_len, const uint8_t* genome, const uint8_t* mask, int64_t n_codes,
+                              int64_t pad, const int32_t* win, int64_t n, int32_t* score, int32_t* bound,
+                              int16_t* best, int32_t* tb_len, uint8_t* tb, int64_t tb_stride) {
+  if (!params || read_len <= 0 || read_len > STORMGPU_MAX_READ_LEN || n < 0 ||
+      params->allowed_indels < 0 || params->allowed_indels > STORMGPU_MAX_INDELS) {
+    sg_set_error("bad align arguments");
+    return STORMGPU_EINVAL;
+  }
+  const int I = params->allowed_indels;
+  if (tb_stride < (read_len + I + 1) / 2) { sg_set_error("tb_stride too small"); return STORMGPU_EINVAL; }
+  for (int64_t k = 0; k < n; ++k)
+    if (win[k] < -(4 * (int64_t)kPadBytes - 64) || win[k] + read_len + 2 * I > n_codes + 4 * (int64_t)kPadBytes - 64) {
+      sg_set_error("window outside the padded genome");
+      return STORMGPU_EINVAL;
+    }
+  ScoreParams sp = make_score_params(*params);
+  sp.Is = 1 << 28;              // window = diag - I exactly
+  sp.min_score = -(1 << 29);    // always trace back
+  uint8_t *ga, *gb, *ma, *mb;
+  if (upload_padded(genome, n_codes, pad, 0, &ga, &gb)) return STORMGPU_ECUDA;
+  if (upload_padded(mask, n_codes, pad, 0x55, &ma, &mb)) return STORMGPU_ECUDA;
+  const int64_t rb = ((read_len + 3) / 4 + 15) & ~7;
+  std::vector<uint8_t> hr(rb, 0), hq(rb, 0);
+  memcpy(hr.data(), read, (read_len + 3) / 4);
+  if (levels) memcpy(hq.data(), levels, (read_len + 3) / 4);
+  uint8_t *dr, *dq = nullptr;
+  int16_t* dl;
+  SG_CUDA(cudaMalloc(&dr, rb));
+  SG_CUDA(cudaMemcpy(dr, hr.data(), rb, cudaMemcpyHostToDevice));
+  if (levels) {
+    SG_CUDA(cudaMalloc(&dq, rb));
+    SG_CUDA(cudaMemcpy(dq, hq.data(), rb, cudaMemcpyHostToDevice));
+  }
+  int16_t L16 = (int16_t)read_len;
+  SG_CUDA(cudaMalloc(&dl, sizeof(int16_t)));
+  SG_CUDA(cudaMemcpy(dl, &L16, sizeof(int16_t), cudaMemcpyHostToDevice));
+  ReadsDev rd{1, dr, rb, dq, rb, dl};
+  PassBuffers pb;
+  memset(&pb, 0, sizeof(pb));
+  const int64_t nn = std::max<int64_t>(n, 1);
+  const int BW = 2 * I + 1;
+  const int wpr = (2 * BW + 31) / 32 + (params->colour ? (BW + 31) / 32 : 0);
+  const int64_t tbs = ((read_len + I + 1) / 2 + 7) & ~7LL;
+  std::vector<int32_t> zeros(nn, 0), diag(nn, 0);
+  for (int64_t k = 0; k < n; ++k) diag[k] = win[k] + I;
+  SG_CUDA(cudaMalloc(&pb.p_read, sizeof(int32_t) * nn));
+  SG_CUDA(cudaMalloc(&pb.p_diag, sizeof(int32_t) * nn));
+  SG_CUDA(cudaMalloc(&pb.a_score, sizeof(int32_t) * nn));
+  SG_CUDA(cudaMalloc(&pb.a_bound, sizeof(int32_t) * nn));
+  SG_CUDA(cudaMalloc(&pb.a_tblen, sizeof(int32_t) * nn));
+  SG_CUDA(cudaMalloc(&pb.a_pos, sizeof(int16_t) * 4 * nn));
+  SG_CUDA(cudaMalloc(&pb.a_tb, tbs * nn));
+  SG_CUDA(cudaMalloc(&pb.a_scratch, sizeof(uint32_t) * (size_t)read_len * wpr * nn));
+  pb.tbs = tbs;
+  SG_CUDA(cudaMemcpy(pb.p_read, zeros.data(), sizeof(int32_t) * nn, cudaMemcpyHostToDevice));
+  SG_CUDA(cudaMemcpy(pb.p_diag, diag.data(), sizeof(int32_t) * nn, cudaMemcpyHostToDevice));
+  launch_align(rd, sp, gb, mb, 0, n, pb, 0);
+  SG_CUDA(cudaGetLastError());
+  SG_CUDA(cudaDeviceSynchronize());
+  if (n) {
+    SG_CUDA(cudaMemcpy(score, pb.a_score, sizeof(int32_t) * n, cudaMemcpyDeviceToHost));
+    SG_CUDA(cudaMemcpy(bound, pb.a_bound, sizeof(int32_t) * n, cudaMemcpyDeviceToHost));
+    SG_CUDA(cudaMemcpy(best, pb.a_pos, sizeof(int16_t) * 4 * n, cudaMemcpyDeviceToHost));
+    SG_CUDA(cudaMemcpy(tb_len, pb.a_tblen, sizeof(int32_t) * n, cudaMemcpyDeviceToHost));
+    std::vector<uint8_t> htb(tbs * n);
+    SG_CUDA(cudaMemcpy(htb.data(), pb.a_tb, tbs * n, cudaMemcpyDeviceToHost));
+    for (int64_t k = 0; k < n; ++k) {
+      memset(tb + k * tb_stride, 0, tb_stride);
+      memcpy(tb + k * tb_stride, htb.data() + k * tbs, std::min<int64_t>(tbs, tb_stride));
+    }
+  }
+  cudaFree(ga); cudaFree(ma); cudaFree(dr); if (dq) cudaFree(dq); cudaFree(dl);
+  cudaFree(pb.p_read); cudaFree(pb.p_diag); cudaFree(pb.a_score); cudaFree(pb.a_bound);
+  cudaFree(pb.a_tblen); cudaFree(pb.a_pos); cudaFree(pb.a_tb); cudaFree(pb.a_scratch);
+  return 0;
+}
+
+extern "C" int stormgpu_index_one(const char* seed, int32_t stdev_distance, const uint8_t* codes, int64_t n_codes,
+                                  int64_t pad, const int32_t* rs, const int32_t* re, int32_t n_regions,
+                                  int32_t* first, int32_t* map, int64_t map_capacity, int64_t* map_len) {
+  SeedSet ss;
+  if (parse_seeds(seed, &ss) != 0 || ss.n < 1) { sg_set_error("invalid seed"); return STORMGPU_EINVAL; }
+  uint8_t *ga, *gb;
+  if (upload_padded(codes, n_codes, pad, 0, &ga, &gb)) return STORMGPU_ECUDA;
+  DevIndex ix;
+  int rc = build_one_index(gb, n_codes, rs, re, n_regions, ss.s[0], stdev_distance, &ix, 0, nullptr);
+  if (rc) { cudaFree(ga); return rc; }
+  SG_CUDA(cudaDeviceSynchronize());
+  SG_CUDA(cudaMemcpy(first, ix.first, sizeof(int32_t) * (ix.nkeys + 1), cudaMemcpyDeviceToHost));
+  if (ix.n > map_capacity) { sg_set_error("map_capacity too small"); cudaFree(ga); return STORMGPU_EINVAL; }
+  if (ix.n) SG_CUDA(cudaMemcpy(map, ix.map, sizeof(int32_t) * ix.n, cudaMemcpyDeviceToHost));
+  *map_len = ix.n;
+  cudaFree(ix.first);
+  if (ix.map) cudaFree(ix.map);
+  cudaFree(ga);
+  return 0;
+}

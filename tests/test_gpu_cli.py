@@ -1,0 +1,46 @@
+"""End to end on the GPU: the storm-nucleotide / storm-color binaries (CUDA library behind the
+reference's command line) against the golden SAM / FASTQ produced by the reference itself,
+and, when oracle/_ref is present, against a live reference run on a larger input."""
+import os
+import subprocess
+
+import pytest
+
+import ffi
+import golden_cases
+from storm_b200 import api, build, synth
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _built():
+    build.build()
+
+
+def _exe(mode):
+    return os.path.join(build.BIN_DIR, "storm-color" if mode == "colour" else "storm-nucleotide")
+
+
+@pytest.mark.parametrize("name", sorted(golden_cases.meta()))
+def test_gpu_cli_matches_golden(name, tmp_path):
+    assert golden_cases.check_case(name, str(tmp_path), _exe) > 0
+
+
+@pytest.mark.skipif(not ffi.ref_available(), reason="oracle/_ref not built")
+@pytest.mark.parametrize("cfg,scale,extra", [(0, 0.2, []), (1, 0.02, []), (0, 0.05, ["-M", "4", "-A", "-i", "20", "-z", "70"])])
+def test_gpu_cli_matches_reference(cfg, scale, extra, tmp_path):
+    w = synth.generate(cfg, scale, str(tmp_path / "ref.fa"), str(tmp_path / "reads.fq"))
+    args = w["args"] + extra
+    colour = w["mode"] == "colour"
+    outs = {}
+    for tag, exe in (("ref", os.path.join(ffi.REF_DIR, "storm-color" if colour else "storm-nucleotide")),
+                     ("gpu", _exe(w["mode"]))):
+        p = subprocess.run([exe, "-g", "ref.fa", "-r", "reads.fq", "-o", tag + ".sam", "-O", tag + ".fq", "-v", "0"] + args,
+                           cwd=str(tmp_path), env=dict(os.environ, MALLOC_PERTURB_="255"), capture_output=True,
+                           timeout=1800)
+        assert p.returncode == 0, p.stderr[-3000:]
+        lines = (tmp_path / (tag + ".sam")).read_bytes().split(b"\n")
+        outs[tag] = [l for l in lines if not l.startswith(b"@PG")], (tmp_path / (tag + ".fq")).read_bytes()
+    assert outs["gpu"][0] == outs["ref"][0]
+    assert outs["gpu"][1] == outs["ref"][1]

@@ -1,0 +1,200 @@
+"""GPU parity: every CUDA kernel against the oracle on seeded inputs, through the C ABI.
+
+Bar: bit-exact (integer work).  The oracle itself is pinned to the reference by
+tests/test_oracle_pin.py and tests/test_e2e_cpu.py."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import ffi
+from storm_b200 import api, build
+
+pytestmark = pytest.mark.gpu
+
+PADB = 128
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _built():
+    build.build()
+    if not api.device_available():
+        pytest.fail("no CUDA device: GPU tests need a B200")
+
+
+def _mutate(rng, s, rate):
+    s = s.copy()
+    m = rng.random(len(s)) < rate
+    s[m] = (s[m] + rng.integers(1, 4, size=int(m.sum()))) % 4
+    return s
+
+
+@pytest.mark.parametrize("W", [2, 4, 8, 16])
+def test_filter_kernel_vs_oracle(W):
+    rng = np.random.default_rng(200 + W)
+    orc = ffi.oracle()
+    G = 5000
+    g = rng.integers(0, 4, size=G).astype(np.uint8)
+    gp = ffi.pack2(g, PADB)
+    base = gp.ctypes.data + PADB
+    total = passed = 0
+    for trial in range(40):
+        L = int(rng.choice([3, 12, 35, 49, 50, 75, 100, 150, 151, 250]))
+        match = int(rng.choice([5, 5, 3, 9, 300]))
+        mism, go, ge = int(rng.choice([4, 3])), int(rng.choice([9, 7])), int(rng.choice([4, 2]))
+        thr = int(rng.choice([40, 80, 100, 150, 254, 400]))
+        src = int(rng.integers(0, G - L - 40))
+        read = _mutate(rng, g[src:src + L], rng.choice([0.0, 0.05, 0.2, 0.75]))
+        rp = np.concatenate([ffi.pack2(read), np.zeros(64, np.uint8)])
+        n = 96
+        pos = np.concatenate([src - rng.integers(0, 2 * W, size=n // 3),
+                              rng.integers(-L - 8, G + 8, size=n - n // 3)]).astype(np.int32)
+        got = api.sw_filter(W, L, match, mism, go, ge, thr, gp[PADB:PADB + (G + 3) // 4], G, pos, rp)
+        for k in range(n):
+            exp = orc.or_sw_filter(W, L, match, mism, go, ge, thr, C.c_void_p(base), int(pos[k]), rp.ctypes.data)
+            assert got[k] == exp, (trial, k, W, L, match, thr, int(pos[k]))
+        total += n
+        passed += int(got.sum())
+    assert 0 < passed < total
+
+
+@pytest.mark.parametrize("colour", [0, 1])
+def test_align_kernel_vs_oracle(colour):
+    rng = np.random.default_rng(31 + colour)
+    orc = ffi.oracle()
+    G = 2000
+    for trial in range(60):
+        I = int(rng.choice([0, 1, 2, 3, 5, 7, 10, 15, 20, 31]))
+        L = int(rng.choice([8, 20, 35, 49, 50, 75, 100, 150, 300]))
+        match, mism = int(rng.choice([5, 3])), int(rng.choice([-4, -3, -6]))
+        go, ge = int(rng.choice([-9, -7])), int(rng.choice([-4, -2]))
+        g = rng.integers(0, 4, size=G).astype(np.uint8)
+        m = np.zeros(G, np.uint8)
+        for _ in range(int(rng.integers(0, 3))):
+            a = int(rng.integers(0, G - 10))
+            m[a:a + int(rng.integers(1, 8))] = 1
+        gp = ffi.pack2(g, PADB)
+        mp = ffi.pack2(m, PADB, fill=0x55)
+        src = int(rng.integers(0, G - L - 2 * I))
+        read = _mutate(rng, g[src + I:src + I + L], rng.choice([0.0, 0.03, 0.1, 0.3]))
+        lv = rng.integers(0, 4, size=L).astype(np.uint8)
+        rp = ffi.pack2(read)
+        qp = ffi.pack2(lv)
+        use_q = rng.random() < 0.8
+        wins = np.concatenate([[src], src + rng.integers(-3, 4, size=3),
+                               rng.integers(-L - 2 * I, G, size=4)]).astype(np.int32)
+        prm = api.params(colour=colour, match=match, mismatch=mism, gap_open=go, gap_extend=ge, indels=I)
+        score, bound, best, tbl, tb = api.align(prm, rp, qp if use_q else None, L, gp[PADB:PADB + (G + 3) // 4],
+                                                mp[PADB:PADB + (G + 3) // 4], G, wins)
+        p = ffi.make_params(colour=colour, match=match, mismatch=mism, gap_open=go, gap_extend=ge, indels=I)
+        for k, w in enumerate(wins):
+            o = ffi.OrAlignOut()
+            orc.or_align(C.byref(p), C.c_void_p(rp.ctypes.data), C.c_void_p(qp.ctypes.data if use_q else 0),
+                         L, C.c_void_p(gp.ctypes.data + PADB), C.c_void_p(mp.ctypes.data + PADB),
+                         C.c_int64(int(w)), C.byref(o))
+            ctx = (trial, k, colour, I, L, int(w))
+            assert score[k] == o.score and bound[k] == o.bound, ctx
+            assert tuple(best[k]) == (o.best_i, o.best_j, o.best_i0, o.best_j0), ctx
+            assert tbl[k] == o.tb_len, ctx
+            nb = (o.tb_len + 1) // 2
+            assert bytes(tb[k, :nb]) == bytes(o.tb)[:nb], ctx
+
+
+def test_index_kernel_vs_oracle():
+    rng = np.random.default_rng(17)
+    orc = ffi.oracle()
+    for trial, (N, seed, l) in enumerate([(100000, "####--#-#--##--####", 100), (50000, "#####-##-###", 3),
+                                          (30000, "##-##-###-###", 0), (20000, "###-#-###", 1),
+                                          (5000, "######", 100), (300, "####-##", 2)]):
+        g = rng.integers(0, 4, size=N).astype(np.uint8)
+        for _ in range(30 if N > 1000 else 0):
+            a, b = rng.integers(0, N - 300, size=2)
+            g[b:b + 200] = g[a:a + 200]
+        regs = [(N // 3, N // 3 + 50), (N // 2, N // 2 + 3), (N - 7, N)]
+        gp = ffi.pack2(g, PADB)
+        first, mp = api.index_one(seed, l, gp[PADB:PADB + (N + 3) // 4], N, regs)
+        sb = C.create_string_buffer(16 * 2048)
+        assert orc.or_parse_seeds(seed.encode(), sb, 16) == 1
+        f2 = np.zeros_like(first)
+        m2 = np.zeros(N + 64, np.int32)
+        rs = np.array([a for a, _ in regs], np.int32)
+        re_ = np.array([b for _, b in regs], np.int32)
+        n2 = orc.or_index_build(sb, l, C.c_void_p(gp.ctypes.data + PADB), C.c_int64(N), rs.ctypes.data,
+                                re_.ctypes.data, len(regs), f2.ctypes.data, m2.ctypes.data, C.c_int64(len(m2)))
+        assert n2 == len(mp), trial
+        assert np.array_equal(first, f2), trial
+        assert np.array_equal(mp, m2[:n2]), trial
+
+
+def _reads_arrays(seqs, quals, colour_first_levels=None):
+    n = len(seqs)
+    maxl = max(len(s) for s in seqs)
+    stride = ((maxl + 3) // 4 + 7) & ~7
+    codes = np.zeros((n, stride), np.uint8)
+    levels = np.zeros((n, stride), np.uint8)
+    for i, (s, q) in enumerate(zip(seqs, quals)):
+        p = ffi.pack2(s)
+        codes[i, :len(p)] = p
+        lv = np.searchsorted(np.array([2, 7, 10]), np.asarray(q), side="left").astype(np.uint8)
+        lp = ffi.pack2(lv)
+        levels[i, :len(lp)] = lp
+    return codes, levels, np.array([len(s) for s in seqs], np.int16)
+
+
+@pytest.mark.parametrize("colour,indels,seeds", [
+    (0, 3, "####--#-#--##--####;#####--###-#-###;###-##-#######"),
+    (0, 15, "##-##-###-###;###--#-#--#--####"),
+    (1, 7, "####-##-#-####;###-#--##-##--###;####-#---#----#--####"),
+])
+def test_map_api_vs_oracle(colour, indels, seeds):
+    from storm_b200 import synth
+    genome = synth.make_genome([40000, 15000], 21, gc=0.45, repeat_frac=0.2)
+    if colour:
+        pr, cols, q = synth.simulate_colour_reads(genome, 1500, 40, 22)
+        seqs = [c for c in cols]
+        quals = [qq for qq in q]
+        # colour-space reference: colours of consecutive bases
+        refs = [(n, (s[1:] ^ s[:-1]).astype(np.uint8)) for n, s in genome]
+    else:
+        seqs, quals = synth.simulate_nucleotide_reads(genome, 2000, [35, 50, 75, 100, 150], 23)
+        refs = genome
+    codes, levels, lengths = _reads_arrays(seqs, quals)
+    first_levels = np.full(len(seqs), 2, np.uint8) if colour else None
+    prm = api.params(colour=colour, indels=indels, min_score=100 if not colour else 110,
+                     min_score_filter=95)
+    m = api.Mapper(prm, seeds)
+    packed = []
+    for name, s in refs:
+        cp = ffi.pack2(s, PADB)
+        mk = ffi.pack2(np.zeros(len(s), np.uint8), PADB, fill=0x55)
+        packed.append((cp, mk, len(s)))
+        m.add_reference(cp[PADB:], mk[PADB:], len(s))
+    m.build_index()
+    batch = api.ReadBatch(codes, lengths, levels, first_levels)
+    res = m.map(batch)
+    st = m.stats()
+    m.close()
+    # oracle
+    orc = ffi.oracle()
+    R = (ffi.OrRef * len(packed))()
+    keep = []
+    for k, (cp, mk, n) in enumerate(packed):
+        zr = np.zeros(1, np.int32)
+        keep.append(zr)
+        R[k] = ffi.OrRef(cp.ctypes.data + PADB, mk.ctypes.data + PADB, n, zr.ctypes.data, zr.ctypes.data, 0)
+    rd = ffi.ReadsT(len(seqs), codes.ctypes.data, codes.shape[1], levels.ctypes.data, levels.shape[1],
+                    lengths.ctypes.data, first_levels.ctypes.data if colour else None)
+    hits = np.zeros(len(seqs) * 4, dtype=api.HIT_DTYPE)
+    tb = np.zeros((len(seqs) * 4, res.tb_stride), np.uint8)
+    mapped = np.zeros(len(seqs), np.uint8)
+    out = ffi.ResultsT(hits.ctypes.data, tb.ctypes.data, res.tb_stride, mapped.ctypes.data)
+    p = ffi.make_params(colour=colour, indels=indels, min_score=prm.min_score, min_score_filter=95)
+    cnt = np.zeros(3, np.int64)
+    assert orc.or_map(C.byref(p), seeds.encode(), R, len(packed), C.byref(rd), C.byref(out), cnt.ctypes.data) == 0
+    assert np.array_equal(res.mapped, mapped)
+    assert np.array_equal(res.hits, hits)
+    for k in range(len(hits)):
+        nb = (hits[k]["tb_len"] + 1) // 2
+        assert bytes(res.tb[k, :nb]) == bytes(tb[k, :nb]), k
+    assert mapped.sum() > len(seqs) // 4
+    assert st["filter_passed"] == cnt[1]
