@@ -1,0 +1,395 @@
+#!/usr/bin/env python
+"""Benchmark of the mapping hot path on B200.
+
+One step = the hot path over one batch: build the spaced-seed index of the resident
+reference (every seed), then map every read of the batch on both strands (hit gather,
+banded filter, full alignment with traceback, top-4 update) into device-resident results.
+The default workload is the colour-space one (10 Mbp, 41% GC, 20% mutated repeats, 2M reads
+of a primer + 50 colours, storm-color -M 1 -z 105 -t 120 -i 7 and its three w11 seeds),
+generated here from fixed seeds.
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl reference] [--cfg 0..4 --scale s]
+
+value   reads/s with reads, reference and results resident in HBM (device-timed, CUDA events);
+e2e     the same through the host-buffer C ABI call (stormgpu_map: reads copied in, results
+        copied out inside the timed region) plus the index build;
+roofline the dominant kernel against its measured ceiling; cpu_baseline the reference's
+        OpenMP/AVX2 build (oracle/_ref) on this host's cores on a bounded read sample.
+Multi-GPU: one process per GPU (torchrun), each maps its own batch (weak scaling), no
+collective on the data path; time = max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+from storm_b200 import synth  # noqa: E402
+
+PEAKS_PATH = os.path.join(ROOT, "MEASURED_PEAKS.json")
+TRAFFIC_PATH = os.path.join(ROOT, "profiles", "traffic.json")
+REF_DIR = os.path.join(ROOT, "oracle", "_ref")
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def workload_files(cfg: int, scale: float, rank: int, nreads: int | None = None):
+    """Generate (once) the FASTA + FASTQ of workload `cfg` for this rank; returns paths + spec."""
+    w = synth.workload(cfg, scale)
+    d = os.path.join(tempfile.gettempdir(), "storm_bench_c%d_s%g_r%d" % (cfg, scale, rank))
+    os.makedirs(d, exist_ok=True)
+    ref, reads = os.path.join(d, "ref.fa"), os.path.join(d, "reads.fq")
+    done = os.path.join(d, "done")
+    if not os.path.exists(done):
+        genome = synth.make_genome(w["ref_sizes"], w["ref_seed"], w["gc"], w["repeat"])
+        synth.write_fasta(ref, genome)
+        model = synth.ReadModel(**w.get("model", {}))
+        if w["mode"] == "colour":
+            pr, cols, q = synth.simulate_colour_reads(genome, w["reads"], w["lengths"], w["read_seed"] + 1000 * rank, model)
+            synth.write_colour_fastq(reads, pr, cols, q)
+        else:
+            seqs, quals = synth.simulate_nucleotide_reads(genome, w["reads"], w["lengths"], w["read_seed"] + 1000 * rank, model)
+            synth.write_fastq(reads, seqs, quals)
+        open(done, "w").write("ok")
+    return w, ref, reads, d
+
+
+def parse_cli_args(args):
+    """The mapping parameters of a storm command line (main.c semantics)."""
+    p = dict(match=5, mismatch=-4, gap_open=-9, gap_extend=-4, indels=3, min_score=115,
+             min_score_filter=100, stdev=100, senses=3)
+    seeds = None
+    it = iter(range(len(args)))
+    i = 0
+    while i < len(args):
+        a = args[i]
+        v = args[i + 1] if i + 1 < len(args) else None
+        key = {"-m": "match", "-x": "mismatch", "-d": "gap_open", "-e": "gap_extend", "-i": "indels",
+               "-t": "min_score", "-z": "min_score_filter", "-l": "stdev"}.get(a)
+        if key:
+            p[key] = int(v)
+            i += 2
+        elif a == "-s":
+            seeds = v
+            i += 2
+        elif a in ("-M", "-b", "-o", "-O"):
+            i += 2
+        else:
+            i += 1
+    del it
+    return p, seeds
+
+
+DEFAULT_SEEDS = {0: "####--#-#--##--####;#####--###-#-###;###-##-#######",
+                 1: "####----##--##-####;####-###--#----####;####-####-####"}
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.Q,
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True,
+                                     timeout=5).stdout.strip()
+                if out:
+                    self.samples.append([x.strip() for x in out.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for s in self.samples for k in range(4)
+                          if len(s) > 5 + k and s[5 + k].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def reference_exe(colour: bool) -> str:
+    name = "storm-color" if colour else "storm-nucleotide"
+    flags = open("/proc/cpuinfo").read() if os.path.exists("/proc/cpuinfo") else ""
+    if " avx2" not in flags:
+        name += "-sse2"
+    return os.path.join(REF_DIR, name)
+
+
+def sample_fastq(reads: str, d: str, n: int) -> str:
+    path = os.path.join(d, "sample_%d.fq" % n)
+    if not os.path.exists(path):
+        with open(reads, "rb") as f, open(path, "wb") as o:
+            for k, line in enumerate(f):
+                if k >= 4 * n:
+                    break
+                o.write(line)
+    return path
+
+
+def run_reference_once(w, ref, sample, d, threads):
+    exe = reference_exe(w["mode"] == "colour")
+    cmd = [exe, "-g", ref, "-r", sample, "-o", os.path.join(d, "ref_out.sam"), "-v", "0", "-N", str(threads)] + w["args"]
+    t0 = time.perf_counter()
+    p = subprocess.run(cmd, cwd=d, capture_output=True, env=dict(os.environ, MALLOC_PERTURB_="255"))
+    dt = time.perf_counter() - t0
+    if p.returncode != 0:
+        raise RuntimeError("reference run failed: %s" % p.stderr[-500:])
+    return dt
+
+
+def cpu_sample_size(cfg):
+    return {0: 100000, 1: 60000, 2: 20000, 3: 20000, 4: 20000}[cfg]
+
+
+def reference_arm(a, w, ref, reads, d):
+    threads = os.cpu_count() or 1
+    if not os.path.exists(reference_exe(w["mode"] == "colour")):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref not built (reference sources absent)"}))
+        return
+    n = min(cpu_sample_size(a.cfg), w["reads"])
+    sample = sample_fastq(reads, d, n)
+    for _ in range(a.warmup):
+        run_reference_once(w, ref, sample, d, threads)
+    times = [run_reference_once(w, ref, sample, d, threads) for _ in range(a.steps)]
+    tot = sum(times)
+    value = n * a.steps / tot
+    line = {"metric": "mapped reads/sec", "value": value, "unit": "reads/s", "n_gpus": a.gpus,
+            "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1000 * tot / a.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8/int32",
+            "data": "synthetic", "impl": "reference",
+            "config": {"workload": workload_name(a.cfg, a.scale), "reads_per_step": n,
+                       "reference_codes": sum(w["ref_sizes"]), "args": " ".join(w["args"])},
+            "cpu_baseline": {"value": value, "unit": "reads/s", "cores": threads, "kind": "reference",
+                             "sample": "%d of the workload's reads, full reference, index build included" % n},
+            "e2e": {"value": value, "unit": "reads/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def workload_name(cfg, scale):
+    names = {0: "cfg0 nucleotide 1 Mbp, 100k x 50 bp", 1: "cfg1 colour 10 Mbp, 2M x 50 colours",
+             2: "cfg2 nucleotide 100 Mbp, 10M x 35-150 bp, -i 15", 3: "cfg3 served -O chain",
+             4: "cfg4 3.1 Gbp, 100M x 100 bp"}
+    return names[cfg] + ("" if scale == 1.0 else " (scale %g)" % scale)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--cfg", type=int, default=1)
+    ap.add_argument("--scale", type=float, default=1.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    a = ap.parse_args()
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if a.impl == "reference":
+        if rank != 0:
+            return
+        w, ref, reads, d = workload_files(a.cfg, a.scale, 0)
+        reference_arm(a, w, ref, reads, d)
+        return
+
+    import torch
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+
+    from storm_b200 import api, build, host
+    build.build()
+    w, ref_path, reads_path, d = workload_files(a.cfg, a.scale, rank)
+    colour = 1 if w["mode"] == "colour" else 0
+    prm_d, seeds = parse_cli_args(w["args"])
+    seeds = seeds or DEFAULT_SEEDS[colour]
+    prm = api.params(colour=colour, device=local, **prm_d)
+    t0 = time.perf_counter()
+    reads = host.ReadSet(reads_path, colour)
+    reference = host.Reference(ref_path, colour)
+    log("rank %d: loaded %d reads, %d sequence(s) in %.1f s" % (rank, reads.n, reference.n, time.perf_counter() - t0))
+    n = reads.n
+    tbs = ((reads.max_len + prm.allowed_indels + 1) // 2 + 7) & ~7
+
+    mapper = api.Mapper(prm, seeds)
+    reference.add_to(mapper)
+
+    # device-resident inputs and outputs
+    batch = reads.batch()
+    d_codes = torch.from_numpy(batch.codes).to(dev)
+    d_levels = torch.from_numpy(batch.levels).to(dev) if batch.levels is not None else None
+    d_len = torch.from_numpy(batch.lengths.copy()).to(dev)
+    d_fl = torch.from_numpy(batch.first_levels).to(dev) if batch.first_levels is not None else None
+    import ctypes
+    d_hits = torch.empty(n * 4 * ctypes.sizeof(api.Hit), dtype=torch.uint8, device=dev)
+    d_tb = torch.empty(n * 4 * tbs, dtype=torch.uint8, device=dev)
+    d_mapped = torch.empty(n, dtype=torch.uint8, device=dev)
+    rstruct = api.Reads(n, d_codes.data_ptr(), batch.codes.shape[1],
+                        d_levels.data_ptr() if d_levels is not None else None,
+                        batch.levels.shape[1] if batch.levels is not None else 0, d_len.data_ptr(),
+                        d_fl.data_ptr() if d_fl is not None else None)
+    ostruct = api.Results(d_hits.data_ptr(), d_tb.data_ptr(), tbs, d_mapped.data_ptr())
+    stream = torch.cuda.Stream(device=dev)
+    flush = torch.empty(512 << 20, dtype=torch.uint8, device=dev)  # > 126 MB L2
+
+    def step():
+        mapper.build_index()
+        mapper.map_device(rstruct, ostruct, stream.cuda_stream)
+
+    for _ in range(a.warmup):
+        step()
+    torch.cuda.synchronize()
+
+    ms_steps, stage = [], []
+    with ClockSampler(local) as clk:
+        for _ in range(a.steps):
+            flush.fill_(1)
+            torch.cuda.synchronize()
+            if dist:
+                dist.barrier()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            step()
+            e1.record(stream)
+            e1.synchronize()
+            ms_steps.append(e0.elapsed_time(e1))
+            stage.append(mapper.stats())
+    torch.cuda.synchronize()
+    mapped = int(d_mapped.sum().item())
+    t_local = sum(ms_steps)
+    t_max = t_local
+    if dist:
+        t = torch.tensor([t_local], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_max = float(t.item())
+    value = world * n * a.steps / (t_max / 1000.0)
+
+    # end to end through the host-buffer ABI call
+    e2e_ms = []
+    for _ in range(max(1, min(a.steps, 3))):
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        t0 = time.perf_counter()
+        mapper.build_index()
+        res = mapper.map(batch, tbs)
+        e2e_ms.append(1000 * (time.perf_counter() - t0))
+    e2e_t = sum(e2e_ms)
+    if dist:
+        t = torch.tensor([e2e_t], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_t = float(t.item())
+    h2d = batch.codes.nbytes + (batch.levels.nbytes if batch.levels is not None else 0) + batch.lengths.nbytes + \
+        (batch.first_levels.nbytes if batch.first_levels is not None else 0)
+    d2h = res.hits.nbytes + res.tb.nbytes + res.mapped.nbytes
+    e2e = {"value": world * n * len(e2e_ms) / (e2e_t / 1000.0), "unit": "reads/s", "h2d_bytes_per_step": int(h2d),
+           "d2h_bytes_per_step": int(d2h), "includes": "index build + reads H2D + map + results D2H"}
+
+    # roofline of the dominant kernel, from the last timed step's per-stage device times
+    st = stage[-1]
+    peaks = json.load(open(PEAKS_PATH)) if os.path.exists(PEAKS_PATH) else {}
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    ops_s, ms_peak = _int_peak(api, local)
+    filter_ops = st["filter_cells"] * 10
+    gather_bytes = st["seed_lookups"] * 8 + st["hit_positions"] * 4 + n * (reads.max_len / 4) * 2 + st["candidates"] * 4
+    stages = {
+        "sw_filter": {"ms": st["ms_filter"], "bound": "int", "achieved": filter_ops / (st["ms_filter"] * 1e-3) / 1e12,
+                      "peak": ops_s / 1e12, "unit": "Tops/s", "gcups": st["filter_cells"] / (st["ms_filter"] * 1e-3) / 1e9},
+        "hit_gather": {"ms": st["ms_gather"], "bound": "hbm", "achieved": gather_bytes / (st["ms_gather"] * 1e-3) / 1e9,
+                       "peak": hbm, "unit": "GB/s"},
+        "full_align": {"ms": st["ms_align"], "aligned": st["aligned"]},
+        "replay": {"ms": st["ms_replay"]},
+        "index_build": {"ms": st["ms_index"]},
+    }
+    for v in stages.values():
+        if "achieved" in v:
+            v["frac"] = v["achieved"] / v["peak"]
+    dom = max(("sw_filter", "hit_gather"), key=lambda k: stages[k]["ms"])
+    traffic = None
+    if os.path.exists(TRAFFIC_PATH):
+        tr = json.load(open(TRAFFIC_PATH))
+        traffic = tr.get(dom, {}).get("bytes_per_launch")
+    roof = {"kernel": dom, "bound": stages[dom]["bound"], "achieved": stages[dom]["achieved"],
+            "peak": stages[dom]["peak"], "unit": stages[dom]["unit"], "frac": stages[dom]["frac"],
+            "traffic": traffic,
+            "peak_source": "measured: stormgpu_int_peak add/max lane-ops" if dom == "sw_filter" else "MEASURED_PEAKS.json hbm_gbs"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu_baseline and os.path.exists(reference_exe(colour)):
+        ns = min(cpu_sample_size(a.cfg), w["reads"])
+        sample = sample_fastq(reads_path, d, ns)
+        dt = run_reference_once(w, ref_path, sample, d, os.cpu_count() or 1)
+        cpu = {"value": ns / dt, "unit": "reads/s", "cores": os.cpu_count(), "kind": "reference",
+               "sample": "%d of the workload's reads, full reference, index build included, one run" % ns}
+
+    if rank == 0:
+        line = {"metric": "mapped reads/sec", "value": value, "unit": "reads/s", "n_gpus": world, "steps": a.steps,
+                "warmup": a.warmup, "ms_per_step": t_max / a.steps, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "u8/int32", "data": "synthetic",
+                "config": {"workload": workload_name(a.cfg, a.scale), "reads_per_gpu": n,
+                           "reference_codes": sum(w["ref_sizes"]), "args": " ".join(w["args"]),
+                           "step": "index build (all seeds) + map all reads, both strands",
+                           "l2": "flushed (512 MB write) between timed steps", "parallelism": "dp%d (reads)" % world},
+                "mapped_fraction": mapped / n, "sw_filter_gcups": stages["sw_filter"]["gcups"],
+                "gpu_launches": int(st["kernels"]), "roofline": roof, "stages": stages,
+                "clocks": clk.summary(), "e2e": e2e, "cpu_baseline": cpu,
+                "int_peak": {"ops_per_s": ops_s, "ms": ms_peak}}
+        print(json.dumps(line))
+    mapper.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def _int_peak(api, device):
+    import ctypes as C
+    ops, ms = C.c_double(0), C.c_double(0)
+    api.lib().stormgpu_int_peak.argtypes = [C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+    api._check(api.lib().stormgpu_int_peak(device, C.byref(ops), C.byref(ms)))
+    return ops.value, ms.value
+
+
+if __name__ == "__main__":
+    main()

@@ -191,6 +191,11 @@ int stormgpu_index_one(const char *seed, int32_t stdev_distance, const uint8_t *
                        const int32_t *region_ends, int32_t n_regions, int32_t *first,
                        int32_t *map, int64_t map_capacity, int64_t *map_len);
 
+/* Measurement helper: sustained 32-bit integer add/max lane-operations per second of the
+ * device (the instruction mix of the banded filter), used as the integer-pipe roofline.
+ * No counterpart in the reference (it has no GPU). */
+int stormgpu_int_peak(int device, double *ops_per_s, double *ms);
+
 #ifdef __cplusplus
 }
 #endif

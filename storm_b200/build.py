@@ -12,7 +12,8 @@ CSRC = os.path.join(PKG, "csrc")
 LIB_DIR = os.path.join(PKG, "lib")
 BIN_DIR = os.path.join(PKG, "bin")
 LIB = os.path.join(LIB_DIR, "libstormgpu.so")
-CU_SOURCES = ["stormgpu.cu", "index_build.cu", "map_kernels.cu"]
+HOST_LIB = os.path.join(LIB_DIR, "libstormhost.so")
+CU_SOURCES = ["stormgpu.cu", "index_build.cu", "map_kernels.cu", "intpeak.cu"]
 HOST_SOURCES = ["host/storm_host.c", "host/storm_cli.c", "host/storm_gpu_main.c"]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
               "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr"]
@@ -60,6 +61,9 @@ def build(verbose: bool = False, force: bool = False) -> str:
                 _run([nvcc()] + NVCC_FLAGS + ["-c", os.path.join(CSRC, src), "-o", obj], verbose)
             objs.append(obj)
         _run([nvcc(), "-shared", "-gencode", "arch=compute_100a,code=sm_100a", "-o", LIB] + objs + ["-cudart", "static"], verbose)
+    if force or _stale(HOST_LIB, deps):
+        _run(["gcc", "-O2", "-std=gnu11", "-fPIC", "-shared", "-o", HOST_LIB,
+              os.path.join(CSRC, "host", "storm_host.c"), "-lm"], verbose)
     for colour, name in ((0, "storm-nucleotide"), (1, "storm-color")):
         exe = os.path.join(BIN_DIR, name)
         if force or _stale(exe, deps + [LIB]):

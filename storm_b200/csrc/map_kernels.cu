@@ -380,7 +380,8 @@ __global__ void filter_kernel(ReadsDev rd, ScoreParams sp, const uint8_t* __rest
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int64_t nwarps = (int64_t)gridDim.x * (blockDim.x >> 5);
   const unsigned lt = (1u << lane) - 1u;
-  unsigned long long cells = 0;
+  unsigned long long cells = 0, cands = 0, acells = 0;
+  const int BW = 2 * sp.I + 1;
   for (int64_t r = (int64_t)blockIdx.x * (blockDim.x >> 5) + w; r < rd.n; r += nwarps) {
     const int U = ucount[r];
     if (U == 0) {
@@ -403,6 +404,8 @@ __global__ void filter_kernel(ReadsDev rd, ScoreParams sp, const uint8_t* __rest
       P += __popc(m);
     }
     cells += (unsigned long long)U * L * (2 * sp.Is + 1);
+    cands += (unsigned long long)U;
+    acells += (unsigned long long)P * L * BW;
     int start = 0;
     if (lane == 0) start = (int)atomicAdd(&pb.counters[0], (unsigned long long)P);
     start = __shfl_sync(0xffffffffu, start, 0);
@@ -418,8 +421,11 @@ __global__ void filter_kernel(ReadsDev rd, ScoreParams sp, const uint8_t* __rest
     }
     __syncwarp();
   }
-  for (int o = 16; o > 0; o >>= 1) cells += __shfl_xor_sync(0xffffffffu, cells, o);
-  if (lane == 0) atomicAdd(&pb.counters[2], cells);
+  if (lane == 0) {
+    atomicAdd(&pb.counters[2], cells);
+    atomicAdd(&pb.counters[5], cands);
+    atomicAdd(&pb.counters[6], acells);
+  }
 }
 
 void launch_filter(const ReadsDev& r, const ScoreParams& sp, const uint8_t* genome,

@@ -379,7 +379,8 @@ static int map_device_impl(stormgpu_ctx* c, const stormgpu_reads* reads, stormgp
       SG_CUDA(cudaStreamSynchronize(st));
       if (cnt[1]) { sg_set_error("internal: filter slot overflow"); return STORMGPU_EINVAL; }
       const int64_t npass = (int64_t)cnt[0];
-      S.candidates += 0;  // filled below from ucount via cells
+      S.candidates += (int64_t)cnt[5];
+      S.align_cells += (int64_t)cnt[6];
       S.filter_cells += (int64_t)cnt[2];
       S.seed_lookups += (int64_t)cnt[3];
       S.hit_positions += (int64_t)cnt[4];
@@ -399,7 +400,6 @@ static int map_device_impl(stormgpu_ctx* c, const stormgpu_reads* reads, stormgp
           launches++;
         }
         S.aligned += npass;
-        S.align_cells += npass * 0;  // per-read lengths: accounted on the host below
       }
       SG_CUDA(cudaEventRecord(c->ev[3], st));
       if (npass > 0) {
