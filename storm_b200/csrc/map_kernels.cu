@@ -306,152 +306,6 @@ void launch_segment_unique_big(const int32_t* big_list, int nbig, const int32_t*
 
 // ------------------------------------------------------------------------------ filter
 
-// The banded saturating-u8 SW of alignment_avx2__align_* (alignment_simd.c:2613-3404) for one
-// hit: W cells; before the loop the genome register holds window codes 0..W-1 (cell k = code
-// W-1-k); odd steps shift one more genome code in at cell 0, even steps one more read code in
-// at cell W-1; per cell M = subs(adds(M[l-2], match if equal), mismatch if different),
-// I = max(subs(max(I[l-1], I[l-1] of the neighbour), ext), subs(max(M[l-1], M[l-1] of the
-// neighbour), open)) (neighbour below at odd steps, above at even steps, 0 at the edge),
-// M = max(M, I) & mask[l], Max = max(Max, M); pass iff Max > thr.  The mask table of
-// alignment_avx2__setlength_* (:2282-2507) is rebuilt incrementally per step.
-template <int W>
-__device__ __forceinline__ bool sw_filter_one(const uint8_t* __restrict__ genome, int64_t pos,
-                                              const uint8_t* read, int L, int fm, int fx, int fo,
-                                              int fe, int fthr) {
-  constexpr uint32_t FULLC = (W == 16) ? 0xffffffffu : ((1u << (2 * W)) - 1u);
-  constexpr uint32_t FULLM = (1u << W) - 1u;
-  int M1[W], M2[W], I1[W];
-#pragma unroll
-  for (int k = 0; k < W; ++k) { M1[k] = 0; M2[k] = 0; I1[k] = 0; }
-  uint32_t A = 0, B = 0;
-  int64_t g = pos;
-#pragma unroll
-  for (int d = 0; d < W; ++d) B = ((B << 2) | (uint32_t)code_at(genome, g++)) & FULLC;
-  const int prlength = 2 * (L + W - 1);
-  uint32_t msk = 1u << (W - 1);
-  int Max = 0, r = 0;
-  for (int l = 0; l < prlength; ++l) {
-    if (l > 0 && !(l & 1)) {
-      if (l >= prlength - 2 * (W - 1)) msk = (msk >> 1) & FULLM;
-      else if (l <= 2 * (W - 1)) msk = msk | ((msk >> 1) & FULLM);
-    }
-    const bool odd = l & 1;
-    if (odd) B = ((B << 2) | (uint32_t)code_at(genome, g++)) & FULLC;
-    else A = (A >> 2) | ((uint32_t)code_at(read, r++) << (2 * (W - 1)));
-    const uint32_t x = A ^ B;
-    int Mn[W], In[W];
-#pragma unroll
-    for (int k = 0; k < W; ++k) {
-      const bool eq = ((x >> (2 * k)) & 3u) == 0u;
-      int m = eq ? min(M2[k] + fm, 255) : max(M2[k] - fx, 0);
-      int Is_, Ms_;
-      if (odd) { Is_ = k > 0 ? I1[k - 1] : 0; Ms_ = k > 0 ? M1[k - 1] : 0; }
-      else { Is_ = k < W - 1 ? I1[k + 1] : 0; Ms_ = k < W - 1 ? M1[k + 1] : 0; }
-      const int Im = max(I1[k], Is_), Mm = max(M1[k], Ms_);
-      const int iv = max(max(Im - fe, 0), max(Mm - fo, 0));
-      m = max(m, iv);
-      if (!((msk >> k) & 1u)) m = 0;
-      Max = max(Max, m);
-      Mn[k] = m;
-      In[k] = iv;
-    }
-#pragma unroll
-    for (int k = 0; k < W; ++k) { M2[k] = M1[k]; M1[k] = Mn[k]; I1[k] = In[k]; }
-  }
-  return Max > fthr;
-}
-
-__device__ __forceinline__ bool sw_filter_dispatch(int W, const uint8_t* genome, int64_t pos,
-                                                   const uint8_t* read, int L, const ScoreParams& sp) {
-  switch (W) {
-  case 2: return sw_filter_one<2>(genome, pos, read, L, sp.fm, sp.fx, sp.fo, sp.fe, sp.fthr);
-  case 4: return sw_filter_one<4>(genome, pos, read, L, sp.fm, sp.fx, sp.fo, sp.fe, sp.fthr);
-  case 8: return sw_filter_one<8>(genome, pos, read, L, sp.fm, sp.fx, sp.fo, sp.fe, sp.fthr);
-  default: return sw_filter_one<16>(genome, pos, read, L, sp.fm, sp.fx, sp.fo, sp.fe, sp.fthr);
-  }
-}
-
-constexpr int kReadSmem = (STORMGPU_MAX_READ_LEN + 64) / 4;
-
-__global__ void filter_kernel(ReadsDev rd, ScoreParams sp, const uint8_t* __restrict__ genome,
-                              const int64_t* __restrict__ hoff, int32_t* __restrict__ cand,
-                              const int32_t* __restrict__ ucount, PassBuffers pb) {
-  __shared__ uint8_t sread[8][kReadSmem];
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const int64_t nwarps = (int64_t)gridDim.x * (blockDim.x >> 5);
-  const unsigned lt = (1u << lane) - 1u;
-  unsigned long long cells = 0, cands = 0, acells = 0;
-  const int BW = 2 * sp.I + 1;
-  for (int64_t r = (int64_t)blockIdx.x * (blockDim.x >> 5) + w; r < rd.n; r += nwarps) {
-    const int U = ucount[r];
-    if (U == 0) {
-      if (lane == 0) { pb.pcount[r] = 0; pb.pstart[r] = 0; }
-      continue;
-    }
-    const int L = rd.lengths[r];
-    const uint8_t* src = rd.codes + r * rd.cstride;
-    const int nb = (L + sp.W + 8) / 4;
-    for (int b = lane; b < kReadSmem; b += 32) sread[w][b] = (b < nb && b < rd.cstride) ? src[b] : 0;
-    __syncwarp();
-    int32_t* seg = cand + hoff[r];
-    int P = 0;
-    for (int c0 = 0; c0 < U; c0 += 32) {
-      const int c = c0 + lane;
-      int32_t d = c < U ? seg[c] : 0;
-      bool pass = c < U && sw_filter_dispatch(sp.W, genome, (int64_t)d - sp.Is, sread[w], L, sp);
-      unsigned m = __ballot_sync(0xffffffffu, pass);
-      if (pass) seg[P + __popc(m & lt)] = d;  // in-place compaction (writes trail reads)
-      P += __popc(m);
-    }
-    cells += (unsigned long long)U * L * (2 * sp.Is + 1);
-    cands += (unsigned long long)U;
-    acells += (unsigned long long)P * L * BW;
-    int start = 0;
-    if (lane == 0) start = (int)atomicAdd(&pb.counters[0], (unsigned long long)P);
-    start = __shfl_sync(0xffffffffu, start, 0);
-    if (lane == 0) { pb.pstart[r] = start; pb.pcount[r] = P; }
-    if ((int64_t)start + P > pb.p_cap) {
-      if (lane == 0) atomicExch(&pb.counters[1], 1ull);
-      continue;
-    }
-    __syncwarp();
-    for (int k = lane; k < P; k += 32) {
-      pb.p_read[start + k] = (int32_t)r;
-      pb.p_diag[start + k] = seg[k];
-    }
-    __syncwarp();
-  }
-  if (lane == 0) {
-    atomicAdd(&pb.counters[2], cells);
-    atomicAdd(&pb.counters[5], cands);
-    atomicAdd(&pb.counters[6], acells);
-  }
-}
-
-void launch_filter(const ReadsDev& r, const ScoreParams& sp, const uint8_t* genome,
-                   const int64_t* hoff, const int32_t* cand, const int32_t* ucount,
-                   PassBuffers& pb, cudaStream_t st) {
-  if (r.n <= 0) return;
-  int64_t blocks = (r.n + 7) / 8;
-  if (blocks > 148 * 64) blocks = 148 * 64;
-  filter_kernel<<<(unsigned)blocks, 256, 0, st>>>(r, sp, genome, hoff, (int32_t*)cand, ucount, pb);
-}
-
-__global__ void filter_flat_kernel(int W, int L, ScoreParams sp, const uint8_t* __restrict__ genome,
-                                   const int32_t* __restrict__ pos, int64_t n, const uint8_t* __restrict__ read,
-                                   uint8_t* __restrict__ pass) {
-  int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= n) return;
-  pass[t] = sw_filter_dispatch(W, genome, pos[t], read, L, sp) ? 1 : 0;
-}
-
-void launch_filter_flat(int W, int L, const ScoreParams& sp, const uint8_t* genome,
-                        const int32_t* pos, int64_t n, const uint8_t* read, uint8_t* pass,
-                        cudaStream_t st) {
-  if (n <= 0) return;
-  filter_flat_kernel<<<(unsigned)((n + 127) / 128), 128, 0, st>>>(W, L, sp, genome, pos, n, read, pass);
-}
-
 // ------------------------------------------------------------------------------ align
 
 // Cell state packed in 16 bits: from (2) | indels (7) | colour checksum (2) | auto-correct (2)

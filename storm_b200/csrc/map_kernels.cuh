@@ -73,18 +73,11 @@ void launch_segment_unique(const ReadsDev& r, const int32_t* hits, const int64_t
 void launch_segment_unique_big(const int32_t* big_list, int nbig, const int32_t* hits,
                                const int64_t* hoff, int32_t* cand, int32_t* ucount, int I,
                                int32_t* tmp, int64_t tmp_elems, cudaStream_t st);
-void launch_filter(const ReadsDev& r, const ScoreParams& sp, const uint8_t* genome,
-                   const int64_t* hoff, const int32_t* cand, const int32_t* ucount,
-                   PassBuffers& pb, cudaStream_t st);
 void launch_align(const ReadsDev& r, const ScoreParams& sp, const uint8_t* genome,
                   const uint8_t* mask, int64_t slot0, int64_t nslots, PassBuffers& pb,
                   cudaStream_t st);
 void launch_replay(int64_t n, const ScoreParams& sp, int ref_id, int sense, PassBuffers& pb,
                    stormgpu_hit* hits, uint8_t* tb, int64_t tbs, uint8_t* mapped, cudaStream_t st);
 
-// unit-level kernels
-void launch_filter_flat(int W, int L, const ScoreParams& sp, const uint8_t* genome,
-                        const int32_t* pos, int64_t n, const uint8_t* read, uint8_t* pass,
-                        cudaStream_t st);
 
 }  // namespace sg

@@ -12,6 +12,7 @@
 #include "index_build.cuh"
 #include "map_kernels.cuh"
 #include "scan.cuh"
+#include "sw_filter.cuh"
 
 static thread_local char g_err[1024];
 
@@ -152,7 +153,9 @@ struct stormgpu_ctx {
   DevBuf<uint8_t> tb, mapped;
   // pass buffers
   DevBuf<int32_t> hitsc, ucount, cand, pstart, pcount, p_read, p_diag, big_list, big_count;
-  DevBuf<int64_t> hoff, scan_tmp64;
+  DevBuf<int64_t> hoff, scan_tmp64, uoff, foff;
+  DevBuf<int32_t> fr, fd;
+  DevBuf<uint8_t> flag;
   DevBuf<int32_t> a_score, a_bound, a_tblen, big_tmp;
   DevBuf<int16_t> a_pos;
   DevBuf<uint8_t> a_tb;
@@ -206,6 +209,7 @@ extern "C" void stormgpu_close(stormgpu_ctx* c) {
   c->big_list.release(); c->big_count.release(); c->hoff.release(); c->scan_tmp64.release();
   c->a_score.release(); c->a_bound.release(); c->a_tblen.release(); c->big_tmp.release();
   c->a_pos.release(); c->a_tb.release(); c->scratch.release(); c->counters.release();
+  c->uoff.release(); c->foff.release(); c->fr.release(); c->fd.release(); c->flag.release();
   for (auto& e : c->ev) cudaEventDestroy(e);
   cudaStreamDestroy(c->st);
   delete c;
@@ -300,7 +304,7 @@ static int map_device_impl(stormgpu_ctx* c, const stormgpu_reads* reads, stormgp
     rev.levels = reads->levels ? c->rlevels.p : nullptr;
   }
   if (c->hitsc.grow(n) || c->ucount.grow(n) || c->pstart.grow(n) || c->pcount.grow(n) ||
-      c->hoff.grow(n + 1) || c->scan_tmp64.grow(scan_tmp_elems(n) + 8) || c->big_list.grow(n) ||
+      c->hoff.grow(n + 1) || c->uoff.grow(n + 1) || c->scan_tmp64.grow(scan_tmp_elems(n) + 8) || c->big_list.grow(n) ||
       c->big_count.grow(1) || c->counters.grow(8))
     return STORMGPU_ENOMEM;
   const int BW = 2 * sp.I + 1;
@@ -324,9 +328,7 @@ static int map_device_impl(stormgpu_ctx* c, const stormgpu_reads* reads, stormgp
       int64_t htot = 0;
       SG_CUDA(cudaMemcpyAsync(&htot, c->hoff.p + n, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
       SG_CUDA(cudaStreamSynchronize(st));
-      if (c->cand.grow(std::max<int64_t>(htot, 1)) || c->p_read.grow(std::max<int64_t>(htot, 1)) ||
-          c->p_diag.grow(std::max<int64_t>(htot, 1)))
-        return STORMGPU_ENOMEM;
+      if (c->cand.grow(std::max<int64_t>(htot, 1))) return STORMGPU_ENOMEM;
       launch_gather_expand(rd, c->seeds, ix, c->hoff.p, c->cand.p, st);
       SG_CUDA(cudaMemsetAsync(c->big_count.p, 0, sizeof(int32_t), st));
       launch_segment_unique(rd, c->hitsc.p, c->hoff.p, c->cand.p, c->ucount.p, sp.I, c->big_list.p,
@@ -364,31 +366,52 @@ static int map_device_impl(stormgpu_ctx* c, const stormgpu_reads* reads, stormgp
           launches++;
         }
       }
+      // flat candidate list (read, diagonal), reads in order, diagonals ascending per read
+      exclusive_scan<int32_t, int64_t>(c->ucount.p, c->uoff.p, n, c->uoff.p + n, c->scan_tmp64.p, st);
+      int64_t utot = 0;
+      SG_CUDA(cudaMemcpyAsync(&utot, c->uoff.p + n, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+      SG_CUDA(cudaStreamSynchronize(st));
+      if (c->fr.grow(std::max<int64_t>(utot, 1)) || c->fd.grow(std::max<int64_t>(utot, 1)) ||
+          c->flag.grow(std::max<int64_t>(utot, 1)) || c->foff.grow(utot + 1) ||
+          c->scan_tmp64.grow(scan_tmp_elems(std::max<int64_t>(utot, n)) + 8))
+        return STORMGPU_ENOMEM;
+      launch_flatten(n, c->hoff.p, c->cand.p, c->ucount.p, c->uoff.p, c->fr.p, c->fd.p, st);
+      launches += 5;
       SG_CUDA(cudaEventRecord(c->ev[1], st));
-      PassBuffers pb;
-      memset(&pb, 0, sizeof(pb));
-      pb.hits = c->hitsc.p; pb.hoff = c->hoff.p; pb.ucount = c->ucount.p; pb.cand = c->cand.p;
-      pb.cand_cap = c->cand.cap; pb.pstart = c->pstart.p; pb.pcount = c->pcount.p;
-      pb.p_read = c->p_read.p; pb.p_diag = c->p_diag.p; pb.p_cap = c->p_read.cap;
-      pb.counters = c->counters.p;
-      launch_filter(rd, sp, R.d_codes, c->hoff.p, c->cand.p, c->ucount.p, pb, st);
+      FilterJob job;
+      job.n = utot; job.fr = c->fr.p; job.fd = c->fd.p; job.flag = c->flag.p; job.codes = rd.codes;
+      job.cstride = rd.cstride; job.lengths = rd.lengths; job.genome = R.d_codes; job.W = sp.W; job.Is = sp.Is;
+      job.fm = sp.fm; job.fx = sp.fx; job.fo = sp.fo; job.fe = sp.fe; job.fthr = sp.fthr;
+      job.counters = c->counters.p;
+      launch_filter_flat_job(job, sp, filter_dpx_ok(sp, maxL), st);
       launches++;
       SG_CUDA(cudaEventRecord(c->ev[2], st));
+      exclusive_scan<uint8_t, int64_t>(c->flag.p, c->foff.p, utot, c->foff.p + utot, c->scan_tmp64.p, st);
       unsigned long long cnt[8];
+      int64_t npass = 0;
+      SG_CUDA(cudaMemcpyAsync(&npass, c->foff.p + utot, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
       SG_CUDA(cudaMemcpyAsync(cnt, c->counters.p, sizeof(cnt), cudaMemcpyDeviceToHost, st));
       SG_CUDA(cudaStreamSynchronize(st));
-      if (cnt[1]) { sg_set_error("internal: filter slot overflow"); return STORMGPU_EINVAL; }
-      const int64_t npass = (int64_t)cnt[0];
+      if (utot == 0) npass = 0;
       S.candidates += (int64_t)cnt[5];
-      S.align_cells += (int64_t)cnt[6];
       S.filter_cells += (int64_t)cnt[2];
       S.seed_lookups += (int64_t)cnt[3];
       S.hit_positions += (int64_t)cnt[4];
       S.filter_passed += npass;
+      PassBuffers pb;
+      memset(&pb, 0, sizeof(pb));
+      pb.hits = c->hitsc.p; pb.hoff = c->hoff.p; pb.ucount = c->ucount.p; pb.cand = c->cand.p;
+      pb.cand_cap = c->cand.cap; pb.pstart = c->pstart.p; pb.pcount = c->pcount.p;
+      pb.counters = c->counters.p;
+      SG_CUDA(cudaMemsetAsync(c->pcount.p, 0, sizeof(int32_t) * n, st));
       if (npass > 0) {
-        if (c->a_score.grow(npass) || c->a_bound.grow(npass) || c->a_tblen.grow(npass) ||
-            c->a_pos.grow(npass * 4) || c->a_tb.grow(npass * tbs))
+        if (c->p_read.grow(npass) || c->p_diag.grow(npass) || c->a_score.grow(npass) || c->a_bound.grow(npass) ||
+            c->a_tblen.grow(npass) || c->a_pos.grow(npass * 4) || c->a_tb.grow(npass * tbs))
           return STORMGPU_ENOMEM;
+        pb.p_read = c->p_read.p; pb.p_diag = c->p_diag.p; pb.p_cap = c->p_read.cap;
+        launch_compact(utot, c->flag.p, c->foff.p, c->fr.p, c->fd.p, c->p_read.p, c->p_diag.p, st);
+        launch_slot_bounds(npass, c->p_read.p, c->pstart.p, c->pcount.p, st);
+        launches += 3;
         pb.a_score = c->a_score.p; pb.a_bound = c->a_bound.p; pb.a_tblen = c->a_tblen.p;
         pb.a_pos = c->a_pos.p; pb.a_tb = c->a_tb.p; pb.tbs = tbs;
         const int64_t per_slot = (int64_t)maxL * wpr;
@@ -400,6 +423,7 @@ static int map_device_impl(stormgpu_ctx* c, const stormgpu_reads* reads, stormgp
           launches++;
         }
         S.aligned += npass;
+        S.align_cells += npass * (int64_t)maxL * BW;
       }
       SG_CUDA(cudaEventRecord(c->ev[3], st));
       if (npass > 0) {
@@ -550,7 +574,25 @@ extern "C" int stormgpu_sw_filter(int W, int read_len, uint32_t match, uint32_t 
   SG_CUDA(cudaMalloc(&dpos, sizeof(int32_t) * std::max<int64_t>(n, 1)));
   SG_CUDA(cudaMalloc(&dp, std::max<int64_t>(n, 1)));
   if (n) SG_CUDA(cudaMemcpy(dpos, pos, sizeof(int32_t) * n, cudaMemcpyHostToDevice));
-  launch_filter_flat(W, read_len, sp, gb, dpos, n, dr, dp, 0);
+  {
+    int16_t L16 = (int16_t)read_len;
+    int16_t* dl;
+    int32_t* dzero;
+    SG_CUDA(cudaMalloc(&dl, sizeof(int16_t)));
+    SG_CUDA(cudaMemcpy(dl, &L16, sizeof(int16_t), cudaMemcpyHostToDevice));
+    SG_CUDA(cudaMalloc(&dzero, sizeof(int32_t) * std::max<int64_t>(n, 1)));
+    SG_CUDA(cudaMemset(dzero, 0, sizeof(int32_t) * std::max<int64_t>(n, 1)));
+    FilterJob job;
+    memset(&job, 0, sizeof(job));
+    job.n = n; job.fr = dzero; job.fd = dpos; job.flag = dp; job.codes = dr; job.cstride = rb;
+    job.lengths = dl; job.genome = gb; job.W = W; job.Is = 0;
+    job.fm = sp.fm; job.fx = sp.fx; job.fo = sp.fo; job.fe = sp.fe; job.fthr = sp.fthr;
+    launch_filter_flat_job(job, sp, filter_dpx_ok(sp, read_len), 0);
+    SG_CUDA(cudaGetLastError());
+    SG_CUDA(cudaDeviceSynchronize());
+    cudaFree(dl);
+    cudaFree(dzero);
+  }
   SG_CUDA(cudaGetLastError());
   SG_CUDA(cudaDeviceSynchronize());
   if (n) SG_CUDA(cudaMemcpy(pass, dp, n, cudaMemcpyDeviceToHost));

@@ -1,0 +1,171 @@
+// sw_filter.cu -- the banded SW filter on packed 16-bit pairs (DPX), one candidate diagonal
+// per thread over a flat candidate list, and the order-preserving compaction of the
+// candidates that pass.
+//
+// Semantics: those of alignment_avx2__align_{hexa,octa,quad,pair} (alignment_simd.c:2613-3404)
+// for one hit of W cells, as restated in map_kernels.cu (sw_filter_one).  Here the W cells of
+// one anti-diagonal step live in W/2 registers, two signed 16-bit cells each:
+//   * codes: one byte per cell holding the code twice (c | c << 4), so that
+//     sel = (A ^ B) | 0x8080 is directly a byte_perm selector whose nibbles pick
+//     T = [match, -mismatch, -mismatch, -mismatch] and sign-replicate it: the per-cell score
+//     is one PRMT (code 0 = equal symbols);
+//   * I = max(P, P of the neighbour cell, 0) with P = max(I[l-1] - ext, M[l-1] - open): the
+//     neighbour is the same cell one register-half over (PRMT 0x5432);
+//   * M = max(M[l-2] + score, I, 0) in one __viaddmax_s16x2_relu.
+// The upper u8 saturation of the reference (adds at 255) is not reproduced: the threshold is
+// at most 254, so the first cell that would saturate already has a value above it and the
+// hit passes in both; cells are masked before they propagate, so an unmasked run and a
+// saturating one agree on pass/fail.  Values stay below 2^15 when L * match < 32768 (checked
+// by the host, which otherwise uses the plain 32-bit kernel).
+#include "map_kernels.cuh"
+#include "sw_filter.cuh"
+#include "filter_ref.cuh"
+#include "filter_core.cuh"
+
+namespace sg {
+
+template <int W>
+__global__ void __launch_bounds__(256) filter_flat_dpx_kernel(FilterJob job) {
+  const uint32_t T = (uint32_t)(job.fm & 0xff) | ((uint32_t)((256 - job.fx) & 0xff) << 8) |
+                     ((uint32_t)((256 - job.fx) & 0xff) << 16) | ((uint32_t)((256 - job.fx) & 0xff) << 24);
+  const uint32_t NFE = (uint32_t)(uint16_t)(-job.fe) * 0x10001u;
+  const uint32_t NFO = (uint32_t)(uint16_t)(-job.fo) * 0x10001u;
+  unsigned long long cells = 0, cands = 0;
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < job.n; t += (int64_t)gridDim.x * blockDim.x) {
+    const int r = job.fr[t];
+    const int d = job.fd[t];
+    const int L = job.lengths[r];
+    const int mx = filter_dpx<W>(job.genome, (int64_t)d - job.Is, job.codes + (int64_t)r * job.cstride,
+                                 job.cstride, L, T, NFE, NFO);
+    job.flag[t] = mx > job.fthr ? 1 : 0;
+    cells += (unsigned long long)L * (2 * job.Is + 1);
+    cands++;
+  }
+  if (job.counters) {
+    for (int o = 16; o > 0; o >>= 1) {
+      cells += __shfl_xor_sync(0xffffffffu, cells, o);
+      cands += __shfl_xor_sync(0xffffffffu, cands, o);
+    }
+    if ((threadIdx.x & 31) == 0 && cands) {
+      atomicAdd(&job.counters[2], cells);
+      atomicAdd(&job.counters[5], cands);
+    }
+  }
+}
+
+// Plain 32-bit variant (any score values), the restatement in map_kernels.cu.
+__global__ void filter_flat_scalar_kernel(FilterJob job, ScoreParams sp) {
+  unsigned long long cells = 0, cands = 0;
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < job.n; t += (int64_t)gridDim.x * blockDim.x) {
+    const int r = job.fr[t];
+    const int L = job.lengths[r];
+    job.flag[t] = sw_filter_dispatch_ext(job.W, job.genome, (int64_t)job.fd[t] - job.Is,
+                                         job.codes + (int64_t)r * job.cstride, L, sp) ? 1 : 0;
+    cells += (unsigned long long)L * (2 * job.Is + 1);
+    cands++;
+  }
+  if (job.counters) {
+    for (int o = 16; o > 0; o >>= 1) {
+      cells += __shfl_xor_sync(0xffffffffu, cells, o);
+      cands += __shfl_xor_sync(0xffffffffu, cands, o);
+    }
+    if ((threadIdx.x & 31) == 0 && cands) {
+      atomicAdd(&job.counters[2], cells);
+      atomicAdd(&job.counters[5], cands);
+    }
+  }
+}
+
+bool filter_dpx_ok(const ScoreParams& sp, int max_len) {
+  return sp.fm <= 127 && sp.fx <= 128 && (int64_t)max_len * sp.fm < 32000 && sp.fe <= 32000 && sp.fo <= 32000;
+}
+
+void launch_filter_flat_job(const FilterJob& job, const ScoreParams& sp, bool dpx, cudaStream_t st) {
+  if (job.n <= 0) return;
+  int64_t blocks = (job.n + 255) / 256;
+  if (blocks > 148 * 32) blocks = 148 * 32;
+  if (!dpx) {
+    filter_flat_scalar_kernel<<<(unsigned)blocks, 256, 0, st>>>(job, sp);
+    return;
+  }
+  switch (job.W) {
+  case 2: filter_flat_dpx_kernel<2><<<(unsigned)blocks, 256, 0, st>>>(job); break;
+  case 4: filter_flat_dpx_kernel<4><<<(unsigned)blocks, 256, 0, st>>>(job); break;
+  case 8: filter_flat_dpx_kernel<8><<<(unsigned)blocks, 256, 0, st>>>(job); break;
+  default: filter_flat_dpx_kernel<16><<<(unsigned)blocks, 256, 0, st>>>(job); break;
+  }
+}
+
+// ------------------------------------------------------------------ flat lists, compaction
+
+// per read: its unique diagonals (segment at hoff[r], ucount[r] long) -> flat arrays at uoff[r]
+__global__ void flatten_kernel(int64_t n, const int64_t* __restrict__ hoff, const int32_t* __restrict__ cand,
+                               const int32_t* __restrict__ ucount, const int64_t* __restrict__ uoff,
+                               int32_t* __restrict__ fr, int32_t* __restrict__ fd) {
+  const int lane = threadIdx.x & 31;
+  const int64_t nwarps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  for (int64_t r = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); r < n; r += nwarps) {
+    const int U = ucount[r];
+    const int32_t* src = cand + hoff[r];
+    const int64_t o = uoff[r];
+    for (int k = lane; k < U; k += 32) {
+      fr[o + k] = (int32_t)r;
+      fd[o + k] = src[k];
+    }
+  }
+}
+
+void launch_flatten(int64_t n, const int64_t* hoff, const int32_t* cand, const int32_t* ucount,
+                    const int64_t* uoff, int32_t* fr, int32_t* fd, cudaStream_t st) {
+  if (n <= 0) return;
+  int64_t blocks = (n + 7) / 8;
+  if (blocks > 148 * 32) blocks = 148 * 32;
+  flatten_kernel<<<(unsigned)blocks, 256, 0, st>>>(n, hoff, cand, ucount, uoff, fr, fd);
+}
+
+// passing candidates, in order, into (p_read, p_diag); pcount/pstart per read
+__global__ void compact_kernel(int64_t n, const uint8_t* __restrict__ flag, const int64_t* __restrict__ off,
+                               const int32_t* __restrict__ fr, const int32_t* __restrict__ fd,
+                               int32_t* __restrict__ p_read, int32_t* __restrict__ p_diag) {
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) {
+    if (flag[t]) {
+      const int64_t o = off[t];
+      p_read[o] = fr[t];
+      p_diag[o] = fd[t];
+    }
+  }
+}
+
+__global__ void slot_bounds_kernel(int64_t npass, const int32_t* __restrict__ p_read, int32_t* __restrict__ pstart,
+                                   int32_t* __restrict__ pcount) {
+  for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < npass; s += (int64_t)gridDim.x * blockDim.x) {
+    const int r = p_read[s];
+    if (s == 0 || p_read[s - 1] != r) pstart[r] = (int32_t)s;
+  }
+}
+
+__global__ void slot_count_kernel(int64_t npass, const int32_t* __restrict__ p_read, const int32_t* __restrict__ pstart,
+                                  int32_t* __restrict__ pcount) {
+  for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < npass; s += (int64_t)gridDim.x * blockDim.x) {
+    const int r = p_read[s];
+    if (s == npass - 1 || p_read[s + 1] != r) pcount[r] = (int32_t)(s - pstart[r] + 1);
+  }
+}
+
+void launch_compact(int64_t n, const uint8_t* flag, const int64_t* off, const int32_t* fr, const int32_t* fd,
+                    int32_t* p_read, int32_t* p_diag, cudaStream_t st) {
+  if (n <= 0) return;
+  int64_t blocks = (n + 255) / 256;
+  if (blocks > 148 * 32) blocks = 148 * 32;
+  compact_kernel<<<(unsigned)blocks, 256, 0, st>>>(n, flag, off, fr, fd, p_read, p_diag);
+}
+
+void launch_slot_bounds(int64_t npass, const int32_t* p_read, int32_t* pstart, int32_t* pcount, cudaStream_t st) {
+  if (npass <= 0) return;
+  int64_t blocks = (npass + 255) / 256;
+  if (blocks > 148 * 32) blocks = 148 * 32;
+  slot_bounds_kernel<<<(unsigned)blocks, 256, 0, st>>>(npass, p_read, pstart, pcount);
+  slot_count_kernel<<<(unsigned)blocks, 256, 0, st>>>(npass, p_read, pstart, pcount);
+}
+
+}  // namespace sg
