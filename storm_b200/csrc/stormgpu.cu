@@ -108,6 +108,8 @@ ScoreParams make_score_params(const stormgpu_params& p) {
 
 struct RefSeq {
   int64_t n = 0;
+  uint8_t* d_gexp_alloc = nullptr;
+  uint8_t* d_gexp = nullptr;     // byte-expanded codes (filter streams)
   uint8_t* d_codes_alloc = nullptr;
   uint8_t* d_mask_alloc = nullptr;
   uint8_t* d_codes = nullptr;
@@ -155,7 +157,7 @@ struct stormgpu_ctx {
   DevBuf<int32_t> hitsc, ucount, cand, pstart, pcount, p_read, p_diag, big_list, big_count;
   DevBuf<int64_t> hoff, scan_tmp64, uoff, foff;
   DevBuf<int32_t> fr, fd;
-  DevBuf<uint8_t> flag;
+  DevBuf<uint8_t> flag, rexp;
   DevBuf<int32_t> a_score, a_bound, a_tblen, big_tmp;
   DevBuf<int16_t> a_pos;
   DevBuf<uint8_t> a_tb;
@@ -179,6 +181,14 @@ extern "C" int stormgpu_open(const stormgpu_params* params, const char* seeds, s
   }
   if (params->device < 0 || params->device >= ndev) { sg_set_error("bad device ordinal"); return STORMGPU_EINVAL; }
   SG_CUDA(cudaSetDevice(params->device));
+  {
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, params->device) == cudaSuccess) {
+      uint64_t keep = UINT64_MAX;
+      cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+    cudaGetLastError();
+  }
   stormgpu_ctx* c = new stormgpu_ctx();
   c->p = *params;
   c->seeds = ss;
@@ -200,6 +210,7 @@ extern "C" void stormgpu_close(stormgpu_ctx* c) {
   for (auto& r : c->refs) {
     cudaFree(r.d_codes_alloc);
     cudaFree(r.d_mask_alloc);
+    cudaFree(r.d_gexp_alloc);
     for (auto& ix : r.idx) { cudaFree(ix.first); cudaFree(ix.map); }
   }
   c->rcodes.release(); c->rlevels.release(); c->fcodes.release(); c->flevels.release();
@@ -210,6 +221,7 @@ extern "C" void stormgpu_close(stormgpu_ctx* c) {
   c->a_score.release(); c->a_bound.release(); c->a_tblen.release(); c->big_tmp.release();
   c->a_pos.release(); c->a_tb.release(); c->scratch.release(); c->counters.release();
   c->uoff.release(); c->foff.release(); c->fr.release(); c->fd.release(); c->flag.release();
+  c->rexp.release();
   for (auto& e : c->ev) cudaEventDestroy(e);
   cudaStreamDestroy(c->st);
   delete c;
@@ -238,6 +250,10 @@ extern "C" int stormgpu_add_reference(stormgpu_ctx* c, const uint8_t* codes, con
   if (mask) memcpy(hm.data(), mask, nb);
   for (int64_t k = n_codes; k & 3; ++k) hm[k >> 2] |= (uint8_t)(1u << ((k & 3) << 1));  // masked past the end
   SG_CUDA(cudaMemcpyAsync(r.d_mask, hm.data(), nb, cudaMemcpyHostToDevice, c->st));
+  SG_CUDA(cudaMalloc(&r.d_gexp_alloc, n_codes + 2 * kGexpPad + 16));
+  SG_CUDA(cudaMemsetAsync(r.d_gexp_alloc, 0, n_codes + 2 * kGexpPad + 16, c->st));
+  r.d_gexp = r.d_gexp_alloc + kGexpPad;
+  launch_expand_genome(r.d_codes, n_codes, r.d_gexp, c->st);
   r.rs.assign(rs, rs + std::max(n_regions, 0));
   r.re.assign(re, re + std::max(n_regions, 0));
   SG_CUDA(cudaStreamSynchronize(c->st));
@@ -383,8 +399,12 @@ static int map_device_impl(stormgpu_ctx* c, const stormgpu_reads* reads, stormgp
       job.cstride = rd.cstride; job.lengths = rd.lengths; job.genome = R.d_codes; job.W = sp.W; job.Is = sp.Is;
       job.fm = sp.fm; job.fx = sp.fx; job.fo = sp.fo; job.fe = sp.fe; job.fthr = sp.fthr;
       job.counters = c->counters.p;
+      const int64_t rstride = rexp_stride(maxL);
+      if (c->rexp.grow(n * rstride)) return STORMGPU_ENOMEM;
+      launch_expand_reads(rd, c->rexp.p, rstride, st);
+      job.gexp = R.d_gexp; job.rexp = c->rexp.p; job.rstride = rstride;
       launch_filter_flat_job(job, sp, filter_dpx_ok(sp, maxL), st);
-      launches++;
+      launches += 2;
       SG_CUDA(cudaEventRecord(c->ev[2], st));
       exclusive_scan<uint8_t, int64_t>(c->flag.p, c->foff.p, utot, c->foff.p + utot, c->scan_tmp64.p, st);
       unsigned long long cnt[8];
@@ -582,16 +602,27 @@ extern "C" int stormgpu_sw_filter(int W, int read_len, uint32_t match, uint32_t 
     SG_CUDA(cudaMemcpy(dl, &L16, sizeof(int16_t), cudaMemcpyHostToDevice));
     SG_CUDA(cudaMalloc(&dzero, sizeof(int32_t) * std::max<int64_t>(n, 1)));
     SG_CUDA(cudaMemset(dzero, 0, sizeof(int32_t) * std::max<int64_t>(n, 1)));
+    uint8_t *gx, *rx;
+    const int64_t rstride = rexp_stride(read_len);
+    SG_CUDA(cudaMalloc(&gx, n_codes + 2 * kGexpPad + 16));
+    SG_CUDA(cudaMemset(gx, 0, n_codes + 2 * kGexpPad + 16));
+    SG_CUDA(cudaMalloc(&rx, rstride));
+    launch_expand_genome(gb, n_codes, gx + kGexpPad, 0);
+    ReadsDev one{1, dr, rb, nullptr, 0, dl};
+    launch_expand_reads(one, rx, rstride, 0);
     FilterJob job;
     memset(&job, 0, sizeof(job));
     job.n = n; job.fr = dzero; job.fd = dpos; job.flag = dp; job.codes = dr; job.cstride = rb;
     job.lengths = dl; job.genome = gb; job.W = W; job.Is = 0;
+    job.gexp = gx + kGexpPad; job.rexp = rx; job.rstride = rstride;
     job.fm = sp.fm; job.fx = sp.fx; job.fo = sp.fo; job.fe = sp.fe; job.fthr = sp.fthr;
     launch_filter_flat_job(job, sp, filter_dpx_ok(sp, read_len), 0);
     SG_CUDA(cudaGetLastError());
     SG_CUDA(cudaDeviceSynchronize());
     cudaFree(dl);
     cudaFree(dzero);
+    cudaFree(gx);
+    cudaFree(rx);
   }
   SG_CUDA(cudaGetLastError());
   SG_CUDA(cudaDeviceSynchronize());

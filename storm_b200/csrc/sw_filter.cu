@@ -30,13 +30,19 @@ __global__ void __launch_bounds__(256) filter_flat_dpx_kernel(FilterJob job) {
                      ((uint32_t)((256 - job.fx) & 0xff) << 16) | ((uint32_t)((256 - job.fx) & 0xff) << 24);
   const uint32_t NFE = (uint32_t)(uint16_t)(-job.fe) * 0x10001u;
   const uint32_t NFO = (uint32_t)(uint16_t)(-job.fo) * 0x10001u;
+  uint32_t TLO, THI, CFE, CFO;
+  filter_v3_consts(job.fm, job.fx, job.fo, job.fe, TLO, THI, CFE, CFO);
   unsigned long long cells = 0, cands = 0;
   for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < job.n; t += (int64_t)gridDim.x * blockDim.x) {
     const int r = job.fr[t];
     const int d = job.fd[t];
     const int L = job.lengths[r];
-    const int mx = filter_dpx<W>(job.genome, (int64_t)d - job.Is, job.codes + (int64_t)r * job.cstride,
-                                 job.cstride, L, T, NFE, NFO);
+    const int64_t pos = (int64_t)d - job.Is;
+    int mx;
+    if (L >= W && job.gexp)
+      mx = filter_v3<W>(job.gexp, pos, job.rexp + (int64_t)r * job.rstride, L, TLO, THI, CFE, CFO);
+    else
+      mx = filter_dpx<W>(job.genome, pos, job.codes + (int64_t)r * job.cstride, job.cstride, L, T, NFE, NFO);
     job.flag[t] = mx > job.fthr ? 1 : 0;
     cells += (unsigned long long)L * (2 * job.Is + 1);
     cands++;
@@ -51,6 +57,46 @@ __global__ void __launch_bounds__(256) filter_flat_dpx_kernel(FilterJob job) {
       atomicAdd(&job.counters[5], cands);
     }
   }
+}
+
+__global__ void expand_genome_kernel(const uint8_t* __restrict__ codes, int64_t n_codes, uint8_t* __restrict__ gexp) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n_codes; i += (int64_t)gridDim.x * blockDim.x)
+    gexp[i] = (uint8_t)(code_at(codes, i) * 0x11);
+}
+
+void launch_expand_genome(const uint8_t* codes, int64_t n_codes, uint8_t* gexp, cudaStream_t st) {
+  if (n_codes <= 0) return;
+  int64_t blocks = (n_codes + 255) / 256;
+  if (blocks > 148 * 64) blocks = 148 * 64;
+  expand_genome_kernel<<<(unsigned)blocks, 256, 0, st>>>(codes, n_codes, gexp);
+}
+
+// one warp per read: bytes 0xC4 + c * 0x11 for the L codes, 0xC4 (code 0) after
+__global__ void expand_reads_kernel(ReadsDev rd, uint8_t* __restrict__ rexp, int64_t rstride) {
+  const int lane = threadIdx.x & 31;
+  const int64_t nwarps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  for (int64_t r = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); r < rd.n; r += nwarps) {
+    const int L = rd.lengths[r];
+    const uint8_t* c = rd.codes + r * rd.cstride;
+    uint32_t* o = reinterpret_cast<uint32_t*>(rexp + r * rstride);
+    for (int64_t w = lane; w < rstride / 4; w += 32) {
+      uint32_t v = 0;
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const int i = (int)(4 * w + k);
+        const uint32_t b = i < L ? 0xC4u + 0x11u * (uint32_t)code_at(c, i) : 0xC4u;
+        v |= b << (8 * k);
+      }
+      o[w] = v;
+    }
+  }
+}
+
+void launch_expand_reads(const ReadsDev& rd, uint8_t* rexp, int64_t rstride, cudaStream_t st) {
+  if (rd.n <= 0) return;
+  int64_t blocks = (rd.n + 7) / 8;
+  if (blocks > 148 * 32) blocks = 148 * 32;
+  expand_reads_kernel<<<(unsigned)blocks, 256, 0, st>>>(rd, rexp, rstride);
 }
 
 // Plain 32-bit variant (any score values), the restatement in map_kernels.cu.

@@ -17,7 +17,15 @@ struct FilterJob {
   int W, Is;
   int fm, fx, fo, fe, fthr;
   unsigned long long* counters;  // [2] += filter cells L*(2*Is+1), [5] += candidates
+  const uint8_t* gexp;          // byte-expanded genome (code c -> c * 0x11), code 0
+  const uint8_t* rexp;          // read streams (bytes 0xC4 + c * 0x11), rstride bytes per read
+  int64_t rstride;
 };
+
+constexpr int64_t kGexpPad = 4096;   // bytes of padding around a byte-expanded sequence
+inline int64_t rexp_stride(int max_len) { return ((int64_t)max_len + 16 + 8 + 15) & ~15LL; }
+void launch_expand_genome(const uint8_t* codes, int64_t n_codes, uint8_t* gexp, cudaStream_t st);
+void launch_expand_reads(const ReadsDev& rd, uint8_t* rexp, int64_t rstride, cudaStream_t st);
 
 bool filter_dpx_ok(const ScoreParams& sp, int max_len);
 void launch_filter_flat_job(const FilterJob& job, const ScoreParams& sp, bool dpx, cudaStream_t st);

@@ -18,6 +18,13 @@ static void pack(const std::vector<int>& c, uint8_t* out) {
 }
 
 template <int W>
+static int filter_w3(const uint8_t* gexp, int64_t pos, const uint8_t* rexp, int L, int fm, int fx, int fo, int fe) {
+  uint32_t TLO, THI, CFE, CFO;
+  sg::filter_v3_consts(fm, fx, fo, fe, TLO, THI, CFE, CFO);
+  return sg::filter_v3<W>(gexp, pos, rexp, L, TLO, THI, CFE, CFO);
+}
+
+template <int W>
 static int filter_w(const uint8_t* g, int64_t pos, const uint8_t* r, int64_t rstride, int L, int fm, int fx,
                     int fo, int fe) {
   const uint32_t T = (uint32_t)(fm & 0xff) | ((uint32_t)((256 - fx) & 0xff) << 8) |
@@ -35,6 +42,10 @@ int main(int argc, char** argv) {
   std::vector<int> g(G);
   for (int i = 0; i < G; ++i) g[i] = rng() & 3;
   pack(g, gen);
+  std::vector<uint8_t> gxbuf(PAD * 4 + G + PAD * 4, 0);
+  uint8_t* gexp = gxbuf.data() + PAD * 4;
+  for (int i = 0; i < G; ++i) gexp[i] = (uint8_t)(g[i] * 0x11);
+  int checked3 = 0;
   int checked = 0;
   for (int t = 0; t < cases; ++t) {
     const int Ws[4] = {2, 4, 8, 16};
@@ -60,6 +71,25 @@ int main(int argc, char** argv) {
     default: got = filter_w<16>(gen, pos, rb.data(), stride, L, fm, fx, fo, fe); break;
     }
     const int pass = got > (thr >= 255 ? 254 : thr);
+    if (L >= W) {
+      std::vector<uint8_t> rexp(((L + W + 8 + 3) & ~3) + 16, 0xC4);
+      for (int i = 0; i < L; ++i) rexp[i] = (uint8_t)(0xC4 + read[i] * 0x11);
+      int got3;
+      switch (W) {
+      case 2: got3 = filter_w3<2>(gexp, pos, rexp.data(), L, fm, fx, fo, fe); break;
+      case 4: got3 = filter_w3<4>(gexp, pos, rexp.data(), L, fm, fx, fo, fe); break;
+      case 8: got3 = filter_w3<8>(gexp, pos, rexp.data(), L, fm, fx, fo, fe); break;
+      default: got3 = filter_w3<16>(gexp, pos, rexp.data(), L, fm, fx, fo, fe); break;
+      }
+      const int pass3 = got3 > (thr >= 255 ? 254 : thr);
+      const int exp3 = or_sw_filter(W, L, fm, fx, fo, fe, thr, gen, pos, rb.data());
+      if (pass3 != exp3) {
+        printf("MISMATCH v3 case %d: W=%d L=%d fm=%d fx=%d fo=%d fe=%d thr=%d pos=%lld max=%d v2max=%d exp=%d\n", t, W, L,
+               fm, fx, fo, fe, thr, (long long)pos, got3, got, exp3);
+        return 1;
+      }
+      checked3++;
+    }
     const int exp = or_sw_filter(W, L, fm, fx, fo, fe, thr, gen, pos, rb.data());
     if (pass != exp) {
       printf("MISMATCH case %d: W=%d L=%d fm=%d fx=%d fo=%d fe=%d thr=%d pos=%lld max=%d exp=%d\n", t, W, L, fm,
@@ -68,6 +98,6 @@ int main(int argc, char** argv) {
     }
     checked++;
   }
-  printf("checked %d\n", checked);
+  printf("checked %d (v3 %d)\n", checked, checked3);
   return 0;
 }
