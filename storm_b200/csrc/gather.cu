@@ -1,0 +1,267 @@
+// gather.cu -- hit gather: for one read-strand, every (seed, read position) key's CSR list
+// (index.c:212-241) shifted by the read position, merged into the ascending, de-duplicated
+// diagonals that process_read's heap yields (run.c:577-698): a diagonal is kept iff it is
+// strictly greater than the previous one in sorted order, the previous of the first being -I
+// (run.c:617, :648, :697).
+//
+// One warp per read: keys computed from the packed read, CSR offsets read from the
+// (L2-resident) key table, positions gathered straight into the warp's shared memory, bitonic
+// sort there, de-duplication by ballot, and the surviving diagonals appended to the flat
+// candidate list (reads contiguous, diagonals ascending within a read).  Reads with more index
+// positions than a warp can hold go to a block-per-read kernel (shared memory up to 32768
+// positions) and, beyond that, to a global-memory variant run one read at a time.
+#include "gather.cuh"
+
+namespace sg {
+
+__constant__ SeedSet c_gseeds;
+
+// Seed key at read position rp; codes beyond the read's end read as 0 (seed.c:203-213).
+__device__ __forceinline__ uint32_t read_key(const SeedDev& s, const uint8_t* rd, int L, int rp) {
+  uint32_t key = 0;
+  for (int c = 0; c < s.n_care; ++c) {
+    const int p = rp + s.care[c];
+    key = (key << 2) | (uint32_t)(p < L ? code_at(rd, p) : 0);
+  }
+  return key;
+}
+
+__device__ __forceinline__ int seed_npos(const SeedDev& s, int L) {
+  return s.n_positions ? s.n_positions : (L - s.span + 1 > 0 ? L - s.span + 1 : 0);
+}
+
+// (index offset, count, read position) of item t of seed si
+__device__ __forceinline__ void seed_item(const IndexView& ix, int si, int t, const uint8_t* read, int L,
+                                          int& a, int& cnt, int& rp) {
+  const SeedDev& s = c_gseeds.s[si];
+  a = 0; cnt = 0; rp = 0;
+  if (t >= seed_npos(s, L)) return;
+  rp = s.n_positions ? s.positions[t] : t;
+  if (rp < 0 || rp >= L) return;
+  const uint32_t key = read_key(s, read, L, rp);
+  a = __ldg(ix.first[si] + key);
+  cnt = __ldg(ix.first[si] + key + 1) - a;
+}
+
+__device__ __forceinline__ void warp_bitonic(int32_t* s, int P) {
+  const int lane = threadIdx.x & 31;
+  for (int k = 2; k <= P; k <<= 1)
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      for (int i = lane; i < P; i += 32) {
+        const int ixj = i ^ j;
+        if (ixj > i) {
+          const int32_t a = s[i], b = s[ixj];
+          if ((a > b) == ((i & k) == 0)) { s[i] = b; s[ixj] = a; }
+        }
+      }
+      __syncwarp();
+    }
+}
+
+// sorted s[0..H) -> accepted diagonals appended to the flat list (one warp)
+__device__ __forceinline__ void warp_emit(int32_t* s, int H, int I, int r, const GatherOut& go) {
+  const int lane = threadIdx.x & 31;
+  const unsigned lt = (1u << lane) - 1u;
+  int U = 0;
+  for (int t0 = 0; t0 < H; t0 += 32) {
+    const int t = t0 + lane;
+    const int32_t v = t < H ? s[t] : 0;
+    const int32_t prev = t == 0 ? -I : (t < H ? s[t - 1] : 0);
+    const bool keep = t < H && v > prev;
+    const unsigned m = __ballot_sync(0xffffffffu, keep);
+    __syncwarp();
+    if (keep) s[U + __popc(m & lt)] = v;  // compaction in place (writes trail reads)
+    U += __popc(m);
+    __syncwarp();
+  }
+  unsigned long long base = 0;
+  if (lane == 0 && U) base = atomicAdd(&go.counters[7], (unsigned long long)U);
+  base = __shfl_sync(0xffffffffu, base, 0);
+  if ((int64_t)(base + U) > go.cap) {
+    if (lane == 0) atomicExch(&go.counters[8], 1ull);
+    return;
+  }
+  for (int k = lane; k < U; k += 32) {
+    go.fr[base + k] = r;
+    go.fd[base + k] = s[k];
+  }
+}
+
+constexpr int kWarpCap = 1024;
+constexpr int kGWarps = 8;
+
+__global__ void __launch_bounds__(kGWarps * 32) gather_fused_kernel(ReadsDev rd, IndexView ix, int I, GatherOut go) {
+  __shared__ int32_t sm[kGWarps][kWarpCap];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  int32_t* s = sm[w];
+  const int64_t nwarps = (int64_t)gridDim.x * kGWarps;
+  unsigned long long lookups = 0, positions = 0;
+  for (int64_t r = (int64_t)blockIdx.x * kGWarps + w; r < rd.n; r += nwarps) {
+    const int L = rd.lengths[r];
+    const uint8_t* read = rd.codes + r * rd.cstride;
+    int H = 0;
+    for (int si = 0; si < c_gseeds.n; ++si) {
+      const int np = seed_npos(c_gseeds.s[si], L);
+      const int32_t* mp = ix.map[si];
+      for (int t0 = 0; t0 < np; t0 += 32) {
+        int a, cnt, rp;
+        seed_item(ix, si, t0 + lane, read, L, a, cnt, rp);
+        lookups += (t0 + lane < np) ? 1 : 0;
+        const int incl = warp_incl_scan(cnt);
+        const int dst = H + incl - cnt;
+        H += __shfl_sync(0xffffffffu, incl, 31);
+        if (cnt <= 8) {
+          for (int u = 0; u < cnt; ++u)
+            if (dst + u < kWarpCap) s[dst + u] = __ldg(mp + a + u) - rp;
+        }
+        unsigned m = __ballot_sync(0xffffffffu, cnt > 8);
+        while (m) {
+          const int j = __ffs(m) - 1;
+          m &= m - 1;
+          const int aj = __shfl_sync(0xffffffffu, a, j), cj = __shfl_sync(0xffffffffu, cnt, j);
+          const int dj = __shfl_sync(0xffffffffu, dst, j), rj = __shfl_sync(0xffffffffu, rp, j);
+          for (int u = lane; u < cj; u += 32)
+            if (dj + u < kWarpCap) s[dj + u] = __ldg(mp + aj + u) - rj;
+        }
+      }
+    }
+    positions += (unsigned long long)H;
+    if (H > kWarpCap) {
+      if (lane == 0) go.big_list[atomicAdd(go.big_count, 1)] = (int32_t)r;
+      __syncwarp();
+      continue;
+    }
+    __syncwarp();
+    int P = 1;
+    while (P < H) P <<= 1;
+    for (int i = H + lane; i < P; i += 32) s[i] = 0x7fffffff;
+    __syncwarp();
+    warp_bitonic(s, P);
+    warp_emit(s, H, I, (int)r, go);
+    __syncwarp();
+  }
+  for (int o = 16; o > 0; o >>= 1) lookups += __shfl_xor_sync(0xffffffffu, lookups, o);
+  if (lane == 0) {
+    atomicAdd(&go.counters[3], lookups);
+    atomicAdd(&go.counters[4], positions);
+  }
+}
+
+// One block per read: the same steps with a block-wide scan, in dynamic shared memory (`cap`
+// positions) or, when gbuf is given, in that global buffer.  Reads with more than `cap`
+// positions are recorded in the huge list with their count.
+__global__ void gather_block_kernel(ReadsDev rd, IndexView ix, int I, const int32_t* __restrict__ list, GatherOut go,
+                                    int cap, int32_t* gbuf, int32_t* huge_list, int32_t* huge_h, int32_t* huge_count) {
+  extern __shared__ int32_t dsm[];
+  __shared__ int wtot[32];
+  __shared__ int s_H;
+  int32_t* s = gbuf ? gbuf : dsm;
+  const int r = list[blockIdx.x];
+  const int L = rd.lengths[r];
+  const uint8_t* read = rd.codes + (int64_t)r * rd.cstride;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  if (threadIdx.x == 0) s_H = 0;
+  __syncthreads();
+  for (int si = 0; si < c_gseeds.n; ++si) {
+    const int np = seed_npos(c_gseeds.s[si], L);
+    const int32_t* mp = ix.map[si];
+    for (int t0 = 0; t0 < np; t0 += blockDim.x) {
+      int a, cnt, rp;
+      seed_item(ix, si, t0 + threadIdx.x, read, L, a, cnt, rp);
+      const int incl = warp_incl_scan(cnt);
+      if (lane == 31) wtot[w] = incl;
+      __syncthreads();
+      int before = 0, tot = 0;
+      for (int q = 0; q < nw; ++q) { if (q < w) before += wtot[q]; tot += wtot[q]; }
+      const int dst = s_H + before + incl - cnt;
+      for (int u = 0; u < cnt; ++u)
+        if (dst + u < cap) s[dst + u] = __ldg(mp + a + u) - rp;
+      __syncthreads();
+      if (threadIdx.x == 0) s_H += tot;
+      __syncthreads();
+    }
+  }
+  const int H = s_H;
+  if (H > cap) {
+    if (threadIdx.x == 0) {
+      const int k = atomicAdd(huge_count, 1);
+      huge_list[k] = r;
+      huge_h[k] = H;
+    }
+    return;
+  }
+  int P = 1;
+  while (P < H) P <<= 1;
+  for (int i = H + threadIdx.x; i < P; i += blockDim.x) s[i] = 0x7fffffff;
+  __syncthreads();
+  for (int k = 2; k <= P; k <<= 1)
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      for (int i = threadIdx.x; i < P; i += blockDim.x) {
+        const int ixj = i ^ j;
+        if (ixj > i) {
+          const int32_t x = s[i], y = s[ixj];
+          if ((x > y) == ((i & k) == 0)) { s[i] = y; s[ixj] = x; }
+        }
+      }
+      __syncthreads();
+    }
+  // de-duplicate in chunks of blockDim, appending in order
+  const unsigned lt = (1u << lane) - 1u;
+  int U = 0;
+  for (int t0 = 0; t0 < H; t0 += blockDim.x) {
+    const int t = t0 + threadIdx.x;
+    const int32_t v = t < H ? s[t] : 0;
+    const int32_t prev = t == 0 ? -I : (t < H ? s[t - 1] : 0);
+    const bool keep = t < H && v > prev;
+    const unsigned m = __ballot_sync(0xffffffffu, keep);
+    if (lane == 0) wtot[w] = __popc(m);
+    __syncthreads();
+    int before = 0, tot = 0;
+    for (int q = 0; q < nw; ++q) { if (q < w) before += wtot[q]; tot += wtot[q]; }
+    if (keep) s[U + before + __popc(m & lt)] = v;
+    U += tot;
+    __syncthreads();
+  }
+  __shared__ unsigned long long s_base;
+  if (threadIdx.x == 0) s_base = U ? atomicAdd(&go.counters[7], (unsigned long long)U) : 0ull;
+  __syncthreads();
+  const unsigned long long base = s_base;
+  if ((int64_t)(base + U) > go.cap) {
+    if (threadIdx.x == 0) atomicExch(&go.counters[8], 1ull);
+    return;
+  }
+  for (int k = threadIdx.x; k < U; k += blockDim.x) {
+    go.fr[base + k] = r;
+    go.fd[base + k] = s[k];
+  }
+}
+
+void upload_gather_seeds(const SeedSet& seeds, cudaStream_t st) {
+  cudaMemcpyToSymbolAsync(c_gseeds, &seeds, sizeof(SeedSet), 0, cudaMemcpyHostToDevice, st);
+}
+
+void launch_gather_fused(const ReadsDev& rd, const IndexView& ix, int I, const GatherOut& go, cudaStream_t st) {
+  if (rd.n <= 0) return;
+  int64_t blocks = (rd.n + kGWarps - 1) / kGWarps;
+  if (blocks > 148 * 16) blocks = 148 * 16;
+  gather_fused_kernel<<<(unsigned)blocks, kGWarps * 32, 0, st>>>(rd, ix, I, go);
+}
+
+void launch_gather_block(const ReadsDev& rd, const IndexView& ix, int I, const int32_t* list, int nlist,
+                         const GatherOut& go, int32_t* gbuf, int gcap, int32_t* huge_list, int32_t* huge_h,
+                         int32_t* huge_count, cudaStream_t st) {
+  if (nlist <= 0) return;
+  const int smem_cap = kBlockGatherCap;
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(gather_block_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_cap * 4);
+    attr = true;
+  }
+  if (gbuf)
+    gather_block_kernel<<<nlist, 1024, 0, st>>>(rd, ix, I, list, go, gcap, gbuf, huge_list, huge_h, huge_count);
+  else
+    gather_block_kernel<<<nlist, 1024, smem_cap * 4, st>>>(rd, ix, I, list, go, smem_cap, nullptr, huge_list,
+                                                              huge_h, huge_count);
+}
+
+}  // namespace sg

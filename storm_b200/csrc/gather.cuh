@@ -1,0 +1,27 @@
+// gather.cuh -- fused hit gather (gather.cu).
+#pragma once
+
+#include "map_kernels.cuh"
+
+namespace sg {
+
+struct GatherOut {
+  int32_t* fr;                   // flat list: read of each candidate
+  int32_t* fd;                   // flat list: diagonal of each candidate
+  int64_t cap;                   // capacity of fr / fd
+  unsigned long long* counters;  // [3] key lookups, [4] index positions, [7] flat cursor, [8] overflow
+  int32_t* big_list;             // reads with more positions than a warp holds
+  int32_t* big_count;
+};
+
+constexpr int kBlockGatherCap = 32768;
+
+void upload_gather_seeds(const SeedSet& seeds, cudaStream_t st);
+void launch_gather_fused(const ReadsDev& rd, const IndexView& ix, int I, const GatherOut& go, cudaStream_t st);
+// one block per listed read; gbuf == nullptr: shared memory (kBlockGatherCap positions),
+// reads beyond it are appended to (huge_list, huge_h); else the global buffer gbuf of gcap.
+void launch_gather_block(const ReadsDev& rd, const IndexView& ix, int I, const int32_t* list, int nlist,
+                         const GatherOut& go, int32_t* gbuf, int gcap, int32_t* huge_list, int32_t* huge_h,
+                         int32_t* huge_count, cudaStream_t st);
+
+}  // namespace sg

@@ -1,15 +1,12 @@
 // map_kernels.cu -- the kernels of one mapping pass (one reference sequence x one strand).
 //
-//  gather_count / gather_expand / segment_unique   hit gather (run.c:577-698, index.c:212-241)
-//  filter                                           banded u8 SW filter (alignment_simd.c)
+//  (hit gather: gather.cu; banded filter: sw_filter.cu)
 //  align                                            banded DP + traceback (alignment.c:488-734)
 //  replay                                           per-read top-4 update (run.c:664-691,
 //                                                   hit_map.c:50-144)
 #include "map_kernels.cuh"
 
 namespace sg {
-
-__constant__ SeedSet c_seeds;
 
 // ------------------------------------------------------------------------------ reads
 
@@ -69,242 +66,6 @@ void launch_init_results(int64_t n, stormgpu_hit* hits, uint8_t* mapped, uint8_t
   if (n <= 0) return;
   init_results_kernel<<<(unsigned)((n * 4 + 255) / 256), 256, 0, st>>>(n, hits, mapped, tb, tbs);
 }
-
-// ------------------------------------------------------------------------------ gather
-
-// Seed key at read position rp; codes beyond the read's end read as 0 (seed.c:203-213).
-__device__ __forceinline__ uint32_t read_key(const SeedDev& s, const uint8_t* rd, int L, int rp) {
-  uint32_t key = 0;
-  for (int c = 0; c < s.n_care; ++c) {
-    int p = rp + s.care[c];
-    key = (key << 2) | (uint32_t)(p < L ? code_at(rd, p) : 0);
-  }
-  return key;
-}
-
-__device__ __forceinline__ int seed_npos(const SeedDev& s, int L) {
-  return s.n_positions ? s.n_positions : (L - s.span + 1 > 0 ? L - s.span + 1 : 0);
-}
-
-__global__ void gather_count_kernel(ReadsDev rd, IndexView ix, int32_t* __restrict__ hits,
-                                    unsigned long long* __restrict__ counters) {
-  const int lane = threadIdx.x & 31;
-  const int64_t nwarps = (int64_t)gridDim.x * (blockDim.x >> 5);
-  unsigned long long lookups = 0, positions = 0;
-  for (int64_t r = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); r < rd.n; r += nwarps) {
-    const int L = rd.lengths[r];
-    const uint8_t* read = rd.codes + r * rd.cstride;
-    long long tot = 0;
-    for (int si = 0; si < c_seeds.n; ++si) {
-      const SeedDev& s = c_seeds.s[si];
-      const int np = seed_npos(s, L);
-      for (int t = lane; t < np; t += 32) {
-        int rp = s.n_positions ? s.positions[t] : t;
-        if (rp < 0 || rp >= L) continue;
-        uint32_t key = read_key(s, read, L, rp);
-        int a = __ldg(ix.first[si] + key), b = __ldg(ix.first[si] + key + 1);
-        tot += b - a;
-        lookups++;
-      }
-    }
-    for (int o = 16; o > 0; o >>= 1) tot += __shfl_xor_sync(0xffffffffu, tot, o);
-    if (lane == 0) hits[r] = tot > 0x7fffffffLL ? 0x7fffffff : (int32_t)tot;
-    positions += (unsigned long long)tot;
-  }
-  for (int o = 16; o > 0; o >>= 1) lookups += __shfl_xor_sync(0xffffffffu, lookups, o);
-  if (lane == 0) {
-    atomicAdd(&counters[3], lookups);
-    atomicAdd(&counters[4], positions);
-  }
-}
-
-void launch_gather_count(const ReadsDev& r, const SeedSet& seeds, const IndexView& ix,
-                         int32_t* hits, unsigned long long* counters, cudaStream_t st) {
-  cudaMemcpyToSymbolAsync(c_seeds, &seeds, sizeof(SeedSet), 0, cudaMemcpyHostToDevice, st);
-  if (r.n <= 0) return;
-  int64_t blocks = (r.n + 7) / 8;
-  if (blocks > 148 * 64) blocks = 148 * 64;
-  gather_count_kernel<<<(unsigned)blocks, 256, 0, st>>>(r, ix, hits, counters);
-}
-
-__global__ void gather_expand_kernel(ReadsDev rd, IndexView ix, const int64_t* __restrict__ hoff,
-                                     int32_t* __restrict__ cand) {
-  const int lane = threadIdx.x & 31;
-  const int64_t nwarps = (int64_t)gridDim.x * (blockDim.x >> 5);
-  for (int64_t r = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); r < rd.n; r += nwarps) {
-    const int L = rd.lengths[r];
-    const uint8_t* read = rd.codes + r * rd.cstride;
-    int32_t* out = cand + hoff[r];
-    int run = 0;
-    for (int si = 0; si < c_seeds.n; ++si) {
-      const SeedDev& s = c_seeds.s[si];
-      const int np = seed_npos(s, L);
-      const int32_t* mp = ix.map[si];
-      for (int t0 = 0; t0 < np; t0 += 32) {
-        int t = t0 + lane, a = 0, cnt = 0, rp = 0;
-        if (t < np) {
-          rp = s.n_positions ? s.positions[t] : t;
-          if (rp >= 0 && rp < L) {
-            uint32_t key = read_key(s, read, L, rp);
-            a = __ldg(ix.first[si] + key);
-            cnt = __ldg(ix.first[si] + key + 1) - a;
-          }
-        }
-        int incl = warp_incl_scan(cnt);
-        int dst = run + incl - cnt;
-        run += __shfl_sync(0xffffffffu, incl, 31);
-        unsigned m = __ballot_sync(0xffffffffu, cnt > 0);
-        while (m) {
-          int j = __ffs(m) - 1;
-          m &= m - 1;
-          int sj = __shfl_sync(0xffffffffu, a, j), cj = __shfl_sync(0xffffffffu, cnt, j);
-          int dj = __shfl_sync(0xffffffffu, dst, j), rj = __shfl_sync(0xffffffffu, rp, j);
-          for (int u = lane; u < cj; u += 32) out[dj + u] = __ldg(mp + sj + u) - rj;
-        }
-      }
-    }
-  }
-}
-
-void launch_gather_expand(const ReadsDev& r, const SeedSet& seeds, const IndexView& ix,
-                          const int64_t* hoff, int32_t* cand, cudaStream_t st) {
-  (void)seeds;
-  if (r.n <= 0) return;
-  int64_t blocks = (r.n + 7) / 8;
-  if (blocks > 148 * 64) blocks = 148 * 64;
-  gather_expand_kernel<<<(unsigned)blocks, 256, 0, st>>>(r, ix, hoff, cand);
-}
-
-// Sorted, de-duplicated diagonals with the accept rule of run.c:617/648/697: a diagonal is
-// kept iff it is strictly greater than the previous one in sorted order, the "previous" of the
-// first being -I.
-constexpr int kWarpSortMax = 1024;
-
-__device__ __forceinline__ void warp_bitonic(int32_t* s, int P) {
-  const int lane = threadIdx.x & 31;
-  for (int k = 2; k <= P; k <<= 1)
-    for (int j = k >> 1; j > 0; j >>= 1) {
-      for (int i = lane; i < P; i += 32) {
-        int ixj = i ^ j;
-        if (ixj > i) {
-          int32_t a = s[i], b = s[ixj];
-          bool up = (i & k) == 0;
-          if ((a > b) == up) { s[i] = b; s[ixj] = a; }
-        }
-      }
-      __syncwarp();
-    }
-}
-
-__global__ void segment_unique_kernel(int64_t n, const int32_t* __restrict__ hits,
-                                      const int64_t* __restrict__ hoff, int32_t* __restrict__ cand,
-                                      int32_t* __restrict__ ucount, int I, int32_t* __restrict__ big_list,
-                                      int32_t* __restrict__ big_count) {
-  __shared__ int32_t sm[8][kWarpSortMax];
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  int32_t* s = sm[w];
-  const int64_t nwarps = (int64_t)gridDim.x * (blockDim.x >> 5);
-  const unsigned lt = (1u << lane) - 1u;
-  for (int64_t r = (int64_t)blockIdx.x * (blockDim.x >> 5) + w; r < n; r += nwarps) {
-    const int H = hits[r];
-    if (H > kWarpSortMax) {
-      if (lane == 0) { int k = atomicAdd(big_count, 1); big_list[k] = (int32_t)r; }
-      continue;
-    }
-    int32_t* seg = cand + hoff[r];
-    int P = 1;
-    while (P < H) P <<= 1;
-    for (int i = lane; i < P; i += 32) s[i] = i < H ? seg[i] : 0x7fffffff;
-    __syncwarp();
-    warp_bitonic(s, P);
-    int out = 0;
-    for (int t0 = 0; t0 < H; t0 += 32) {
-      int t = t0 + lane;
-      int32_t v = t < H ? s[t] : 0;
-      int32_t prev = t == 0 ? -I : (t < H ? s[t - 1] : 0);
-      bool keep = t < H && v > prev;
-      unsigned m = __ballot_sync(0xffffffffu, keep);
-      if (keep) seg[out + __popc(m & lt)] = v;
-      out += __popc(m);
-    }
-    if (lane == 0) ucount[r] = out;
-    __syncwarp();
-  }
-}
-
-void launch_segment_unique(const ReadsDev& r, const int32_t* hits, const int64_t* hoff, int32_t* cand,
-                           int32_t* ucount, int I, int32_t* big_list, int32_t* big_count,
-                           cudaStream_t st) {
-  if (r.n <= 0) return;
-  int64_t blocks = (r.n + 7) / 8;
-  if (blocks > 148 * 32) blocks = 148 * 32;
-  segment_unique_kernel<<<(unsigned)blocks, 256, 0, st>>>(r.n, hits, hoff, cand, ucount, I, big_list, big_count);
-}
-
-// One block per long segment: bitonic sort in shared memory (<= 32768 elements) or, beyond
-// that, in the global scratch `tmp` (padded to a power of two).
-__global__ void segment_unique_big_kernel(const int32_t* __restrict__ big_list, const int32_t* __restrict__ hits,
-                                          const int64_t* __restrict__ hoff, int32_t* __restrict__ cand,
-                                          int32_t* __restrict__ ucount, int I, int32_t* __restrict__ tmp,
-                                          int smem_elems) {
-  extern __shared__ int32_t dsm[];
-  __shared__ int wsum[32];
-  const int64_t r = big_list[blockIdx.x];
-  const int H = hits[r];
-  int32_t* seg = cand + hoff[r];
-  int P = 1;
-  while (P < H) P <<= 1;
-  int32_t* s = (P <= smem_elems) ? dsm : tmp;
-  for (int i = threadIdx.x; i < P; i += blockDim.x) s[i] = i < H ? seg[i] : 0x7fffffff;
-  __syncthreads();
-  for (int k = 2; k <= P; k <<= 1)
-    for (int j = k >> 1; j > 0; j >>= 1) {
-      for (int i = threadIdx.x; i < P; i += blockDim.x) {
-        int ixj = i ^ j;
-        if (ixj > i) {
-          int32_t a = s[i], b = s[ixj];
-          bool up = (i & k) == 0;
-          if ((a > b) == up) { s[i] = b; s[ixj] = a; }
-        }
-      }
-      __syncthreads();
-    }
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  const unsigned lt = (1u << lane) - 1u;
-  int out = 0;
-  for (int t0 = 0; t0 < H; t0 += blockDim.x) {
-    int t = t0 + threadIdx.x;
-    int32_t v = t < H ? s[t] : 0;
-    int32_t prev = t == 0 ? -I : (t < H ? s[t - 1] : 0);
-    bool keep = t < H && v > prev;
-    unsigned m = __ballot_sync(0xffffffffu, keep);
-    if (lane == 0) wsum[w] = __popc(m);
-    __syncthreads();
-    int before = 0, tot = 0;
-    for (int q = 0; q < nw; ++q) { if (q < w) before += wsum[q]; tot += wsum[q]; }
-    if (keep) seg[out + before + __popc(m & lt)] = v;
-    out += tot;
-    __syncthreads();
-  }
-  if (threadIdx.x == 0) ucount[r] = out;
-}
-
-void launch_segment_unique_big(const int32_t* big_list, int nbig, const int32_t* hits,
-                               const int64_t* hoff, int32_t* cand, int32_t* ucount, int I,
-                               int32_t* tmp, int64_t tmp_elems, cudaStream_t st) {
-  if (nbig <= 0) return;
-  const int smem_elems = 32768;
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(segment_unique_big_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         smem_elems * 4);
-    attr = true;
-  }
-  (void)tmp_elems;
-  segment_unique_big_kernel<<<nbig, 1024, smem_elems * 4, st>>>(big_list, hits, hoff, cand, ucount, I, tmp, smem_elems);
-}
-
-// ------------------------------------------------------------------------------ filter
 
 // ------------------------------------------------------------------------------ align
 

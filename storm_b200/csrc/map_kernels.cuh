@@ -33,12 +33,6 @@ struct IndexView {
 };
 
 struct PassBuffers {
-  // gather
-  int32_t* hits;        // per read: number of index positions (G1)
-  int64_t* hoff;        // per read: offset in cand (scan of hits)
-  int32_t* ucount;      // per read: unique candidate diagonals (G3)
-  int32_t* cand;        // candidate diagonals, per-read segments
-  int64_t cand_cap;
   // filter -> flat list of passing candidates
   int32_t* pstart;      // per read: first slot
   int32_t* pcount;      // per read: number of passing candidates
@@ -55,24 +49,12 @@ struct PassBuffers {
   int64_t tbs;
   uint32_t* a_scratch;  // direction bits, see align kernel
   int64_t scratch_words;
-  int32_t* big_list;    // reads whose segment is too long for the warp sort
-  int32_t* big_count;
 };
 
 void launch_reverse_reads(const ReadsDev& in, const uint8_t* first_levels, int colour,
                           uint8_t* rcodes, uint8_t* rlevels, cudaStream_t st);
 void launch_init_results(int64_t n, stormgpu_hit* hits, uint8_t* mapped, uint8_t* tb, int64_t tbs,
                          cudaStream_t st);
-void launch_gather_count(const ReadsDev& r, const SeedSet& seeds, const IndexView& ix,
-                         int32_t* hits, unsigned long long* counters, cudaStream_t st);
-void launch_gather_expand(const ReadsDev& r, const SeedSet& seeds, const IndexView& ix,
-                          const int64_t* hoff, int32_t* cand, cudaStream_t st);
-void launch_segment_unique(const ReadsDev& r, const int32_t* hits, const int64_t* hoff, int32_t* cand,
-                           int32_t* ucount, int I, int32_t* big_list, int32_t* big_count,
-                           cudaStream_t st);
-void launch_segment_unique_big(const int32_t* big_list, int nbig, const int32_t* hits,
-                               const int64_t* hoff, int32_t* cand, int32_t* ucount, int I,
-                               int32_t* tmp, int64_t tmp_elems, cudaStream_t st);
 void launch_align(const ReadsDev& r, const ScoreParams& sp, const uint8_t* genome,
                   const uint8_t* mask, int64_t slot0, int64_t nslots, PassBuffers& pb,
                   cudaStream_t st);

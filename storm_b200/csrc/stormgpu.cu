@@ -13,6 +13,7 @@
 #include "map_kernels.cuh"
 #include "scan.cuh"
 #include "sw_filter.cuh"
+#include "gather.cuh"
 
 static thread_local char g_err[1024];
 
@@ -154,8 +155,8 @@ struct stormgpu_ctx {
   DevBuf<stormgpu_hit> hits;
   DevBuf<uint8_t> tb, mapped;
   // pass buffers
-  DevBuf<int32_t> hitsc, ucount, cand, pstart, pcount, p_read, p_diag, big_list, big_count;
-  DevBuf<int64_t> hoff, scan_tmp64, uoff, foff;
+  DevBuf<int32_t> pstart, pcount, p_read, p_diag, big_list, big_count, huge_list, huge_h;
+  DevBuf<int64_t> scan_tmp64, foff;
   DevBuf<int32_t> fr, fd;
   DevBuf<uint8_t> flag, rexp;
   DevBuf<int32_t> a_score, a_bound, a_tblen, big_tmp;
@@ -215,12 +216,13 @@ extern "C" void stormgpu_close(stormgpu_ctx* c) {
   }
   c->rcodes.release(); c->rlevels.release(); c->fcodes.release(); c->flevels.release();
   c->first_levels.release(); c->lengths.release(); c->hits.release(); c->tb.release();
-  c->mapped.release(); c->hitsc.release(); c->ucount.release(); c->cand.release();
+  c->mapped.release();
   c->pstart.release(); c->pcount.release(); c->p_read.release(); c->p_diag.release();
-  c->big_list.release(); c->big_count.release(); c->hoff.release(); c->scan_tmp64.release();
+  c->big_list.release(); c->big_count.release(); c->huge_list.release(); c->huge_h.release();
+  c->scan_tmp64.release();
   c->a_score.release(); c->a_bound.release(); c->a_tblen.release(); c->big_tmp.release();
   c->a_pos.release(); c->a_tb.release(); c->scratch.release(); c->counters.release();
-  c->uoff.release(); c->foff.release(); c->fr.release(); c->fd.release(); c->flag.release();
+  c->foff.release(); c->fr.release(); c->fd.release(); c->flag.release();
   c->rexp.release();
   for (auto& e : c->ev) cudaEventDestroy(e);
   cudaStreamDestroy(c->st);
@@ -319,10 +321,12 @@ static int map_device_impl(stormgpu_ctx* c, const stormgpu_reads* reads, stormgp
     rev.codes = c->rcodes.p;
     rev.levels = reads->levels ? c->rlevels.p : nullptr;
   }
-  if (c->hitsc.grow(n) || c->ucount.grow(n) || c->pstart.grow(n) || c->pcount.grow(n) ||
-      c->hoff.grow(n + 1) || c->uoff.grow(n + 1) || c->scan_tmp64.grow(scan_tmp_elems(n) + 8) || c->big_list.grow(n) ||
-      c->big_count.grow(1) || c->counters.grow(8))
+  if (c->pstart.grow(n) || c->pcount.grow(n) || c->scan_tmp64.grow(scan_tmp_elems(n) + 8) ||
+      c->big_list.grow(n) || c->huge_list.grow(n) || c->huge_h.grow(n) || c->big_count.grow(2) ||
+      c->counters.grow(16) || c->fr.grow(std::max<int64_t>(n * 64, 1 << 20)) ||
+      c->fd.grow(std::max<int64_t>(n * 64, 1 << 20)))
     return STORMGPU_ENOMEM;
+  upload_gather_seeds(c->seeds, st);
   const int BW = 2 * sp.I + 1;
   const int wpr = (2 * BW + 31) / 32 + (sp.colour ? (BW + 31) / 32 : 0);
   const int64_t tbs = ((maxL + sp.I + 1) / 2 + 7) & ~7LL;
@@ -336,63 +340,52 @@ static int map_device_impl(stormgpu_ctx* c, const stormgpu_reads* reads, stormgp
     for (int strand = 0; strand < 2; ++strand) {
       if (!(c->p.senses & (1 << strand))) continue;
       const ReadsDev& rd = strand ? rev : fwd;
-      SG_CUDA(cudaMemsetAsync(c->counters.p, 0, sizeof(unsigned long long) * 8, st));
-      SG_CUDA(cudaEventRecord(c->ev[0], st));
-      launch_gather_count(rd, c->seeds, ix, c->hitsc.p, c->counters.p, st);
-      exclusive_scan<int32_t, int64_t>(c->hitsc.p, c->hoff.p, n, c->hoff.p + n, c->scan_tmp64.p, st);
-      launches += 4;
-      int64_t htot = 0;
-      SG_CUDA(cudaMemcpyAsync(&htot, c->hoff.p + n, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
-      SG_CUDA(cudaStreamSynchronize(st));
-      if (c->cand.grow(std::max<int64_t>(htot, 1))) return STORMGPU_ENOMEM;
-      launch_gather_expand(rd, c->seeds, ix, c->hoff.p, c->cand.p, st);
-      SG_CUDA(cudaMemsetAsync(c->big_count.p, 0, sizeof(int32_t), st));
-      launch_segment_unique(rd, c->hitsc.p, c->hoff.p, c->cand.p, c->ucount.p, sp.I, c->big_list.p,
-                            c->big_count.p, st);
-      launches += 2;
-      int32_t nbig = 0;
-      SG_CUDA(cudaMemcpyAsync(&nbig, c->big_count.p, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
-      SG_CUDA(cudaStreamSynchronize(st));
-      if (nbig > 0) {
-        std::vector<int32_t> bl(nbig), bh(nbig);
-        SG_CUDA(cudaMemcpy(bl.data(), c->big_list.p, sizeof(int32_t) * nbig, cudaMemcpyDeviceToHost));
-        std::vector<int32_t> medium, huge;
-        for (int k = 0; k < nbig; ++k) {
-          int32_t h;
-          SG_CUDA(cudaMemcpy(&h, c->hitsc.p + bl[k], sizeof(int32_t), cudaMemcpyDeviceToHost));
-          (h <= 32768 ? medium : huge).push_back(bl[k]);
-          bh[k] = h;
-        }
-        if (!medium.empty()) {
-          SG_CUDA(cudaMemcpyAsync(c->big_list.p, medium.data(), sizeof(int32_t) * medium.size(), cudaMemcpyHostToDevice, st));
-          launch_segment_unique_big(c->big_list.p, (int)medium.size(), c->hitsc.p, c->hoff.p, c->cand.p,
-                                    c->ucount.p, sp.I, nullptr, 0, st);
-          launches++;
-        }
-        for (size_t k = 0; k < huge.size(); ++k) {
-          int32_t h;
-          SG_CUDA(cudaMemcpy(&h, c->hitsc.p + huge[k], sizeof(int32_t), cudaMemcpyDeviceToHost));
-          int64_t P = 1;
-          while (P < h) P <<= 1;
-          if (c->big_tmp.grow(P)) return STORMGPU_ENOMEM;
-          SG_CUDA(cudaMemcpyAsync(c->big_list.p + n - 1, &huge[k], sizeof(int32_t), cudaMemcpyHostToDevice, st));
-          launch_segment_unique_big(c->big_list.p + n - 1, 1, c->hitsc.p, c->hoff.p, c->cand.p,
-                                    c->ucount.p, sp.I, c->big_tmp.p, P, st);
-          SG_CUDA(cudaStreamSynchronize(st));
-          launches++;
-        }
-      }
-      // flat candidate list (read, diagonal), reads in order, diagonals ascending per read
-      exclusive_scan<int32_t, int64_t>(c->ucount.p, c->uoff.p, n, c->uoff.p + n, c->scan_tmp64.p, st);
       int64_t utot = 0;
-      SG_CUDA(cudaMemcpyAsync(&utot, c->uoff.p + n, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
-      SG_CUDA(cudaStreamSynchronize(st));
-      if (c->fr.grow(std::max<int64_t>(utot, 1)) || c->fd.grow(std::max<int64_t>(utot, 1)) ||
-          c->flag.grow(std::max<int64_t>(utot, 1)) || c->foff.grow(utot + 1) ||
+      SG_CUDA(cudaEventRecord(c->ev[0], st));
+      for (int attempt = 0;; ++attempt) {
+        // fused hit gather: sorted, de-duplicated diagonals of every read, appended to the flat
+        // candidate list (fr, fd); reads with many index positions go to the block kernel
+        SG_CUDA(cudaMemsetAsync(c->counters.p, 0, sizeof(unsigned long long) * 16, st));
+        SG_CUDA(cudaMemsetAsync(c->big_count.p, 0, sizeof(int32_t) * 2, st));
+        GatherOut go;
+        go.fr = c->fr.p; go.fd = c->fd.p; go.cap = c->fr.cap; go.counters = c->counters.p;
+        go.big_list = c->big_list.p; go.big_count = c->big_count.p;
+        launch_gather_fused(rd, ix, sp.I, go, st);
+        launches++;
+        int32_t nbig[2] = {0, 0};
+        SG_CUDA(cudaMemcpyAsync(nbig, c->big_count.p, sizeof(nbig), cudaMemcpyDeviceToHost, st));
+        SG_CUDA(cudaStreamSynchronize(st));
+        if (nbig[0] > 0) {
+          launch_gather_block(rd, ix, sp.I, c->big_list.p, nbig[0], go, nullptr, 0, c->huge_list.p, c->huge_h.p,
+                              c->big_count.p + 1, st);
+          launches++;
+          SG_CUDA(cudaMemcpyAsync(nbig, c->big_count.p, sizeof(nbig), cudaMemcpyDeviceToHost, st));
+          SG_CUDA(cudaStreamSynchronize(st));
+          if (nbig[1] > 0) {
+            std::vector<int32_t> hl(nbig[1]), hh(nbig[1]);
+            SG_CUDA(cudaMemcpy(hl.data(), c->huge_list.p, sizeof(int32_t) * nbig[1], cudaMemcpyDeviceToHost));
+            SG_CUDA(cudaMemcpy(hh.data(), c->huge_h.p, sizeof(int32_t) * nbig[1], cudaMemcpyDeviceToHost));
+            for (int k = 0; k < nbig[1]; ++k) {
+              int64_t P = 1;
+              while (P < hh[k]) P <<= 1;
+              if (c->big_tmp.grow(P)) return STORMGPU_ENOMEM;
+              launch_gather_block(rd, ix, sp.I, c->huge_list.p + k, 1, go, c->big_tmp.p, (int)P, c->huge_list.p,
+                                  c->huge_h.p, c->big_count.p + 1, st);
+              launches++;
+            }
+          }
+        }
+        unsigned long long g[9];
+        SG_CUDA(cudaMemcpyAsync(g, c->counters.p, sizeof(g), cudaMemcpyDeviceToHost, st));
+        SG_CUDA(cudaStreamSynchronize(st));
+        utot = (int64_t)g[7];
+        if (!g[8]) break;
+        if (attempt > 2) { sg_set_error("internal: candidate list overflow"); return STORMGPU_EINVAL; }
+        if (c->fr.grow(utot + utot / 4 + 1024) || c->fd.grow(utot + utot / 4 + 1024)) return STORMGPU_ENOMEM;
+      }
+      if (c->flag.grow(std::max<int64_t>(utot, 1)) || c->foff.grow(utot + 1) ||
           c->scan_tmp64.grow(scan_tmp_elems(std::max<int64_t>(utot, n)) + 8))
         return STORMGPU_ENOMEM;
-      launch_flatten(n, c->hoff.p, c->cand.p, c->ucount.p, c->uoff.p, c->fr.p, c->fd.p, st);
-      launches += 5;
       SG_CUDA(cudaEventRecord(c->ev[1], st));
       FilterJob job;
       job.n = utot; job.fr = c->fr.p; job.fd = c->fd.p; job.flag = c->flag.p; job.codes = rd.codes;
@@ -420,8 +413,7 @@ static int map_device_impl(stormgpu_ctx* c, const stormgpu_reads* reads, stormgp
       S.filter_passed += npass;
       PassBuffers pb;
       memset(&pb, 0, sizeof(pb));
-      pb.hits = c->hitsc.p; pb.hoff = c->hoff.p; pb.ucount = c->ucount.p; pb.cand = c->cand.p;
-      pb.cand_cap = c->cand.cap; pb.pstart = c->pstart.p; pb.pcount = c->pcount.p;
+      pb.pstart = c->pstart.p; pb.pcount = c->pcount.p;
       pb.counters = c->counters.p;
       SG_CUDA(cudaMemsetAsync(c->pcount.p, 0, sizeof(int32_t) * n, st));
       if (npass > 0) {

@@ -142,32 +142,7 @@ void launch_filter_flat_job(const FilterJob& job, const ScoreParams& sp, bool dp
   }
 }
 
-// ------------------------------------------------------------------ flat lists, compaction
-
-// per read: its unique diagonals (segment at hoff[r], ucount[r] long) -> flat arrays at uoff[r]
-__global__ void flatten_kernel(int64_t n, const int64_t* __restrict__ hoff, const int32_t* __restrict__ cand,
-                               const int32_t* __restrict__ ucount, const int64_t* __restrict__ uoff,
-                               int32_t* __restrict__ fr, int32_t* __restrict__ fd) {
-  const int lane = threadIdx.x & 31;
-  const int64_t nwarps = (int64_t)gridDim.x * (blockDim.x >> 5);
-  for (int64_t r = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); r < n; r += nwarps) {
-    const int U = ucount[r];
-    const int32_t* src = cand + hoff[r];
-    const int64_t o = uoff[r];
-    for (int k = lane; k < U; k += 32) {
-      fr[o + k] = (int32_t)r;
-      fd[o + k] = src[k];
-    }
-  }
-}
-
-void launch_flatten(int64_t n, const int64_t* hoff, const int32_t* cand, const int32_t* ucount,
-                    const int64_t* uoff, int32_t* fr, int32_t* fd, cudaStream_t st) {
-  if (n <= 0) return;
-  int64_t blocks = (n + 7) / 8;
-  if (blocks > 148 * 32) blocks = 148 * 32;
-  flatten_kernel<<<(unsigned)blocks, 256, 0, st>>>(n, hoff, cand, ucount, uoff, fr, fd);
-}
+// ------------------------------------------------------------------ compaction of passing candidates
 
 // passing candidates, in order, into (p_read, p_diag); pcount/pstart per read
 __global__ void compact_kernel(int64_t n, const uint8_t* __restrict__ flag, const int64_t* __restrict__ off,

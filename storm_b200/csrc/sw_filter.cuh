@@ -29,8 +29,6 @@ void launch_expand_reads(const ReadsDev& rd, uint8_t* rexp, int64_t rstride, cud
 
 bool filter_dpx_ok(const ScoreParams& sp, int max_len);
 void launch_filter_flat_job(const FilterJob& job, const ScoreParams& sp, bool dpx, cudaStream_t st);
-void launch_flatten(int64_t n, const int64_t* hoff, const int32_t* cand, const int32_t* ucount,
-                    const int64_t* uoff, int32_t* fr, int32_t* fd, cudaStream_t st);
 void launch_compact(int64_t n, const uint8_t* flag, const int64_t* off, const int32_t* fr, const int32_t* fd,
                     int32_t* p_read, int32_t* p_diag, cudaStream_t st);
 void launch_slot_bounds(int64_t npass, const int32_t* p_read, int32_t* pstart, int32_t* pcount, cudaStream_t st);
