@@ -215,6 +215,7 @@ def main():
     ap.add_argument("--cfg", type=int, default=1)
     ap.add_argument("--scale", type=float, default=1.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--reads", type=int, default=0, help="map only the first N reads of the workload (profiling)")
     a = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -247,6 +248,8 @@ def main():
     seeds = seeds or DEFAULT_SEEDS[colour]
     prm = api.params(colour=colour, device=local, **prm_d)
     t0 = time.perf_counter()
+    if a.reads:
+        reads_path = sample_fastq(reads_path, d, a.reads)
     reads = host.ReadSet(reads_path, colour)
     reference = host.Reference(ref_path, colour)
     log("rank %d: loaded %d reads, %d sequence(s) in %.1f s" % (rank, reads.n, reference.n, time.perf_counter() - t0))

@@ -87,18 +87,110 @@ __device__ __forceinline__ void warp_emit(int32_t* s, int H, int I, int r, const
   }
 }
 
+// Bitonic sort of 32*E values held E per lane (value k of lane l is element k*32 + l):
+// partners 32 or more apart are in the same lane (register compare-exchange), closer ones are
+// exchanged with __shfl_xor_sync.
+template <int E>
+__device__ __forceinline__ void reg_bitonic(int32_t (&v)[E]) {
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int kk = 2; kk <= 32 * E; kk <<= 1) {
+#pragma unroll
+    for (int j = kk >> 1; j > 0; j >>= 1) {
+      if (j >= 32) {
+#pragma unroll
+        for (int k = 0; k < E; ++k) {
+          const int k2 = k ^ (j >> 5);
+          if (k2 > k) {
+            const bool up = ((k * 32 + lane) & kk) == 0;
+            const int32_t a = v[k], b = v[k2];
+            const bool sw = (a > b) == up;
+            v[k] = sw ? b : a;
+            v[k2] = sw ? a : b;
+          }
+        }
+      } else {
+#pragma unroll
+        for (int k = 0; k < E; ++k) {
+          const int32_t o = __shfl_xor_sync(0xffffffffu, v[k], j);
+          const bool up = ((k * 32 + lane) & kk) == 0;
+          const bool lower = (lane & j) == 0;
+          v[k] = (lower == up) ? min(v[k], o) : max(v[k], o);
+        }
+      }
+    }
+  }
+}
+
+// accepted diagonals of the sorted register array (first H valid) -> flat list
+template <int E>
+__device__ __forceinline__ void reg_emit(const int32_t (&v)[E], int H, int I, int r, const GatherOut& go) {
+  const int lane = threadIdx.x & 31;
+  const unsigned lt = (1u << lane) - 1u;
+  unsigned m[E];
+  int U = 0;
+#pragma unroll
+  for (int k = 0; k < E; ++k) {
+    const int32_t up = __shfl_up_sync(0xffffffffu, v[k], 1);
+    const int32_t last = __shfl_sync(0xffffffffu, k ? v[k > 0 ? k - 1 : 0] : 0, 31);
+    const int32_t prev = lane ? up : (k ? last : -I);
+    const bool keep = (k * 32 + lane) < H && v[k] > prev;
+    m[k] = __ballot_sync(0xffffffffu, keep);
+    U += __popc(m[k]);
+  }
+  unsigned long long base = 0;
+  if (lane == 0 && U) base = atomicAdd(&go.counters[7], (unsigned long long)U);
+  base = __shfl_sync(0xffffffffu, base, 0);
+  if ((int64_t)(base + U) > go.cap) {
+    if (lane == 0) atomicExch(&go.counters[8], 1ull);
+    return;
+  }
+  int off = 0;
+#pragma unroll
+  for (int k = 0; k < E; ++k) {
+    if ((m[k] >> lane) & 1u) {
+      const int64_t o = (int64_t)base + off + __popc(m[k] & lt);
+      go.fr[o] = r;
+      go.fd[o] = v[k];
+    }
+    off += __popc(m[k]);
+  }
+}
+
+template <int E>
+__device__ __forceinline__ void sort_emit_regs(const int32_t* s, int H, int I, int r, const GatherOut& go) {
+  const int lane = threadIdx.x & 31;
+  int32_t v[E];
+#pragma unroll
+  for (int k = 0; k < E; ++k) {
+    const int i = k * 32 + lane;
+    v[k] = i < H ? s[i] : 0x7fffffff;
+  }
+  reg_bitonic<E>(v);
+  reg_emit<E>(v, H, I, r, go);
+}
+
 constexpr int kWarpCap = 1024;
 constexpr int kGWarps = 8;
+constexpr int kReadBytes = STORMGPU_MAX_READ_LEN / 4 + 16;
 
 __global__ void __launch_bounds__(kGWarps * 32) gather_fused_kernel(ReadsDev rd, IndexView ix, int I, GatherOut go) {
   __shared__ int32_t sm[kGWarps][kWarpCap];
+  __shared__ __align__(16) uint8_t srd[kGWarps][kReadBytes];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   int32_t* s = sm[w];
+  uint8_t* rs = srd[w];
   const int64_t nwarps = (int64_t)gridDim.x * kGWarps;
   unsigned long long lookups = 0, positions = 0;
   for (int64_t r = (int64_t)blockIdx.x * kGWarps + w; r < rd.n; r += nwarps) {
     const int L = rd.lengths[r];
-    const uint8_t* read = rd.codes + r * rd.cstride;
+    {  // the read's packed codes into shared memory
+      const uint8_t* src = rd.codes + r * rd.cstride;
+      const int nb = (L + 3) >> 2;
+      for (int b = lane; b < nb; b += 32) rs[b] = src[b];
+      __syncwarp();
+    }
+    const uint8_t* read = rs;
     int H = 0;
     for (int si = 0; si < c_gseeds.n; ++si) {
       const int np = seed_npos(c_gseeds.s[si], L);
@@ -132,12 +224,18 @@ __global__ void __launch_bounds__(kGWarps * 32) gather_fused_kernel(ReadsDev rd,
       continue;
     }
     __syncwarp();
-    int P = 1;
-    while (P < H) P <<= 1;
-    for (int i = H + lane; i < P; i += 32) s[i] = 0x7fffffff;
-    __syncwarp();
-    warp_bitonic(s, P);
-    warp_emit(s, H, I, (int)r, go);
+    if (H <= 32) sort_emit_regs<1>(s, H, I, (int)r, go);
+    else if (H <= 64) sort_emit_regs<2>(s, H, I, (int)r, go);
+    else if (H <= 128) sort_emit_regs<4>(s, H, I, (int)r, go);
+    else if (H <= 256) sort_emit_regs<8>(s, H, I, (int)r, go);
+    else {
+      int P = 1;
+      while (P < H) P <<= 1;
+      for (int i = H + lane; i < P; i += 32) s[i] = 0x7fffffff;
+      __syncwarp();
+      warp_bitonic(s, P);
+      warp_emit(s, H, I, (int)r, go);
+    }
     __syncwarp();
   }
   for (int o = 16; o > 0; o >>= 1) lookups += __shfl_xor_sync(0xffffffffu, lookups, o);
