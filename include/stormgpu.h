@@ -152,7 +152,7 @@ typedef struct stormgpu_stats {
   int64_t aligned;           /* full alignments computed */
   int64_t seed_lookups;      /* (seed, read position) key lookups */
   int64_t hit_positions;     /* index positions read by the hit gather */
-  int64_t filter_cells;      /* algorithmic filter cells: L * (2*min(i,15)+1) per diagonal */
+  int64_t filter_cells;      /* filter cell updates: W * 2 * (L + W - 1) per candidate, W = 2..16 */
   int64_t align_cells;       /* L * (2*i+1) per full alignment */
   int64_t kernels;           /* kernel launches */
   double  ms_index, ms_gather, ms_filter, ms_align, ms_replay, ms_total;
@@ -191,10 +191,11 @@ int stormgpu_index_one(const char *seed, int32_t stdev_distance, const uint8_t *
                        const int32_t *region_ends, int32_t n_regions, int32_t *first,
                        int32_t *map, int64_t map_capacity, int64_t *map_len);
 
-/* Measurement helper: sustained 32-bit integer add/max lane-operations per second of the
- * device (the instruction mix of the banded filter), used as the integer-pipe roofline.
+/* Measurement helper: the device's rate, in 32-bit lane instructions per second, for the
+ * instruction mix of one step of the packed 16-bit filter recurrence (7.5 instructions per
+ * register of two cells), run register-resident; the roofline denominator of the filter.
  * No counterpart in the reference (it has no GPU). */
-int stormgpu_int_peak(int device, double *ops_per_s, double *ms);
+int stormgpu_filter_peak(int device, double *ops_per_s, double *ms);
 
 #ifdef __cplusplus
 }

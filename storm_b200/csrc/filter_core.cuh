@@ -205,125 +205,230 @@ SG_HD int filter_dpx(const uint8_t* __restrict__ genome, int64_t pos, const uint
 // (4 + c - g) | (12 + c - g) << 4: a prmt selector (no borrow between bytes) that picks the
 // match score when c == g (byte 4 of {lo, hi}) and the mismatch score otherwise, with the
 // sign replicated into the high byte.  Codes enter the band registers with constant-selector
-// prmts from 4-byte stream words: four read codes and four genome codes per block of 4 step
-// pairs.  Pair p of the band covers read positions i = p - W + 1 + k (cell k); blocks whose
-// pairs all have 0 <= i < L for every cell run without the mask.
+// prmts from 4-byte stream words: four read codes and four genome codes per 4 step pairs.
+// Pair p of the band covers read positions i = p - W + 1 + k (cell k); blocks whose pairs all
+// have 0 <= i < L for every cell run without the mask.
+//
+// Split layout: register j of the band holds cells j (low half) and j + H (high half),
+// H = W / 2.  The neighbour of cell k (k - 1 on genome steps, k + 1 on read steps) is then the
+// same half of register j - 1 or j + 1, and shifting a code stream by one cell is a renaming
+// of the registers: logical register j of the read codes is A[(j + ra) mod H] after ra read
+// steps, and of the genome codes B[(j - rb) mod H] after rb genome steps.  Only the seam
+// register (where a half crosses over) needs a prmt, for the neighbour values and for the
+// entering code.  Blocks of BP = max(4, H) step pairs return the rotation to 0, so every
+// index is a constant.
 constexpr uint32_t kFB = 256u;
 constexpr uint32_t kFBB = kFB * 0x10001u;
 
-template <int W, bool ODD, bool MASKED, int T>
-SG_HD void fstep3(uint32_t (&A)[W / 2], uint32_t (&B)[W / 2], uint32_t (&M1)[W / 2], uint32_t (&M2)[W / 2],
-                  uint32_t (&I1)[W / 2], uint32_t& Max, uint32_t rcur, uint32_t gcur, uint32_t TLO,
-                  uint32_t THI, uint32_t CFE, uint32_t CFO, const uint32_t (&mw)[W / 2]) {
-  constexpr int NR = W / 2;
-  if (ODD) {
-#pragma unroll
-    for (int j = NR - 1; j > 0; --j) B[j] = prmt(B[j - 1], B[j], 0x0041);
-    B[0] = prmt(gcur, B[0], 0x0040u | (uint32_t)T);
-  } else {
-#pragma unroll
-    for (int j = 0; j < NR - 1; ++j) A[j] = prmt(A[j], A[j + 1], 0x0041);
-    A[NR - 1] = prmt(A[NR - 1], rcur, 0x0001u | ((uint32_t)(4 + T) << 4));
+// Cells of pair p inside the read (0 <= p - W + 1 + k <= L - 1), for the pairs where that is
+// a constant: prologue pairs p < W - 1 (cells k >= W - 1 - p) and epilogue pairs p = L + e,
+// e < W - 1 (cells k <= W - 2 - e).  Every pair in between has all W cells inside.
+template <int W> __host__ __device__ constexpr uint32_t full_mask() { return (uint32_t)((1ull << W) - 1ull); }
+template <int W, int MODE, int K> __host__ __device__ constexpr uint32_t split_pair_mask() {
+  return MODE == 0 ? full_mask<W>()
+       : MODE == 1 ? full_mask<W>() & ~((1u << (W - 1 - K)) - 1u)
+                   : (2u << (W - 2 - K)) - 1u;
+}
+
+// One step of a pair whose index is Q mod H: ODD = genome step.  T = byte of the stream words
+// holding the entering codes; MB = the pair's cells inside the read (a constant, so that a
+// register with both halves outside costs nothing and one with a half outside one LOP3).
+template <int W, bool ODD, int T, int Q, uint32_t MB>
+SG_HD void fstep_split(uint32_t (&A)[W / 2], uint32_t (&B)[W / 2], uint32_t (&M1)[W / 2], uint32_t (&M2)[W / 2],
+                       uint32_t (&I1)[W / 2], uint32_t& Max, uint32_t rcur, uint32_t gcur, uint32_t TLO,
+                       uint32_t THI, uint32_t CFE, uint32_t CFO) {
+  constexpr int H = W / 2;
+  constexpr int RA = (Q + 1) % H;                // read steps done (mod H), this one included
+  constexpr int RB = (ODD ? Q + 1 : Q) % H;      // genome steps done (mod H)
+  if (ODD) {  // new code into cell 0; old cell H - 1 moves to cell H
+    constexpr int idx = (H - 1 - Q % H + H) % H;
+    B[idx] = prmt(gcur, B[idx], 0x0040u | (uint32_t)T);
+  } else {    // old cell H moves to cell H - 1; new code into cell W - 1
+    constexpr int idx = Q % H;
+    A[idx] = prmt(A[idx], rcur, 0x0001u | ((uint32_t)(4 + T) << 4));
   }
-  uint32_t P[NR], Mn[NR], In[NR];
+  uint32_t P[H], Mn[H], In[H];
 #pragma unroll
-  for (int j = 0; j < NR; ++j) P[j] = __vimax_s16x2_relu(I1[j] - CFE, M1[j] - CFO);  // halves are positive: relu is a no-op
+  for (int j = 0; j < H; ++j) P[j] = __vimax_s16x2_relu(I1[j] - CFE, M1[j] - CFO);  // halves are positive
 #pragma unroll
-  for (int j = 0; j < NR; ++j) {
-    const uint32_t nbr = ODD ? prmt(j > 0 ? P[j - 1] : kFBB, P[j], 0x5432)
-                             : prmt(P[j], j < NR - 1 ? P[j + 1] : kFBB, 0x5432);
+  for (int j = 0; j < H; ++j) {
+    uint32_t nbr;
+    if (ODD) nbr = j > 0 ? P[j - 1] : prmt(kFBB, P[H - 1], 0x5410);
+    else     nbr = j < H - 1 ? P[j + 1] : prmt(P[0], kFBB, 0x5432);
     In[j] = __vimax3_s16x2(P[j], nbr, kFBB);
-    const uint32_t sc = prmt(TLO, THI, A[j] - B[j]);
-    uint32_t mv = __viaddmax_s16x2(M2[j], sc, In[j]);
-    if (MASKED) mv = (mv & mw[j]) | (kFBB & ~mw[j]);
-    Mn[j] = mv;
+    const bool lo = (MB >> j) & 1u, hi = (MB >> (j + H)) & 1u;
+    if (!lo && !hi) {
+      Mn[j] = kFBB;  // M of cells outside the read is 0; their I still propagates
+    } else {
+      const uint32_t sc = prmt(TLO, THI, A[(j + RA) % H] - B[(j - RB + H) % H]);
+      const uint32_t mv = __viaddmax_s16x2(M2[j], sc, In[j]);
+      Mn[j] = (lo && hi) ? mv : lo ? ((mv & 0x0000FFFFu) | (kFBB & 0xFFFF0000u))
+                                   : ((mv & 0xFFFF0000u) | (kFBB & 0x0000FFFFu));
+    }
   }
-  if (NR == 1) {
+  if (H == 1) {
     Max = __vimax_s16x2_relu(Max, Mn[0]);
   } else {
 #pragma unroll
-    for (int j = 0; j + 1 < NR; j += 2) Max = __vimax3_s16x2(Max, Mn[j], Mn[j + 1]);
+    for (int j = 0; j + 1 < H; j += 2) Max = __vimax3_s16x2(Max, Mn[j], Mn[j + 1]);
   }
 #pragma unroll
-  for (int j = 0; j < NR; ++j) {
+  for (int j = 0; j < H; ++j) {
     M2[j] = M1[j];
     M1[j] = Mn[j];
     I1[j] = In[j];
   }
 }
 
-// mask words of pair p: cell k enabled iff 0 <= p - W + 1 + k <= L - 1
-template <int W>
-SG_HD void pair_mask(int p, int L, uint32_t (&mw)[W / 2]) {
-  const int kmin = (W - 1 - p) > 0 ? (W - 1 - p) : 0;
-  const int kmax = (L + W - 2 - p) < (W - 1) ? (L + W - 2 - p) : (W - 1);
-  uint32_t m = 0;
-  if (kmax >= kmin) m = ((kmax >= 31) ? 0xffffffffu : ((2u << kmax) - 1u)) & ~((1u << kmin) - 1u);
-#pragma unroll
-  for (int j = 0; j < W / 2; ++j) mw[j] = mask_word(m, j);
+// Pairs K..NP-1 of a group whose pair 0 has index QB mod H; pair k takes byte k % 4 of the
+// stream words rc[k / 4], gc[k / 4].  MODE: 0 main (all cells inside), 1 prologue (pair index
+// k), 2 epilogue (pair L + k).
+template <int W, int MODE, int QB, int K, int NP, int NWD>
+SG_HD void run_pairs_split(uint32_t (&A)[W / 2], uint32_t (&B)[W / 2], uint32_t (&M1)[W / 2], uint32_t (&M2)[W / 2],
+                           uint32_t (&I1)[W / 2], uint32_t& Max, const uint32_t (&rc)[NWD],
+                           const uint32_t (&gc)[NWD], uint32_t TLO, uint32_t THI, uint32_t CFE, uint32_t CFO) {
+  if constexpr (K < NP) {
+    constexpr uint32_t MB = split_pair_mask<W, MODE, K>();
+    fstep_split<W, false, K % 4, QB + K, MB>(A, B, M1, M2, I1, Max, rc[K / 4], gc[K / 4], TLO, THI, CFE, CFO);
+    fstep_split<W, true, K % 4, QB + K, MB>(A, B, M1, M2, I1, Max, rc[K / 4], gc[K / 4], TLO, THI, CFE, CFO);
+    run_pairs_split<W, MODE, QB, K + 1, NP, NWD>(A, B, M1, M2, I1, Max, rc, gc, TLO, THI, CFE, CFO);
+  }
 }
 
-template <int W, bool MASKED>
-SG_HD void fblock3(int p0, int L, uint32_t (&A)[W / 2], uint32_t (&B)[W / 2], uint32_t (&M1)[W / 2],
-                   uint32_t (&M2)[W / 2], uint32_t (&I1)[W / 2], uint32_t& Max, uint32_t rcur, uint32_t gcur,
-                   uint32_t TLO, uint32_t THI, uint32_t CFE, uint32_t CFO) {
-  uint32_t mw[W / 2];
-#pragma unroll
-  for (int j = 0; j < W / 2; ++j) mw[j] = 0xffffffffu;
-  if (MASKED) pair_mask<W>(p0 + 0, L, mw);
-  fstep3<W, false, MASKED, 0>(A, B, M1, M2, I1, Max, rcur, gcur, TLO, THI, CFE, CFO, mw);
-  fstep3<W, true, MASKED, 0>(A, B, M1, M2, I1, Max, rcur, gcur, TLO, THI, CFE, CFO, mw);
-  if (MASKED) pair_mask<W>(p0 + 1, L, mw);
-  fstep3<W, false, MASKED, 1>(A, B, M1, M2, I1, Max, rcur, gcur, TLO, THI, CFE, CFO, mw);
-  fstep3<W, true, MASKED, 1>(A, B, M1, M2, I1, Max, rcur, gcur, TLO, THI, CFE, CFO, mw);
-  if (MASKED) pair_mask<W>(p0 + 2, L, mw);
-  fstep3<W, false, MASKED, 2>(A, B, M1, M2, I1, Max, rcur, gcur, TLO, THI, CFE, CFO, mw);
-  fstep3<W, true, MASKED, 2>(A, B, M1, M2, I1, Max, rcur, gcur, TLO, THI, CFE, CFO, mw);
-  if (MASKED) pair_mask<W>(p0 + 3, L, mw);
-  fstep3<W, false, MASKED, 3>(A, B, M1, M2, I1, Max, rcur, gcur, TLO, THI, CFE, CFO, mw);
-  fstep3<W, true, MASKED, 3>(A, B, M1, M2, I1, Max, rcur, gcur, TLO, THI, CFE, CFO, mw);
+// remainder pairs K.. while K < r (r < NP): guarded, constant rotation
+template <int W, int QB, int K, int NP, int NWD>
+SG_HD void run_rest_split(int r, uint32_t (&A)[W / 2], uint32_t (&B)[W / 2], uint32_t (&M1)[W / 2],
+                          uint32_t (&M2)[W / 2], uint32_t (&I1)[W / 2], uint32_t& Max, const uint32_t (&rc)[NWD],
+                          const uint32_t (&gc)[NWD], uint32_t TLO, uint32_t THI, uint32_t CFE, uint32_t CFO) {
+  if constexpr (K < NP) {
+    if (K < r) {
+      run_pairs_split<W, 0, QB, K, K + 1, NWD>(A, B, M1, M2, I1, Max, rc, gc, TLO, THI, CFE, CFO);
+      run_rest_split<W, QB, K + 1, NP, NWD>(r, A, B, M1, M2, I1, Max, rc, gc, TLO, THI, CFE, CFO);
+    }
+  }
 }
+
+// selector of prmt(w0, w1, .) picking bytes s..s+3 of the 8-byte pair (s < 4)
+SG_HD uint32_t funnel_sel(uint32_t s) { return s | ((s + 1) << 4) | ((s + 2) << 8) | ((s + 3) << 12); }
 
 // gexp: byte-expanded genome (code c -> c * 0x11) at code 0, 4-byte aligned, readable in its
-// padding; rexp: read stream bytes 0xC4 + c * 0x11, 4-byte aligned, readable for L + W + 8
+// padding; rexp: read stream bytes 0xC4 + c * 0x11, 4-byte aligned, readable for L + 24
 // bytes.  Returns the band maximum (unbiased).  Requires L >= W.
+//
+// Pairs 0..W-2 (prologue) and L..L+W-2 (epilogue) run with their constant cell masks, pairs
+// W-1..L-1 (main) unmasked in blocks of BP pairs; the main remainder (fewer than BP pairs)
+// keeps constant rotations, and the registers are rotated back to rotation 0 once, before
+// the epilogue.
 template <int W>
-SG_HD int filter_v3(const uint8_t* __restrict__ gexp, int64_t pos, const uint8_t* __restrict__ rexp, int L,
-                    uint32_t TLO, uint32_t THI, uint32_t CFE, uint32_t CFO) {
-  constexpr int NR = W / 2;
-  uint32_t A[NR], B[NR], M1[NR], M2[NR], I1[NR];
+SG_HD int filter_split(const uint8_t* __restrict__ gexp, int64_t pos, const uint8_t* __restrict__ rexp, int L,
+                       uint32_t TLO, uint32_t THI, uint32_t CFE, uint32_t CFO) {
+  constexpr int H = W / 2;
+  constexpr int BP = H > 4 ? H : 4;
+  constexpr int NPRO = W - 1;
+  constexpr int NWP = (NPRO + 3) / 4;  // stream words of the prologue / epilogue
+  constexpr int NWB = BP / 4;          // stream words of a main block
+  uint32_t A[H], B[H], M1[H], M2[H], I1[H];
 #pragma unroll
-  for (int j = 0; j < NR; ++j) {
-    A[j] = 0xC4C4u;  // code 0 in read format
+  for (int j = 0; j < H; ++j) {
+    A[j] = 0xC4C4u;  // code 0 in read format (cells outside the read)
     // window codes 0..W-1, cell k = code W-1-k
-    B[j] = (uint32_t)gexp[pos + W - 1 - 2 * j] | ((uint32_t)gexp[pos + W - 2 - 2 * j] << 8);
+    B[j] = (uint32_t)gexp[pos + W - 1 - j] | ((uint32_t)gexp[pos + W - 1 - j - H] << 8);
     M1[j] = kFBB; M2[j] = kFBB; I1[j] = kFBB;
   }
   uint32_t Max = kFBB;
-  const int64_t g0 = pos + W;
-  const uint32_t* gw = reinterpret_cast<const uint32_t*>(gexp) + (g0 >> 2);
-  const uint32_t s = (uint32_t)(g0 & 3);
-  const uint32_t fsel = s | ((s + 1) << 4) | ((s + 2) << 8) | ((s + 3) << 12);
+  const uint32_t* gx = reinterpret_cast<const uint32_t*>(gexp);
   const uint32_t* rw = reinterpret_cast<const uint32_t*>(rexp);
-  const int npairs = L + W - 1;
-  const int nblocks = (npairs + 3) >> 2;
-  uint32_t w0 = ldg32(gw), w1 = ldg32(gw + 1);
-  for (int b = 0; b < nblocks; ++b) {
-    const uint32_t gcur = prmt(w0, w1, fsel);
-    const uint32_t rcur = ldg32(rw + b);
-    w0 = w1;
-    w1 = ldg32(gw + b + 2);
-    const int p0 = 4 * b;
-    if (p0 >= W - 1 && p0 + 3 <= L - 1)
-      fblock3<W, false>(p0, L, A, B, M1, M2, I1, Max, rcur, gcur, TLO, THI, CFE, CFO);
-    else
-      fblock3<W, true>(p0, L, A, B, M1, M2, I1, Max, rcur, gcur, TLO, THI, CFE, CFO);
+  const int64_t g0 = pos + W;  // genome byte entering at pair 0
+  {  // prologue: pairs 0..W-2, read bytes 0.., genome bytes g0..
+    uint32_t rc[NWP], gc[NWP];
+    const uint32_t* gw = gx + (g0 >> 2);
+    const uint32_t sel = funnel_sel((uint32_t)(g0 & 3));
+    uint32_t wp = ldg32(gw);
+#pragma unroll
+    for (int k = 0; k < NWP; ++k) {
+      rc[k] = ldg32(rw + k);
+      const uint32_t wn = ldg32(gw + k + 1);
+      gc[k] = prmt(wp, wn, sel);
+      wp = wn;
+    }
+    run_pairs_split<W, 1, 0, 0, NPRO, NWP>(A, B, M1, M2, I1, Max, rc, gc, TLO, THI, CFE, CFO);
+  }
+  {  // main: pairs W-1..L-1, index W-1 = H-1 mod H at every block start
+    const int nmain = L - W + 1;
+    const int64_t gb = g0 + W - 1;
+    const uint32_t* gw = gx + (gb >> 2);
+    const uint32_t gsel = funnel_sel((uint32_t)(gb & 3));
+    const uint32_t* rwm = rw + ((W - 1) >> 2);
+    constexpr uint32_t rsel = ((W - 1) & 3) | ((((W - 1) & 3) + 1) << 4) | ((((W - 1) & 3) + 2) << 8) |
+                              ((((W - 1) & 3) + 3) << 12);
+    uint32_t gp = ldg32(gw), rp = ldg32(rwm);
+    int pm = 0;
+    for (; pm + BP <= nmain; pm += BP) {
+      uint32_t rc[NWB], gc[NWB];
+      const int q = pm >> 2;
+#pragma unroll
+      for (int k = 0; k < NWB; ++k) {
+        const uint32_t gn = ldg32(gw + q + k + 1), rn = ldg32(rwm + q + k + 1);
+        gc[k] = prmt(gp, gn, gsel);
+        rc[k] = prmt(rp, rn, rsel);
+        gp = gn;
+        rp = rn;
+      }
+      run_pairs_split<W, 0, H - 1, 0, BP, NWB>(A, B, M1, M2, I1, Max, rc, gc, TLO, THI, CFE, CFO);
+    }
+    const int r = nmain - pm;
+    if (r > 0) {
+      uint32_t rc[NWB], gc[NWB];
+      const int q = pm >> 2;
+#pragma unroll
+      for (int k = 0; k < NWB; ++k) {
+        const uint32_t gn = ldg32(gw + q + k + 1), rn = ldg32(rwm + q + k + 1);
+        gc[k] = prmt(gp, gn, gsel);
+        rc[k] = prmt(rp, rn, rsel);
+        gp = gn;
+        rp = rn;
+      }
+      run_rest_split<W, H - 1, 0, BP, NWB>(r, A, B, M1, M2, I1, Max, rc, gc, TLO, THI, CFE, CFO);
+    }
+  }
+  if (H > 1) {  // back to rotation 0: logical read register j = A[(j + L) mod H], genome B[(j - L) mod H]
+    const int s = L & (H - 1);
+#pragma unroll
+    for (int b = 1; b < H; b <<= 1) {
+      const bool on = (s & b) != 0;
+      uint32_t ta[H], tb[H];
+#pragma unroll
+      for (int j = 0; j < H; ++j) {
+        ta[j] = A[(j + b) % H];
+        tb[j] = B[(j - b + H) % H];
+      }
+#pragma unroll
+      for (int j = 0; j < H; ++j) {
+        A[j] = on ? ta[j] : A[j];
+        B[j] = on ? tb[j] : B[j];
+      }
+    }
+  }
+  {  // epilogue: pairs L..L+W-2; the entering read codes stay in cells outside the read
+    uint32_t rc[NWP], gc[NWP];
+    const int64_t ge = g0 + L;
+    const uint32_t* gw = gx + (ge >> 2);
+    const uint32_t sel = funnel_sel((uint32_t)(ge & 3));
+    uint32_t wp = ldg32(gw);
+#pragma unroll
+    for (int k = 0; k < NWP; ++k) {
+      rc[k] = 0xC4C4C4C4u;
+      const uint32_t wn = ldg32(gw + k + 1);
+      gc[k] = prmt(wp, wn, sel);
+      wp = wn;
+    }
+    run_pairs_split<W, 2, 0, 0, NPRO, NWP>(A, B, M1, M2, I1, Max, rc, gc, TLO, THI, CFE, CFO);
   }
   const int lo = (int)(int16_t)(Max & 0xffffu), hi = (int)(int16_t)(Max >> 16);
   return (lo > hi ? lo : hi) - (int)kFB;
 }
 
-SG_HD void filter_v3_consts(int fm, int fx, int fo, int fe, uint32_t& TLO, uint32_t& THI, uint32_t& CFE,
+SG_HD void filter_split_consts(int fm, int fx, int fo, int fe, uint32_t& TLO, uint32_t& THI, uint32_t& CFE,
                             uint32_t& CFO) {
   const uint32_t mis = (uint32_t)((256 - fx) & 0xff);
   TLO = (mis << 8) | (mis << 16) | (mis << 24);

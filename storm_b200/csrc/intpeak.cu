@@ -1,50 +1,72 @@
-// intpeak.cu -- integer-pipe peak of this GPU, measured: every thread runs 16 independent
-// chains of add + max (the instruction mix of the banded filter), so that the figure is the
-// chip's issue rate for those 32-bit integer operations, not a datasheet number.
+// intpeak.cu -- the roofline denominator of the banded filter, measured on this GPU: every
+// thread runs 16 independent register-resident copies of one step of the packed 16-bit filter
+// recurrence (filter_core.cuh), with no memory traffic, so that the figure is the chip's rate
+// for that exact instruction mix rather than a datasheet number.
+//
+// Per copy and step (one register = two 16-bit cells): two gap subtractions and a max (P), a
+// three-way max (I), a subtraction and a byte permute (score), an add-max (M), and half of a
+// three-way max (running maximum): 7.5 32-bit lane instructions per two cells.
 #include "common.cuh"
+#include "filter_core.cuh"
 
 namespace {
 
-__global__ void intpeak_kernel(int iters, int seed, int* out) {
-  int a[16];
+__global__ void filter_mix_kernel(int iters, uint32_t seed, uint32_t* out) {
+  uint32_t M1[16], M2[16], I1[16];
 #pragma unroll
-  for (int k = 0; k < 16; ++k) a[k] = seed + k * 7 + threadIdx.x;
-  const int b = seed * 3 + 1, c = seed ^ 0x55;
+  for (int k = 0; k < 16; ++k) {
+    M1[k] = (seed + 977u * k + threadIdx.x) & 0x00ff00ffu;
+    M2[k] = (seed * 3u + 131u * k) & 0x00ff00ffu;
+    I1[k] = (seed ^ (k * 0x01010101u)) & 0x00ff00ffu;
+  }
+  const uint32_t CFE = (seed & 3u) * 0x10001u, CFO = ((seed >> 2) & 7u) * 0x10001u;
+  const uint32_t TLO = seed * 0x9E3779B9u, THI = TLO ^ 0x5A5A5A5Au;
+  uint32_t mx0 = 0, mx1 = 0;
   for (int it = 0; it < iters; ++it) {
 #pragma unroll
     for (int k = 0; k < 16; ++k) {
-      a[k] = a[k] + b;          // IADD
-      a[k] = max(a[k], c);      // IMNMX
+      const uint32_t p = __vimax_s16x2_relu(I1[k] - CFE, M1[k] - CFO);
+      const uint32_t in = __vimax3_s16x2(p, I1[(k + 1) & 15], sg::kFBB);
+      const uint32_t sc = sg::prmt(TLO, THI, M1[k] - M2[k]);
+      const uint32_t mn = __viaddmax_s16x2(M2[k], sc, in);
+      M2[k] = M1[k];
+      M1[k] = mn;
+      I1[k] = in;
+    }
+#pragma unroll
+    for (int k = 0; k < 16; k += 4) {
+      mx0 = __vimax3_s16x2(mx0, M1[k], M1[k + 1]);
+      mx1 = __vimax3_s16x2(mx1, M1[k + 2], M1[k + 3]);
     }
   }
-  int s = 0;
+  uint32_t s = mx0 ^ mx1;
 #pragma unroll
-  for (int k = 0; k < 16; ++k) s ^= a[k];
-  if (s == 0x7fffffff) out[0] = s;  // keep the work alive
+  for (int k = 0; k < 16; ++k) s ^= M1[k] ^ I1[k];
+  if (s == 0x7fffffffu) out[0] = s;  // keep the work alive
 }
 
 }  // namespace
 
-// Sustained 32-bit integer add/max lane-operations per second (ops counted per thread).
-extern "C" int stormgpu_int_peak(int device, double* ops_per_s, double* ms) {
+// 32-bit lane instructions of the filter recurrence per second (7.5 per register step).
+extern "C" int stormgpu_filter_peak(int device, double* ops_per_s, double* ms) {
   SG_CUDA(cudaSetDevice(device));
   int sms = 0;
   SG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
-  int* d;
-  SG_CUDA(cudaMalloc(&d, sizeof(int)));
+  uint32_t* d;
+  SG_CUDA(cudaMalloc(&d, sizeof(uint32_t)));
   cudaEvent_t e0, e1;
-  cudaEventCreate(&e0);
-  cudaEventCreate(&e1);
-  const int blocks = sms * 8, threads = 256, iters = 20000;
-  intpeak_kernel<<<blocks, threads>>>(100, 1, d);  // warm-up
-  cudaEventRecord(e0);
-  intpeak_kernel<<<blocks, threads>>>(iters, 2, d);
-  cudaEventRecord(e1);
+  SG_CUDA(cudaEventCreate(&e0));
+  SG_CUDA(cudaEventCreate(&e1));
+  const int blocks = sms * 8, threads = 256, iters = 4000;
+  filter_mix_kernel<<<blocks, threads>>>(100, 1u, d);  // warm-up
+  SG_CUDA(cudaEventRecord(e0));
+  filter_mix_kernel<<<blocks, threads>>>(iters, 2u, d);
+  SG_CUDA(cudaEventRecord(e1));
   SG_CUDA(cudaEventSynchronize(e1));
   float t = 0;
-  cudaEventElapsedTime(&t, e0, e1);
+  SG_CUDA(cudaEventElapsedTime(&t, e0, e1));
   *ms = t;
-  *ops_per_s = (double)blocks * threads * iters * 16 * 2 / (t * 1e-3);
+  *ops_per_s = (double)blocks * threads * iters * (16 * 7 + 8) / (t * 1e-3);
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   cudaFree(d);

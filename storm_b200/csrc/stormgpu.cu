@@ -298,12 +298,15 @@ static int map_device_impl(stormgpu_ctx* c, const stormgpu_reads* reads, stormgp
   memset(&S, 0, sizeof(S));
   S.ms_index = ms_index;
   int64_t launches = 0;
-  int maxL = 0;
+  int maxL = 0, minL = STORMGPU_MAX_READ_LEN;
   {
     std::vector<int16_t> hl(n > 0 ? n : 1);
     if (n > 0) SG_CUDA(cudaMemcpyAsync(hl.data(), reads->lengths, sizeof(int16_t) * n, cudaMemcpyDeviceToHost, st));
     SG_CUDA(cudaStreamSynchronize(st));
-    for (int64_t r = 0; r < n; ++r) maxL = std::max<int>(maxL, hl[r]);
+    for (int64_t r = 0; r < n; ++r) {
+      maxL = std::max<int>(maxL, hl[r]);
+      minL = std::min<int>(minL, hl[r]);
+    }
     if (maxL > STORMGPU_MAX_READ_LEN) { sg_set_error("read longer than %d", STORMGPU_MAX_READ_LEN); return STORMGPU_EINVAL; }
   }
   if (out->tb_stride < (maxL + c->p.allowed_indels + 1) / 2) { sg_set_error("tb_stride too small"); return STORMGPU_EINVAL; }
@@ -395,7 +398,7 @@ static int map_device_impl(stormgpu_ctx* c, const stormgpu_reads* reads, stormgp
       const int64_t rstride = rexp_stride(maxL);
       if (c->rexp.grow(n * rstride)) return STORMGPU_ENOMEM;
       launch_expand_reads(rd, c->rexp.p, rstride, st);
-      job.gexp = R.d_gexp; job.rexp = c->rexp.p; job.rstride = rstride;
+      job.gexp = R.d_gexp; job.rexp = c->rexp.p; job.rstride = rstride; job.min_len = minL;
       launch_filter_flat_job(job, sp, filter_dpx_ok(sp, maxL), st);
       launches += 2;
       SG_CUDA(cudaEventRecord(c->ev[2], st));
@@ -606,7 +609,7 @@ extern "C" int stormgpu_sw_filter(int W, int read_len, uint32_t match, uint32_t 
     memset(&job, 0, sizeof(job));
     job.n = n; job.fr = dzero; job.fd = dpos; job.flag = dp; job.codes = dr; job.cstride = rb;
     job.lengths = dl; job.genome = gb; job.W = W; job.Is = 0;
-    job.gexp = gx + kGexpPad; job.rexp = rx; job.rstride = rstride;
+    job.gexp = gx + kGexpPad; job.rexp = rx; job.rstride = rstride; job.min_len = read_len;
     job.fm = sp.fm; job.fx = sp.fx; job.fo = sp.fo; job.fe = sp.fe; job.fthr = sp.fthr;
     launch_filter_flat_job(job, sp, filter_dpx_ok(sp, read_len), 0);
     SG_CUDA(cudaGetLastError());

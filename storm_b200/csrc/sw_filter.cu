@@ -3,19 +3,21 @@
 // candidates that pass.
 //
 // Semantics: those of alignment_avx2__align_{hexa,octa,quad,pair} (alignment_simd.c:2613-3404)
-// for one hit of W cells, as restated in map_kernels.cu (sw_filter_one).  Here the W cells of
-// one anti-diagonal step live in W/2 registers, two signed 16-bit cells each:
-//   * codes: one byte per cell holding the code twice (c | c << 4), so that
-//     sel = (A ^ B) | 0x8080 is directly a byte_perm selector whose nibbles pick
-//     T = [match, -mismatch, -mismatch, -mismatch] and sign-replicate it: the per-cell score
-//     is one PRMT (code 0 = equal symbols);
-//   * I = max(P, P of the neighbour cell, 0) with P = max(I[l-1] - ext, M[l-1] - open): the
-//     neighbour is the same cell one register-half over (PRMT 0x5432);
-//   * M = max(M[l-2] + score, I, 0) in one __viaddmax_s16x2_relu.
+// for one hit of W cells, as restated in filter_ref.cuh (sw_filter_one).  Here the W cells of
+// one anti-diagonal step live in W/2 registers, two signed 16-bit cells each (filter_core.cuh):
+//   * the per-cell score is one prmt whose selector is the difference of a read byte and a
+//     genome byte (no compare, no branch);
+//   * I = max(P, P of the neighbour cell, 0) with P = max(I[l-1] - ext, M[l-1] - open), and
+//     M = max(M[l-2] + score, I) in one __viaddmax_s16x2; cells carry a bias of 256 so that the
+//     gap subtractions are plain 32-bit adds;
+//   * in the split layout used for reads of at least W codes (cells j and j + W/2 share a
+//     register) the neighbour cell is in the neighbouring register, and the code streams move
+//     by renaming registers; reads shorter than W use the adjacent-pair layout, which decodes
+//     the packed 2-bit streams directly.
 // The upper u8 saturation of the reference (adds at 255) is not reproduced: the threshold is
 // at most 254, so the first cell that would saturate already has a value above it and the
 // hit passes in both; cells are masked before they propagate, so an unmasked run and a
-// saturating one agree on pass/fail.  Values stay below 2^15 when L * match < 32768 (checked
+// saturating one agree on pass/fail.  Values stay below 2^15 when L * match < 32000 (checked
 // by the host, which otherwise uses the plain 32-bit kernel).
 #include "map_kernels.cuh"
 #include "sw_filter.cuh"
@@ -24,14 +26,17 @@
 
 namespace sg {
 
-template <int W>
-__global__ void __launch_bounds__(256) filter_flat_dpx_kernel(FilterJob job) {
+// SHORT: the batch has reads shorter than W (band longer than the read), which take the
+// stream-decoding variant; without them the kernel holds only the split-layout core and
+// fits in 64 registers for W <= 8.
+template <int W, bool SHORT>
+__global__ void __launch_bounds__(256, (W <= 8 ? 4 : 2)) filter_flat_dpx_kernel(FilterJob job) {
   const uint32_t T = (uint32_t)(job.fm & 0xff) | ((uint32_t)((256 - job.fx) & 0xff) << 8) |
                      ((uint32_t)((256 - job.fx) & 0xff) << 16) | ((uint32_t)((256 - job.fx) & 0xff) << 24);
   const uint32_t NFE = (uint32_t)(uint16_t)(-job.fe) * 0x10001u;
   const uint32_t NFO = (uint32_t)(uint16_t)(-job.fo) * 0x10001u;
   uint32_t TLO, THI, CFE, CFO;
-  filter_v3_consts(job.fm, job.fx, job.fo, job.fe, TLO, THI, CFE, CFO);
+  filter_split_consts(job.fm, job.fx, job.fo, job.fe, TLO, THI, CFE, CFO);
   unsigned long long cells = 0, cands = 0;
   for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < job.n; t += (int64_t)gridDim.x * blockDim.x) {
     const int r = job.fr[t];
@@ -39,12 +44,12 @@ __global__ void __launch_bounds__(256) filter_flat_dpx_kernel(FilterJob job) {
     const int L = job.lengths[r];
     const int64_t pos = (int64_t)d - job.Is;
     int mx;
-    if (L >= W && job.gexp)
-      mx = filter_v3<W>(job.gexp, pos, job.rexp + (int64_t)r * job.rstride, L, TLO, THI, CFE, CFO);
+    if (!SHORT || L >= W)
+      mx = filter_split<W>(job.gexp, pos, job.rexp + (int64_t)r * job.rstride, L, TLO, THI, CFE, CFO);
     else
       mx = filter_dpx<W>(job.genome, pos, job.codes + (int64_t)r * job.cstride, job.cstride, L, T, NFE, NFO);
     job.flag[t] = mx > job.fthr ? 1 : 0;
-    cells += (unsigned long long)L * (2 * job.Is + 1);
+    cells += (unsigned long long)(2 * W) * (unsigned long long)(L + W - 1);
     cands++;
   }
   if (job.counters) {
@@ -107,7 +112,7 @@ __global__ void filter_flat_scalar_kernel(FilterJob job, ScoreParams sp) {
     const int L = job.lengths[r];
     job.flag[t] = sw_filter_dispatch_ext(job.W, job.genome, (int64_t)job.fd[t] - job.Is,
                                          job.codes + (int64_t)r * job.cstride, L, sp) ? 1 : 0;
-    cells += (unsigned long long)L * (2 * job.Is + 1);
+    cells += (unsigned long long)(2 * job.W) * (unsigned long long)(L + job.W - 1);
     cands++;
   }
   if (job.counters) {
@@ -134,11 +139,20 @@ void launch_filter_flat_job(const FilterJob& job, const ScoreParams& sp, bool dp
     filter_flat_scalar_kernel<<<(unsigned)blocks, 256, 0, st>>>(job, sp);
     return;
   }
-  switch (job.W) {
-  case 2: filter_flat_dpx_kernel<2><<<(unsigned)blocks, 256, 0, st>>>(job); break;
-  case 4: filter_flat_dpx_kernel<4><<<(unsigned)blocks, 256, 0, st>>>(job); break;
-  case 8: filter_flat_dpx_kernel<8><<<(unsigned)blocks, 256, 0, st>>>(job); break;
-  default: filter_flat_dpx_kernel<16><<<(unsigned)blocks, 256, 0, st>>>(job); break;
+  if (job.min_len >= job.W) {
+    switch (job.W) {
+    case 2: filter_flat_dpx_kernel<2, false><<<(unsigned)blocks, 256, 0, st>>>(job); break;
+    case 4: filter_flat_dpx_kernel<4, false><<<(unsigned)blocks, 256, 0, st>>>(job); break;
+    case 8: filter_flat_dpx_kernel<8, false><<<(unsigned)blocks, 256, 0, st>>>(job); break;
+    default: filter_flat_dpx_kernel<16, false><<<(unsigned)blocks, 256, 0, st>>>(job); break;
+    }
+  } else {
+    switch (job.W) {
+    case 2: filter_flat_dpx_kernel<2, true><<<(unsigned)blocks, 256, 0, st>>>(job); break;
+    case 4: filter_flat_dpx_kernel<4, true><<<(unsigned)blocks, 256, 0, st>>>(job); break;
+    case 8: filter_flat_dpx_kernel<8, true><<<(unsigned)blocks, 256, 0, st>>>(job); break;
+    default: filter_flat_dpx_kernel<16, true><<<(unsigned)blocks, 256, 0, st>>>(job); break;
+    }
   }
 }
 

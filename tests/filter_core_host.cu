@@ -18,10 +18,10 @@ static void pack(const std::vector<int>& c, uint8_t* out) {
 }
 
 template <int W>
-static int filter_w3(const uint8_t* gexp, int64_t pos, const uint8_t* rexp, int L, int fm, int fx, int fo, int fe) {
+static int filter_ws(const uint8_t* gexp, int64_t pos, const uint8_t* rexp, int L, int fm, int fx, int fo, int fe) {
   uint32_t TLO, THI, CFE, CFO;
-  sg::filter_v3_consts(fm, fx, fo, fe, TLO, THI, CFE, CFO);
-  return sg::filter_v3<W>(gexp, pos, rexp, L, TLO, THI, CFE, CFO);
+  sg::filter_split_consts(fm, fx, fo, fe, TLO, THI, CFE, CFO);
+  return sg::filter_split<W>(gexp, pos, rexp, L, TLO, THI, CFE, CFO);
 }
 
 template <int W>
@@ -50,8 +50,8 @@ int main(int argc, char** argv) {
   for (int t = 0; t < cases; ++t) {
     const int Ws[4] = {2, 4, 8, 16};
     const int W = Ws[rng() % 4];
-    const int Ls[10] = {1, 3, 7, 12, 15, 35, 49, 50, 100, 150};
-    const int L = Ls[rng() % 10];
+    const int Ls[18] = {1, 2, 3, 4, 7, 8, 12, 15, 16, 17, 23, 24, 35, 49, 50, 100, 150, 1000};
+    const int L = Ls[rng() % 18];
     const int fm = (int)(rng() % 2 ? 5 : 1 + rng() % 20), fx = 1 + (int)(rng() % 8);
     const int fo = (int)(rng() % 12), fe = (int)(rng() % 6);
     const int thr = (int)(rng() % 260);
@@ -74,18 +74,23 @@ int main(int argc, char** argv) {
     if (L >= W) {
       std::vector<uint8_t> rexp(((L + W + 8 + 3) & ~3) + 16, 0xC4);
       for (int i = 0; i < L; ++i) rexp[i] = (uint8_t)(0xC4 + read[i] * 0x11);
-      int got3;
+      int got4;
       switch (W) {
-      case 2: got3 = filter_w3<2>(gexp, pos, rexp.data(), L, fm, fx, fo, fe); break;
-      case 4: got3 = filter_w3<4>(gexp, pos, rexp.data(), L, fm, fx, fo, fe); break;
-      case 8: got3 = filter_w3<8>(gexp, pos, rexp.data(), L, fm, fx, fo, fe); break;
-      default: got3 = filter_w3<16>(gexp, pos, rexp.data(), L, fm, fx, fo, fe); break;
+      case 2: got4 = filter_ws<2>(gexp, pos, rexp.data(), L, fm, fx, fo, fe); break;
+      case 4: got4 = filter_ws<4>(gexp, pos, rexp.data(), L, fm, fx, fo, fe); break;
+      case 8: got4 = filter_ws<8>(gexp, pos, rexp.data(), L, fm, fx, fo, fe); break;
+      default: got4 = filter_ws<16>(gexp, pos, rexp.data(), L, fm, fx, fo, fe); break;
       }
-      const int pass3 = got3 > (thr >= 255 ? 254 : thr);
+      if (got4 != got) {
+        printf("MISMATCH split case %d: W=%d L=%d fm=%d fx=%d fo=%d fe=%d pos=%lld max=%d stream-max=%d\n", t, W, L,
+               fm, fx, fo, fe, (long long)pos, got4, got);
+        return 1;
+      }
+      const int pass3 = got4 > (thr >= 255 ? 254 : thr);
       const int exp3 = or_sw_filter(W, L, fm, fx, fo, fe, thr, gen, pos, rb.data());
       if (pass3 != exp3) {
-        printf("MISMATCH v3 case %d: W=%d L=%d fm=%d fx=%d fo=%d fe=%d thr=%d pos=%lld max=%d v2max=%d exp=%d\n", t, W, L,
-               fm, fx, fo, fe, thr, (long long)pos, got3, got, exp3);
+        printf("MISMATCH split case %d: W=%d L=%d fm=%d fx=%d fo=%d fe=%d thr=%d pos=%lld max=%d exp=%d\n", t, W, L,
+               fm, fx, fo, fe, thr, (long long)pos, got4, exp3);
         return 1;
       }
       checked3++;
@@ -98,6 +103,6 @@ int main(int argc, char** argv) {
     }
     checked++;
   }
-  printf("checked %d (v3 %d)\n", checked, checked3);
+  printf("checked %d (split layout %d)\n", checked, checked3);
   return 0;
 }
