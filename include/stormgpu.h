@@ -184,6 +184,35 @@ int stormgpu_align(const stormgpu_params *params, const uint8_t *read, const uin
                    int64_t pad, const int32_t *win, int64_t n, int32_t *score, int32_t *bound,
                    int16_t *best, int32_t *tb_len, uint8_t *tb, int64_t tb_stride);
 
+/* stormgpu_align for callers that cannot allocate device memory: callers whose device memory
+ * belongs to another allocator (a framework's caching allocator, a pool reserved at start-up,
+ * with no room for a cudaMalloc of its own) and callers that cannot afford the device-wide
+ * synchronisation of cudaMalloc / cudaFree.  No counterpart in the reference (it has no GPU).
+ *
+ * Same computation and outputs as stormgpu_align, but every array is device memory of the
+ * current device, owned by the caller, and nothing is allocated: read / levels are packed as
+ * for stormgpu_align (levels may be NULL); genome / mask hold n_codes codes with no padding,
+ * and every window must lie inside them (0 <= win[k], win[k] + read_len + 2 * allowed_indels
+ * <= n_codes; otherwise STORMGPU_EINVAL and unspecified outputs); win, score, bound, tb_len
+ * hold n entries, best 4n, tb n * tb_stride bytes (zero-filled, then the traceback).
+ * params->device is not consulted.  Runs on `stream` (a cudaStream_t; NULL: the default
+ * stream) and returns when the results are in place.
+ *
+ * The kernel works in one fixed device array of STORMGPU_NOALLOC_SCRATCH_BYTES inside the
+ * library, which every GPU that loads the library holds until the process exits.  A call
+ * needs 4 * read_len * words_per_row * n bytes of it plus at most 8n + 768 of bookkeeping
+ * (words_per_row = ceil((4I + 2) / 32), plus ceil((2I + 1) / 32) in colour space,
+ * I = allowed_indels); larger calls fail with STORMGPU_EINVAL: split the windows.  The first
+ * call on a device looks up the array's device address (cudaGetSymbolAddress): make it before
+ * any stream capture.  Every call on a device shares that device's array, so calls that
+ * overlap on the GPU race: serialise them. */
+#define STORMGPU_NOALLOC_SCRATCH_BYTES (8ll << 20)
+int stormgpu_align_noalloc(const stormgpu_params *params, const uint8_t *read, const uint8_t *levels,
+                           int read_len, const uint8_t *genome, const uint8_t *mask, int64_t n_codes,
+                           const int32_t *win, int64_t n, int32_t *score, int32_t *bound,
+                           int16_t *best, int32_t *tb_len, uint8_t *tb, int64_t tb_stride,
+                           void *stream);
+
 /* CSR index of one sequence for one seed (index.c:19-195): first[4^w + 1] offsets and
  * map[first[4^w]] positions, ascending within each key. */
 int stormgpu_index_one(const char *seed, int32_t stdev_distance, const uint8_t *codes,

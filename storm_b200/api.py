@@ -83,6 +83,10 @@ def lib():
                                      C.c_void_p, C.c_int64, C.c_int64, C.c_void_p, C.c_int64,
                                      C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                      C.c_int64]
+        L.stormgpu_align_noalloc.argtypes = [C.POINTER(Params), C.c_void_p, C.c_void_p, C.c_int, C.c_void_p,
+                                             C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_void_p,
+                                             C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64,
+                                             C.c_void_p]
         L.stormgpu_index_one.argtypes = [C.c_char_p, C.c_int32, C.c_void_p, C.c_int64, C.c_int64,
                                          C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p,
                                          C.c_int64, C.POINTER(C.c_int64)]
@@ -214,6 +218,16 @@ def align(prm: Params, read_packed, levels_packed, L, genome_packed, mask_packed
     _check(lib().stormgpu_align(C.byref(prm), _p(r), _p(q), L, _p(g), _p(m), n_codes, 0, _p(wins), n,
                                 _p(score), _p(bound), _p(best), _p(tbl), _p(tb), tbs))
     return score, bound, best, tbl, tb
+
+
+def align_noalloc(prm: Params, read, levels, L, genome, mask, n_codes, win, n, score, bound, best, tb_len, tb,
+                  tb_stride, stream=0):
+    """stormgpu_align_noalloc: every buffer argument is a device address (int) of the current
+    device, owned by the caller (levels may be 0); nothing is allocated.  For callers that
+    cannot allocate device memory themselves at this point (a memory pool owned by another
+    allocator, or no tolerance for the synchronisation of an allocation)."""
+    _check(lib().stormgpu_align_noalloc(C.byref(prm), read, levels or None, L, genome, mask, n_codes, win, n,
+                                        score, bound, best, tb_len, tb, tb_stride, stream or None))
 
 
 def index_one(seed: str, stdev: int, codes_packed, n_codes, regions=()):

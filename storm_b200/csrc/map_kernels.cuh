@@ -18,6 +18,10 @@ struct ScoreParams {
   int min_score;      // -t
 };
 
+// filter width W for the SIMD half-width Is (run.c:64-101), and the scoring of a parameter set
+int filter_width(int is);
+ScoreParams make_score_params(const stormgpu_params& p);
+
 struct ReadsDev {
   int64_t n;
   const uint8_t* codes;

@@ -82,6 +82,10 @@ int parse_seeds(const char* list, SeedSet* out) {
   return out->n > 0 ? 0 : STORMGPU_EINVAL;
 }
 
+}  // namespace
+
+namespace sg {
+
 int filter_width(int is) { return is <= 1 ? 2 : is <= 3 ? 4 : is <= 7 ? 8 : 16; }
 
 ScoreParams make_score_params(const stormgpu_params& p) {
@@ -106,6 +110,10 @@ ScoreParams make_score_params(const stormgpu_params& p) {
   sp.min_score = p.min_score;
   return sp;
 }
+
+}  // namespace sg
+
+namespace {
 
 struct RefSeq {
   int64_t n = 0;
