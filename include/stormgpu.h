@@ -155,6 +155,7 @@ typedef struct stormgpu_stats {
   int64_t filter_cells;      /* filter cell updates: W * 2 * (L + W - 1) per candidate, W = 2..16 */
   int64_t align_cells;       /* L * (2*i+1) per full alignment */
   int64_t kernels;           /* kernel launches */
+  int64_t filter_band_cells; /* band cells of the filtered diagonals: L * (2*min(i,15)+1) each */
   double  ms_index, ms_gather, ms_filter, ms_align, ms_replay, ms_total;
 } stormgpu_stats;
 int stormgpu_get_stats(stormgpu_ctx *ctx, stormgpu_stats *out);

@@ -49,7 +49,8 @@ class Results(C.Structure):
 
 class Stats(C.Structure):
     _fields_ = [(n, C.c_int64) for n in ("candidates", "filter_passed", "aligned", "seed_lookups",
-                                         "hit_positions", "filter_cells", "align_cells", "kernels")] + \
+                                         "hit_positions", "filter_cells", "align_cells", "kernels",
+                                         "filter_band_cells")] + \
                [(n, C.c_double) for n in ("ms_index", "ms_gather", "ms_filter", "ms_align",
                                           "ms_replay", "ms_total")]
 
@@ -131,10 +132,19 @@ class ReadBatch:
 
 
 class MapResults:
-    def __init__(self, n, tb_stride):
-        self.hits = np.zeros(n * 4, dtype=HIT_DTYPE)
-        self.tb = np.zeros((n * 4, tb_stride), dtype=np.uint8)
-        self.mapped = np.zeros(n, dtype=np.uint8)
+    """Per-read results; `buffers` = (hits, tb, mapped) arrays to write into (e.g. views of
+    pinned host memory reused across batches), else fresh ones."""
+
+    def __init__(self, n, tb_stride, buffers=None):
+        if buffers is None:
+            self.hits = np.zeros(n * 4, dtype=HIT_DTYPE)
+            self.tb = np.zeros((n * 4, tb_stride), dtype=np.uint8)
+            self.mapped = np.zeros(n, dtype=np.uint8)
+        else:
+            self.hits, self.tb, self.mapped = buffers
+            if (self.hits.dtype != HIT_DTYPE or self.hits.shape != (n * 4,) or self.tb.shape != (n * 4, tb_stride)
+                    or self.mapped.shape != (n,) or not all(a.flags.c_contiguous for a in buffers)):
+                raise ValueError("result buffers of the wrong shape or type")
         self.tb_stride = tb_stride
 
     def cstruct(self) -> Results:
@@ -160,10 +170,12 @@ class Mapper:
     def build_index(self):
         _check(lib().stormgpu_build_index(self._ctx))
 
-    def map(self, batch: ReadBatch, tb_stride=None) -> MapResults:
-        if tb_stride is None:
+    def map(self, batch: ReadBatch, tb_stride=None, out: MapResults | None = None) -> MapResults:
+        if out is not None:
+            tb_stride = out.tb_stride
+        elif tb_stride is None:
             tb_stride = ((int(batch.lengths.max()) + self.params.allowed_indels + 1) // 2 + 7) & ~7
-        res = MapResults(batch.n, tb_stride)
+        res = out if out is not None else MapResults(batch.n, tb_stride)
         rs, rr = batch.cstruct(), res.cstruct()
         _check(lib().stormgpu_map(self._ctx, C.byref(rs), C.byref(rr)))
         return res

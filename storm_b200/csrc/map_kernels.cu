@@ -88,14 +88,52 @@ constexpr int kMaxBand = 2 * STORMGPU_MAX_INDELS + 1;
 // traceback :642-734.  The direction of every cell (2 bits) and, in colour space, whether its
 // pair score was made positive by the SNP adjustment (the `score > corner score` test of
 // :693) go to the scratch, slot-minor: word (row*wpr + k)*nslots + slot.
-__global__ void align_kernel(ReadsDev rd, ScoreParams sp, const uint8_t* __restrict__ genome,
-                             const uint8_t* __restrict__ mask, int64_t slot0, int64_t nslots, PassBuffers pb) {
+// Genome and mask codes of the band of one row, 2 bits each in registers, for a constant band
+// width: row i + 1 is row i moved by one code, so each row loads one genome and one mask code
+// (instead of BW of each).
+template <int BWT>
+struct BandWindow {
+  static_assert(BWT > 0 && BWT <= 64, "band width");
+  uint64_t g[2] = {0, 0}, m[2] = {0, 0};
+  __device__ __forceinline__ void put(int c, int gc, int mc) {
+    g[c >> 5] |= (uint64_t)gc << (2 * (c & 31));
+    m[c >> 5] |= (uint64_t)mc << (2 * (c & 31));
+  }
+  // codes [base, base + BWT)
+  __device__ __forceinline__ void load(const uint8_t* genome, const uint8_t* mask, int64_t base) {
+#pragma unroll
+    for (int c = 0; c < BWT; ++c) put(c, code_at(genome, base + c), code_at(mask, base + c));
+  }
+  // drop cell 0, the others move down one cell, code `pos` becomes cell BWT - 1
+  __device__ __forceinline__ void advance(const uint8_t* genome, const uint8_t* mask, int64_t pos) {
+    if (BWT > 32) {
+      g[0] = (g[0] >> 2) | (g[1] << 62);
+      m[0] = (m[0] >> 2) | (m[1] << 62);
+      g[1] >>= 2;
+      m[1] >>= 2;
+    } else {
+      g[0] >>= 2;
+      m[0] >>= 2;
+    }
+    put(BWT - 1, code_at(genome, pos), code_at(mask, pos));
+  }
+  __device__ __forceinline__ int gcode(int c) const { return (int)((g[c >> 5] >> (2 * (c & 31))) & 3u); }
+  __device__ __forceinline__ int mcode(int c) const { return (int)((m[c >> 5] >> (2 * (c & 31))) & 3u); }
+};
+
+// BWT > 0: the band width 2I + 1 as a constant, so that the row arrays live in registers;
+// BWT = 0: any width up to kMaxBand (arrays in local memory).
+template <int BWT>
+__global__ void __launch_bounds__(128) align_kernel(ReadsDev rd, ScoreParams sp, const uint8_t* __restrict__ genome,
+                                                    const uint8_t* __restrict__ mask, int64_t slot0, int64_t nslots,
+                                                    PassBuffers pb) {
+  constexpr int NB = BWT > 0 ? BWT : kMaxBand;
   const int64_t sl = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (sl >= nslots) return;
   const int64_t slot = slot0 + sl;
   const int r = pb.p_read[slot];
   const int d = pb.p_diag[slot];
-  const int I = sp.I, BW = 2 * I + 1, colour = sp.colour;
+  const int I = sp.I, BW = BWT > 0 ? BWT : 2 * I + 1, colour = sp.colour;
   const int L = rd.lengths[r];
   const uint8_t* rdc = rd.codes + (int64_t)r * rd.cstride;
   const uint8_t* rdq = rd.levels ? rd.levels + (int64_t)r * rd.lstride : nullptr;
@@ -103,17 +141,20 @@ __global__ void align_kernel(ReadsDev rd, ScoreParams sp, const uint8_t* __restr
   const int wpr_dir = (2 * BW + 31) / 32, wpr = wpr_dir + (colour ? (BW + 31) / 32 : 0);
   uint32_t* scr = pb.a_scratch;
   const int64_t ns = nslots;
-  int sc[kMaxBand], stt[kMaxBand];
+  int sc[NB], stt[NB];
   const int mbest = sp.pair[0][3];
+  BandWindow<(BWT > 0 ? BWT : 1)> bwin;
+  if (BWT > 0) bwin.load(genome, mask, win);
   // row 0
   {
     const int rc = code_at(rdc, 0), q = rdq ? code_at(rdq, 0) : 3;
-    uint32_t wd[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    uint32_t wd[(2 * NB + 31) / 32] = {};
+#pragma unroll
     for (int c = 0; c < BW; ++c) {
       const int64_t j = (int64_t)win + c;
-      const int f = code_at(genome, j);
+      const int f = BWT > 0 ? bwin.gcode(c) : code_at(genome, j);
       int chk = 0, score;
-      if (code_at(mask, j) == 0) {
+      if ((BWT > 0 ? bwin.mcode(c) : code_at(mask, j)) == 0) {
         chk = colour ? (rc ^ f) : 0;
         score = sp.pair[colour ? (chk ? 1 : 0) : (rc != f)][q];
       } else score = kMinScore;
@@ -129,14 +170,16 @@ __global__ void align_kernel(ReadsDev rd, ScoreParams sp, const uint8_t* __restr
     const int rc = code_at(rdc, i), q = rdq ? code_at(rdq, i) : 3;
     int max_on_line = kMinScore;
     int lsc = kMinScore, lst = st_make(3, I, 0, 0, 0);  // left border
-    uint32_t wd[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-    uint32_t wc[5] = {0, 0, 0, 0, 0};
+    uint32_t wd[(2 * NB + 31) / 32] = {};
+    uint32_t wc[(NB + 31) / 32] = {};
+    if (BWT > 0) bwin.advance(genome, mask, (int64_t)win + i + BW - 1);
+#pragma unroll
     for (int c = 0; c < BW; ++c) {
       const int64_t j = (int64_t)win + i + c;
-      const int f = code_at(genome, j);
+      const int f = BWT > 0 ? bwin.gcode(c) : code_at(genome, j);
       // initial values of this cell (alignment__init_matrix)
       int chk0 = 0, ac0 = 0, fr0 = 0, s0;
-      if (code_at(mask, j) == 0) {
+      if ((BWT > 0 ? bwin.mcode(c) : code_at(mask, j)) == 0) {
         if (colour) { chk0 = ac0 = rc ^ f; fr0 = ac0 ? q : 0; s0 = sp.pair[chk0 ? 1 : 0][q]; }
         else s0 = sp.pair[rc != f][q];
       } else s0 = kMinScore;
@@ -201,6 +244,7 @@ __global__ void align_kernel(ReadsDev rd, ScoreParams sp, const uint8_t* __restr
       for (int k = wpr_dir; k < wpr; ++k) scr[((int64_t)i * wpr + k) * ns + sl] = wc[k - wpr_dir];
   }
   int best = kMinScore, bi = -1, bj = -1;
+#pragma unroll
   for (int c = 0; c < BW; ++c)
     if (best < sc[c]) { best = sc[c]; bi = L - 1; bj = L - 1 + c; }
   const int32_t bnd = bound > 0x7fffffffLL ? 0x7fffffff : (int32_t)bound;
@@ -255,7 +299,14 @@ void launch_align(const ReadsDev& r, const ScoreParams& sp, const uint8_t* genom
                   const uint8_t* mask, int64_t slot0, int64_t nslots, PassBuffers& pb,
                   cudaStream_t st) {
   if (nslots <= 0) return;
-  align_kernel<<<(unsigned)((nslots + 127) / 128), 128, 0, st>>>(r, sp, genome, mask, slot0, nslots, pb);
+  const unsigned blocks = (unsigned)((nslots + 127) / 128);
+  switch (2 * sp.I + 1) {
+  case 7: align_kernel<7><<<blocks, 128, 0, st>>>(r, sp, genome, mask, slot0, nslots, pb); break;
+  case 15: align_kernel<15><<<blocks, 128, 0, st>>>(r, sp, genome, mask, slot0, nslots, pb); break;
+  case 31: align_kernel<31><<<blocks, 128, 0, st>>>(r, sp, genome, mask, slot0, nslots, pb); break;
+  case 41: align_kernel<41><<<blocks, 128, 0, st>>>(r, sp, genome, mask, slot0, nslots, pb); break;
+  default: align_kernel<0><<<blocks, 128, 0, st>>>(r, sp, genome, mask, slot0, nslots, pb); break;
+  }
 }
 
 // ------------------------------------------------------------------------------ replay

@@ -419,6 +419,7 @@ static int map_device_impl(stormgpu_ctx* c, const stormgpu_reads* reads, stormgp
       if (utot == 0) npass = 0;
       S.candidates += (int64_t)cnt[5];
       S.filter_cells += (int64_t)cnt[2];
+      S.filter_band_cells += (int64_t)cnt[6];
       S.seed_lookups += (int64_t)cnt[3];
       S.hit_positions += (int64_t)cnt[4];
       S.filter_passed += npass;

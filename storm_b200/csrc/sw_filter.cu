@@ -37,7 +37,7 @@ __global__ void __launch_bounds__(256, (W <= 8 ? 4 : 2)) filter_flat_dpx_kernel(
   const uint32_t NFO = (uint32_t)(uint16_t)(-job.fo) * 0x10001u;
   uint32_t TLO, THI, CFE, CFO;
   filter_split_consts(job.fm, job.fx, job.fo, job.fe, TLO, THI, CFE, CFO);
-  unsigned long long cells = 0, cands = 0;
+  unsigned long long cells = 0, cands = 0, band = 0;
   for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < job.n; t += (int64_t)gridDim.x * blockDim.x) {
     const int r = job.fr[t];
     const int d = job.fd[t];
@@ -50,16 +50,19 @@ __global__ void __launch_bounds__(256, (W <= 8 ? 4 : 2)) filter_flat_dpx_kernel(
       mx = filter_dpx<W>(job.genome, pos, job.codes + (int64_t)r * job.cstride, job.cstride, L, T, NFE, NFO);
     job.flag[t] = mx > job.fthr ? 1 : 0;
     cells += (unsigned long long)(2 * W) * (unsigned long long)(L + W - 1);
+    band += (unsigned long long)L * (2 * job.Is + 1);
     cands++;
   }
   if (job.counters) {
     for (int o = 16; o > 0; o >>= 1) {
       cells += __shfl_xor_sync(0xffffffffu, cells, o);
       cands += __shfl_xor_sync(0xffffffffu, cands, o);
+      band += __shfl_xor_sync(0xffffffffu, band, o);
     }
     if ((threadIdx.x & 31) == 0 && cands) {
       atomicAdd(&job.counters[2], cells);
       atomicAdd(&job.counters[5], cands);
+      atomicAdd(&job.counters[6], band);
     }
   }
 }
@@ -106,23 +109,26 @@ void launch_expand_reads(const ReadsDev& rd, uint8_t* rexp, int64_t rstride, cud
 
 // Plain 32-bit variant (any score values), the restatement in map_kernels.cu.
 __global__ void filter_flat_scalar_kernel(FilterJob job, ScoreParams sp) {
-  unsigned long long cells = 0, cands = 0;
+  unsigned long long cells = 0, cands = 0, band = 0;
   for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < job.n; t += (int64_t)gridDim.x * blockDim.x) {
     const int r = job.fr[t];
     const int L = job.lengths[r];
     job.flag[t] = sw_filter_dispatch_ext(job.W, job.genome, (int64_t)job.fd[t] - job.Is,
                                          job.codes + (int64_t)r * job.cstride, L, sp) ? 1 : 0;
     cells += (unsigned long long)(2 * job.W) * (unsigned long long)(L + job.W - 1);
+    band += (unsigned long long)L * (2 * job.Is + 1);
     cands++;
   }
   if (job.counters) {
     for (int o = 16; o > 0; o >>= 1) {
       cells += __shfl_xor_sync(0xffffffffu, cells, o);
       cands += __shfl_xor_sync(0xffffffffu, cands, o);
+      band += __shfl_xor_sync(0xffffffffu, band, o);
     }
     if ((threadIdx.x & 31) == 0 && cands) {
       atomicAdd(&job.counters[2], cells);
       atomicAdd(&job.counters[5], cands);
+      atomicAdd(&job.counters[6], band);
     }
   }
 }

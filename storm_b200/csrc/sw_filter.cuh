@@ -16,7 +16,7 @@ struct FilterJob {
   const uint8_t* genome;
   int W, Is;
   int fm, fx, fo, fe, fthr;
-  unsigned long long* counters;  // [2] += cell updates W*2*(L+W-1), [5] += candidates
+  unsigned long long* counters;  // [2] += cell updates W*2*(L+W-1), [5] += candidates, [6] += L*(2*Is+1)
   const uint8_t* gexp;          // byte-expanded genome (code c -> c * 0x11), code 0
   const uint8_t* rexp;          // read streams (bytes 0xC4 + c * 0x11), rstride bytes per read
   int64_t rstride;
