@@ -7,9 +7,13 @@
 // One warp per read: keys computed from the packed read, CSR offsets read from the
 // (L2-resident) key table, positions gathered straight into the warp's shared memory, bitonic
 // sort there, de-duplication by ballot, and the surviving diagonals appended to the flat
-// candidate list (reads contiguous, diagonals ascending within a read).  Reads with more index
-// positions than a warp can hold go to a block-per-read kernel (shared memory up to 32768
-// positions) and, beyond that, to a global-memory variant run one read at a time.
+// candidate list (reads contiguous, diagonals ascending within a read).  Every lane looks up
+// several (seed, position) keys before any result is used, so that a read costs two memory
+// latencies (key table, positions) rather than two per seed.  Up to 32 positions are sorted in
+// registers; more are first reduced to distinct values (warp_dedupe), then bucket-sorted
+// (bucket_sort_emit).  Reads with more index positions than a warp can hold go to a
+// block-per-read kernel (shared memory up to 32768 positions) and, beyond that, to a
+// global-memory variant run one read at a time.
 #include "gather.cuh"
 
 namespace sg {
@@ -41,6 +45,18 @@ __device__ __forceinline__ void seed_item(const IndexView& ix, int si, int t, co
   const uint32_t key = read_key(s, read, L, rp);
   a = __ldg(ix.first[si] + key);
   cnt = __ldg(ix.first[si] + key + 1) - a;
+}
+
+// (index offset, count, read position) of position t of seed s, with that seed's key table
+__device__ __forceinline__ void item_lookup(const int32_t* __restrict__ first, const SeedDev& s, int t,
+                                            const uint8_t* read, int L, int& a, int& cnt, int& rp) {
+  a = 0; cnt = 0; rp = 0;
+  if (t >= seed_npos(s, L)) return;
+  rp = s.n_positions ? s.positions[t] : t;
+  if (rp < 0 || rp >= L) return;
+  const uint32_t key = read_key(s, read, L, rp);
+  a = __ldg(first + key);
+  cnt = __ldg(first + key + 1) - a;
 }
 
 __device__ __forceinline__ void warp_bitonic(int32_t* s, int P) {
@@ -170,48 +186,178 @@ __device__ __forceinline__ void sort_emit_regs(const int32_t* s, int H, int I, i
   reg_emit<E>(v, H, I, r, go);
 }
 
-constexpr int kWarpCap = 1024;
-constexpr int kGWarps = 8;
+// Drop repeated values from a[0..H) (one warp), keeping one of each, compacted to the front
+// of a (order not kept); tab[0..cap), cap >= H, is the open-addressing set.  The diagonal a read
+// truly maps to comes once per (seed, position) that hits it, so this removes the one large
+// group of equal values before the sort.  Returns the number of distinct values.
+constexpr int32_t kEmptySlot = 0x7fffffff;  // no diagonal (position - read position) reaches it
+__device__ __forceinline__ int warp_dedupe(int32_t* a, int H, int32_t* tab, int cap) {
+  const int lane = threadIdx.x & 31;
+  const unsigned lt = (1u << lane) - 1u;
+  for (int i = lane; i < cap; i += 32) tab[i] = kEmptySlot;
+  __syncwarp();
+  int U = 0;
+  for (int i0 = 0; i0 < H; i0 += 32) {
+    const int i = i0 + lane;
+    bool keep = false;
+    int32_t v = 0;
+    if (i < H) {
+      v = a[i];
+      uint32_t h = __umulhi((uint32_t)v * 0x9E3779B1u, (uint32_t)cap);
+      for (;;) {
+        const int32_t old = atomicCAS(&tab[h], kEmptySlot, v);
+        if (old == kEmptySlot) { keep = true; break; }
+        if (old == v) break;
+        h = h + 1 == (uint32_t)cap ? 0u : h + 1;
+      }
+    }
+    const unsigned m = __ballot_sync(0xffffffffu, keep);
+    if (keep) a[U + __popc(m & lt)] = v;  // writes trail the reads of this and later chunks
+    U += __popc(m);
+    __syncwarp();
+  }
+  return U;
+}
+
+// Sort a[0..H) (one warp) into b[0..H) and emit: 32 buckets by the high bits of (v - min)
+// (power-of-two aligned, so that bucket order is value order), counted with shared atomics,
+// scattered to b, then every lane insertion-sorts its own bucket.  A bucket holding more than
+// 64 values (clustered diagonals) falls back to the bitonic sort of a, which needs room for
+// the next power of two of H from a on (a and b are adjacent).
+__device__ __forceinline__ void bucket_sort_emit(int32_t* a, int32_t* b, int32_t* hist, int H, int I, int r,
+                                                 const GatherOut& go) {
+  const int lane = threadIdx.x & 31;
+  int32_t vmin = 0x7fffffff, vmax = (int32_t)0x80000000;
+  for (int i = lane; i < H; i += 32) {
+    const int32_t v = a[i];
+    vmin = min(vmin, v);
+    vmax = max(vmax, v);
+  }
+  vmin = __reduce_min_sync(0xffffffffu, vmin);
+  vmax = __reduce_max_sync(0xffffffffu, vmax);
+  const uint32_t range = (uint32_t)vmax - (uint32_t)vmin;
+  const int sh = max(0, 32 - __clz((int)range) - 5);  // (range >> sh) < 32
+  hist[lane] = 0;
+  __syncwarp();
+  for (int i = lane; i < H; i += 32) atomicAdd(&hist[((uint32_t)a[i] - (uint32_t)vmin) >> sh], 1);
+  __syncwarp();
+  const int c = hist[lane];
+  const int incl = warp_incl_scan(c);
+  const int base = incl - c;
+  if (__reduce_max_sync(0xffffffffu, (unsigned)c) > 64u) {
+    int P = 1;
+    while (P < H) P <<= 1;
+    for (int i = H + lane; i < P; i += 32) a[i] = 0x7fffffff;
+    __syncwarp();
+    warp_bitonic(a, P);
+    warp_emit(a, H, I, r, go);
+    return;
+  }
+  __syncwarp();
+  hist[lane] = base;
+  __syncwarp();
+  for (int i = lane; i < H; i += 32) {
+    const int32_t v = a[i];
+    b[atomicAdd(&hist[((uint32_t)v - (uint32_t)vmin) >> sh], 1)] = v;
+  }
+  __syncwarp();
+  for (int x = 1; x < c; ++x) {
+    const int32_t t = b[base + x];
+    int y = x - 1;
+    while (y >= 0 && b[base + y] > t) {
+      b[base + y + 1] = b[base + y];
+      --y;
+    }
+    b[base + y + 1] = t;
+  }
+  __syncwarp();
+  warp_emit(b, H, I, r, go);
+}
+
+constexpr int kWarpCap = 768;
+constexpr int kGWarps = 4;
 constexpr int kReadBytes = STORMGPU_MAX_READ_LEN / 4 + 16;
 
+constexpr int kItems = 4;  // (seed, position) items per lane and round: 128 key lookups in flight per warp
+
 __global__ void __launch_bounds__(kGWarps * 32) gather_fused_kernel(ReadsDev rd, IndexView ix, int I, GatherOut go) {
-  __shared__ int32_t sm[kGWarps][kWarpCap];
+  __shared__ int32_t sm[kGWarps][2 * kWarpCap];  // gathered positions, then the set / sorted copy
+  __shared__ int32_t shist[kGWarps][32];
+  __shared__ int32_t soff[kGWarps][kMaxSeeds + 1];  // first item of every seed, for the current read
+  __shared__ const int32_t* s_first[kMaxSeeds];
+  __shared__ const int32_t* s_map[kMaxSeeds];
   __shared__ __align__(16) uint8_t srd[kGWarps][kReadBytes];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int nseeds = c_gseeds.n;
+  if (threadIdx.x < nseeds) {
+    s_first[threadIdx.x] = ix.first[threadIdx.x];
+    s_map[threadIdx.x] = ix.map[threadIdx.x];
+  }
+  __syncthreads();
   int32_t* s = sm[w];
+  int32_t* so = soff[w];
   uint8_t* rs = srd[w];
   const int64_t nwarps = (int64_t)gridDim.x * kGWarps;
   unsigned long long lookups = 0, positions = 0;
   for (int64_t r = (int64_t)blockIdx.x * kGWarps + w; r < rd.n; r += nwarps) {
     const int L = rd.lengths[r];
-    {  // the read's packed codes into shared memory
+    {  // the read's packed codes into shared memory, and the item offsets of the seeds
       const uint8_t* src = rd.codes + r * rd.cstride;
       const int nb = (L + 3) >> 2;
       for (int b = lane; b < nb; b += 32) rs[b] = src[b];
+      const int np = lane < nseeds ? seed_npos(c_gseeds.s[lane], L) : 0;
+      const int incl = warp_incl_scan(np);
+      if (lane <= nseeds) so[lane] = incl - np;
       __syncwarp();
     }
     const uint8_t* read = rs;
+    const int T = so[nseeds];
     int H = 0;
-    for (int si = 0; si < c_gseeds.n; ++si) {
-      const int np = seed_npos(c_gseeds.s[si], L);
-      const int32_t* mp = ix.map[si];
-      for (int t0 = 0; t0 < np; t0 += 32) {
-        int a, cnt, rp;
-        seed_item(ix, si, t0 + lane, read, L, a, cnt, rp);
-        lookups += (t0 + lane < np) ? 1 : 0;
-        const int incl = warp_incl_scan(cnt);
-        const int dst = H + incl - cnt;
-        H += __shfl_sync(0xffffffffu, incl, 31);
-        if (cnt <= 8) {
-          for (int u = 0; u < cnt; ++u)
-            if (dst + u < kWarpCap) s[dst + u] = __ldg(mp + a + u) - rp;
+    for (int r0 = 0; r0 < T; r0 += 32 * kItems) {
+      // every lane looks up its items (all key-table loads in flight together) ...
+      int a[kItems], cnt[kItems], rp[kItems], sid[kItems];
+#pragma unroll
+      for (int m = 0; m < kItems; ++m) {
+        const int it = r0 + m * 32 + lane;
+        int si = 0;
+        if (it < T)
+          while (it >= so[si + 1]) ++si;
+        sid[m] = si;
+        item_lookup(s_first[si], c_gseeds.s[si], it < T ? it - so[si] : 0x40000000, read, L, a[m], cnt[m], rp[m]);
+        lookups += it < T ? 1 : 0;
+      }
+      // ... then one scan places all of them, and the position loads go out together
+      int tot = 0;
+#pragma unroll
+      for (int m = 0; m < kItems; ++m) tot += cnt[m];
+      const int incl = warp_incl_scan(tot);
+      int dst[kItems];
+      dst[0] = H + incl - tot;
+#pragma unroll
+      for (int m = 1; m < kItems; ++m) dst[m] = dst[m - 1] + cnt[m - 1];
+      H += __shfl_sync(0xffffffffu, incl, 31);
+#pragma unroll
+      for (int m = 0; m < kItems; ++m) {
+        if (cnt[m] <= 8) {
+          const int32_t* mp = s_map[sid[m]] + a[m];
+          int32_t tv[8];
+#pragma unroll
+          for (int u = 0; u < 8; ++u) tv[u] = u < cnt[m] ? __ldg(mp + u) : 0;
+#pragma unroll
+          for (int u = 0; u < 8; ++u)
+            if (u < cnt[m] && dst[m] + u < kWarpCap) s[dst[m] + u] = tv[u] - rp[m];
         }
-        unsigned m = __ballot_sync(0xffffffffu, cnt > 8);
-        while (m) {
-          const int j = __ffs(m) - 1;
-          m &= m - 1;
-          const int aj = __shfl_sync(0xffffffffu, a, j), cj = __shfl_sync(0xffffffffu, cnt, j);
-          const int dj = __shfl_sync(0xffffffffu, dst, j), rj = __shfl_sync(0xffffffffu, rp, j);
+      }
+#pragma unroll
+      for (int m = 0; m < kItems; ++m) {  // long position lists: the whole warp copies each
+        unsigned bm = __ballot_sync(0xffffffffu, cnt[m] > 8);
+        while (bm) {
+          const int j = __ffs(bm) - 1;
+          bm &= bm - 1;
+          const int aj = __shfl_sync(0xffffffffu, a[m], j), cj = __shfl_sync(0xffffffffu, cnt[m], j);
+          const int dj = __shfl_sync(0xffffffffu, dst[m], j), rj = __shfl_sync(0xffffffffu, rp[m], j);
+          const int sj = __shfl_sync(0xffffffffu, sid[m], j);
+          const int32_t* mp = s_map[sj];
           for (int u = lane; u < cj; u += 32)
             if (dj + u < kWarpCap) s[dj + u] = __ldg(mp + aj + u) - rj;
         }
@@ -224,17 +370,12 @@ __global__ void __launch_bounds__(kGWarps * 32) gather_fused_kernel(ReadsDev rd,
       continue;
     }
     __syncwarp();
-    if (H <= 32) sort_emit_regs<1>(s, H, I, (int)r, go);
-    else if (H <= 64) sort_emit_regs<2>(s, H, I, (int)r, go);
-    else if (H <= 128) sort_emit_regs<4>(s, H, I, (int)r, go);
-    else if (H <= 256) sort_emit_regs<8>(s, H, I, (int)r, go);
-    else {
-      int P = 1;
-      while (P < H) P <<= 1;
-      for (int i = H + lane; i < P; i += 32) s[i] = 0x7fffffff;
-      __syncwarp();
-      warp_bitonic(s, P);
-      warp_emit(s, H, I, (int)r, go);
+    if (H <= 32) {
+      sort_emit_regs<1>(s, H, I, (int)r, go);
+    } else {
+      const int U = warp_dedupe(s, H, s + kWarpCap, kWarpCap);
+      if (U <= 32) sort_emit_regs<1>(s, U, I, (int)r, go);
+      else bucket_sort_emit(s, s + kWarpCap, shist[w], U, I, (int)r, go);
     }
     __syncwarp();
   }
