@@ -145,6 +145,32 @@ int stormgpu_map_device(stormgpu_ctx *ctx, const stormgpu_reads *reads,
                         stormgpu_results *out, void *stream);
 int stormgpu_sync(stormgpu_ctx *ctx);
 
+/* Served mapping ----------------------------------------------------------------------------
+ * The reference and the index of every step of an -O seed chain stay resident on the GPU;
+ * batches are submitted from any thread and run concurrently on `slots` workers (own stream and
+ * buffers each).  A batch is admitted, in arrival order, when a worker is free and the device
+ * memory its reads need (stormgpu_submit estimates it) fits what the batches in flight leave of
+ * `budget_bytes`.  Step k of a batch maps, with chain[k], the reads no earlier step mapped, in
+ * their order: the reference run again on its own -O FASTQ output (README:97-101,
+ * hit_map.c:514-579); every read gets the results of the step that mapped it.
+ * No counterpart in the reference (one read file per process there). */
+typedef struct stormgpu_server stormgpu_server;
+int stormgpu_server_open(const stormgpu_params *params, const char *const *chain, int nsteps,
+                         int slots, int64_t budget_bytes, stormgpu_server **out);
+int stormgpu_server_add_reference(stormgpu_server *s, const uint8_t *codes, const uint8_t *mask,
+                                  int64_t n_codes, const int32_t *region_starts,
+                                  const int32_t *region_ends, int32_t n_regions);
+/* Index every step, start the workers. */
+int stormgpu_server_build(stormgpu_server *s);
+/* Queue a batch (host buffers, which must stay valid until stormgpu_poll reports it done).
+ * step[r] (optional, n bytes) receives the chain step that mapped read r, 255 if none did. */
+int stormgpu_submit(stormgpu_server *s, const stormgpu_reads *reads, stormgpu_results *out,
+                    uint8_t *step, int64_t *ticket);
+/* 0: done (results in place, *latency_ms = submit to completion), 1: not yet after
+ * timeout_ms (< 0: wait), < 0: the batch failed (message in stormgpu_last_error). */
+int stormgpu_poll(stormgpu_server *s, int64_t ticket, int timeout_ms, double *latency_ms);
+void stormgpu_server_close(stormgpu_server *s);
+
 /* Statistics of the last stormgpu_map* call. */
 typedef struct stormgpu_stats {
   int64_t candidates;        /* diagonals produced by the hit gather */

@@ -84,6 +84,16 @@ def lib():
                                      C.c_void_p, C.c_int64, C.c_int64, C.c_void_p, C.c_int64,
                                      C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                      C.c_int64]
+        L.stormgpu_server_open.argtypes = [C.POINTER(Params), C.POINTER(C.c_char_p), C.c_int, C.c_int, C.c_int64,
+                                           C.POINTER(C.c_void_p)]
+        L.stormgpu_server_add_reference.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p,
+                                                    C.c_void_p, C.c_int32]
+        L.stormgpu_server_build.argtypes = [C.c_void_p]
+        L.stormgpu_submit.argtypes = [C.c_void_p, C.POINTER(Reads), C.POINTER(Results), C.c_void_p,
+                                      C.POINTER(C.c_int64)]
+        L.stormgpu_poll.argtypes = [C.c_void_p, C.c_int64, C.c_int, C.POINTER(C.c_double)]
+        L.stormgpu_server_close.argtypes = [C.c_void_p]
+        L.stormgpu_server_close.restype = None
         L.stormgpu_align_noalloc.argtypes = [C.POINTER(Params), C.c_void_p, C.c_void_p, C.c_int, C.c_void_p,
                                              C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_void_p,
                                              C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64,
@@ -230,6 +240,60 @@ def align(prm: Params, read_packed, levels_packed, L, genome_packed, mask_packed
     _check(lib().stormgpu_align(C.byref(prm), _p(r), _p(q), L, _p(g), _p(m), n_codes, 0, _p(wins), n,
                                 _p(score), _p(bound), _p(best), _p(tbl), _p(tb), tbs))
     return score, bound, best, tbl, tb
+
+
+class Server:
+    """stormgpu_server_*: a resident -O chain (one seed family per step) serving batches
+    submitted from any thread; `slots` batches run at once within `budget_bytes` of device memory."""
+
+    def __init__(self, prm: Params, chain, slots: int = 2, budget_bytes: int = 16 << 30):
+        self.params = prm
+        self._h = C.c_void_p()
+        arr = (C.c_char_p * len(chain))(*[c.encode() for c in chain])
+        _check(lib().stormgpu_server_open(C.byref(prm), arr, len(chain), slots, budget_bytes, C.byref(self._h)))
+        self._live = {}
+
+    def add_reference(self, codes, mask, n_codes, regions=()):
+        rs = np.array([a for a, _ in regions] or [0], np.int32)
+        re = np.array([b for _, b in regions] or [0], np.int32)
+        _check(lib().stormgpu_server_add_reference(self._h, C.c_void_p(codes) if isinstance(codes, int) else _p(codes),
+                                                   C.c_void_p(mask) if isinstance(mask, int) else _p(mask), n_codes,
+                                                   _p(rs), _p(re), len(regions)))
+
+    def build(self):
+        _check(lib().stormgpu_server_build(self._h))
+
+    def submit(self, batch: ReadBatch, tb_stride=None) -> int:
+        if tb_stride is None:
+            tb_stride = ((int(batch.lengths.max()) + self.params.allowed_indels + 1) // 2 + 7) & ~7
+        res = MapResults(batch.n, tb_stride)
+        step = np.zeros(max(batch.n, 1), np.uint8)
+        rs, rr = batch.cstruct(), res.cstruct()
+        t = C.c_int64(0)
+        _check(lib().stormgpu_submit(self._h, C.byref(rs), C.byref(rr), _p(step), C.byref(t)))
+        self._live[t.value] = (batch, res, step, rs, rr)  # kept alive until done
+        return t.value
+
+    def poll(self, ticket: int, timeout_ms: int = -1):
+        """(results, step per read, latency ms) when done; None if not done within timeout_ms."""
+        lat = C.c_double(0)
+        rc = lib().stormgpu_poll(self._h, ticket, timeout_ms, C.byref(lat))
+        if rc == 1:
+            return None
+        batch, res, step, _, _ = self._live.pop(ticket)
+        _check(rc)
+        return res, step[:batch.n], lat.value
+
+    def close(self):
+        if self._h:
+            lib().stormgpu_server_close(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def align_noalloc(prm: Params, read, levels, L, genome, mask, n_codes, win, n, score, bound, best, tb_len, tb,

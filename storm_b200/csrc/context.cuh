@@ -1,0 +1,81 @@
+// context.cuh -- the mapping context behind the C ABI (stormgpu.cu) and the server
+// (server.cu): the device copies of the reference sequences and their indexes, and the
+// per-batch working buffers.
+#pragma once
+
+#include <algorithm>
+#include <vector>
+
+#include "common.cuh"
+#include "index_build.cuh"
+
+namespace sg {
+
+struct RefSeq {
+  int64_t n = 0;
+  uint8_t* d_gexp_alloc = nullptr;
+  uint8_t* d_gexp = nullptr;     // byte-expanded codes (filter streams)
+  uint8_t* d_codes_alloc = nullptr;
+  uint8_t* d_mask_alloc = nullptr;
+  uint8_t* d_codes = nullptr;
+  uint8_t* d_mask = nullptr;
+  std::vector<int32_t> rs, re;
+  std::vector<DevIndex> idx;
+};
+
+template <typename T>
+struct DevBuf {
+  T* p = nullptr;
+  int64_t cap = 0;
+  int grow(int64_t n) {
+    if (n <= cap) return 0;
+    if (p) cudaFree(p);
+    p = nullptr;
+    int64_t c = std::max<int64_t>(n, cap + cap / 2);
+    if (cudaMalloc(&p, sizeof(T) * (size_t)std::max<int64_t>(c, 1)) != cudaSuccess) {
+      cudaGetLastError();
+      cap = 0;
+      sg_set_error("device allocation of %lld bytes failed", (long long)(sizeof(T) * c));
+      return STORMGPU_ENOMEM;
+    }
+    cap = c;
+    return 0;
+  }
+  void release() { if (p) cudaFree(p); p = nullptr; cap = 0; }
+};
+
+
+}  // namespace sg
+
+struct stormgpu_ctx {
+  bool owns_refs = true;  // false: a view of another context's sequences and indexes
+  stormgpu_params p;
+  sg::SeedSet seeds;
+  cudaStream_t st = nullptr;
+  std::vector<sg::RefSeq> refs;
+  bool indexed = false;
+  stormgpu_stats stats;
+  // per-batch read buffers
+  sg::DevBuf<uint8_t> rcodes, rlevels, fcodes, flevels, first_levels;
+  sg::DevBuf<int16_t> lengths;
+  sg::DevBuf<stormgpu_hit> hits;
+  sg::DevBuf<uint8_t> tb, mapped;
+  // pass buffers
+  sg::DevBuf<int32_t> pstart, pcount, p_read, p_diag, big_list, big_count, huge_list, huge_h;
+  sg::DevBuf<int64_t> scan_tmp64, foff;
+  sg::DevBuf<int32_t> fr, fd;
+  sg::DevBuf<uint8_t> flag, rexp;
+  sg::DevBuf<int32_t> a_score, a_bound, a_tblen, big_tmp;
+  sg::DevBuf<int16_t> a_pos;
+  sg::DevBuf<uint8_t> a_tb;
+  sg::DevBuf<uint32_t> scratch;
+  sg::DevBuf<unsigned long long> counters;
+  cudaEvent_t ev[8];
+};
+
+namespace sg {
+
+// One batch on c's stream (every pointer in reads / out on the device); synchronous.
+int map_device_impl(stormgpu_ctx* c, const stormgpu_reads* reads, stormgpu_results* out);
+
+}  // namespace sg

@@ -18,7 +18,6 @@
 
 namespace sg {
 
-__constant__ SeedSet c_gseeds;
 
 // Seed key at read position rp; codes beyond the read's end read as 0 (seed.c:203-213).
 __device__ __forceinline__ uint32_t read_key(const SeedDev& s, const uint8_t* rd, int L, int rp) {
@@ -35,9 +34,9 @@ __device__ __forceinline__ int seed_npos(const SeedDev& s, int L) {
 }
 
 // (index offset, count, read position) of item t of seed si
-__device__ __forceinline__ void seed_item(const IndexView& ix, int si, int t, const uint8_t* read, int L,
-                                          int& a, int& cnt, int& rp) {
-  const SeedDev& s = c_gseeds.s[si];
+__device__ __forceinline__ void seed_item(const SeedSet& gs, const IndexView& ix, int si, int t, const uint8_t* read,
+                                          int L, int& a, int& cnt, int& rp) {
+  const SeedDev& s = gs.s[si];
   a = 0; cnt = 0; rp = 0;
   if (t >= seed_npos(s, L)) return;
   rp = s.n_positions ? s.positions[t] : t;
@@ -280,7 +279,8 @@ constexpr int kReadBytes = STORMGPU_MAX_READ_LEN / 4 + 16;
 
 constexpr int kItems = 4;  // (seed, position) items per lane and round: 128 key lookups in flight per warp
 
-__global__ void __launch_bounds__(kGWarps * 32) gather_fused_kernel(ReadsDev rd, IndexView ix, int I, GatherOut go) {
+__global__ void __launch_bounds__(kGWarps * 32) gather_fused_kernel(ReadsDev rd, IndexView ix, int I, GatherOut go,
+                                                                   const __grid_constant__ SeedSet gs) {
   __shared__ int32_t sm[kGWarps][2 * kWarpCap];  // gathered positions, then the set / sorted copy
   __shared__ int32_t shist[kGWarps][32];
   __shared__ int32_t soff[kGWarps][kMaxSeeds + 1];  // first item of every seed, for the current read
@@ -288,7 +288,7 @@ __global__ void __launch_bounds__(kGWarps * 32) gather_fused_kernel(ReadsDev rd,
   __shared__ const int32_t* s_map[kMaxSeeds];
   __shared__ __align__(16) uint8_t srd[kGWarps][kReadBytes];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const int nseeds = c_gseeds.n;
+  const int nseeds = gs.n;
   if (threadIdx.x < nseeds) {
     s_first[threadIdx.x] = ix.first[threadIdx.x];
     s_map[threadIdx.x] = ix.map[threadIdx.x];
@@ -305,7 +305,7 @@ __global__ void __launch_bounds__(kGWarps * 32) gather_fused_kernel(ReadsDev rd,
       const uint8_t* src = rd.codes + r * rd.cstride;
       const int nb = (L + 3) >> 2;
       for (int b = lane; b < nb; b += 32) rs[b] = src[b];
-      const int np = lane < nseeds ? seed_npos(c_gseeds.s[lane], L) : 0;
+      const int np = lane < nseeds ? seed_npos(gs.s[lane], L) : 0;
       const int incl = warp_incl_scan(np);
       if (lane <= nseeds) so[lane] = incl - np;
       __syncwarp();
@@ -323,7 +323,7 @@ __global__ void __launch_bounds__(kGWarps * 32) gather_fused_kernel(ReadsDev rd,
         if (it < T)
           while (it >= so[si + 1]) ++si;
         sid[m] = si;
-        item_lookup(s_first[si], c_gseeds.s[si], it < T ? it - so[si] : 0x40000000, read, L, a[m], cnt[m], rp[m]);
+        item_lookup(s_first[si], gs.s[si], it < T ? it - so[si] : 0x40000000, read, L, a[m], cnt[m], rp[m]);
         lookups += it < T ? 1 : 0;
       }
       // ... then one scan places all of them, and the position loads go out together
@@ -390,7 +390,8 @@ __global__ void __launch_bounds__(kGWarps * 32) gather_fused_kernel(ReadsDev rd,
 // positions) or, when gbuf is given, in that global buffer.  Reads with more than `cap`
 // positions are recorded in the huge list with their count.
 __global__ void gather_block_kernel(ReadsDev rd, IndexView ix, int I, const int32_t* __restrict__ list, GatherOut go,
-                                    int cap, int32_t* gbuf, int32_t* huge_list, int32_t* huge_h, int32_t* huge_count) {
+                                    int cap, int32_t* gbuf, int32_t* huge_list, int32_t* huge_h, int32_t* huge_count,
+                                    const __grid_constant__ SeedSet gs) {
   extern __shared__ int32_t dsm[];
   __shared__ int wtot[32];
   __shared__ int s_H;
@@ -401,12 +402,12 @@ __global__ void gather_block_kernel(ReadsDev rd, IndexView ix, int I, const int3
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
   if (threadIdx.x == 0) s_H = 0;
   __syncthreads();
-  for (int si = 0; si < c_gseeds.n; ++si) {
-    const int np = seed_npos(c_gseeds.s[si], L);
+  for (int si = 0; si < gs.n; ++si) {
+    const int np = seed_npos(gs.s[si], L);
     const int32_t* mp = ix.map[si];
     for (int t0 = 0; t0 < np; t0 += blockDim.x) {
       int a, cnt, rp;
-      seed_item(ix, si, t0 + threadIdx.x, read, L, a, cnt, rp);
+      seed_item(gs, ix, si, t0 + threadIdx.x, read, L, a, cnt, rp);
       const int incl = warp_incl_scan(cnt);
       if (lane == 31) wtot[w] = incl;
       __syncthreads();
@@ -475,20 +476,17 @@ __global__ void gather_block_kernel(ReadsDev rd, IndexView ix, int I, const int3
   }
 }
 
-void upload_gather_seeds(const SeedSet& seeds, cudaStream_t st) {
-  cudaMemcpyToSymbolAsync(c_gseeds, &seeds, sizeof(SeedSet), 0, cudaMemcpyHostToDevice, st);
-}
-
-void launch_gather_fused(const ReadsDev& rd, const IndexView& ix, int I, const GatherOut& go, cudaStream_t st) {
+void launch_gather_fused(const ReadsDev& rd, const IndexView& ix, int I, const GatherOut& go, const SeedSet& seeds,
+                         cudaStream_t st) {
   if (rd.n <= 0) return;
   int64_t blocks = (rd.n + kGWarps - 1) / kGWarps;
   if (blocks > 148 * 16) blocks = 148 * 16;
-  gather_fused_kernel<<<(unsigned)blocks, kGWarps * 32, 0, st>>>(rd, ix, I, go);
+  gather_fused_kernel<<<(unsigned)blocks, kGWarps * 32, 0, st>>>(rd, ix, I, go, seeds);
 }
 
 void launch_gather_block(const ReadsDev& rd, const IndexView& ix, int I, const int32_t* list, int nlist,
                          const GatherOut& go, int32_t* gbuf, int gcap, int32_t* huge_list, int32_t* huge_h,
-                         int32_t* huge_count, cudaStream_t st) {
+                         int32_t* huge_count, const SeedSet& seeds, cudaStream_t st) {
   if (nlist <= 0) return;
   const int smem_cap = kBlockGatherCap;
   static bool attr = false;
@@ -497,10 +495,11 @@ void launch_gather_block(const ReadsDev& rd, const IndexView& ix, int I, const i
     attr = true;
   }
   if (gbuf)
-    gather_block_kernel<<<nlist, 1024, 0, st>>>(rd, ix, I, list, go, gcap, gbuf, huge_list, huge_h, huge_count);
+    gather_block_kernel<<<nlist, 1024, 0, st>>>(rd, ix, I, list, go, gcap, gbuf, huge_list, huge_h, huge_count,
+                                                 seeds);
   else
     gather_block_kernel<<<nlist, 1024, smem_cap * 4, st>>>(rd, ix, I, list, go, smem_cap, nullptr, huge_list,
-                                                              huge_h, huge_count);
+                                                              huge_h, huge_count, seeds);
 }
 
 }  // namespace sg

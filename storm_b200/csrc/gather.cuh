@@ -16,12 +16,14 @@ struct GatherOut {
 
 constexpr int kBlockGatherCap = 32768;
 
-void upload_gather_seeds(const SeedSet& seeds, cudaStream_t st);
-void launch_gather_fused(const ReadsDev& rd, const IndexView& ix, int I, const GatherOut& go, cudaStream_t st);
+// The seed family travels with every launch (a kernel parameter), so that mapping calls with
+// different seed families can run concurrently on different streams.
+void launch_gather_fused(const ReadsDev& rd, const IndexView& ix, int I, const GatherOut& go, const SeedSet& seeds,
+                         cudaStream_t st);
 // one block per listed read; gbuf == nullptr: shared memory (kBlockGatherCap positions),
 // reads beyond it are appended to (huge_list, huge_h); else the global buffer gbuf of gcap.
 void launch_gather_block(const ReadsDev& rd, const IndexView& ix, int I, const int32_t* list, int nlist,
                          const GatherOut& go, int32_t* gbuf, int gcap, int32_t* huge_list, int32_t* huge_h,
-                         int32_t* huge_count, cudaStream_t st);
+                         int32_t* huge_count, const SeedSet& seeds, cudaStream_t st);
 
 }  // namespace sg

@@ -14,6 +14,7 @@
 #include "scan.cuh"
 #include "sw_filter.cuh"
 #include "gather.cuh"
+#include "context.cuh"
 
 static thread_local char g_err[1024];
 
@@ -113,67 +114,7 @@ ScoreParams make_score_params(const stormgpu_params& p) {
 
 }  // namespace sg
 
-namespace {
 
-struct RefSeq {
-  int64_t n = 0;
-  uint8_t* d_gexp_alloc = nullptr;
-  uint8_t* d_gexp = nullptr;     // byte-expanded codes (filter streams)
-  uint8_t* d_codes_alloc = nullptr;
-  uint8_t* d_mask_alloc = nullptr;
-  uint8_t* d_codes = nullptr;
-  uint8_t* d_mask = nullptr;
-  std::vector<int32_t> rs, re;
-  std::vector<DevIndex> idx;
-};
-
-template <typename T>
-struct DevBuf {
-  T* p = nullptr;
-  int64_t cap = 0;
-  int grow(int64_t n) {
-    if (n <= cap) return 0;
-    if (p) cudaFree(p);
-    p = nullptr;
-    int64_t c = std::max<int64_t>(n, cap + cap / 2);
-    if (cudaMalloc(&p, sizeof(T) * (size_t)std::max<int64_t>(c, 1)) != cudaSuccess) {
-      cudaGetLastError();
-      cap = 0;
-      sg_set_error("device allocation of %lld bytes failed", (long long)(sizeof(T) * c));
-      return STORMGPU_ENOMEM;
-    }
-    cap = c;
-    return 0;
-  }
-  void release() { if (p) cudaFree(p); p = nullptr; cap = 0; }
-};
-
-}  // namespace
-
-struct stormgpu_ctx {
-  stormgpu_params p;
-  SeedSet seeds;
-  cudaStream_t st = nullptr;
-  std::vector<RefSeq> refs;
-  bool indexed = false;
-  stormgpu_stats stats;
-  // per-batch read buffers
-  DevBuf<uint8_t> rcodes, rlevels, fcodes, flevels, first_levels;
-  DevBuf<int16_t> lengths;
-  DevBuf<stormgpu_hit> hits;
-  DevBuf<uint8_t> tb, mapped;
-  // pass buffers
-  DevBuf<int32_t> pstart, pcount, p_read, p_diag, big_list, big_count, huge_list, huge_h;
-  DevBuf<int64_t> scan_tmp64, foff;
-  DevBuf<int32_t> fr, fd;
-  DevBuf<uint8_t> flag, rexp;
-  DevBuf<int32_t> a_score, a_bound, a_tblen, big_tmp;
-  DevBuf<int16_t> a_pos;
-  DevBuf<uint8_t> a_tb;
-  DevBuf<uint32_t> scratch;
-  DevBuf<unsigned long long> counters;
-  cudaEvent_t ev[8];
-};
 
 extern "C" int stormgpu_open(const stormgpu_params* params, const char* seeds, stormgpu_ctx** out) {
   if (!params || !out) { sg_set_error("null argument"); return STORMGPU_EINVAL; }
@@ -216,12 +157,13 @@ extern "C" void stormgpu_close(stormgpu_ctx* c) {
   if (!c) return;
   cudaSetDevice(c->p.device);
   cudaStreamSynchronize(c->st);
-  for (auto& r : c->refs) {
-    cudaFree(r.d_codes_alloc);
-    cudaFree(r.d_mask_alloc);
-    cudaFree(r.d_gexp_alloc);
-    for (auto& ix : r.idx) { cudaFree(ix.first); cudaFree(ix.map); }
-  }
+  if (c->owns_refs)
+    for (auto& r : c->refs) {
+      cudaFree(r.d_codes_alloc);
+      cudaFree(r.d_mask_alloc);
+      cudaFree(r.d_gexp_alloc);
+      for (auto& ix : r.idx) { cudaFree(ix.first); cudaFree(ix.map); }
+    }
   c->rcodes.release(); c->rlevels.release(); c->fcodes.release(); c->flevels.release();
   c->first_levels.release(); c->lengths.release(); c->hits.release(); c->tb.release();
   c->mapped.release();
@@ -296,7 +238,7 @@ extern "C" int stormgpu_build_index(stormgpu_ctx* c) {
   return 0;
 }
 
-static int map_device_impl(stormgpu_ctx* c, const stormgpu_reads* reads, stormgpu_results* out) {
+int sg::map_device_impl(stormgpu_ctx* c, const stormgpu_reads* reads, stormgpu_results* out) {
   if (!c->indexed) { sg_set_error("stormgpu_build_index must be called before mapping"); return STORMGPU_ESTATE; }
   cudaStream_t st = c->st;
   const int64_t n = reads->n;
@@ -337,7 +279,6 @@ static int map_device_impl(stormgpu_ctx* c, const stormgpu_reads* reads, stormgp
       c->counters.grow(16) || c->fr.grow(std::max<int64_t>(n * 64, 1 << 20)) ||
       c->fd.grow(std::max<int64_t>(n * 64, 1 << 20)))
     return STORMGPU_ENOMEM;
-  upload_gather_seeds(c->seeds, st);
   const int BW = 2 * sp.I + 1;
   const int wpr = (2 * BW + 31) / 32 + (sp.colour ? (BW + 31) / 32 : 0);
   const int64_t tbs = ((maxL + sp.I + 1) / 2 + 7) & ~7LL;
@@ -361,27 +302,28 @@ static int map_device_impl(stormgpu_ctx* c, const stormgpu_reads* reads, stormgp
         GatherOut go;
         go.fr = c->fr.p; go.fd = c->fd.p; go.cap = c->fr.cap; go.counters = c->counters.p;
         go.big_list = c->big_list.p; go.big_count = c->big_count.p;
-        launch_gather_fused(rd, ix, sp.I, go, st);
+        launch_gather_fused(rd, ix, sp.I, go, c->seeds, st);
         launches++;
         int32_t nbig[2] = {0, 0};
         SG_CUDA(cudaMemcpyAsync(nbig, c->big_count.p, sizeof(nbig), cudaMemcpyDeviceToHost, st));
         SG_CUDA(cudaStreamSynchronize(st));
         if (nbig[0] > 0) {
           launch_gather_block(rd, ix, sp.I, c->big_list.p, nbig[0], go, nullptr, 0, c->huge_list.p, c->huge_h.p,
-                              c->big_count.p + 1, st);
+                              c->big_count.p + 1, c->seeds, st);
           launches++;
           SG_CUDA(cudaMemcpyAsync(nbig, c->big_count.p, sizeof(nbig), cudaMemcpyDeviceToHost, st));
           SG_CUDA(cudaStreamSynchronize(st));
           if (nbig[1] > 0) {
             std::vector<int32_t> hl(nbig[1]), hh(nbig[1]);
-            SG_CUDA(cudaMemcpy(hl.data(), c->huge_list.p, sizeof(int32_t) * nbig[1], cudaMemcpyDeviceToHost));
-            SG_CUDA(cudaMemcpy(hh.data(), c->huge_h.p, sizeof(int32_t) * nbig[1], cudaMemcpyDeviceToHost));
+            SG_CUDA(cudaMemcpyAsync(hl.data(), c->huge_list.p, sizeof(int32_t) * nbig[1], cudaMemcpyDeviceToHost, st));
+            SG_CUDA(cudaMemcpyAsync(hh.data(), c->huge_h.p, sizeof(int32_t) * nbig[1], cudaMemcpyDeviceToHost, st));
+            SG_CUDA(cudaStreamSynchronize(st));
             for (int k = 0; k < nbig[1]; ++k) {
               int64_t P = 1;
               while (P < hh[k]) P <<= 1;
               if (c->big_tmp.grow(P)) return STORMGPU_ENOMEM;
               launch_gather_block(rd, ix, sp.I, c->huge_list.p + k, 1, go, c->big_tmp.p, (int)P, c->huge_list.p,
-                                  c->huge_h.p, c->big_count.p + 1, st);
+                                  c->huge_h.p, c->big_count.p + 1, c->seeds, st);
               launches++;
             }
           }
