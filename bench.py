@@ -199,6 +199,132 @@ def reference_arm(a, w, ref, reads, d):
     print(json.dumps(line))
 
 
+def serving_arm(a, w, ref_path, reads_path, d):
+    """The served -O chain (configuration 3): the workload's reads split into batches of
+    log-uniform sizes (1k to 1M reads, scaled), arriving as a Poisson process (seed 7).  The same
+    batches first go through the plain per-batch path (each chain step mapped with stormgpu_map,
+    the unmapped reads picked on the host, one batch at a time); then the server takes them as
+    they arrive (continuous batching over 3 worker streams).  Reports the served reads/s, the
+    plain reads/s, p50/p99 batch latency, and checks that both give the same records."""
+    import threading
+
+    import numpy as np
+
+    from storm_b200 import api, build, host
+    build.build()
+    prm_d, _ = parse_cli_args(w["args"])
+    prm = api.params(colour=0, **prm_d)
+    chain = w["chain"]
+    reads = host.ReadSet(reads_path, 0)
+    reference = host.Reference(ref_path, 0)
+    rng = np.random.default_rng(7)
+    perm = rng.permutation(reads.n)
+    lo, hi = max(1, int(1000 * a.scale)), max(2, int(1000000 * a.scale))
+    batches, k = [], 0
+    while k < reads.n:
+        size = int(np.exp(rng.uniform(np.log(lo), np.log(hi))))
+        idx = np.sort(perm[k:k + size])
+        k += size
+        batches.append(api.ReadBatch(reads.codes[idx], reads.lengths[idx], reads.levels[idx]))
+    tbs = ((reads.max_len + prm.allowed_indels + 1) // 2 + 7) & ~7
+    total = sum(b.n for b in batches)
+
+    # plain per-batch path: one mapper (resident index) per chain step, batches one at a time
+    mappers = []
+    for seeds in chain:
+        m = api.Mapper(prm, seeds)
+        reference.add_to(m)
+        m.build_index()
+        mappers.append(m)
+
+    def plain(batch):
+        n = batch.n
+        out = api.MapResults(n, tbs)
+        step = np.full(n, 255, np.uint8)
+        ids, cur = np.arange(n), batch
+        for s, m in enumerate(mappers):
+            if cur.n == 0:
+                break
+            res = m.map(cur, tbs)
+            got = np.nonzero(res.mapped != 0)[0]
+            o = ids[got]
+            for q in range(4):
+                out.hits[4 * o + q] = res.hits[4 * got + q]
+                out.tb[4 * o + q] = res.tb[4 * got + q]
+            out.mapped[o] = 1
+            step[o] = s
+            keep = np.nonzero(res.mapped == 0)[0]
+            ids = ids[keep]
+            cur = api.ReadBatch(cur.codes[keep], cur.lengths[keep], cur.levels[keep])
+        return out, step
+
+    plain(batches[0])  # warm-up
+    t0 = time.perf_counter()
+    ref_out = [plain(b) for b in batches]
+    t_plain = time.perf_counter() - t0
+    for m in mappers:
+        m.close()
+    plain_rate = total / t_plain
+
+    # served: capacity with every batch waiting at once, then batch latency under Poisson
+    # arrivals at 80 % of that capacity
+    srv = api.Server(prm, chain, slots=3, budget_bytes=48 << 30)
+    reference.add_to_server(srv)
+    srv.build()
+    srv.poll(srv.submit(batches[0], tbs))  # warm-up
+
+    def serve(arrivals):
+        tickets = [None] * len(batches)
+        start = time.perf_counter()
+
+        def submitter():
+            for i, b in enumerate(batches):
+                dt = start + arrivals[i] - time.perf_counter()
+                if dt > 0:
+                    time.sleep(dt)
+                tickets[i] = srv.submit(b, tbs)
+
+        th = threading.Thread(target=submitter)
+        th.start()
+        lat, outs = [], []
+        for i in range(len(batches)):
+            while tickets[i] is None:
+                time.sleep(0.0005)
+            res, step, ms = srv.poll(tickets[i])
+            lat.append(ms)
+            outs.append((res, step))
+        el = time.perf_counter() - start
+        th.join()
+        return el, lat, outs
+
+    t_served, _, outs = serve(np.zeros(len(batches)))
+    cap = total / t_served
+    gaps = rng.exponential(total / (0.8 * cap) / len(batches), size=len(batches))
+    _, lat, outs2 = serve(np.concatenate([[0.0], np.cumsum(gaps[:-1])]))
+    srv.close()
+    same = True
+    for (res, step), (pres, pstep) in list(zip(outs, ref_out)) + list(zip(outs2, ref_out)):
+        live = np.repeat(pres.mapped != 0, 4)
+        same &= bool(np.array_equal(step, pstep) and np.array_equal(res.mapped != 0, pres.mapped != 0) and
+                     res.hits[live].tobytes() == pres.hits[live].tobytes())
+    served_rate = total / t_served
+    line = {"metric": "served reads/sec (3-step -O chain, continuous batching)", "value": served_rate,
+            "unit": "reads/s", "n_gpus": 1, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "u8/int32", "data": "synthetic",
+            "config": {"workload": workload_name(a.cfg, a.scale), "reads": total, "batches": len(batches),
+                       "batch_sizes": [b.n for b in batches], "chain": chain, "args": " ".join(w["args"]),
+                       "arrivals": "capacity: all batches at once; latency: Poisson at 80 % of capacity",
+                       "slots": 3},
+            "serving": {"p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+                        "plain_reads_per_s": plain_rate, "served_over_plain": served_rate / plain_rate,
+                        "same_records": same},
+            "e2e": {"value": served_rate, "unit": "reads/s",
+                    "h2d_bytes_per_step": int(sum(b.codes.nbytes + b.levels.nbytes + b.lengths.nbytes for b in batches)),
+                    "d2h_bytes_per_step": int(sum(b.n * (4 * 28 + 4 * tbs + 2) for b in batches)),
+                    "includes": "host buffers in, every chain step, results out"}}
+    print(json.dumps(line))
+
+
 def workload_name(cfg, scale):
     names = {0: "cfg0 nucleotide 1 Mbp, 100k x 50 bp", 1: "cfg1 colour 10 Mbp, 2M x 50 colours",
              2: "cfg2 nucleotide 100 Mbp, 10M x 35-150 bp, -i 15", 3: "cfg3 served -O chain",
@@ -227,6 +353,12 @@ def main():
             return
         w, ref, reads, d = workload_files(a.cfg, a.scale, 0)
         reference_arm(a, w, ref, reads, d)
+        return
+
+    if a.cfg == 3:
+        if rank == 0:
+            w, ref_path, reads_path, d = workload_files(a.cfg, a.scale, 0)
+            serving_arm(a, w, ref_path, reads_path, d)
         return
 
     import torch

@@ -122,8 +122,12 @@ struct BandWindow {
 };
 
 // BWT > 0: the band width 2I + 1 as a constant, so that the row arrays live in registers;
-// BWT = 0: any width up to kMaxBand (arrays in local memory).
-template <int BWT>
+// BWT = 0: any width up to kMaxBand (arrays in local memory).  CM: 0 nucleotide, 1 colour
+// space (the colour state machine compiled in), -1 either (sp.colour).
+// A candidate whose running abort bound falls below -t stops at that row: the replay
+// threshold never is below -t, so it is aborted whatever comes before it, and neither its score
+// nor its traceback is read.
+template <int BWT, int CM>
 __global__ void __launch_bounds__(128) align_kernel(ReadsDev rd, ScoreParams sp, const uint8_t* __restrict__ genome,
                                                     const uint8_t* __restrict__ mask, int64_t slot0, int64_t nslots,
                                                     PassBuffers pb) {
@@ -133,7 +137,7 @@ __global__ void __launch_bounds__(128) align_kernel(ReadsDev rd, ScoreParams sp,
   const int64_t slot = slot0 + sl;
   const int r = pb.p_read[slot];
   const int d = pb.p_diag[slot];
-  const int I = sp.I, BW = BWT > 0 ? BWT : 2 * I + 1, colour = sp.colour;
+  const int I = sp.I, BW = BWT > 0 ? BWT : 2 * I + 1, colour = CM >= 0 ? CM : sp.colour;
   const int L = rd.lengths[r];
   const uint8_t* rdc = rd.codes + (int64_t)r * rd.cstride;
   const uint8_t* rdq = rd.levels ? rd.levels + (int64_t)r * rd.lstride : nullptr;
@@ -242,6 +246,7 @@ __global__ void __launch_bounds__(128) align_kernel(ReadsDev rd, ScoreParams sp,
     for (int k = 0; k < wpr_dir; ++k) scr[((int64_t)i * wpr + k) * ns + sl] = wd[k];
     if (colour)
       for (int k = wpr_dir; k < wpr; ++k) scr[((int64_t)i * wpr + k) * ns + sl] = wc[k - wpr_dir];
+    if (bound < sp.min_score) break;  // aborted at any threshold
   }
   int best = kMinScore, bi = -1, bj = -1;
 #pragma unroll
@@ -300,13 +305,19 @@ void launch_align(const ReadsDev& r, const ScoreParams& sp, const uint8_t* genom
                   cudaStream_t st) {
   if (nslots <= 0) return;
   const unsigned blocks = (unsigned)((nslots + 127) / 128);
+#define SG_ALIGN(BW)                                                                                    \
+  case BW:                                                                                              \
+    if (sp.colour) align_kernel<BW, 1><<<blocks, 128, 0, st>>>(r, sp, genome, mask, slot0, nslots, pb); \
+    else align_kernel<BW, 0><<<blocks, 128, 0, st>>>(r, sp, genome, mask, slot0, nslots, pb);           \
+    break;
   switch (2 * sp.I + 1) {
-  case 7: align_kernel<7><<<blocks, 128, 0, st>>>(r, sp, genome, mask, slot0, nslots, pb); break;
-  case 15: align_kernel<15><<<blocks, 128, 0, st>>>(r, sp, genome, mask, slot0, nslots, pb); break;
-  case 31: align_kernel<31><<<blocks, 128, 0, st>>>(r, sp, genome, mask, slot0, nslots, pb); break;
-  case 41: align_kernel<41><<<blocks, 128, 0, st>>>(r, sp, genome, mask, slot0, nslots, pb); break;
-  default: align_kernel<0><<<blocks, 128, 0, st>>>(r, sp, genome, mask, slot0, nslots, pb); break;
+    SG_ALIGN(7)
+    SG_ALIGN(15)
+    SG_ALIGN(31)
+    SG_ALIGN(41)
+  default: align_kernel<0, -1><<<blocks, 128, 0, st>>>(r, sp, genome, mask, slot0, nslots, pb); break;
   }
+#undef SG_ALIGN
 }
 
 // ------------------------------------------------------------------------------ replay

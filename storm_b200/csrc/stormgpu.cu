@@ -238,7 +238,13 @@ extern "C" int stormgpu_build_index(stormgpu_ctx* c) {
   return 0;
 }
 
-int sg::map_device_impl(stormgpu_ctx* c, const stormgpu_reads* reads, stormgpu_results* out) {
+// Candidate lists of one strand pass are bounded: a batch that would need more is mapped in
+// halves (reads are independent, so the results are the same).
+constexpr int64_t kMaxCandidatesPerPass = 1000000000;
+constexpr int64_t kMaxPassingPerPass = 100000000;  // their tracebacks are kept until the replay
+constexpr int kSplitBatch = 1;
+
+static int map_device_once(stormgpu_ctx* c, const stormgpu_reads* reads, stormgpu_results* out) {
   if (!c->indexed) { sg_set_error("stormgpu_build_index must be called before mapping"); return STORMGPU_ESTATE; }
   cudaStream_t st = c->st;
   const int64_t n = reads->n;
@@ -332,6 +338,7 @@ int sg::map_device_impl(stormgpu_ctx* c, const stormgpu_reads* reads, stormgpu_r
         SG_CUDA(cudaMemcpyAsync(g, c->counters.p, sizeof(g), cudaMemcpyDeviceToHost, st));
         SG_CUDA(cudaStreamSynchronize(st));
         utot = (int64_t)g[7];
+        if (utot > kMaxCandidatesPerPass) return kSplitBatch;
         if (!g[8]) break;
         if (attempt > 2) { sg_set_error("internal: candidate list overflow"); return STORMGPU_EINVAL; }
         if (c->fr.grow(utot + utot / 4 + 1024) || c->fd.grow(utot + utot / 4 + 1024)) return STORMGPU_ENOMEM;
@@ -365,6 +372,7 @@ int sg::map_device_impl(stormgpu_ctx* c, const stormgpu_reads* reads, stormgpu_r
       S.seed_lookups += (int64_t)cnt[3];
       S.hit_positions += (int64_t)cnt[4];
       S.filter_passed += npass;
+      if (npass > kMaxPassingPerPass && n > 1) return kSplitBatch;
       PassBuffers pb;
       memset(&pb, 0, sizeof(pb));
       pb.pstart = c->pstart.p; pb.pcount = c->pcount.p;
@@ -413,6 +421,38 @@ int sg::map_device_impl(stormgpu_ctx* c, const stormgpu_reads* reads, stormgpu_r
   cudaEventElapsedTime(&tt, c->ev[6], c->ev[7]);
   S.ms_gather = tg; S.ms_filter = tf; S.ms_align = ta; S.ms_replay = tr; S.ms_total = tt;
   S.kernels = launches;
+  return 0;
+}
+
+int sg::map_device_impl(stormgpu_ctx* c, const stormgpu_reads* reads, stormgpu_results* out) {
+  const int rc = map_device_once(c, reads, out);
+  if (rc != kSplitBatch) return rc;
+  const int64_t n = reads->n;
+  if (n <= 1) {
+    sg_set_error("one read has more than %lld candidate diagonals", (long long)kMaxCandidatesPerPass);
+    return STORMGPU_ENOMEM;
+  }
+  const int64_t h = n / 2;
+  stormgpu_reads r1 = *reads, r2 = *reads;
+  stormgpu_results o1 = *out, o2 = *out;
+  r1.n = h;
+  r2.n = n - h;
+  r2.codes += h * reads->code_stride;
+  if (r2.levels) r2.levels += h * reads->level_stride;
+  r2.lengths += h;
+  if (r2.first_levels) r2.first_levels += h;
+  o2.hits += 4 * h;
+  o2.tb += 4 * h * out->tb_stride;
+  o2.mapped += h;
+  if (const int e = map_device_impl(c, &r1, &o1)) return e;
+  const stormgpu_stats s1 = c->stats;
+  if (const int e = map_device_impl(c, &r2, &o2)) return e;
+  stormgpu_stats& S = c->stats;
+  S.candidates += s1.candidates; S.filter_passed += s1.filter_passed; S.aligned += s1.aligned;
+  S.seed_lookups += s1.seed_lookups; S.hit_positions += s1.hit_positions; S.filter_cells += s1.filter_cells;
+  S.align_cells += s1.align_cells; S.kernels += s1.kernels; S.filter_band_cells += s1.filter_band_cells;
+  S.ms_gather += s1.ms_gather; S.ms_filter += s1.ms_filter; S.ms_align += s1.ms_align;
+  S.ms_replay += s1.ms_replay; S.ms_total += s1.ms_total;
   return 0;
 }
 

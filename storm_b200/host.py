@@ -74,6 +74,10 @@ class Reference:
                                                         C.c_void_p(rs.ctypes.data), C.c_void_p(re.ctypes.data),
                                                         len(regs)))
 
+    def add_to_server(self, server: api.Server):
+        for codes, mask, n, regs in self.sequences():
+            server.add_reference(codes, mask, n, regs)
+
     def __del__(self):
         try:
             hostlib().sh_free_reference(C.byref(self._s))
