@@ -171,6 +171,15 @@ int stormgpu_submit(stormgpu_server *s, const stormgpu_reads *reads, stormgpu_re
 int stormgpu_poll(stormgpu_server *s, int64_t ticket, int timeout_ms, double *latency_ms);
 void stormgpu_server_close(stormgpu_server *s);
 
+/* Greedy placement of the mapping without -M (-G; genome_map.c:187-214, order of
+ * genome_map.c:551-796): the reads whose rank-0 alignment exists -- and, when
+ * uniqueness_threshold > 0 (-u), whose rank-0 score leads the rank-1 score by at least that --
+ * in (sequence, rank-0 start) order, reads of one position in read order.  Works on the results
+ * of the last stormgpu_map call on ctx, which stay on the device; order (host) holds n int32,
+ * *n_placed receives how many are placed. */
+int stormgpu_genome_map_greedy(stormgpu_ctx *ctx, int32_t uniqueness_threshold, int32_t *order,
+                               int64_t *n_placed);
+
 /* Statistics of the last stormgpu_map* call. */
 typedef struct stormgpu_stats {
   int64_t candidates;        /* diagonals produced by the hit gather */

@@ -28,7 +28,31 @@ static int oracle_map(void *user, const stormgpu_params *p, const char *seeds, c
   return rc;
 }
 
+/* greedy placement, restated: reads in read order, kept iff their rank-0 alignment exists (and
+ * leads rank 1 by the -u threshold), then a stable insertion into (sequence, start) order
+ * (genome_map.c:187-214, printed position-major by genome_map.c:551-796) */
+static int oracle_place_greedy(void *user, const sh_refs *refs, const stormgpu_results *res, int64_t n,
+                               int uniqueness_threshold, sh_placement *out, int64_t *n_out, char *err, int errlen) {
+  (void)user; (void)refs; (void)err; (void)errlen;
+  int64_t k = 0;
+  for (int64_t r = 0; r < n; ++r) {
+    const stormgpu_hit *h = &res->hits[r * 4];
+    if (!res->mapped[r] || h[0].ref_start == -1) continue;
+    if (uniqueness_threshold > 0 && !(h[0].score - h[1].score >= uniqueness_threshold)) continue;
+    int64_t j = k++;
+    while (j > 0) {  /* stable: move only past strictly later positions */
+      const stormgpu_hit *p = &res->hits[(int64_t)out[j - 1].read * 4];
+      if (p->ref_id < h[0].ref_id || (p->ref_id == h[0].ref_id && p->ref_start <= h[0].ref_start)) break;
+      out[j] = out[j - 1];
+      --j;
+    }
+    out[j] = (sh_placement){(int32_t)r, 0};
+  }
+  *n_out = k;
+  return 0;
+}
+
 int main(int argc, char **argv) {
-  storm_mapper m = {"oracle", oracle_map, NULL};
+  storm_mapper m = {"oracle", oracle_map, oracle_place_greedy, NULL, NULL};
   return storm_cli_main(argc, argv, STORM_COLOUR, &m);
 }

@@ -71,6 +71,9 @@ struct stormgpu_ctx {
   sg::DevBuf<uint32_t> scratch;
   sg::DevBuf<unsigned long long> counters;
   cudaEvent_t ev[8];
+  int64_t last_n = -1;  // reads of the last stormgpu_map call (its results stay in hits / mapped)
+  // genome_map placement
+  sg::DevBuf<uint32_t> gm_k0, gm_v0, gm_k1, gm_v1, gm_tmp, gm_base;
 };
 
 namespace sg {

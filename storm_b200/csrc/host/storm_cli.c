@@ -84,7 +84,7 @@ int storm_cli_main(int argc, char **argv, int colour, const storm_mapper *mapper
   int match = 5, mismatch = -4, gap_open = -9, gap_extend = -4;
   int allowed_indels = 3, simd_diags = 3, min_score = 115, min_score_filter = 100;
   int quality_base = 33, map_unordered = 0, print_all = 0, uniqueness = 0, uniq_thr = 0;
-  int stdev = 100, ignore_lower = 0, senses = 3;
+  int stdev = 100, ignore_lower = 0, senses = 3, map_greedy = 0;
   FILE *output = stdout, *unmapped = NULL;
   char *seeds = seeds_from_file(colour ? DEFAULT_SEED_FILE_COL : DEFAULT_SEED_FILE_NUC);
   if (!seeds) seeds = colour ? DEFAULT_SEEDS_COL : DEFAULT_SEEDS_NUC;
@@ -143,7 +143,7 @@ int storm_cli_main(int argc, char **argv, int colour, const storm_mapper *mapper
     case 'F': senses = 1; break;
     case 'R': senses = 2; break;
     case 'h': usage(argv[0], seeds); return 0;
-    case 'G': break;
+    case 'G': map_greedy = 1; break;
     case 'M':
       INTARG(map_unordered);
       if (map_unordered <= 0) FATAL_VALUE(map_unordered, "a strictly positive integer");
@@ -189,10 +189,6 @@ int storm_cli_main(int argc, char **argv, int colour, const storm_mapper *mapper
     err("\nNot enough mandatory parameters provided.\n");
     usage(argv[0], seeds);
     return 0;
-  }
-  if (!map_unordered) {
-    err("The per-position (ordered) mapping without -M is not part of this build; use -M <1..4>.");
-    exit(1);
   }
   if (min_score < STORMGPU_MIN_SCORE) {
     err("-t below %d is not supported.", STORMGPU_MIN_SCORE);
@@ -250,14 +246,42 @@ int storm_cli_main(int argc, char **argv, int colour, const storm_mapper *mapper
   so.colour = colour; so.max_rank = map_unordered; so.print_all = print_all;
   so.uniqueness = uniqueness; so.uniqueness_threshold = uniq_thr; so.min_score = min_score;
   so.delta_m = delta_m; so.quality_base = quality_base; so.argc = argc; so.argv = argv;
-  if (output) {
-    static char obuf[1 << 22];
-    setvbuf(output, obuf, _IOFBF, sizeof(obuf));
-    sh_write_sam(output, &so, &refs, &reads, &res, 0, reads.n, 1);
-    fflush(output);
+  if (map_unordered) {
+    if (output) {
+      static char obuf[1 << 22];
+      setvbuf(output, obuf, _IOFBF, sizeof(obuf));
+      sh_write_sam(output, &so, &refs, &reads, &res, 0, reads.n, 1);
+      fflush(output);
+    } else {
+      err("No file name provided for SAM output.");
+    }
   } else {
-    err("No file name provided for SAM output.");
+    /* the per-position map (genome_map, run.c:1025-1061) */
+    msg(1, "\n\nReference mapping...\n");
+    sh_placement *pl = malloc(sizeof(sh_placement) * (size_t)(reads.n ? reads.n : 1));
+    int64_t npl = 0;
+    if (map_greedy) {
+      if (!mapper->place_greedy ||
+          mapper->place_greedy(mapper->user, &refs, &res, reads.n, uniqueness ? uniq_thr : 0, pl, &npl, emsg,
+                               sizeof(emsg)) != 0) {
+        err("Mapping failed (%s): %s", mapper->name, emsg);
+        exit(2);
+      }
+    } else {
+      sh_genome_map_contextual(&refs, &res, reads.n, colour, allowed_indels, match, mismatch, uniqueness, uniq_thr,
+                               pl, &npl);
+    }
+    if (output) {
+      static char obuf2[1 << 22];
+      setvbuf(output, obuf2, _IOFBF, sizeof(obuf2));
+      sh_write_genome_map_sam(output, &so, &refs, &reads, &res, pl, npl);
+      fflush(output);
+    } else {
+      err("No file name provided for SAM output.");
+    }
+    free(pl);
   }
+  if (mapper->finish) mapper->finish(mapper->user);
   if (unmapped) sh_write_unmapped_fastq(unmapped, &so, &reads, &res);
   if (output && output != stdout) fclose(output);
   if (unmapped) fclose(unmapped);

@@ -18,6 +18,12 @@ typedef struct storm_mapper {
    * return 0 or a negative error code (message through `err`). */
   int (*map)(void *user, const stormgpu_params *p, const char *seeds, const sh_refs *refs,
              const sh_reads *reads, stormgpu_results *out, char *err, int errlen);
+  /* greedy genome_map placement (no -M, -G) of the results of the last map call: placed reads
+   * in position-major order (rank 0); uniqueness_threshold 0 = no -u. */
+  int (*place_greedy)(void *user, const sh_refs *refs, const stormgpu_results *res, int64_t n,
+                      int uniqueness_threshold, sh_placement *out, int64_t *n_out, char *err, int errlen);
+  /* release what map kept (may be NULL) */
+  void (*finish)(void *user);
   void *user;
 } storm_mapper;
 

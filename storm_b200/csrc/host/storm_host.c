@@ -657,6 +657,269 @@ int sh_write_sam(FILE *f, const sh_sam_opts *o, const sh_refs *refs, const sh_re
 }
 
 /* hit_map.c:514-579 */
+/* ------------------------------------------------------------------------------ genome_map */
+
+#define GM_CODES 4                 /* BASE_CODE_COUNT / COLOR_CODE_COUNT (codes.h:25-29) */
+#define GM_NO_CODE GM_CODES        /* genome_map.c:26 */
+#define GM_BLOCK 4096
+
+/* 6-bit counters, one per code and the no-code symbol, packed in 32 bits (genome_map.c:37-48) */
+static inline int gm_get(uint32_t c, int code) { return (int)((c >> (code * 6)) & 0x3F); }
+static inline uint32_t gm_inc(uint32_t c, int code) {
+  const uint32_t v = (uint32_t)((gm_get(c, code) + 1) & 0x3F);
+  return (c & ~(0x3Fu << (code * 6))) | (v << (code * 6));
+}
+
+/* per-position data, created lazily in blocks of GM_BLOCK positions */
+typedef struct gm_block {
+  uint8_t created[GM_BLOCK];
+  uint32_t aligned[GM_BLOCK];
+  uint32_t *inserted;  /* indels * GM_BLOCK */
+} gm_block;
+
+typedef struct gm_map {
+  int nref, indels;
+  int64_t *npos;
+  gm_block ***blocks;
+} gm_map;
+
+static gm_block *gm_block_of(gm_map *m, int ref, int64_t pos, int create) {
+  gm_block **b = &m->blocks[ref][pos / GM_BLOCK];
+  if (!*b && create) {
+    *b = calloc(1, sizeof(gm_block));
+    if (m->indels) (*b)->inserted = calloc((size_t)m->indels * GM_BLOCK, sizeof(uint32_t));
+  }
+  return *b;
+}
+
+/* genome_map__create_position_data */
+static void gm_create(gm_map *m, int ref, int64_t pos) {
+  gm_block *b = gm_block_of(m, ref, pos, 1);
+  b->created[pos % GM_BLOCK] = 1;
+}
+
+/* genome_map__get_direct_consensus_code (genome_map.c:312-337) */
+static int gm_consensus(gm_map *m, int ref, int64_t pos, int offset, int ref_code) {
+  gm_block *b = gm_block_of(m, ref, pos, 0);
+  if (!b || !b->created[pos % GM_BLOCK]) return ref_code;
+  const uint32_t counts = offset < 0 ? b->aligned[pos % GM_BLOCK]
+                                     : b->inserted[(size_t)offset * GM_BLOCK + (size_t)(pos % GM_BLOCK)];
+  int best = ref_code;
+  for (int i = 0; i <= GM_CODES; ++i)
+    if (gm_get(counts, i) > gm_get(counts, best)) best = i;
+  if (gm_get(counts, best) == 0) best = GM_NO_CODE;
+  return best;
+}
+
+/* genome_map__update_consensus_code (genome_map.c:346-356) */
+static void gm_update(gm_map *m, int ref, int64_t pos, int offset, int code) {
+  gm_create(m, ref, pos);
+  gm_block *b = gm_block_of(m, ref, pos, 0);
+  if (offset >= 0) {
+    uint32_t *c = &b->inserted[(size_t)offset * GM_BLOCK + (size_t)(pos % GM_BLOCK)];
+    *c = gm_inc(*c, code);
+  } else {
+    b->aligned[pos % GM_BLOCK] = gm_inc(b->aligned[pos % GM_BLOCK], code);
+  }
+}
+
+/* GET_PAIR_TYPE (alignment.h:87-94) */
+static inline int pair_type(int code, int colour) {
+  if ((code & 0xC) == 0x4) return 0x4;
+  if (colour && (code & 0xC) == 0x8) return 0x8;
+  if ((code & 0xC) == 0xC) return 0xC;
+  return code;
+}
+
+/* genome_map__compute_adjusted_score (genome_map.c:366-424) */
+static int gm_adjusted(gm_map *m, const sh_refs *refs, const stormgpu_hit *h, const uint8_t *tb, int colour,
+                       int match, int mismatch) {
+  if (h->ref_start == -1) return STORMGPU_MIN_SCORE;
+  int score = 0, indel = 0, ref = h->ref_id;
+  int64_t pos = h->ref_start;
+  for (int i = 0; i < h->tb_len; ++i) {
+    const int cell = tb_get(tb, i);
+    switch (pair_type(cell, colour)) {
+    case 0x3: {
+      const int rc = get2(refs->codes[ref], pos);
+      score += rc == gm_consensus(m, ref, pos, -1, rc) ? match : mismatch;
+      ++pos;
+      indel = 0;
+      break;
+    }
+    case 0x1:
+      score += gm_consensus(m, ref, pos, -1, GM_NO_CODE) == GM_NO_CODE ? match : mismatch;
+      ++pos;
+      indel = 0;
+      break;
+    case 0x4:
+    case 0x8: {
+      const int c = cell & 3;
+      score += c == gm_consensus(m, ref, pos, -1, c) ? match : mismatch;
+      ++pos;
+      indel = 0;
+      break;
+    }
+    case 0xC: {
+      const int c = cell & 3;
+      score += c == gm_consensus(m, ref, pos, indel, c) ? match : mismatch;
+      ++indel;
+      break;
+    }
+    default:
+      break;
+    }
+  }
+  return score;
+}
+
+int sh_genome_map_contextual(const sh_refs *refs, const stormgpu_results *res, int64_t n, int colour, int indels,
+                             int match, int mismatch, int uniqueness, int uniqueness_threshold,
+                             sh_placement *out, int64_t *n_out) {
+  *n_out = 0;
+  gm_map m;
+  m.nref = refs->n;
+  m.indels = indels;
+  m.npos = calloc((size_t)refs->n, sizeof(int64_t));
+  m.blocks = calloc((size_t)refs->n, sizeof(gm_block **));
+  for (int s = 0; s < refs->n; ++s) {
+    m.npos[s] = refs->sizes[s] + 1;  /* GENOME_MAP_SIZE */
+    m.blocks[s] = calloc((size_t)(m.npos[s] / GM_BLOCK + 1), sizeof(gm_block *));
+  }
+  /* mapped reads in read order, then a stable sort by descending unsigned best score
+   * (genome_map.c:233-299: 4-bit digits, bucket 15 - digit) */
+  int64_t nm = 0;
+  for (int64_t r = 0; r < n; ++r) nm += res->mapped[r] != 0;
+  int32_t *idx = malloc(sizeof(int32_t) * (size_t)(nm ? nm : 1)), *tmp = malloc(sizeof(int32_t) * (size_t)(nm ? nm : 1));
+  for (int64_t r = 0, j = 0; r < n; ++r)
+    if (res->mapped[r]) idx[j++] = (int32_t)r;
+  for (int d = 0; d < 8; ++d) {
+    int64_t count[16] = {0}, index[16];
+    for (int64_t j = 0; j < nm; ++j) count[15 - (((uint32_t)res->hits[(int64_t)idx[j] * 4].score >> (4 * d)) & 15)]++;
+    index[0] = 0;
+    for (int b = 1; b < 16; ++b) index[b] = index[b - 1] + count[b - 1];
+    for (int64_t j = 0; j < nm; ++j)
+      tmp[index[15 - (((uint32_t)res->hits[(int64_t)idx[j] * 4].score >> (4 * d)) & 15)]++] = idx[j];
+    int32_t *sw = tmp; tmp = idx; idx = sw;
+  }
+  for (int64_t j = 0; j < nm; ++j) {
+    const int64_t r = idx[j];
+    const stormgpu_hit *h = &res->hits[r * 4];
+    int adj[STORMGPU_MAP_DETAIL];
+    for (int k = 0; k < STORMGPU_MAP_DETAIL; ++k) adj[k] = STORMGPU_MIN_SCORE;
+    int best_rank = -1, best = STORMGPU_MIN_SCORE;
+    for (int k = 0; k < STORMGPU_MAP_DETAIL && h[k].ref_start != -1; ++k) {
+      adj[k] = gm_adjusted(&m, refs, &h[k], res->tb + (size_t)(r * 4 + k) * (size_t)res->tb_stride, colour, match,
+                           mismatch);
+      if (adj[k] > best) { best = adj[k]; best_rank = k; }
+    }
+    if (best_rank < 0 || (uniqueness && !(adj[0] - adj[1] > uniqueness_threshold))) continue;
+    const stormgpu_hit *b = &h[best_rank];
+    const int ref = b->ref_id;
+    int64_t pos = b->ref_start;
+    gm_create(&m, ref, pos);
+    out[(*n_out)++] = (sh_placement){(int32_t)r, best_rank};
+    const uint8_t *tb = res->tb + (size_t)(r * 4 + best_rank) * (size_t)res->tb_stride;
+    int insertions = -1;
+    for (int k = 0; k < b->tb_len; ++k) {
+      const int cell = tb_get(tb, k);
+      switch (pair_type(cell, colour)) {
+      case 0xC: insertions++; gm_update(&m, ref, pos, insertions, cell & 3); break;
+      case 0x3: insertions = -1; gm_update(&m, ref, pos, -1, get2(refs->codes[ref], pos)); break;
+      case 0x4: insertions = -1; gm_update(&m, ref, pos, -1, cell & 3); break;
+      case 0x1: insertions = -1; gm_update(&m, ref, pos, -1, GM_NO_CODE); break;
+      case 0x8: insertions = -1; gm_update(&m, ref, pos, -1, cell & 3); break;
+      default: break;
+      }
+      for (int p = insertions + 1; p < indels; ++p) gm_update(&m, ref, pos, p, GM_NO_CODE);
+      if (insertions < 0) pos++;
+    }
+  }
+  free(idx);
+  free(tmp);
+  for (int s = 0; s < refs->n; ++s) {
+    for (int64_t k = 0; k <= m.npos[s] / GM_BLOCK; ++k)
+      if (m.blocks[s][k]) { free(m.blocks[s][k]->inserted); free(m.blocks[s][k]); }
+    free(m.blocks[s]);
+  }
+  free(m.blocks);
+  free(m.npos);
+  sh_sort_placements(res, out, *n_out);
+  return 0;
+}
+
+typedef struct { int32_t ref; int64_t pos; int64_t seq; sh_placement p; } gm_key;
+static int gm_key_cmp(const void *a, const void *b) {
+  const gm_key *x = a, *y = b;
+  if (x->ref != y->ref) return x->ref < y->ref ? -1 : 1;
+  if (x->pos != y->pos) return x->pos < y->pos ? -1 : 1;
+  return x->seq < y->seq ? -1 : x->seq > y->seq;
+}
+
+void sh_sort_placements(const stormgpu_results *res, sh_placement *pl, int64_t n) {
+  if (n <= 1) return;
+  gm_key *k = malloc(sizeof(gm_key) * (size_t)n);
+  for (int64_t i = 0; i < n; ++i) {
+    const stormgpu_hit *h = &res->hits[(int64_t)pl[i].read * 4 + pl[i].rank];
+    k[i] = (gm_key){h->ref_id, h->ref_start, i, pl[i]};
+  }
+  qsort(k, (size_t)n, sizeof(gm_key), gm_key_cmp);
+  for (int64_t i = 0; i < n; ++i) pl[i] = k[i].p;
+  free(k);
+}
+
+int sh_write_genome_map_sam(FILE *f, const sh_sam_opts *o, const sh_refs *refs, const sh_reads *reads,
+                            const stormgpu_results *res, const sh_placement *pl, int64_t n_pl) {
+  const int colour = o->colour;
+  fprintf(f, "@HD\tVN:1.4\tSO:coordinate\n");
+  for (int s = 0; s < refs->n; ++s)
+    fprintf(f, "@SQ\tSN:%s\tLN:%ld\n", refs->names[s] ? refs->names[s] : "*", (long)(refs->sizes[s] + (colour ? 1 : 0)));
+  const char *rg = reads->db_name ? reads->db_name : "*";
+  fprintf(f, "@RG\tID:%s\tSM:%s\n", rg, rg);
+  fprintf(f, "@PG\tID:%s\tVN:%s\tCL:\"", "SToRM", "0.0101");
+  for (int i = 0; i < o->argc; ++i) fprintf(f, "%s ", o->argv[i]);
+  fprintf(f, "\"\n");
+  char cigar[4 * STORMGPU_MAX_READ_LEN + 64], seq[2 * STORMGPU_MAX_READ_LEN + 8];
+  char *qbuf = malloc((size_t)reads->max_len + 8);
+  int cur_ref = -1, sym = 0;
+  int64_t cur_pos = 0;
+  for (int64_t i = 0; i < n_pl; ++i) {
+    const int64_t r = pl[i].read;
+    const int k = pl[i].rank;
+    const stormgpu_hit *h = &res->hits[r * 4];
+    const int ref = h[k].ref_id;
+    const int64_t start = h[k].ref_start;
+    if (colour) {  /* the reference's running ref_symbol: first base transformed by every colour before */
+      if (ref != cur_ref) { cur_ref = ref; cur_pos = 0; sym = refs->first_base[ref]; }
+      for (; cur_pos < start && cur_pos < refs->sizes[ref]; ++cur_pos) sym ^= get2(refs->codes[ref], cur_pos);
+    }
+    const int rev = (h[k].sense & 2) != 0;
+    const int mapq = sh_mapq(k, h[0].score, h[1].score, h[k].score, o->min_score, o->delta_m);
+    const int ed = sh_traceback_to_cigar(res->tb + (size_t)(r * 4 + k) * (size_t)res->tb_stride, h[k].tb_len,
+                                         refs->codes[ref], start, colour, sym & 3, cigar, seq);
+    fprintf(f, "%s\t%d\t%s\t%ld\t%d\t%s\t*\t0\t0\t%s\t", reads->names[r], rev ? 0x10 : 0,
+            refs->names[ref] ? refs->names[ref] : "*", (long)(start + 1), mapq, cigar, seq);
+    const int L = reads->lengths[r];
+    if (reads->levels) {
+      const uint8_t *lv = reads->levels + r * reads->level_stride;
+      int qi = 0;
+      if (rev) {
+        for (int q = L - 1; q >= 0; --q) { int c = o->quality_base + LEVEL_UB[get2(lv, q)]; qbuf[qi++] = (char)(c < 126 ? c : 126); }
+        if (colour) { int c = o->quality_base + LEVEL_UB[reads->first_level[r]]; qbuf[qi++] = (char)(c < 126 ? c : 126); }
+      } else {
+        if (colour) { int c = o->quality_base + LEVEL_UB[reads->first_level[r]]; qbuf[qi++] = (char)(c < 126 ? c : 126); }
+        for (int q = 0; q < L; ++q) { int c = o->quality_base + LEVEL_UB[get2(lv, q)]; qbuf[qi++] = (char)(c < 126 ? c : 126); }
+      }
+      fwrite(qbuf, 1, (size_t)qi, f);
+    } else {
+      fputc('*', f);
+    }
+    fprintf(f, "\tAS:i:%d\tNM:i:%d\n", h[k].score, ed);
+  }
+  free(qbuf);
+  return 0;
+}
+
 int sh_write_unmapped_fastq(FILE *f, const sh_sam_opts *o, const sh_reads *reads,
                             const stormgpu_results *res) {
   static const char B[4] = {'A', 'C', 'G', 'T'}, CL[4] = {'0', '1', '2', '3'};

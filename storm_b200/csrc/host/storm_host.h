@@ -91,6 +91,32 @@ int sh_write_sam(FILE *f, const sh_sam_opts *o, const sh_refs *refs, const sh_re
 int sh_write_unmapped_fastq(FILE *f, const sh_sam_opts *o, const sh_reads *reads,
                             const stormgpu_results *res);
 
+/* genome_map (the mapping without -M): the reads placed on the references, in the order
+ * genome_map__generate_SAM_output prints them (sequence, position, then placement order),
+ * each with the rank of its alignment that was placed. */
+typedef struct sh_placement {
+  int32_t read;
+  int32_t rank;
+} sh_placement;
+
+/* Contextual placement (the default, genome_map.c:253-536): reads by descending best score
+ * (a stable sort on the unsigned value, as the reference's radix sort); every alignment of the
+ * read rescored against the consensus of the reads placed so far (6-bit counters per code that
+ * wrap, genome_map.c:37-48), the best placed and the consensus updated along its traceback.
+ * out holds n entries; *n_out receives the number placed.  Inherently sequential: it runs
+ * here, on the GPU's top-4 records. */
+int sh_genome_map_contextual(const sh_refs *refs, const stormgpu_results *res, int64_t n, int colour, int indels,
+                             int match, int mismatch, int uniqueness, int uniqueness_threshold,
+                             sh_placement *out, int64_t *n_out);
+
+/* Order placements by (sequence, position of the placed alignment), keeping their order
+ * within a position. */
+void sh_sort_placements(const stormgpu_results *res, sh_placement *pl, int64_t n);
+
+/* The SAM of a genome map (genome_map.c:551-796): @HD SO:coordinate, records position-major. */
+int sh_write_genome_map_sam(FILE *f, const sh_sam_opts *o, const sh_refs *refs, const sh_reads *reads,
+                            const stormgpu_results *res, const sh_placement *pl, int64_t n_pl);
+
 /* alignment.c:749-887 (exposed for tests). */
 int sh_traceback_to_cigar(const uint8_t *tb, int tb_len, const uint8_t *ref_codes,
                           int64_t ref_start, int colour, int ref_start_symbol, char *cigar,

@@ -17,7 +17,7 @@ constexpr int kSortThreads = 256;
 constexpr int kSortRounds = 16;
 constexpr int kSortTile = kSortThreads * kSortRounds;
 
-__global__ void radix_hist_kernel(const uint32_t* __restrict__ keys, int64_t n, int shift,
+static __global__ void radix_hist_kernel(const uint32_t* __restrict__ keys, int64_t n, int shift,
                                   uint32_t* __restrict__ hist, int ntiles) {
   __shared__ uint32_t h[kRadixBins];
   for (int i = threadIdx.x; i < kRadixBins; i += blockDim.x) h[i] = 0;
@@ -32,7 +32,7 @@ __global__ void radix_hist_kernel(const uint32_t* __restrict__ keys, int64_t n, 
     hist[(int64_t)d * ntiles + blockIdx.x] = h[d];
 }
 
-__global__ void radix_scatter_kernel(const uint32_t* __restrict__ keys_in,
+static __global__ void radix_scatter_kernel(const uint32_t* __restrict__ keys_in,
                                      const uint32_t* __restrict__ vals_in, int64_t n, int shift,
                                      const uint32_t* __restrict__ offs, int ntiles,
                                      uint32_t* __restrict__ keys_out, uint32_t* __restrict__ vals_out) {

@@ -174,6 +174,8 @@ extern "C" void stormgpu_close(stormgpu_ctx* c) {
   c->a_pos.release(); c->a_tb.release(); c->scratch.release(); c->counters.release();
   c->foff.release(); c->fr.release(); c->fd.release(); c->flag.release();
   c->rexp.release();
+  c->gm_k0.release(); c->gm_v0.release(); c->gm_k1.release(); c->gm_v1.release(); c->gm_tmp.release();
+  c->gm_base.release();
   for (auto& e : c->ev) cudaEventDestroy(e);
   cudaStreamDestroy(c->st);
   delete c;
@@ -514,6 +516,7 @@ extern "C" int stormgpu_map(stormgpu_ctx* c, const stormgpu_reads* reads, stormg
   dres.mapped = c->mapped.p;
   int rc = map_device_impl(c, &dr, &dres);
   if (rc) return rc;
+  c->last_n = n;
   if (n > 0) {
     SG_CUDA(cudaMemcpyAsync(out->hits, c->hits.p, sizeof(stormgpu_hit) * n * 4, cudaMemcpyDeviceToHost, st));
     SG_CUDA(cudaMemcpyAsync(out->tb, c->tb.p, n * 4 * out->tb_stride, cudaMemcpyDeviceToHost, st));

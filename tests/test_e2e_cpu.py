@@ -149,3 +149,39 @@ def test_masked_multi_sequence(tmp_path):
     (tmp_path / "reads.fq").write_bytes(b"\n".join(lines))
     run_pair(str(tmp_path), 0, ["-M", "4", "-A", "-z", "90", "-t", "95"])
     run_pair(str(tmp_path), 0, ["-M", "4", "-j", "-z", "90", "-t", "95"])
+
+
+@pytest.mark.parametrize("args", [
+    ["-z", "100", "-t", "100", "-i", "3"],          # contextual placement (default without -M)
+    ["-G", "-z", "100", "-t", "100", "-i", "3"],    # greedy placement
+    ["-i", "7", "-z", "80", "-t", "90"],            # more indels: inserted-code counters
+    ["-u", "5", "-z", "90", "-t", "95"],
+    ["-G", "-u", "5", "-z", "90", "-t", "95"],
+    ["-i", "0", "-z", "60", "-t", "60"],
+])
+def test_genome_map_nucleotide(nuc_data, args):
+    """The mapping without -M (genome_map.c): reads placed per reference position, SAM written
+    position-major."""
+    lines = run_pair(nuc_data, 0, args)
+    assert _mapped(lines) > 0
+
+
+@pytest.mark.parametrize("args", [
+    ["-z", "105", "-t", "120", "-i", "7"],
+    ["-G", "-i", "3"],
+])
+def test_genome_map_colour(col_data, args):
+    lines = run_pair(col_data, 1, args)
+    assert _mapped(lines) > 0
+
+
+def test_genome_map_repeats_stack_reads(tmp_path):
+    """Reads piled on repeated and overlapping positions, so that the contextual rescoring
+    against the consensus decides between copies."""
+    genome = synth.make_genome([40000], 12, 0.45, 0.5)
+    synth.write_fasta(str(tmp_path / "ref.fa"), genome)
+    seqs, quals = synth.simulate_nucleotide_reads(genome, 4000, 50, 13,
+                                                  synth.ReadModel(indel_rate=0.01, indel_max=2))
+    synth.write_fastq(str(tmp_path / "reads.fq"), seqs, quals)
+    lines = run_pair(str(tmp_path), 0, ["-i", "5", "-z", "90", "-t", "95"])
+    assert _mapped(lines) > 1000

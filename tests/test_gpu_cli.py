@@ -30,8 +30,32 @@ def test_gpu_cli_matches_golden(name, tmp_path):
 @pytest.mark.skipif(not ffi.ref_available(), reason="oracle/_ref not built")
 @pytest.mark.parametrize("cfg,scale,extra", [(0, 0.2, []), (1, 0.02, []), (0, 0.05, ["-M", "4", "-A", "-i", "20", "-z", "70"])])
 def test_gpu_cli_matches_reference(cfg, scale, extra, tmp_path):
+    _live(cfg, scale, extra, tmp_path)
+
+
+def _without_m(args):
+    out, i = [], 0
+    while i < len(args):
+        if args[i] == "-M":
+            i += 2
+            continue
+        out.append(args[i])
+        i += 1
+    return out
+
+
+@pytest.mark.skipif(not ffi.ref_available(), reason="oracle/_ref not built")
+@pytest.mark.parametrize("cfg,scale,extra", [(0, 0.2, []), (0, 0.2, ["-G"]), (0, 0.05, ["-G", "-u", "5", "-i", "7"]),
+                                             (1, 0.02, []), (1, 0.02, ["-G"])])
+def test_gpu_cli_genome_map_matches_reference(cfg, scale, extra, tmp_path):
+    """Without -M: the per-position map (greedy placement sorted on the GPU, contextual placement
+    on the mapped records), SAM written position-major."""
+    _live(cfg, scale, extra, tmp_path, strip_m=True)
+
+
+def _live(cfg, scale, extra, tmp_path, strip_m=False):
     w = synth.generate(cfg, scale, str(tmp_path / "ref.fa"), str(tmp_path / "reads.fq"))
-    args = w["args"] + extra
+    args = (_without_m(w["args"]) if strip_m else w["args"]) + extra
     colour = w["mode"] == "colour"
     outs = {}
     for tag, exe in (("ref", os.path.join(ffi.REF_DIR, "storm-color" if colour else "storm-nucleotide")),
