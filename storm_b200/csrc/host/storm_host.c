@@ -387,13 +387,126 @@ static int load_fastq(const char *path, int colour, int quality_base, int allow_
   return rc;
 }
 
+/* FASTA reads, or CSFASTA (a primer base, then colours) with an optional quality file of
+ * space-separated integers (reads_data.c:73-345).  After leading '#' comments (a "# Title: "
+ * names the read set), a record is a '>' header and one or more sequence lines; a header not
+ * followed by sequence lines leaves its name to the next record (the reference overwrites it).
+ * Quality lines are the quality file's lines that are neither comments nor headers, one per read
+ * in order; a short line keeps the values of the previous read for the missing positions (the
+ * reference parses into one buffer reused across reads, load_data.c:15-33). */
+static int load_fasta(const char *path, const char *qual_path, int colour, int allow_mixed, sh_reads *out) {
+  size_t len;
+  char *buf = slurp(path, &len);
+  if (!buf) return fail(STORMGPU_EINVAL, "Failed to read input file %s (read sequences).", path);
+  size_t pos = 0;
+  const char *line;
+  size_t ll;
+  char *title = NULL;
+  size_t rec_start = 0;
+  while (1) {
+    rec_start = pos;
+    if (!next_line(buf, len, &pos, &line, &ll)) { free(buf); return fail(STORMGPU_EINVAL, "Failed to read input file %s (read sequences) first line.", path); }
+    if (ll >= 9 && !title && strncmp(line, "# Title: ", 9) == 0) {
+      size_t nl = strcspn(line + 9, "\r\n");
+      if (nl > ll - 9) nl = ll - 9;
+      title = malloc(nl + 1);
+      memcpy(title, line + 9, nl);
+      title[nl] = 0;
+    }
+    if (ll > 0 && line[0] == '#') continue;
+    break;
+  }
+  pos = rec_start;
+  /* sequences may span lines: gather each record's sequence into one contiguous copy */
+  growbuf seq = {0};
+  int64_t cap = 1 << 16, n = 0;
+  rawread *rr = malloc(sizeof(rawread) * (size_t)cap);
+  size_t name_off = 0;
+  int name_len = -1;
+  int in_seq = 0;
+  while (next_line(buf, len, &pos, &line, &ll)) {
+    size_t l2 = ll;
+    while (l2 > 0 && (line[l2 - 1] == '\r' || line[l2 - 1] == '\n')) l2--;
+    const int type = ll == 0 || line[0] == '\r' ? 0 : line[0] == '#' ? 0 : line[0] == '>' ? 1 : 2;
+    if (type == 2 && name_len >= 0) {
+      if (!in_seq) {
+        if (n == cap) { cap *= 2; rr = realloc(rr, sizeof(rawread) * (size_t)cap); }
+        rr[n].name_off = name_off;
+        rr[n].name_len = name_len;
+        rr[n].seq_off = seq.n;
+        rr[n].seq_len = 0;
+        rr[n].has_qual = 0;
+        rr[n].qual_len = 0;
+        n++;
+        in_seq = 1;
+      }
+      gb_put(&seq, line, l2);
+      rr[n - 1].seq_len += (int)l2;
+    } else {
+      in_seq = 0;
+      if (type == 1) {
+        name_off = (size_t)(line - buf) + 1;
+        name_len = header_name_len(line, l2);
+      }
+    }
+  }
+  if (n == 0) { free(rr); free(buf); free(seq.p); free(title); return fail(STORMGPU_EINVAL, "Reads could not be loaded."); }
+  /* names live in buf, sequences in seq: copy the names next to the sequences */
+  const size_t names_at = seq.n;
+  for (int64_t i = 0; i < n; ++i) {
+    const size_t o = seq.n;
+    gb_put(&seq, buf + rr[i].name_off, (size_t)rr[i].name_len);
+    rr[i].name_off = o;
+  }
+  (void)names_at;
+  memset(out, 0, sizeof(*out));
+  int rc = fill_reads(out, seq.p, rr, n, colour, 33, allow_mixed, 0);
+  if (rc == 0 && qual_path) {
+    size_t qlen;
+    char *qb = slurp(qual_path, &qlen);
+    if (!qb) rc = fail(STORMGPU_EINVAL, "Failed to read input file %s (quality of read sequences).", qual_path);
+    else {
+      out->has_quality = 1;
+      out->levels = calloc((size_t)n, (size_t)out->level_stride);
+      const int need = out->max_len + (colour ? 1 : 0);
+      short *qv = calloc((size_t)need + 1, sizeof(short));  /* kept across reads */
+      size_t qp = 0;
+      int64_t i = 0;
+      char *tmp = malloc(qlen + 1);
+      while (i < n && next_line(qb, qlen, &qp, &line, &ll)) {
+        if (ll == 0 || line[0] == '\r' || line[0] == '#' || line[0] == '>') continue;
+        memcpy(tmp, line, ll);
+        tmp[ll] = 0;
+        const int L = out->lengths[i];
+        const int want = L + (colour ? 1 : 0);
+        char *save = NULL, *tok = strtok_r(tmp, " ", &save);
+        for (int j = 0; j < want && tok; ++j, tok = strtok_r(NULL, " ", &save)) qv[j] = (short)atoi(tok);
+        uint8_t *lv = out->levels + i * out->level_stride;
+        if (colour) out->first_level[i] = (uint8_t)quality_level(qv[0]);
+        for (int k = 0; k < L; ++k) put2(lv, k, quality_level(qv[k + (colour ? 1 : 0)]));
+        i++;
+      }
+      free(tmp);
+      free(qv);
+      free(qb);
+    }
+  }
+  if (rc == 0) {
+    if (title) out->db_name = title;
+    else out->db_name = common_name(out->names[0], out->names[n - 1]);
+  } else free(title);
+  free(rr);
+  free(seq.p);
+  free(buf);
+  return rc;
+}
+
 int sh_load_reads(const char *path, const char *qual_path, int colour, int quality_base,
                   int allow_mixed, sh_reads *out) {
   const char *dot = strrchr(path, '.');
   if (dot && (!strcmp(dot, ".fastq") || !strcmp(dot, ".fq") || !strcmp(dot, ".fastq2") || !strcmp(dot, ".fq2")))
     return load_fastq(path, colour, quality_base, allow_mixed, out);
-  (void)qual_path;
-  return fail(STORMGPU_EINVAL, "Reads file %s: only FASTQ input (.fastq/.fq) is supported by this build.", path);
+  return load_fasta(path, qual_path, colour, allow_mixed, out);
 }
 
 void sh_free_reads(sh_reads *r) {

@@ -185,3 +185,46 @@ def test_genome_map_repeats_stack_reads(tmp_path):
     synth.write_fastq(str(tmp_path / "reads.fq"), seqs, quals)
     lines = run_pair(str(tmp_path), 0, ["-i", "5", "-z", "90", "-t", "95"])
     assert _mapped(lines) > 1000
+
+
+def test_fasta_reads(tmp_path):
+    """Nucleotide reads as FASTA (no qualities): some sequences wrapped over two lines, a header
+    without a sequence (its name passes to the next record), comments and a title first."""
+    genome = synth.make_genome([30000], 17)
+    synth.write_fasta(str(tmp_path / "ref.fa"), genome)
+    seqs, _ = synth.simulate_nucleotide_reads(genome, 1500, 50, 18)
+    with open(tmp_path / "reads.fa", "wb") as f:
+        f.write(b"# Title: fasta reads\n# another comment\n")
+        for k, s in enumerate(seqs):
+            b = synth.BASES[s].tobytes()
+            if k == 10:
+                f.write(b">orphan header\n")
+            f.write(b">r%d some text\n" % k)
+            f.write(b[:20] + b"\n" + b[20:] + b"\n" if k % 7 == 0 else b + b"\n")
+    lines = run_pair(str(tmp_path), 0, ["-M", "2", "-z", "90", "-t", "95"], reads="reads.fa")
+    assert _mapped(lines) > 500
+
+
+@pytest.mark.parametrize("with_qual", [True, False])
+def test_csfasta_reads(tmp_path, with_qual):
+    """Colour reads as CSFASTA (primer base + colours), with the qualities in a .qual file of
+    integers (-q): comments and headers there too, a negative value, and one short line."""
+    genome = synth.make_genome([40000], 19)
+    synth.write_fasta(str(tmp_path / "ref.fa"), genome)
+    pr, cols, q = synth.simulate_colour_reads(genome, 1500, 50, 20)
+    with open(tmp_path / "reads.csfasta", "wb") as f:
+        f.write(b"# Title: solid set\n")
+        for k in range(len(cols)):
+            f.write(b">r%d_F3\n%c%s\n" % (k, synth.BASES[pr[k]], synth.COLOURS[cols[k]].tobytes()))
+    with open(tmp_path / "reads.qual", "wb") as f:
+        f.write(b"# qualities\n")
+        for k in range(len(cols)):
+            v = [int(x) for x in q[k]]
+            if k % 50 == 3:
+                v[5] = -1
+            if k == 77:
+                v = v[:30]  # short line: the rest keeps the previous read's values
+            f.write(b">r%d_F3\n%s\n" % (k, b" ".join(b"%d" % x for x in v)))
+    args = ["-M", "2", "-z", "90", "-t", "100", "-i", "5"] + (["-q", "reads.qual"] if with_qual else [])
+    lines = run_pair(str(tmp_path), 1, args, reads="reads.csfasta")
+    assert _mapped(lines) > 500
