@@ -64,7 +64,9 @@ struct stormgpu_ctx {
   sg::DevBuf<int32_t> pstart, pcount, p_read, p_diag, big_list, big_count, huge_list, huge_h;
   sg::DevBuf<int64_t> scan_tmp64, foff;
   sg::DevBuf<int32_t> fr, fd;
-  sg::DevBuf<uint8_t> flag, rexp;
+  sg::DevBuf<uint8_t> flag;       // pass byte per candidate
+  sg::DevBuf<uint32_t> flagw;     // pass bits, one word per 32 candidates
+  sg::DevBuf<uint8_t> rexp;
   sg::DevBuf<int32_t> a_score, a_bound, a_tblen, big_tmp;
   sg::DevBuf<int16_t> a_pos;
   sg::DevBuf<uint8_t> a_tb;

@@ -218,8 +218,8 @@ __device__ __forceinline__ int warp_dedupe(int32_t* a, int H, int32_t* tab, int 
   return U;
 }
 
-// Sort a[0..H) (one warp) into b[0..H) and emit: 32 buckets by the high bits of (v - min)
-// (power-of-two aligned, so that bucket order is value order), counted with shared atomics,
+// Sort a[0..H) (one warp) into b[0..H) and emit: 32 buckets of equal width over [min, max]
+// (so that bucket order is value order), counted with shared atomics,
 // scattered to b, then every lane insertion-sorts its own bucket.  A bucket holding more than
 // 64 values (clustered diagonals) falls back to the bitonic sort of a, which needs room for
 // the next power of two of H from a on (a and b are adjacent).
@@ -234,11 +234,16 @@ __device__ __forceinline__ void bucket_sort_emit(int32_t* a, int32_t* b, int32_t
   }
   vmin = __reduce_min_sync(0xffffffffu, vmin);
   vmax = __reduce_max_sync(0xffffffffu, vmax);
+  // bucket = floor(32 * (v - min) / (range + 1)) as a multiply-high: monotone, all 32 buckets used
   const uint32_t range = (uint32_t)vmax - (uint32_t)vmin;
-  const int sh = max(0, 32 - __clz((int)range) - 5);  // (range >> sh) < 32
+  const uint32_t mul = range < 32u ? 0u : (uint32_t)((32ull << 32) / ((uint64_t)range + 1ull));
+  auto bucket = [&](int32_t v) -> int {
+    const uint32_t x = (uint32_t)v - (uint32_t)vmin;
+    return range < 32u ? (int)x : (int)__umulhi(x, mul);
+  };
   hist[lane] = 0;
   __syncwarp();
-  for (int i = lane; i < H; i += 32) atomicAdd(&hist[((uint32_t)a[i] - (uint32_t)vmin) >> sh], 1);
+  for (int i = lane; i < H; i += 32) atomicAdd(&hist[bucket(a[i])], 1);
   __syncwarp();
   const int c = hist[lane];
   const int incl = warp_incl_scan(c);
@@ -257,7 +262,7 @@ __device__ __forceinline__ void bucket_sort_emit(int32_t* a, int32_t* b, int32_t
   __syncwarp();
   for (int i = lane; i < H; i += 32) {
     const int32_t v = a[i];
-    b[atomicAdd(&hist[((uint32_t)v - (uint32_t)vmin) >> sh], 1)] = v;
+    b[atomicAdd(&hist[bucket(v)], 1)] = v;
   }
   __syncwarp();
   for (int x = 1; x < c; ++x) {

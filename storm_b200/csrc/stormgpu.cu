@@ -172,7 +172,7 @@ extern "C" void stormgpu_close(stormgpu_ctx* c) {
   c->scan_tmp64.release();
   c->a_score.release(); c->a_bound.release(); c->a_tblen.release(); c->big_tmp.release();
   c->a_pos.release(); c->a_tb.release(); c->scratch.release(); c->counters.release();
-  c->foff.release(); c->fr.release(); c->fd.release(); c->flag.release();
+  c->foff.release(); c->fr.release(); c->fd.release(); c->flag.release(); c->flagw.release();
   c->rexp.release();
   c->gm_k0.release(); c->gm_v0.release(); c->gm_k1.release(); c->gm_v1.release(); c->gm_tmp.release();
   c->gm_base.release();
@@ -345,8 +345,10 @@ static int map_device_once(stormgpu_ctx* c, const stormgpu_reads* reads, stormgp
         if (attempt > 2) { sg_set_error("internal: candidate list overflow"); return STORMGPU_EINVAL; }
         if (c->fr.grow(utot + utot / 4 + 1024) || c->fd.grow(utot + utot / 4 + 1024)) return STORMGPU_ENOMEM;
       }
-      if (c->flag.grow(std::max<int64_t>(utot, 1)) || c->foff.grow(utot + 1) ||
-          c->scan_tmp64.grow(scan_tmp_elems(std::max<int64_t>(utot, n)) + 8))
+      const int64_t nwords = (utot + 31) / 32;
+      if (c->flag.grow(std::max<int64_t>(nwords * 32, 1)) || c->flagw.grow(std::max<int64_t>(nwords, 1)) ||
+          c->foff.grow(nwords + 1) ||
+          c->scan_tmp64.grow(scan_tmp_elems(std::max<int64_t>(nwords, n)) + 8))
         return STORMGPU_ENOMEM;
       SG_CUDA(cudaEventRecord(c->ev[1], st));
       FilterJob job;
@@ -361,10 +363,12 @@ static int map_device_once(stormgpu_ctx* c, const stormgpu_reads* reads, stormgp
       launch_filter_flat_job(job, sp, filter_dpx_ok(sp, maxL), st);
       launches += 2;
       SG_CUDA(cudaEventRecord(c->ev[2], st));
-      exclusive_scan<uint8_t, int64_t>(c->flag.p, c->foff.p, utot, c->foff.p + utot, c->scan_tmp64.p, st);
+      launch_pack_flags(utot, c->flag.p, c->flagw.p, st);
+      exclusive_scan<PassWord, int64_t>(reinterpret_cast<const PassWord*>(c->flagw.p), c->foff.p, nwords,
+                                        c->foff.p + nwords, c->scan_tmp64.p, st);
       unsigned long long cnt[8];
       int64_t npass = 0;
-      SG_CUDA(cudaMemcpyAsync(&npass, c->foff.p + utot, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+      SG_CUDA(cudaMemcpyAsync(&npass, c->foff.p + nwords, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
       SG_CUDA(cudaMemcpyAsync(cnt, c->counters.p, sizeof(cnt), cudaMemcpyDeviceToHost, st));
       SG_CUDA(cudaStreamSynchronize(st));
       if (utot == 0) npass = 0;
@@ -385,7 +389,7 @@ static int map_device_once(stormgpu_ctx* c, const stormgpu_reads* reads, stormgp
             c->a_tblen.grow(npass) || c->a_pos.grow(npass * 4) || c->a_tb.grow(npass * tbs))
           return STORMGPU_ENOMEM;
         pb.p_read = c->p_read.p; pb.p_diag = c->p_diag.p; pb.p_cap = c->p_read.cap;
-        launch_compact(utot, c->flag.p, c->foff.p, c->fr.p, c->fd.p, c->p_read.p, c->p_diag.p, st);
+        launch_compact(nwords, c->flagw.p, c->foff.p, c->fr.p, c->fd.p, c->p_read.p, c->p_diag.p, st);
         launch_slot_bounds(npass, c->p_read.p, c->pstart.p, c->pcount.p, st);
         launches += 3;
         pb.a_score = c->a_score.p; pb.a_bound = c->a_bound.p; pb.a_tblen = c->a_tblen.p;

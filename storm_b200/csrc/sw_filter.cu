@@ -164,15 +164,48 @@ void launch_filter_flat_job(const FilterJob& job, const ScoreParams& sp, bool dp
 
 // ------------------------------------------------------------------ compaction of passing candidates
 
-// passing candidates, in order, into (p_read, p_diag); pcount/pstart per read
-__global__ void compact_kernel(int64_t n, const uint8_t* __restrict__ flag, const int64_t* __restrict__ off,
+// pass bytes -> pass bits, one word per 32 candidates (the scan then runs over words)
+__global__ void pack_flags_kernel(int64_t n, const uint8_t* __restrict__ flag, uint32_t* __restrict__ words) {
+  const int64_t nw = (n + 31) / 32;
+  for (int64_t w = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; w < nw; w += (int64_t)gridDim.x * blockDim.x) {
+    uint32_t bits = 0;
+    const int64_t t0 = w * 32;
+    if (t0 + 32 <= n) {
+      const uint4* p = reinterpret_cast<const uint4*>(flag + t0);  // flag is 16-byte aligned, t0 a multiple of 32
+      const uint4 q0 = p[0], q1 = p[1];
+      const uint32_t v[8] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w};
+#pragma unroll
+      for (int k = 0; k < 8; ++k)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) bits |= ((v[k] >> (8 * b)) & 1u) << (4 * k + b);
+    } else {
+      for (int64_t t = t0; t < n; ++t) bits |= (uint32_t)(flag[t] & 1) << (t - t0);
+    }
+    words[w] = bits;
+  }
+}
+
+void launch_pack_flags(int64_t n, const uint8_t* flag, uint32_t* words, cudaStream_t st) {
+  if (n <= 0) return;
+  int64_t blocks = ((n + 31) / 32 + 255) / 256;
+  if (blocks > 148 * 32) blocks = 148 * 32;
+  pack_flags_kernel<<<(unsigned)blocks, 256, 0, st>>>(n, flag, words);
+}
+
+// passing candidates, in order, into (p_read, p_diag): one thread per word of pass bits
+__global__ void compact_kernel(int64_t nwords, const uint32_t* __restrict__ flag, const int64_t* __restrict__ woff,
                                const int32_t* __restrict__ fr, const int32_t* __restrict__ fd,
                                int32_t* __restrict__ p_read, int32_t* __restrict__ p_diag) {
-  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) {
-    if (flag[t]) {
-      const int64_t o = off[t];
+  for (int64_t w = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; w < nwords; w += (int64_t)gridDim.x * blockDim.x) {
+    uint32_t m = flag[w];
+    if (!m) continue;
+    int64_t o = woff[w];
+    while (m) {
+      const int64_t t = w * 32 + (__ffs(m) - 1);
       p_read[o] = fr[t];
       p_diag[o] = fd[t];
+      ++o;
+      m &= m - 1;
     }
   }
 }
@@ -193,12 +226,12 @@ __global__ void slot_count_kernel(int64_t npass, const int32_t* __restrict__ p_r
   }
 }
 
-void launch_compact(int64_t n, const uint8_t* flag, const int64_t* off, const int32_t* fr, const int32_t* fd,
+void launch_compact(int64_t nwords, const uint32_t* flag, const int64_t* woff, const int32_t* fr, const int32_t* fd,
                     int32_t* p_read, int32_t* p_diag, cudaStream_t st) {
-  if (n <= 0) return;
-  int64_t blocks = (n + 255) / 256;
+  if (nwords <= 0) return;
+  int64_t blocks = (nwords + 255) / 256;
   if (blocks > 148 * 32) blocks = 148 * 32;
-  compact_kernel<<<(unsigned)blocks, 256, 0, st>>>(n, flag, off, fr, fd, p_read, p_diag);
+  compact_kernel<<<(unsigned)blocks, 256, 0, st>>>(nwords, flag, woff, fr, fd, p_read, p_diag);
 }
 
 void launch_slot_bounds(int64_t npass, const int32_t* p_read, int32_t* pstart, int32_t* pcount, cudaStream_t st) {

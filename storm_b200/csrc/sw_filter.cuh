@@ -30,7 +30,21 @@ void launch_expand_reads(const ReadsDev& rd, uint8_t* rexp, int64_t rstride, cud
 
 bool filter_dpx_ok(const ScoreParams& sp, int max_len);
 void launch_filter_flat_job(const FilterJob& job, const ScoreParams& sp, bool dpx, cudaStream_t st);
-void launch_compact(int64_t n, const uint8_t* flag, const int64_t* off, const int32_t* fr, const int32_t* fd,
+// pass bytes of n candidates -> words of 32 pass bits (bit t & 31 of word t >> 5)
+void launch_pack_flags(int64_t n, const uint8_t* flag, uint32_t* words, cudaStream_t st);
+// A word of pass bits, counted as its number of passing candidates when scanned.
+struct PassWord {
+  uint32_t bits;
+  __host__ __device__ explicit operator int64_t() const {
+#if defined(__CUDA_ARCH__)
+    return __popc(bits);
+#else
+    return __builtin_popcount(bits);
+#endif
+  }
+};
+// passing candidates, in order: word w's set bits go to woff[w], woff[w] + 1, ...
+void launch_compact(int64_t nwords, const uint32_t* flag, const int64_t* woff, const int32_t* fr, const int32_t* fd,
                     int32_t* p_read, int32_t* p_diag, cudaStream_t st);
 void launch_slot_bounds(int64_t npass, const int32_t* p_read, int32_t* pstart, int32_t* pcount, cudaStream_t st);
 
