@@ -62,12 +62,12 @@ def build(verbose: bool = False, force: bool = False) -> str:
             objs.append(obj)
         _run([nvcc(), "-shared", "-gencode", "arch=compute_100a,code=sm_100a", "-o", LIB] + objs + ["-cudart", "static"], verbose)
     if force or _stale(HOST_LIB, deps):
-        _run(["gcc", "-O2", "-std=gnu11", "-fPIC", "-shared", "-o", HOST_LIB,
+        _run(["gcc", "-O2", "-std=gnu11", "-fopenmp", "-fPIC", "-shared", "-o", HOST_LIB,
               os.path.join(CSRC, "host", "storm_host.c"), "-lm"], verbose)
     for colour, name in ((0, "storm-nucleotide"), (1, "storm-color")):
         exe = os.path.join(BIN_DIR, name)
         if force or _stale(exe, deps + [LIB]):
-            _run(["gcc", "-O2", "-std=gnu11", "-DSTORM_COLOUR=%d" % colour, "-o", exe]
+            _run(["gcc", "-O2", "-std=gnu11", "-fopenmp", "-DSTORM_COLOUR=%d" % colour, "-o", exe]
                  + [os.path.join(CSRC, s) for s in HOST_SOURCES]
                  + ["-L" + LIB_DIR, "-lstormgpu", "-Wl,-rpath,$ORIGIN/../lib", "-lm"], verbose)
     return LIB

@@ -3,6 +3,10 @@
  */
 #include "storm_host.h"
 
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
 #include <ctype.h>
 #include <math.h>
 #include <stdarg.h>
@@ -518,19 +522,29 @@ void sh_free_reads(sh_reads *r) {
 
 /* ---------------------------------------------------------------------------- ordering */
 
+/* order: length, then tag, then file position */
 typedef struct sortkey { int16_t len; uint64_t tag; int64_t idx; } sortkey;
-static int cmp_sortkey(const void *a, const void *b) {
-  const sortkey *x = a, *y = b;
-  if (x->len != y->len) return x->len < y->len ? -1 : 1;
-  if (x->tag != y->tag) return x->tag < y->tag ? -1 : 1;
-  return (x->idx > y->idx) - (x->idx < y->idx);
-}
 
 void sh_sort_reads(sh_reads *r) {
   int64_t n = r->n;
   sortkey *k = malloc(sizeof(sortkey) * (size_t)(n ? n : 1));
   for (int64_t i = 0; i < n; ++i) { k[i].len = r->lengths[i]; k[i].tag = r->tags[i]; k[i].idx = i; }
-  qsort(k, (size_t)n, sizeof(sortkey), cmp_sortkey);
+  /* stable LSD radix sort on (length, tag), bytes of the tag first: from file order, equal keys
+   * keep file order */
+  {
+    sortkey *t = malloc(sizeof(sortkey) * (size_t)(n ? n : 1));
+    for (int pass = 0; pass < 10 && n > 0; ++pass) {
+      int64_t cnt[257] = {0};
+#define SK_BYTE(x) (pass < 8 ? (int)(((x).tag >> (8 * pass)) & 0xff) : (int)((((uint16_t)(x).len) >> (8 * (pass - 8))) & 0xff))
+      for (int64_t i = 0; i < n; ++i) cnt[SK_BYTE(k[i]) + 1]++;
+      if (cnt[SK_BYTE(k[0]) + 1] == n) continue;  /* one value of this byte: order unchanged */
+      for (int b = 0; b < 256; ++b) cnt[b + 1] += cnt[b];
+      for (int64_t i = 0; i < n; ++i) t[cnt[SK_BYTE(k[i])]++] = k[i];
+#undef SK_BYTE
+      sortkey *sw = k; k = t; t = sw;
+    }
+    free(t);
+  }
   uint8_t *codes = malloc((size_t)(n ? n : 1) * (size_t)r->code_stride);
   uint8_t *levels = r->levels ? malloc((size_t)(n ? n : 1) * (size_t)r->level_stride) : NULL;
   int16_t *lengths = malloc(sizeof(int16_t) * (size_t)(n ? n : 1));
@@ -658,43 +672,38 @@ int sh_mapq(int rank, int score0, int score1, int score_rank, int min_score, int
 }
 
 /* base of sequence s at position pos in colour space, from its first base and colours */
-static int ref_symbol_at(const sh_refs *refs, int s, int64_t pos) {
-  int b = refs->first_base[s];
-  for (int64_t p = 0; p < pos && p < refs->sizes[s]; ++p) b ^= get2(refs->codes[s], p);
-  return b & 3;
-}
 
 typedef struct colour_cursor { int seq; int64_t pos; int base; } colour_cursor;
 
-int sh_write_sam(FILE *f, const sh_sam_opts *o, const sh_refs *refs, const sh_reads *reads,
-                 const stormgpu_results *res, int64_t first, int64_t count, int header) {
-  const int colour = o->colour;
-  if (header) {
-    fprintf(f, "@HD\tVN:1.4\tSO:unsorted\n");
-    for (int s = 0; s < refs->n; ++s)
-      fprintf(f, "@SQ\tSN:%s\tLN:%ld\n", refs->names[s] ? refs->names[s] : "*",
-              (long)(refs->sizes[s] + (colour ? 1 : 0)));
-    const char *rg = reads->db_name ? reads->db_name : "*";
-    fprintf(f, "@RG\tID:%s\tSM:%s\n", rg, rg);
-    fprintf(f, "@PG\tID:%s\tVN:%s\tCL:\"", "SToRM", "0.0101");
-    for (int i = 0; i < o->argc; ++i) fprintf(f, "%s ", o->argv[i]);
-    fprintf(f, "\"\n");
-  }
-  /* colour space: prefix bases per sequence, computed lazily from a checkpoint table */
-  int64_t **chk = NULL;
-  const int64_t STEP = 4096;
-  if (colour) {
-    chk = calloc((size_t)refs->n, sizeof(int64_t *));
-    for (int s = 0; s < refs->n; ++s) {
-      int64_t nck = refs->sizes[s] / STEP + 2;
-      chk[s] = malloc(sizeof(int64_t) * (size_t)nck);
-      int b = refs->first_base[s];
-      for (int64_t p = 0, k = 0; k < nck; ++k) {
-        chk[s][k] = b;
-        for (int64_t e = (k + 1) * STEP; p < e && p < refs->sizes[s]; ++p) b ^= get2(refs->codes[s], p);
-      }
+/* colour space: base of each sequence at every multiple of SYM_STEP positions (the first
+ * base transformed by the colours before it), so that a record's reference base needs at most
+ * SYM_STEP - 1 more steps */
+#define SYM_STEP 64
+static uint8_t **symbol_checkpoints(const sh_refs *refs) {
+  uint8_t **chk = calloc((size_t)refs->n, sizeof(uint8_t *));
+  for (int s = 0; s < refs->n; ++s) {
+    const int64_t nck = refs->sizes[s] / SYM_STEP + 2;
+    chk[s] = malloc((size_t)nck);
+    int b = refs->first_base[s];
+    for (int64_t p = 0, k = 0; k < nck; ++k) {
+      chk[s][k] = (uint8_t)b;
+      for (int64_t e = (k + 1) * SYM_STEP; p < e && p < refs->sizes[s]; ++p) b ^= get2(refs->codes[s], p);
     }
   }
+  return chk;
+}
+
+static int symbol_at(const sh_refs *refs, uint8_t *const *chk, int s, int64_t pos) {
+  const int64_t ck = pos / SYM_STEP;
+  int b = chk[s][ck];
+  for (int64_t p = ck * SYM_STEP; p < pos && p < refs->sizes[s]; ++p) b ^= get2(refs->codes[s], p);
+  return b & 3;
+}
+
+/* the records of reads [first, first + count) (hit_map.c:197-504) */
+static void write_sam_records(FILE *f, const sh_sam_opts *o, const sh_refs *refs, const sh_reads *reads,
+                              const stormgpu_results *res, int64_t first, int64_t count, uint8_t *const *chk) {
+  const int colour = o->colour;
   char cigar[4 * STORMGPU_MAX_READ_LEN + 64], seq[2 * STORMGPU_MAX_READ_LEN + 8];
   static const char B[4] = {'A', 'C', 'G', 'T'};
   char *qbuf = malloc((size_t)reads->max_len + 8);
@@ -715,12 +724,7 @@ int sh_write_sam(FILE *f, const sh_sam_opts *o, const sh_refs *refs, const sh_re
         int mapq = sh_mapq(k, h[0].score, h[1].score, h[k].score, o->min_score, o->delta_m);
         int sym = 0;
         if (colour) {
-          if (ref_start >= 0) {
-            int64_t ck = ref_start / STEP;
-            int b = (int)chk[ref_id][ck];
-            for (int64_t p = ck * STEP; p < ref_start && p < refs->sizes[ref_id]; ++p) b ^= get2(refs->codes[ref_id], p);
-            sym = b & 3;
-          } else sym = ref_symbol_at(refs, ref_id, 0);
+          sym = symbol_at(refs, chk, ref_id, ref_start >= 0 ? ref_start : 0);
         }
         int ed = sh_traceback_to_cigar(res->tb + (size_t)(r * 4 + k) * (size_t)res->tb_stride, h[k].tb_len,
                                        refs->codes[ref_id], ref_start, colour, sym, cigar, seq);
@@ -762,6 +766,51 @@ int sh_write_sam(FILE *f, const sh_sam_opts *o, const sh_refs *refs, const sh_re
     }
   }
   free(qbuf);
+}
+
+int sh_write_sam(FILE *f, const sh_sam_opts *o, const sh_refs *refs, const sh_reads *reads,
+                 const stormgpu_results *res, int64_t first, int64_t count, int header) {
+  const int colour = o->colour;
+  if (header) {
+    fprintf(f, "@HD\tVN:1.4\tSO:unsorted\n");
+    for (int s = 0; s < refs->n; ++s)
+      fprintf(f, "@SQ\tSN:%s\tLN:%ld\n", refs->names[s] ? refs->names[s] : "*",
+              (long)(refs->sizes[s] + (colour ? 1 : 0)));
+    const char *rg = reads->db_name ? reads->db_name : "*";
+    fprintf(f, "@RG\tID:%s\tSM:%s\n", rg, rg);
+    fprintf(f, "@PG\tID:%s\tVN:%s\tCL:\"", "SToRM", "0.0101");
+    for (int i = 0; i < o->argc; ++i) fprintf(f, "%s ", o->argv[i]);
+    fprintf(f, "\"\n");
+  }
+  /* records formatted in chunks, several chunks at once, written in read order */
+  uint8_t **chk = colour ? symbol_checkpoints(refs) : NULL;
+  int nthreads = 1;
+#ifdef _OPENMP
+  nthreads = omp_get_max_threads();
+#endif
+  int64_t CH = count / (4 * (int64_t)nthreads);
+  CH = CH < 256 ? 256 : CH > 16384 ? 16384 : CH;
+  const int64_t per_round = CH * nthreads * 2;
+  char **bufs = calloc((size_t)nthreads * 2, sizeof(char *));
+  size_t *lens = calloc((size_t)nthreads * 2, sizeof(size_t));
+  for (int64_t lo = first; lo < first + count; lo += per_round) {
+    const int64_t hi = lo + per_round < first + count ? lo + per_round : first + count;
+    const int nchunks = (int)((hi - lo + CH - 1) / CH);
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int c = 0; c < nchunks; ++c) {
+      const int64_t a = lo + (int64_t)c * CH, e = a + CH < hi ? a + CH : hi;
+      FILE *m = open_memstream(&bufs[c], &lens[c]);
+      write_sam_records(m, o, refs, reads, res, a, e - a, chk);
+      fclose(m);
+    }
+    for (int c = 0; c < nchunks; ++c) {
+      fwrite(bufs[c], 1, lens[c], f);
+      free(bufs[c]);
+      bufs[c] = NULL;
+    }
+  }
+  free(bufs);
+  free(lens);
   if (chk) {
     for (int s = 0; s < refs->n; ++s) free(chk[s]);
     free(chk);
