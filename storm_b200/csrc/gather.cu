@@ -280,6 +280,11 @@ __device__ __forceinline__ void bucket_sort_emit(int32_t* a, int32_t* b, int32_t
 
 constexpr int kWarpCap = 768;
 constexpr int kGWarps = 4;
+// Reads per warp: block b takes the contiguous reads [32 b, 32 b + 32), warp w the reads
+// 32 b + w + 4 k.  Blocks start in index order, so warps finish, and append their candidates,
+// in close to read order: a batch whose reads are grouped by length gives a candidate list
+// grouped by length, which the filter needs to keep one read length per SM.
+constexpr int kGReadsPerWarp = 8;
 constexpr int kReadBytes = STORMGPU_MAX_READ_LEN / 4 + 16;
 
 constexpr int kItems = 4;  // (seed, position) items per lane and round: 128 key lookups in flight per warp
@@ -302,9 +307,11 @@ __global__ void __launch_bounds__(kGWarps * 32) gather_fused_kernel(ReadsDev rd,
   int32_t* s = sm[w];
   int32_t* so = soff[w];
   uint8_t* rs = srd[w];
-  const int64_t nwarps = (int64_t)gridDim.x * kGWarps;
   unsigned long long lookups = 0, positions = 0;
-  for (int64_t r = (int64_t)blockIdx.x * kGWarps + w; r < rd.n; r += nwarps) {
+  const int64_t rbase = (int64_t)blockIdx.x * kGWarps * kGReadsPerWarp + w;
+  for (int k = 0; k < kGReadsPerWarp; ++k) {
+    const int64_t r = rbase + (int64_t)k * kGWarps;
+    if (r >= rd.n) break;
     const int L = rd.lengths[r];
     {  // the read's packed codes into shared memory, and the item offsets of the seeds
       const uint8_t* src = rd.codes + r * rd.cstride;
@@ -484,8 +491,7 @@ __global__ void gather_block_kernel(ReadsDev rd, IndexView ix, int I, const int3
 void launch_gather_fused(const ReadsDev& rd, const IndexView& ix, int I, const GatherOut& go, const SeedSet& seeds,
                          cudaStream_t st) {
   if (rd.n <= 0) return;
-  int64_t blocks = (rd.n + kGWarps - 1) / kGWarps;
-  if (blocks > 148 * 16) blocks = 148 * 16;
+  const int64_t blocks = (rd.n + kGWarps * kGReadsPerWarp - 1) / (kGWarps * kGReadsPerWarp);
   gather_fused_kernel<<<(unsigned)blocks, kGWarps * 32, 0, st>>>(rd, ix, I, go, seeds);
 }
 
