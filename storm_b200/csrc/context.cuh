@@ -72,6 +72,7 @@ struct stormgpu_ctx {
   sg::DevBuf<uint8_t> a_tb;
   sg::DevBuf<uint32_t> scratch;
   sg::DevBuf<unsigned long long> counters;
+  sg::DevBuf<uint32_t> ord, ord_tmp;  // length order of a mixed-length batch: sort keys and values, sort scratch
   cudaEvent_t ev[8];
   int64_t last_n = -1;  // reads of the last stormgpu_map call (its results stay in hits / mapped)
   // genome_map placement

@@ -310,8 +310,9 @@ __global__ void __launch_bounds__(kGWarps * 32) gather_fused_kernel(ReadsDev rd,
   unsigned long long lookups = 0, positions = 0;
   const int64_t rbase = (int64_t)blockIdx.x * kGWarps * kGReadsPerWarp + w;
   for (int k = 0; k < kGReadsPerWarp; ++k) {
-    const int64_t r = rbase + (int64_t)k * kGWarps;
-    if (r >= rd.n) break;
+    const int64_t kr = rbase + (int64_t)k * kGWarps;
+    if (kr >= rd.n) break;
+    const int64_t r = rd.order ? (int64_t)rd.order[kr] : kr;
     const int L = rd.lengths[r];
     {  // the read's packed codes into shared memory, and the item offsets of the seeds
       const uint8_t* src = rd.codes + r * rd.cstride;

@@ -29,6 +29,9 @@ struct ReadsDev {
   const uint8_t* levels;   // may be null
   int64_t lstride;
   const int16_t* lengths;
+  // may be null; else the fused gather visits read order[k] k-th (reads grouped by length, so
+  // that the candidate list, and with it the filter's and the alignment's blocks, is too)
+  const int32_t* order;
 };
 
 struct IndexView {

@@ -14,6 +14,7 @@
 #include "scan.cuh"
 #include "sw_filter.cuh"
 #include "gather.cuh"
+#include "radix.cuh"
 #include "context.cuh"
 
 static thread_local char g_err[1024];
@@ -246,6 +247,15 @@ constexpr int64_t kMaxCandidatesPerPass = 1000000000;
 constexpr int64_t kMaxPassingPerPass = 100000000;  // their tracebacks are kept until the replay
 constexpr int kSplitBatch = 1;
 
+// sort keys of the length order: key = read length, value = read index
+static __global__ void length_keys_kernel(const int16_t* __restrict__ lengths, int64_t n, uint32_t* __restrict__ keys,
+                                          uint32_t* __restrict__ vals) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    keys[i] = (uint32_t)(uint16_t)lengths[i];
+    vals[i] = (uint32_t)i;
+  }
+}
+
 static int map_device_once(stormgpu_ctx* c, const stormgpu_reads* reads, stormgpu_results* out) {
   if (!c->indexed) { sg_set_error("stormgpu_build_index must be called before mapping"); return STORMGPU_ESTATE; }
   cudaStream_t st = c->st;
@@ -271,7 +281,19 @@ static int map_device_once(stormgpu_ctx* c, const stormgpu_reads* reads, stormgp
   launch_init_results(n, out->hits, out->mapped, out->tb, out->tb_stride, st);
   launches++;
   if (n == 0) return 0;
-  ReadsDev fwd{n, reads->codes, reads->code_stride, reads->levels, reads->level_stride, reads->lengths};
+  ReadsDev fwd{n, reads->codes, reads->code_stride, reads->levels, reads->level_stride, reads->lengths, nullptr};
+  if (minL != maxL) {
+    // reads of several lengths: the gather visits them grouped by length (a stable sort of the
+    // read indices by length); a batch in any read order then runs like one sorted by length
+    if (c->ord.grow(4 * n) || c->ord_tmp.grow(radix_tmp_bytes(n) / 4 + 16)) return STORMGPU_ENOMEM;
+    uint32_t *k0 = c->ord.p, *v0 = k0 + n, *k1 = v0 + n, *v1 = k1 + n;
+    length_keys_kernel<<<(unsigned)std::min<int64_t>((n + 255) / 256, 148 * 8), 256, 0, st>>>(reads->lengths, n, k0, v0);
+    int bits = 1;
+    while ((1 << bits) <= maxL) ++bits;
+    const int which = radix_sort_pairs(k0, v0, k1, v1, n, bits, c->ord_tmp.p, st);
+    fwd.order = reinterpret_cast<const int32_t*>(which ? v1 : v0);
+    launches += 1 + 3 * ((bits + kRadixBits - 1) / kRadixBits);
+  }
   ReadsDev rev = fwd;
   if (c->p.senses & 2) {
     if (c->rcodes.grow(n * reads->code_stride)) return STORMGPU_ENOMEM;

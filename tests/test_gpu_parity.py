@@ -198,3 +198,35 @@ def test_map_api_vs_oracle(colour, indels, seeds):
         assert bytes(res.tb[k, :nb]) == bytes(tb[k, :nb]), k
     assert mapped.sum() > len(seqs) // 4
     assert st["filter_passed"] == cnt[1]
+
+
+def test_map_is_invariant_to_read_order_in_a_mixed_length_batch():
+    """A batch of reads of several lengths is gathered grouped by length (a device sort of the
+    read indices); the results of a read must not depend on where it sits in the batch."""
+    from storm_b200 import synth
+    genome = synth.make_genome([60000], 31, gc=0.42, repeat_frac=0.25)
+    seqs, quals = synth.simulate_nucleotide_reads(genome, 3000, [35, 50, 75, 100, 150], 31)
+    codes, levels, lengths = _reads_arrays(seqs, quals)
+    prm = api.params(indels=15, min_score=100, min_score_filter=95)
+    m = api.Mapper(prm, "##-##-###-###;###--#-#--#--####")
+    for _, s in genome:
+        cp = ffi.pack2(s, PADB)
+        mk = ffi.pack2(np.zeros(len(s), np.uint8), PADB, fill=0x55)
+        m.add_reference(cp[PADB:], mk[PADB:], len(s))
+    m.build_index()
+    tbs = ((150 + 15 + 1) // 2 + 7) & ~7
+    base = m.map(api.ReadBatch(codes, lengths, levels), tbs)
+    perm = np.random.default_rng(5).permutation(len(seqs))
+    shuf = m.map(api.ReadBatch(codes[perm], lengths[perm], levels[perm]), tbs)
+    order = np.argsort(lengths, kind="stable")
+    srt = m.map(api.ReadBatch(codes[order], lengths[order], levels[order]), tbs)
+    m.close()
+    assert base.mapped.sum() > len(seqs) // 4
+    for got, p in ((shuf, perm), (srt, order)):
+        assert np.array_equal(got.mapped, base.mapped[p])
+        h4 = (4 * p[:, None] + np.arange(4)).ravel()
+        assert got.hits.tobytes() == base.hits[h4].tobytes()
+        live = np.nonzero(got.hits["ref_id"] >= 0)[0]
+        for k in live:
+            nb = (int(got.hits["tb_len"][k]) + 1) // 2
+            assert bytes(got.tb[k, :nb]) == bytes(base.tb[h4[k], :nb]), k
