@@ -538,12 +538,12 @@ def main():
     st = stage[-1]
     peaks = json.load(open(PEAKS_PATH)) if os.path.exists(PEAKS_PATH) else {}
     hbm = peaks.get("hbm_gbs", 6650.0)
-    # filter: algorithmic work = 3.75 lane instructions per cell update (7.5 per register of two
-    # packed 16-bit cells: 2 gap subtractions, max, 3-way max, selector subtraction, permute,
+    # filter: algorithmic work = 3.25 lane instructions per cell update (6.5 per register of two
+    # packed 16-bit cells: gap subtraction, add-max, 3-way max, selector subtraction, permute,
     # add-max, half a running max), over W * 2 * (L + W - 1) cell updates per candidate; peak =
     # the measured rate of that instruction mix (stormgpu_filter_peak)
     ops_s, ms_peak = _filter_peak(api, local)
-    filter_ops = st["filter_cells"] * 3.75
+    filter_ops = st["filter_cells"] * 3.25
     gather_bytes = st["seed_lookups"] * 8 + st["hit_positions"] * 4 + n * (reads.max_len / 4) * 2 + st["candidates"] * 4
     stages = {
         "sw_filter": {"ms": st["ms_filter"], "bound": "int", "achieved": filter_ops / (st["ms_filter"] * 1e-3) / 1e12,

@@ -257,7 +257,7 @@ int stormgpu_index_one(const char *seed, int32_t stdev_distance, const uint8_t *
                        int32_t *map, int64_t map_capacity, int64_t *map_len);
 
 /* Measurement helper: the device's rate, in 32-bit lane instructions per second, for the
- * instruction mix of one step of the packed 16-bit filter recurrence (7.5 instructions per
+ * instruction mix of one step of the packed 16-bit filter recurrence (6.5 instructions per
  * register of two cells), run register-resident; the roofline denominator of the filter.
  * No counterpart in the reference (it has no GPU). */
 int stormgpu_filter_peak(int device, double *ops_per_s, double *ms);

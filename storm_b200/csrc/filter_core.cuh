@@ -236,7 +236,7 @@ template <int W, int MODE, int K> __host__ __device__ constexpr uint32_t split_p
 template <int W, bool ODD, int T, int Q, uint32_t MB>
 SG_HD void fstep_split(uint32_t (&A)[W / 2], uint32_t (&B)[W / 2], uint32_t (&M1)[W / 2], uint32_t (&M2)[W / 2],
                        uint32_t (&I1)[W / 2], uint32_t& Max, uint32_t rcur, uint32_t gcur, uint32_t TLO,
-                       uint32_t THI, uint32_t CFE, uint32_t CFO) {
+                       uint32_t THI, uint32_t NFE, uint32_t CFO) {
   constexpr int H = W / 2;
   constexpr int RA = (Q + 1) % H;                // read steps done (mod H), this one included
   constexpr int RB = (ODD ? Q + 1 : Q) % H;      // genome steps done (mod H)
@@ -249,7 +249,9 @@ SG_HD void fstep_split(uint32_t (&A)[W / 2], uint32_t (&B)[W / 2], uint32_t (&M1
   }
   uint32_t P[H], Mn[H], In[H];
 #pragma unroll
-  for (int j = 0; j < H; ++j) P[j] = __vimax_s16x2_relu(I1[j] - CFE, M1[j] - CFO);  // halves are positive
+  // P = max(I1 - ext, M1 - open) as one add-max: NFE holds -ext in both halves, and every half
+  // stays positive (cells are biased by 256, ext and open are below 256)
+  for (int j = 0; j < H; ++j) P[j] = __viaddmax_s16x2(I1[j], NFE, M1[j] - CFO);
 #pragma unroll
   for (int j = 0; j < H; ++j) {
     uint32_t nbr;
@@ -286,12 +288,12 @@ SG_HD void fstep_split(uint32_t (&A)[W / 2], uint32_t (&B)[W / 2], uint32_t (&M1
 template <int W, int MODE, int QB, int K, int NP, int NWD>
 SG_HD void run_pairs_split(uint32_t (&A)[W / 2], uint32_t (&B)[W / 2], uint32_t (&M1)[W / 2], uint32_t (&M2)[W / 2],
                            uint32_t (&I1)[W / 2], uint32_t& Max, const uint32_t (&rc)[NWD],
-                           const uint32_t (&gc)[NWD], uint32_t TLO, uint32_t THI, uint32_t CFE, uint32_t CFO) {
+                           const uint32_t (&gc)[NWD], uint32_t TLO, uint32_t THI, uint32_t NFE, uint32_t CFO) {
   if constexpr (K < NP) {
     constexpr uint32_t MB = split_pair_mask<W, MODE, K>();
-    fstep_split<W, false, K % 4, QB + K, MB>(A, B, M1, M2, I1, Max, rc[K / 4], gc[K / 4], TLO, THI, CFE, CFO);
-    fstep_split<W, true, K % 4, QB + K, MB>(A, B, M1, M2, I1, Max, rc[K / 4], gc[K / 4], TLO, THI, CFE, CFO);
-    run_pairs_split<W, MODE, QB, K + 1, NP, NWD>(A, B, M1, M2, I1, Max, rc, gc, TLO, THI, CFE, CFO);
+    fstep_split<W, false, K % 4, QB + K, MB>(A, B, M1, M2, I1, Max, rc[K / 4], gc[K / 4], TLO, THI, NFE, CFO);
+    fstep_split<W, true, K % 4, QB + K, MB>(A, B, M1, M2, I1, Max, rc[K / 4], gc[K / 4], TLO, THI, NFE, CFO);
+    run_pairs_split<W, MODE, QB, K + 1, NP, NWD>(A, B, M1, M2, I1, Max, rc, gc, TLO, THI, NFE, CFO);
   }
 }
 
@@ -299,11 +301,11 @@ SG_HD void run_pairs_split(uint32_t (&A)[W / 2], uint32_t (&B)[W / 2], uint32_t 
 template <int W, int QB, int K, int NP, int NWD>
 SG_HD void run_rest_split(int r, uint32_t (&A)[W / 2], uint32_t (&B)[W / 2], uint32_t (&M1)[W / 2],
                           uint32_t (&M2)[W / 2], uint32_t (&I1)[W / 2], uint32_t& Max, const uint32_t (&rc)[NWD],
-                          const uint32_t (&gc)[NWD], uint32_t TLO, uint32_t THI, uint32_t CFE, uint32_t CFO) {
+                          const uint32_t (&gc)[NWD], uint32_t TLO, uint32_t THI, uint32_t NFE, uint32_t CFO) {
   if constexpr (K < NP) {
     if (K < r) {
-      run_pairs_split<W, 0, QB, K, K + 1, NWD>(A, B, M1, M2, I1, Max, rc, gc, TLO, THI, CFE, CFO);
-      run_rest_split<W, QB, K + 1, NP, NWD>(r, A, B, M1, M2, I1, Max, rc, gc, TLO, THI, CFE, CFO);
+      run_pairs_split<W, 0, QB, K, K + 1, NWD>(A, B, M1, M2, I1, Max, rc, gc, TLO, THI, NFE, CFO);
+      run_rest_split<W, QB, K + 1, NP, NWD>(r, A, B, M1, M2, I1, Max, rc, gc, TLO, THI, NFE, CFO);
     }
   }
 }
@@ -321,7 +323,7 @@ SG_HD uint32_t funnel_sel(uint32_t s) { return s | ((s + 1) << 4) | ((s + 2) << 
 // the epilogue.
 template <int W>
 SG_HD int filter_split(const uint8_t* __restrict__ gexp, int64_t pos, const uint8_t* __restrict__ rexp, int L,
-                       uint32_t TLO, uint32_t THI, uint32_t CFE, uint32_t CFO) {
+                       uint32_t TLO, uint32_t THI, uint32_t NFE, uint32_t CFO) {
   constexpr int H = W / 2;
   constexpr int BP = H > 4 ? H : 4;
   constexpr int NPRO = W - 1;
@@ -351,7 +353,7 @@ SG_HD int filter_split(const uint8_t* __restrict__ gexp, int64_t pos, const uint
       gc[k] = prmt(wp, wn, sel);
       wp = wn;
     }
-    run_pairs_split<W, 1, 0, 0, NPRO, NWP>(A, B, M1, M2, I1, Max, rc, gc, TLO, THI, CFE, CFO);
+    run_pairs_split<W, 1, 0, 0, NPRO, NWP>(A, B, M1, M2, I1, Max, rc, gc, TLO, THI, NFE, CFO);
   }
   {  // main: pairs W-1..L-1, index W-1 = H-1 mod H at every block start
     const int nmain = L - W + 1;
@@ -374,7 +376,7 @@ SG_HD int filter_split(const uint8_t* __restrict__ gexp, int64_t pos, const uint
         gp = gn;
         rp = rn;
       }
-      run_pairs_split<W, 0, H - 1, 0, BP, NWB>(A, B, M1, M2, I1, Max, rc, gc, TLO, THI, CFE, CFO);
+      run_pairs_split<W, 0, H - 1, 0, BP, NWB>(A, B, M1, M2, I1, Max, rc, gc, TLO, THI, NFE, CFO);
     }
     const int r = nmain - pm;
     if (r > 0) {
@@ -388,7 +390,7 @@ SG_HD int filter_split(const uint8_t* __restrict__ gexp, int64_t pos, const uint
         gp = gn;
         rp = rn;
       }
-      run_rest_split<W, H - 1, 0, BP, NWB>(r, A, B, M1, M2, I1, Max, rc, gc, TLO, THI, CFE, CFO);
+      run_rest_split<W, H - 1, 0, BP, NWB>(r, A, B, M1, M2, I1, Max, rc, gc, TLO, THI, NFE, CFO);
     }
   }
   if (H > 1) {  // back to rotation 0: logical read register j = A[(j + L) mod H], genome B[(j - L) mod H]
@@ -422,18 +424,18 @@ SG_HD int filter_split(const uint8_t* __restrict__ gexp, int64_t pos, const uint
       gc[k] = prmt(wp, wn, sel);
       wp = wn;
     }
-    run_pairs_split<W, 2, 0, 0, NPRO, NWP>(A, B, M1, M2, I1, Max, rc, gc, TLO, THI, CFE, CFO);
+    run_pairs_split<W, 2, 0, 0, NPRO, NWP>(A, B, M1, M2, I1, Max, rc, gc, TLO, THI, NFE, CFO);
   }
   const int lo = (int)(int16_t)(Max & 0xffffu), hi = (int)(int16_t)(Max >> 16);
   return (lo > hi ? lo : hi) - (int)kFB;
 }
 
-SG_HD void filter_split_consts(int fm, int fx, int fo, int fe, uint32_t& TLO, uint32_t& THI, uint32_t& CFE,
+SG_HD void filter_split_consts(int fm, int fx, int fo, int fe, uint32_t& TLO, uint32_t& THI, uint32_t& NFE,
                             uint32_t& CFO) {
   const uint32_t mis = (uint32_t)((256 - fx) & 0xff);
   TLO = (mis << 8) | (mis << 16) | (mis << 24);
   THI = (uint32_t)(fm & 0xff) | (mis << 8) | (mis << 16) | (mis << 24);
-  CFE = (uint32_t)fe * 0x10001u;
+  NFE = (uint32_t)(uint16_t)(-fe) * 0x10001u;
   CFO = (uint32_t)fo * 0x10001u;
 }
 

@@ -67,10 +67,9 @@ template <int W, bool SHORT>
 __global__ void __launch_bounds__(256, (W <= 8 ? 4 : 2)) filter_flat_dpx_kernel(FilterJob job) {
   const uint32_t T = (uint32_t)(job.fm & 0xff) | ((uint32_t)((256 - job.fx) & 0xff) << 8) |
                      ((uint32_t)((256 - job.fx) & 0xff) << 16) | ((uint32_t)((256 - job.fx) & 0xff) << 24);
-  const uint32_t NFE = (uint32_t)(uint16_t)(-job.fe) * 0x10001u;
   const uint32_t NFO = (uint32_t)(uint16_t)(-job.fo) * 0x10001u;
-  uint32_t TLO, THI, CFE, CFO;
-  filter_split_consts(job.fm, job.fx, job.fo, job.fe, TLO, THI, CFE, CFO);
+  uint32_t TLO, THI, NFE, CFO;  // NFE: -ext in both halves (both layouts)
+  filter_split_consts(job.fm, job.fx, job.fo, job.fe, TLO, THI, NFE, CFO);
   unsigned long long cells = 0, cands = 0, band = 0;
   const int64_t t0 = (int64_t)blockIdx.x * blockDim.x * kFilterTile + threadIdx.x;
   for (int i = 0; i < kFilterTile; ++i) {
@@ -82,7 +81,7 @@ __global__ void __launch_bounds__(256, (W <= 8 ? 4 : 2)) filter_flat_dpx_kernel(
     const int64_t pos = (int64_t)d - job.Is;
     int mx;
     if (!SHORT || L >= W)
-      mx = filter_split<W>(job.gexp, pos, job.rexp + (int64_t)r * job.rstride, L, TLO, THI, CFE, CFO);
+      mx = filter_split<W>(job.gexp, pos, job.rexp + (int64_t)r * job.rstride, L, TLO, THI, NFE, CFO);
     else
       mx = filter_dpx<W>(job.genome, pos, job.codes + (int64_t)r * job.cstride, job.cstride, L, T, NFE, NFO);
     job.flag[t] = mx > job.fthr ? 1 : 0;
