@@ -217,6 +217,7 @@ def batched_arm(a, w, ref_path, reads_path, d):
     reference.add_to(mapper)
     mapper.build_index()
     batch = reads.batch()
+    tuning = mapper.autotune(batch, sample=200000)  # launch parameters (no effect on results)
     tbs = ((reads.max_len + prm.allowed_indels + 1) // 2 + 7) & ~7
     L = reads.lengths
     cuts = [0] + [int(i) for i in np.nonzero(np.diff(L))[0] + 1] + [reads.n]
@@ -247,7 +248,7 @@ def batched_arm(a, w, ref_path, reads_path, d):
             "n_gpus": 1, "steps": a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "u8/int32", "data": "synthetic",
             "config": {"workload": workload_name(a.cfg, a.scale), "reads": n, "lengths": sorted(set(int(x) for x in L)),
-                       "reference_codes": sum(w["ref_sizes"]), "args": " ".join(w["args"])},
+                       "reference_codes": sum(w["ref_sizes"]), "args": " ".join(w["args"]), "tuning": tuning},
             "batched": {"reads_per_s": n / min(batched_t), "ms": 1000 * min(batched_t)},
             "plain_per_length": {"reads_per_s": n / min(plain_t), "ms": 1000 * min(plain_t), "batches": len(buckets)},
             "batched_over_plain": min(plain_t) / min(batched_t), "same_records": same,
@@ -452,6 +453,13 @@ def main():
 
     # device-resident inputs and outputs
     batch = reads.batch()
+    # launch parameters picked by the autotuner on a sample of the workload (setup, untimed;
+    # they change no result)
+    t0 = time.perf_counter()
+    mapper.build_index()
+    tuning = mapper.autotune(batch, sample=200000)
+    tune_s = time.perf_counter() - t0
+    log("rank %d: autotuned %s in %.1f s" % (rank, tuning, tune_s))
     d_codes = torch.from_numpy(batch.codes).to(dev)
     d_levels = torch.from_numpy(batch.levels).to(dev) if batch.levels is not None else None
     d_len = torch.from_numpy(batch.lengths.copy()).to(dev)
@@ -584,7 +592,8 @@ def main():
                 "config": {"workload": workload_name(a.cfg, a.scale), "reads_per_gpu": n,
                            "reference_codes": sum(w["ref_sizes"]), "args": " ".join(w["args"]),
                            "step": "index build (all seeds) + map all reads, both strands",
-                           "l2": "flushed (512 MB write) between timed steps", "parallelism": "dp%d (reads)" % world},
+                           "l2": "flushed (512 MB write) between timed steps", "parallelism": "dp%d (reads)" % world,
+                           "tuning": tuning, "tuning_s": round(tune_s, 2)},
                 "mapped_fraction": mapped / n, "sw_filter_gcups": stages["sw_filter"]["gcups"],
                 "gpu_launches": int(st["kernels"]), "roofline": roof, "stages": stages,
                 "counts": {k: int(st[k]) for k in ("candidates", "filter_passed", "aligned", "seed_lookups",

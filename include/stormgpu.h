@@ -195,6 +195,31 @@ typedef struct stormgpu_stats {
 } stormgpu_stats;
 int stormgpu_get_stats(stormgpu_ctx *ctx, stormgpu_stats *out);
 
+/* Launch parameters of the mapping stages.  None of them changes a result: they trade
+ * occupancy, load balance and atomics against each other, and the best values depend on the
+ * read lengths, the band and the index.  No counterpart in the reference (it has no GPU). */
+typedef struct stormgpu_tuning {
+  int32_t gather_warp_cap;        /* index positions one gather warp holds in shared memory (the
+                                     hit bucket), 256..1536; reads with more go to a block per read */
+  int32_t gather_reads_per_steal; /* reads a gather warp takes from the work cursor at a time, 1..64 */
+  int32_t filter_rows;            /* rows of 256 candidates in a filter block's tile, 1..64 */
+  int32_t align_steal;            /* passing candidates an alignment warp takes at a time, 32..1024,
+                                     a multiple of 32 */
+  int32_t filter_cursor;          /* 1: the filter runs as a persistent grid whose blocks take tiles
+                                     from a work cursor; 0: one block per tile */
+} stormgpu_tuning;
+/* The context's parameters (defaults 768, 4, 8, 32, 0). */
+int stormgpu_get_tuning(stormgpu_ctx *ctx, stormgpu_tuning *out);
+/* Set them; STORMGPU_EINVAL (nothing changed) if one is outside its range. */
+int stormgpu_set_tuning(stormgpu_ctx *ctx, const stormgpu_tuning *t);
+/* Autotuner: maps the reads (or `sample` of them, spread evenly over the batch, when
+ * 0 < sample < n) once per candidate value of each parameter,
+ * stage by stage, times the stage it affects with CUDA events, and keeps the fastest value of
+ * each (the result is in the context and, when `out` is not null, in *out).  The reads are
+ * on the host, as for stormgpu_map.  Requires stormgpu_build_index.  Afterwards the context's
+ * last results (used by stormgpu_genome_map_greedy) are those of the sample. */
+int stormgpu_autotune(stormgpu_ctx *ctx, const stormgpu_reads *reads, int64_t sample, stormgpu_tuning *out);
+
 /* Unit-level entry points (host buffers), one kernel each, used by the parity tests.
  * ------------------------------------------------------------------------------------- */
 

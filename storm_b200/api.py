@@ -55,6 +55,15 @@ class Stats(C.Structure):
                                           "ms_replay", "ms_total")]
 
 
+class Tuning(C.Structure):
+    """stormgpu_tuning: launch parameters of the stages (none changes a result)."""
+    _fields_ = [(n, C.c_int32) for n in ("gather_warp_cap", "gather_reads_per_steal", "filter_rows", "align_steal",
+                                         "filter_cursor")]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 _lib = None
 
 
@@ -77,6 +86,9 @@ def lib():
         L.stormgpu_map_device.argtypes = [C.c_void_p, C.POINTER(Reads), C.POINTER(Results), C.c_void_p]
         L.stormgpu_sync.argtypes = [C.c_void_p]
         L.stormgpu_get_stats.argtypes = [C.c_void_p, C.POINTER(Stats)]
+        L.stormgpu_get_tuning.argtypes = [C.c_void_p, C.POINTER(Tuning)]
+        L.stormgpu_set_tuning.argtypes = [C.c_void_p, C.POINTER(Tuning)]
+        L.stormgpu_autotune.argtypes = [C.c_void_p, C.POINTER(Reads), C.c_int64, C.POINTER(Tuning)]
         L.stormgpu_sw_filter.argtypes = [C.c_int, C.c_int, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
                                          C.c_uint32, C.c_void_p, C.c_int64, C.c_int64, C.c_void_p,
                                          C.c_int64, C.c_void_p, C.c_void_p]
@@ -196,6 +208,25 @@ class Mapper:
 
     def sync(self):
         _check(lib().stormgpu_sync(self._ctx))
+
+    def tuning(self) -> dict:
+        t = Tuning()
+        _check(lib().stormgpu_get_tuning(self._ctx, C.byref(t)))
+        return t.as_dict()
+
+    def set_tuning(self, **kw):
+        t = Tuning()
+        _check(lib().stormgpu_get_tuning(self._ctx, C.byref(t)))
+        for k, v in kw.items():
+            setattr(t, k, int(v))
+        _check(lib().stormgpu_set_tuning(self._ctx, C.byref(t)))
+
+    def autotune(self, batch: ReadBatch, sample: int = 200000) -> dict:
+        """Pick the launch parameters by timing them on (up to `sample` of) the batch."""
+        t = Tuning()
+        rs = batch.cstruct()
+        _check(lib().stormgpu_autotune(self._ctx, C.byref(rs), int(sample), C.byref(t)))
+        return t.as_dict()
 
     def stats(self) -> dict:
         s = Stats()

@@ -1,0 +1,129 @@
+// autotune.cu -- the launch parameters of the mapping stages (stormgpu_tuning) and the
+// autotuner that picks them by timing.
+//
+// None of the parameters changes a result: the gather's hit bucket (positions a warp holds in
+// shared memory) trades occupancy against reads sent to the block-per-read kernel, its reads
+// per steal trade work-cursor atomics against load balance, the filter's tile rows trade
+// block barriers against the tail, its persistent grid (tiles from a work cursor) trades
+// the cursor's atomics and barriers against the block scheduler's tail, and the alignment's
+// run per steal trades atomics against
+// balance across candidates that stop early.  The best values depend on the read lengths, the
+// band and how repetitive the index is, so they are measured on the caller's own reads: every
+// candidate value of one parameter is run on a sample (the others at their best so far), the
+// stage it affects is timed with the CUDA events of stormgpu_map, and the fastest stays.
+// The reference has no counterpart (it has no GPU).
+#include <cstring>
+#include <vector>
+
+#include "common.cuh"
+#include "context.cuh"
+#include "gather.cuh"
+
+namespace {
+
+bool tuning_ok(const stormgpu_tuning& t) {
+  return t.gather_warp_cap >= 256 && t.gather_warp_cap <= sg::kMaxWarpCap &&
+         t.gather_reads_per_steal >= 1 && t.gather_reads_per_steal <= 64 && t.filter_rows >= 1 &&
+         t.filter_rows <= 64 && t.align_steal >= 32 && t.align_steal <= 1024 && t.align_steal % 32 == 0 &&
+         (t.filter_cursor == 0 || t.filter_cursor == 1);
+}
+
+}  // namespace
+
+extern "C" int stormgpu_get_tuning(stormgpu_ctx* c, stormgpu_tuning* out) {
+  if (!c || !out) { sg_set_error("null argument"); return STORMGPU_EINVAL; }
+  *out = c->tune;
+  return 0;
+}
+
+extern "C" int stormgpu_set_tuning(stormgpu_ctx* c, const stormgpu_tuning* t) {
+  if (!c || !t) { sg_set_error("null argument"); return STORMGPU_EINVAL; }
+  if (!tuning_ok(*t)) {
+    sg_set_error("tuning out of range (warp cap %d, reads per steal %d, filter rows %d, align steal %d, "
+                 "filter cursor %d)", t->gather_warp_cap, t->gather_reads_per_steal, t->filter_rows, t->align_steal,
+                 t->filter_cursor);
+    return STORMGPU_EINVAL;
+  }
+  c->tune = *t;
+  return 0;
+}
+
+extern "C" int stormgpu_autotune(stormgpu_ctx* c, const stormgpu_reads* reads, int64_t sample,
+                                 stormgpu_tuning* out) {
+  if (!c || !reads || reads->n < 0) { sg_set_error("null argument"); return STORMGPU_EINVAL; }
+  if (!c->indexed) { sg_set_error("stormgpu_build_index must be called before stormgpu_autotune"); return STORMGPU_ESTATE; }
+  // the sample: reads spread evenly over the batch (a batch sorted by length keeps its mix)
+  stormgpu_reads r = *reads;
+  std::vector<uint8_t> sc, sl, sf;
+  std::vector<int16_t> slen;
+  if (sample > 0 && r.n > sample) {
+    const int64_t m = sample;
+    sc.resize((size_t)(m * r.code_stride));
+    if (r.levels) sl.resize((size_t)(m * r.level_stride));
+    if (r.first_levels) sf.resize((size_t)m);
+    slen.resize((size_t)m);
+    for (int64_t k = 0; k < m; ++k) {
+      const int64_t j = k * reads->n / m;
+      memcpy(sc.data() + k * r.code_stride, reads->codes + j * r.code_stride, (size_t)r.code_stride);
+      if (r.levels) memcpy(sl.data() + k * r.level_stride, reads->levels + j * r.level_stride, (size_t)r.level_stride);
+      if (r.first_levels) sf[(size_t)k] = reads->first_levels[j];
+      slen[(size_t)k] = reads->lengths[j];
+    }
+    r.n = m;
+    r.codes = sc.data();
+    r.levels = r.levels ? sl.data() : nullptr;
+    r.first_levels = r.first_levels ? sf.data() : nullptr;
+    r.lengths = slen.data();
+  }
+  int maxL = 0;
+  for (int64_t k = 0; k < r.n; ++k) maxL = std::max<int>(maxL, r.lengths[k]);
+  const int64_t tbs = ((maxL + c->p.allowed_indels + 1) / 2 + 7) & ~7LL;
+  std::vector<stormgpu_hit> hits((size_t)std::max<int64_t>(r.n * 4, 1));
+  std::vector<uint8_t> tb((size_t)std::max<int64_t>(r.n * 4 * tbs, 1)), mapped((size_t)std::max<int64_t>(r.n, 1));
+  stormgpu_results res{hits.data(), tb.data(), tbs, mapped.data()};
+  const stormgpu_stats saved = c->stats;
+
+  // stage time of one setting: best of two runs after a warm-up (which also sizes the buffers)
+  auto time_of = [&](const stormgpu_tuning& t, double stormgpu_stats::*stage, double* ms) -> int {
+    c->tune = t;
+    double best = 1e300;
+    for (int k = 0; k < 3; ++k) {
+      if (const int rc = stormgpu_map(c, &r, &res)) return rc;
+      if (k > 0) best = std::min(best, c->stats.*stage);
+    }
+    *ms = best;
+    return 0;
+  };
+  struct Knob {
+    int32_t stormgpu_tuning::*field;
+    double stormgpu_stats::*stage;
+    std::vector<int32_t> values;
+  };
+  const Knob knobs[] = {
+      {&stormgpu_tuning::gather_warp_cap, &stormgpu_stats::ms_gather, {512, 768, 1024, 1536}},
+      {&stormgpu_tuning::gather_reads_per_steal, &stormgpu_stats::ms_gather, {1, 2, 4, 8, 16}},
+      {&stormgpu_tuning::filter_cursor, &stormgpu_stats::ms_filter, {0, 1}},
+      {&stormgpu_tuning::filter_rows, &stormgpu_stats::ms_filter, {2, 4, 8, 16}},
+      {&stormgpu_tuning::align_steal, &stormgpu_stats::ms_align, {32, 64, 128}},
+  };
+  stormgpu_tuning best = c->tune;
+  int rc = 0;
+  for (const Knob& kn : knobs) {
+    double best_ms = 1e300;
+    int32_t best_v = best.*kn.field;
+    for (int32_t v : kn.values) {
+      stormgpu_tuning t = best;
+      t.*kn.field = v;
+      double ms = 0;
+      if ((rc = time_of(t, kn.stage, &ms))) break;
+      if (ms < best_ms) { best_ms = ms; best_v = v; }
+    }
+    if (rc) break;
+    best.*kn.field = best_v;
+  }
+  c->tune = best;
+  c->stats = saved;
+  if (rc) return rc;
+  if (out) *out = best;
+  return 0;
+}

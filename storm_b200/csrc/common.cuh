@@ -1,8 +1,12 @@
 // common.cuh -- shared device helpers of libstormgpu (sm_100a).
 #pragma once
 
+#include <algorithm>
 #include <cstdint>
 #include <cstdio>
+#include <map>
+#include <mutex>
+#include <tuple>
 #include <cuda_runtime.h>
 
 #include "../../include/stormgpu.h"
@@ -49,6 +53,29 @@ __device__ __forceinline__ int warp_sum(int v) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
   return v;
+}
+
+// Blocks of `threads` threads of kernel k that fit on the current device at once (the grid of
+// a persistent launch), at least one; queried once per (kernel, device, threads, smem).
+inline int64_t resident_grid_of(const void* k, int threads, size_t smem) {
+  static std::mutex mu;
+  static std::map<std::tuple<const void*, int, int, size_t>, int64_t> cache;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  const auto key = std::make_tuple(k, dev, threads, smem);
+  std::lock_guard<std::mutex> lock(mu);
+  auto it = cache.find(key);
+  if (it != cache.end()) return it->second;
+  int sms = 0, per = 0;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k, threads, smem);
+  const int64_t g = (int64_t)(per > 0 ? per : 1) * (sms > 0 ? sms : 1);
+  cache[key] = g;
+  return g;
+}
+template <class K>
+inline int64_t resident_grid(K* k, int threads, size_t smem = 0) {
+  return resident_grid_of(reinterpret_cast<const void*>(k), threads, smem);
 }
 
 }  // namespace sg

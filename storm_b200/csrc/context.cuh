@@ -55,6 +55,7 @@ struct stormgpu_ctx {
   std::vector<sg::RefSeq> refs;
   bool indexed = false;
   stormgpu_stats stats;
+  stormgpu_tuning tune = {768, 4, 8, 32, 0};  // launch parameters of the stages (no effect on results)
   // per-batch read buffers
   sg::DevBuf<uint8_t> rcodes, rlevels, fcodes, flevels, first_levels;
   sg::DevBuf<int16_t> lengths;

@@ -278,20 +278,19 @@ __device__ __forceinline__ void bucket_sort_emit(int32_t* a, int32_t* b, int32_t
   warp_emit(b, H, I, r, go);
 }
 
-constexpr int kWarpCap = 768;
 constexpr int kGWarps = 4;
-// Reads per warp: block b takes the contiguous reads [32 b, 32 b + 32), warp w the reads
-// 32 b + w + 4 k.  Blocks start in index order, so warps finish, and append their candidates,
-// in close to read order: a batch whose reads are grouped by length gives a candidate list
-// grouped by length, which the filter needs to keep one read length per SM.
-constexpr int kGReadsPerWarp = 8;
+// Reads per steal (GatherOut.reads_per_steal, 4 by default): the grid is the resident set, and
+// every warp takes the next reads_per_steal reads (in the order of rd.order, or of the batch) from a work cursor until none is left, so
+// reads with many index positions balance out, and warps append their candidates in close to
+// read order: a batch whose reads are grouped by length gives a candidate list grouped by
+// length, which the filter needs to keep one read length per SM.
 constexpr int kReadBytes = STORMGPU_MAX_READ_LEN / 4 + 16;
 
 constexpr int kItems = 4;  // (seed, position) items per lane and round: 128 key lookups in flight per warp
 
-__global__ void __launch_bounds__(kGWarps * 32) gather_fused_kernel(ReadsDev rd, IndexView ix, int I, GatherOut go,
+__global__ void __launch_bounds__(kGWarps * 32, 8) gather_fused_kernel(ReadsDev rd, IndexView ix, int I, GatherOut go,
                                                                    const __grid_constant__ SeedSet gs) {
-  __shared__ int32_t sm[kGWarps][2 * kWarpCap];  // gathered positions, then the set / sorted copy
+  extern __shared__ int32_t sm[];  // per warp 2 * cap: gathered positions, then the set / sorted copy
   __shared__ int32_t shist[kGWarps][32];
   __shared__ int32_t soff[kGWarps][kMaxSeeds + 1];  // first item of every seed, for the current read
   __shared__ const int32_t* s_first[kMaxSeeds];
@@ -304,14 +303,18 @@ __global__ void __launch_bounds__(kGWarps * 32) gather_fused_kernel(ReadsDev rd,
     s_map[threadIdx.x] = ix.map[threadIdx.x];
   }
   __syncthreads();
-  int32_t* s = sm[w];
+  const int cap = go.warp_cap;
+  int32_t* s = sm + (size_t)w * 2 * cap;
   int32_t* so = soff[w];
   uint8_t* rs = srd[w];
   unsigned long long lookups = 0, positions = 0;
-  const int64_t rbase = (int64_t)blockIdx.x * kGWarps * kGReadsPerWarp + w;
-  for (int k = 0; k < kGReadsPerWarp; ++k) {
-    const int64_t kr = rbase + (int64_t)k * kGWarps;
-    if (kr >= rd.n) break;
+  for (;;) {
+  unsigned long long k0 = 0;
+  if (lane == 0) k0 = atomicAdd(go.cursor, (unsigned long long)go.reads_per_steal);
+  k0 = __shfl_sync(0xffffffffu, k0, 0);
+  if ((int64_t)k0 >= rd.n) break;
+  const int64_t kend = (int64_t)k0 + go.reads_per_steal < rd.n ? (int64_t)k0 + go.reads_per_steal : rd.n;
+  for (int64_t kr = (int64_t)k0; kr < kend; ++kr) {
     const int64_t r = rd.order ? (int64_t)rd.order[kr] : kr;
     const int L = rd.lengths[r];
     {  // the read's packed codes into shared memory, and the item offsets of the seeds
@@ -358,7 +361,7 @@ __global__ void __launch_bounds__(kGWarps * 32) gather_fused_kernel(ReadsDev rd,
           for (int u = 0; u < 8; ++u) tv[u] = u < cnt[m] ? __ldg(mp + u) : 0;
 #pragma unroll
           for (int u = 0; u < 8; ++u)
-            if (u < cnt[m] && dst[m] + u < kWarpCap) s[dst[m] + u] = tv[u] - rp[m];
+            if (u < cnt[m] && dst[m] + u < cap) s[dst[m] + u] = tv[u] - rp[m];
         }
       }
 #pragma unroll
@@ -372,12 +375,12 @@ __global__ void __launch_bounds__(kGWarps * 32) gather_fused_kernel(ReadsDev rd,
           const int sj = __shfl_sync(0xffffffffu, sid[m], j);
           const int32_t* mp = s_map[sj];
           for (int u = lane; u < cj; u += 32)
-            if (dj + u < kWarpCap) s[dj + u] = __ldg(mp + aj + u) - rj;
+            if (dj + u < cap) s[dj + u] = __ldg(mp + aj + u) - rj;
         }
       }
     }
     positions += (unsigned long long)H;
-    if (H > kWarpCap) {
+    if (H > cap) {
       if (lane == 0) go.big_list[atomicAdd(go.big_count, 1)] = (int32_t)r;
       __syncwarp();
       continue;
@@ -386,11 +389,12 @@ __global__ void __launch_bounds__(kGWarps * 32) gather_fused_kernel(ReadsDev rd,
     if (H <= 32) {
       sort_emit_regs<1>(s, H, I, (int)r, go);
     } else {
-      const int U = warp_dedupe(s, H, s + kWarpCap, kWarpCap);
+      const int U = warp_dedupe(s, H, s + cap, cap);
       if (U <= 32) sort_emit_regs<1>(s, U, I, (int)r, go);
-      else bucket_sort_emit(s, s + kWarpCap, shist[w], U, I, (int)r, go);
+      else bucket_sort_emit(s, s + cap, shist[w], U, I, (int)r, go);
     }
     __syncwarp();
+  }
   }
   for (int o = 16; o > 0; o >>= 1) lookups += __shfl_xor_sync(0xffffffffu, lookups, o);
   if (lane == 0) {
@@ -492,8 +496,15 @@ __global__ void gather_block_kernel(ReadsDev rd, IndexView ix, int I, const int3
 void launch_gather_fused(const ReadsDev& rd, const IndexView& ix, int I, const GatherOut& go, const SeedSet& seeds,
                          cudaStream_t st) {
   if (rd.n <= 0) return;
-  const int64_t blocks = (rd.n + kGWarps * kGReadsPerWarp - 1) / (kGWarps * kGReadsPerWarp);
-  gather_fused_kernel<<<(unsigned)blocks, kGWarps * 32, 0, st>>>(rd, ix, I, go, seeds);
+  static std::once_flag attr;
+  std::call_once(attr, [] {
+    cudaFuncSetAttribute(gather_fused_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kGWarps * 2 * kMaxWarpCap * 4);
+  });
+  const size_t smem = (size_t)kGWarps * 2 * go.warp_cap * sizeof(int32_t);
+  const int64_t per_block = (int64_t)kGWarps * go.reads_per_steal;
+  const int64_t blocks = std::min<int64_t>((rd.n + per_block - 1) / per_block,
+                                          resident_grid(gather_fused_kernel, kGWarps * 32, smem));
+  gather_fused_kernel<<<(unsigned)blocks, kGWarps * 32, smem, st>>>(rd, ix, I, go, seeds);
 }
 
 void launch_gather_block(const ReadsDev& rd, const IndexView& ix, int I, const int32_t* list, int nlist,
@@ -501,11 +512,10 @@ void launch_gather_block(const ReadsDev& rd, const IndexView& ix, int I, const i
                          int32_t* huge_count, const SeedSet& seeds, cudaStream_t st) {
   if (nlist <= 0) return;
   const int smem_cap = kBlockGatherCap;
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(gather_block_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_cap * 4);
-    attr = true;
-  }
+  static std::once_flag attr;
+  std::call_once(attr, [] {
+    cudaFuncSetAttribute(gather_block_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kBlockGatherCap * 4);
+  });
   if (gbuf)
     gather_block_kernel<<<nlist, 1024, 0, st>>>(rd, ix, I, list, go, gcap, gbuf, huge_list, huge_h, huge_count,
                                                  seeds);

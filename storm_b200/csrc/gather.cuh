@@ -12,7 +12,13 @@ struct GatherOut {
   unsigned long long* counters;  // [3] key lookups, [4] index positions, [7] flat cursor, [8] overflow
   int32_t* big_list;             // reads with more positions than a warp holds
   int32_t* big_count;
+  unsigned long long* cursor;    // zeroed work cursor of the fused gather (reads taken so far)
+  int reads_per_steal;           // reads a warp takes from the cursor at a time (>= 1)
+  int warp_cap;                  // index positions a warp holds in shared memory, <= kMaxWarpCap;
+                                 // reads with more go to the block kernel
 };
+
+constexpr int kMaxWarpCap = 1536;
 
 constexpr int kBlockGatherCap = 32768;
 

@@ -127,14 +127,12 @@ struct BandWindow {
 // A candidate whose running abort bound falls below -t stops at that row: the replay
 // threshold never is below -t, so it is aborted whatever comes before it, and neither its score
 // nor its traceback is read.
+// One slot; its direction bits in scratch column sl of ns.
 template <int BWT, int CM>
-__global__ void __launch_bounds__(128) align_kernel(ReadsDev rd, ScoreParams sp, const uint8_t* __restrict__ genome,
-                                                    const uint8_t* __restrict__ mask, int64_t slot0, int64_t nslots,
-                                                    PassBuffers pb) {
+__device__ __forceinline__ void align_one(const ReadsDev& rd, const ScoreParams& sp, const uint8_t* __restrict__ genome,
+                                          const uint8_t* __restrict__ mask, int64_t slot, int64_t sl, int64_t ns,
+                                          const PassBuffers& pb) {
   constexpr int NB = BWT > 0 ? BWT : kMaxBand;
-  const int64_t sl = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (sl >= nslots) return;
-  const int64_t slot = slot0 + sl;
   const int r = pb.p_read[slot];
   const int d = pb.p_diag[slot];
   const int I = sp.I, BW = BWT > 0 ? BWT : 2 * I + 1, colour = CM >= 0 ? CM : sp.colour;
@@ -144,7 +142,6 @@ __global__ void __launch_bounds__(128) align_kernel(ReadsDev rd, ScoreParams sp,
   const int win = max(d - I, -sp.Is);  // run.c:667
   const int wpr_dir = (2 * BW + 31) / 32, wpr = wpr_dir + (colour ? (BW + 31) / 32 : 0);
   uint32_t* scr = pb.a_scratch;
-  const int64_t ns = nslots;
   int sc[NB], stt[NB];
   const int mbest = sp.pair[0][3];
   BandWindow<(BWT > 0 ? BWT : 1)> bwin;
@@ -300,24 +297,63 @@ __global__ void __launch_bounds__(128) align_kernel(ReadsDev rd, ScoreParams sp,
   pb.a_pos[slot * 4 + 3] = (int16_t)j0;
 }
 
-void launch_align(const ReadsDev& r, const ScoreParams& sp, const uint8_t* genome,
-                  const uint8_t* mask, int64_t slot0, int64_t nslots, PassBuffers& pb,
-                  cudaStream_t st) {
-  if (nslots <= 0) return;
-  const unsigned blocks = (unsigned)((nslots + 127) / 128);
-#define SG_ALIGN(BW)                                                                                    \
-  case BW:                                                                                              \
-    if (sp.colour) align_kernel<BW, 1><<<blocks, 128, 0, st>>>(r, sp, genome, mask, slot0, nslots, pb); \
-    else align_kernel<BW, 0><<<blocks, 128, 0, st>>>(r, sp, genome, mask, slot0, nslots, pb);           \
-    break;
+// Slots slot0 .. slot0 + nslots: one per thread (scratch column = slot - slot0), or with
+// pb.cursor a persistent grid whose warps take the next 32 slots from the cursor (the slot
+// count read from pb.npass_dev when it is given; scratch column = the thread's index in the
+// grid, so the scratch holds align_workers() columns).
+template <int BWT, int CM>
+__global__ void __launch_bounds__(128, (BWT > 0 && BWT <= 15 ? 5 : 1)) align_kernel(ReadsDev rd, ScoreParams sp, const uint8_t* __restrict__ genome,
+                                                    const uint8_t* __restrict__ mask, int64_t slot0, int64_t nslots,
+                                                    PassBuffers pb) {
+  // one call site of align_one (its band code is large and fully unrolled)
+  const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const bool steal = pb.cursor != nullptr;
+  const int64_t n = steal && pb.npass_dev ? *pb.npass_dev : nslots;
+  const int64_t ns = steal ? (int64_t)gridDim.x * blockDim.x : nslots;
+  const int lane = threadIdx.x & 31;
+  const int take = pb.steal >= 32 ? pb.steal & ~31 : 32;
+  int64_t s = tid, end = steal ? 0 : tid + 1;  // stealing: every lane takes the first run together
+  for (;;) {
+    if (steal && s >= end) {  // the warp's next run of `take` slots
+      unsigned long long b = 0;
+      if (lane == 0) b = atomicAdd(pb.cursor, (unsigned long long)take);
+      s = (int64_t)__shfl_sync(0xffffffffu, b, 0);
+      if (s >= n) break;
+      end = s + take;
+      s += lane;
+    }
+    if (s < n) align_one<BWT, CM>(rd, sp, genome, mask, slot0 + s, steal ? tid : s, ns, pb);
+    if (!steal) break;
+    s += 32;
+  }
+}
+
+static const void* align_kernel_of(const ScoreParams& sp) {
+#define SG_ALIGN(BW) \
+  case BW: return sp.colour ? (const void*)align_kernel<BW, 1> : (const void*)align_kernel<BW, 0>;
   switch (2 * sp.I + 1) {
     SG_ALIGN(7)
     SG_ALIGN(15)
     SG_ALIGN(31)
     SG_ALIGN(41)
-  default: align_kernel<0, -1><<<blocks, 128, 0, st>>>(r, sp, genome, mask, slot0, nslots, pb); break;
+  default: return (const void*)align_kernel<0, -1>;
   }
 #undef SG_ALIGN
+}
+
+int64_t align_workers(int64_t nslots, const ScoreParams& sp) {
+  const int64_t g = resident_grid_of(align_kernel_of(sp), 128, 0) * 128;
+  return std::min<int64_t>(g, (nslots + 127) / 128 * 128);
+}
+
+void launch_align(const ReadsDev& r, const ScoreParams& sp, const uint8_t* genome,
+                  const uint8_t* mask, int64_t slot0, int64_t nslots, PassBuffers& pb,
+                  cudaStream_t st) {
+  if (nslots <= 0) return;
+  const void* k = align_kernel_of(sp);
+  const unsigned blocks = (unsigned)(pb.cursor ? align_workers(nslots, sp) / 128 : (nslots + 127) / 128);
+  void* args[] = {(void*)&r, (void*)&sp, (void*)&genome, (void*)&mask, (void*)&slot0, (void*)&nslots, (void*)&pb};
+  cudaLaunchKernel(k, dim3(blocks), dim3(128), args, 0, st);  // errors surface at the caller's next check
 }
 
 // ------------------------------------------------------------------------------ replay

@@ -56,6 +56,11 @@ struct PassBuffers {
   int64_t tbs;
   uint32_t* a_scratch;  // direction bits, see align kernel
   int64_t scratch_words;
+  // may be null; else a zeroed work cursor, and the align launch is a persistent grid of
+  // align_workers() threads (scratch columns) taking slots from it
+  unsigned long long* cursor;
+  const int64_t* npass_dev;  // may be null; else the slot count is read from here
+  int steal;                 // with a cursor: slots a warp takes at a time, a multiple of 32 (0 = 32)
 };
 
 void launch_reverse_reads(const ReadsDev& in, const uint8_t* first_levels, int colour,
@@ -65,6 +70,8 @@ void launch_init_results(int64_t n, stormgpu_hit* hits, uint8_t* mapped, uint8_t
 void launch_align(const ReadsDev& r, const ScoreParams& sp, const uint8_t* genome,
                   const uint8_t* mask, int64_t slot0, int64_t nslots, PassBuffers& pb,
                   cudaStream_t st);
+// scratch columns of a launch_align with a cursor (the threads of its persistent grid)
+int64_t align_workers(int64_t nslots, const ScoreParams& sp);
 void launch_replay(int64_t n, const ScoreParams& sp, int ref_id, int sense, PassBuffers& pb,
                    stormgpu_hit* hits, uint8_t* tb, int64_t tbs, uint8_t* mapped, cudaStream_t st);
 

@@ -332,6 +332,9 @@ static int map_device_once(stormgpu_ctx* c, const stormgpu_reads* reads, stormgp
         GatherOut go;
         go.fr = c->fr.p; go.fd = c->fd.p; go.cap = c->fr.cap; go.counters = c->counters.p;
         go.big_list = c->big_list.p; go.big_count = c->big_count.p;
+        go.cursor = c->counters.p + 12;  // zeroed just above
+        go.reads_per_steal = c->tune.gather_reads_per_steal;
+        go.warp_cap = c->tune.gather_warp_cap;
         launch_gather_fused(rd, ix, sp.I, go, c->seeds, st);
         launches++;
         int32_t nbig[2] = {0, 0};
@@ -374,6 +377,9 @@ static int map_device_once(stormgpu_ctx* c, const stormgpu_reads* reads, stormgp
         return STORMGPU_ENOMEM;
       SG_CUDA(cudaEventRecord(c->ev[1], st));
       FilterJob job;
+      memset(&job, 0, sizeof(job));
+      if (c->tune.filter_cursor) job.cursor = c->counters.p + 10;  // zeroed with the counters of the pass
+      job.rows = c->tune.filter_rows;
       job.n = utot; job.fr = c->fr.p; job.fd = c->fd.p; job.flag = c->flag.p; job.codes = rd.codes;
       job.cstride = rd.cstride; job.lengths = rd.lengths; job.genome = R.d_codes; job.W = sp.W; job.Is = sp.Is;
       job.fm = sp.fm; job.fx = sp.fx; job.fo = sp.fo; job.fe = sp.fe; job.fthr = sp.fthr;
@@ -416,14 +422,14 @@ static int map_device_once(stormgpu_ctx* c, const stormgpu_reads* reads, stormgp
         launches += 3;
         pb.a_score = c->a_score.p; pb.a_bound = c->a_bound.p; pb.a_tblen = c->a_tblen.p;
         pb.a_pos = c->a_pos.p; pb.a_tb = c->a_tb.p; pb.tbs = tbs;
+        // one persistent launch over all passing candidates; scratch for its threads only
+        pb.cursor = c->counters.p + 11;  // zeroed with the counters at the start of the pass
+        pb.steal = c->tune.align_steal;
         const int64_t per_slot = (int64_t)maxL * wpr;
-        int64_t chunk = std::min<int64_t>(npass, std::max<int64_t>(4096, (int64_t)(256ll << 20) / (per_slot * 4)));
-        if (c->scratch.grow(chunk * per_slot)) return STORMGPU_ENOMEM;
+        if (c->scratch.grow(align_workers(npass, sp) * per_slot)) return STORMGPU_ENOMEM;
         pb.a_scratch = c->scratch.p;
-        for (int64_t s0 = 0; s0 < npass; s0 += chunk) {
-          launch_align(rd, sp, R.d_codes, R.d_mask, s0, std::min(chunk, npass - s0), pb, st);
-          launches++;
-        }
+        launch_align(rd, sp, R.d_codes, R.d_mask, 0, npass, pb, st);
+        launches++;
         S.aligned += npass;
         S.align_cells += npass * (int64_t)maxL * BW;
       }

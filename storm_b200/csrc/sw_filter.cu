@@ -26,14 +26,35 @@
 
 namespace sg {
 
-// Candidates per thread: a block of 256 threads takes the contiguous tile of 256 * kFilterTile
-// candidates at blockIdx.x * 256 * kFilterTile (lane-consecutive within each of its rows).
-// Blocks start in index order, so the blocks resident at any time work on neighbouring
-// candidates: in a batch whose reads are grouped by length, an SM runs warps of one read
-// length.  A grid-stride loop over a grid larger than the resident set makes every resident
-// block walk the whole list instead, which mixes all lengths on every SM; on a 35-150 bp batch
-// that ran the same instructions 1.48x slower, stalled on instruction fetch.
-constexpr int kFilterTile = 8;
+// Candidates per thread: a block of 256 threads takes a tile of 256 * rows contiguous
+// candidates (rows of 256; FilterJob.rows, kFilterTile by default).  Tiles go out in list order -- from a work cursor to a persistent
+// grid (a block takes the next tile when all its warps are done with the last: uneven tiles
+// balance), or by block index to a grid of one tile per block -- so the warps resident at any
+// time work on neighbouring candidates: in a batch whose reads are grouped by length, an SM runs
+// warps of one read length.  A grid-stride loop over a grid larger than the resident set makes
+// every resident block walk the whole list instead, which mixes all lengths on every SM; on a
+// 35-150 bp batch that ran the same instructions 1.48x slower, stalled on instruction fetch.
+// The tile goes to the whole block, not warp by warp, for the same reason: the warps of a
+// block start every tile together and stay close in the long unrolled band code (warps taking
+// tiles one by one drift apart in it, which measured 5-15 % slower).
+constexpr int kFilterTile = 8;  // rows of a tile unless FilterJob.rows says otherwise
+
+// The block's tiles in list order: by block index, or with a cursor taken from it one at a
+// time (all threads of the block make the same calls).  Taking the next tile ahead, to hide
+// the atomic's round trip, measured no faster.
+struct FilterTiles {
+  unsigned long long* cursor;
+  int64_t T;  // candidates per tile
+  __device__ __forceinline__ int64_t first() { return cursor ? after() : (int64_t)blockIdx.x * T; }
+  __device__ __forceinline__ int64_t after() {
+    __shared__ unsigned long long s_tile;
+    if (!cursor) return INT64_MAX;
+    __syncthreads();  // every thread has read the previous tile
+    if (threadIdx.x == 0) s_tile = atomicAdd(cursor, 1ull);
+    __syncthreads();
+    return (int64_t)s_tile * T;
+  }
+};
 
 // one block's filter counters (cells, candidates, band cells) into the stats: three global
 // atomics per block.  `counters` is uniform over the block.
@@ -71,10 +92,13 @@ __global__ void __launch_bounds__(256, (W <= 8 ? 4 : 2)) filter_flat_dpx_kernel(
   uint32_t TLO, THI, NFE, CFO;  // NFE: -ext in both halves (both layouts)
   filter_split_consts(job.fm, job.fx, job.fo, job.fe, TLO, THI, NFE, CFO);
   unsigned long long cells = 0, cands = 0, band = 0;
-  const int64_t t0 = (int64_t)blockIdx.x * blockDim.x * kFilterTile + threadIdx.x;
-  for (int i = 0; i < kFilterTile; ++i) {
-    const int64_t t = t0 + (int64_t)i * blockDim.x;
-    if (t >= job.n) break;
+  const int64_t n = job.n_dev ? (int64_t)*job.n_dev : job.n;
+  const int rows = job.rows > 0 ? job.rows : kFilterTile;
+  FilterTiles tiles{job.cursor, 256 * (int64_t)rows};
+  for (int64_t base = tiles.first(); base < n; base = tiles.after())
+  for (int i = 0; i < rows; ++i) {
+    const int64_t t = base + i * 256 + threadIdx.x;
+    if (t >= n) break;
     const int r = job.fr[t];
     const int d = job.fd[t];
     const int L = job.lengths[r];
@@ -135,10 +159,13 @@ void launch_expand_reads(const ReadsDev& rd, uint8_t* rexp, int64_t rstride, cud
 // Plain 32-bit variant (any score values), the restatement in map_kernels.cu.
 __global__ void filter_flat_scalar_kernel(FilterJob job, ScoreParams sp) {
   unsigned long long cells = 0, cands = 0, band = 0;
-  const int64_t t0 = (int64_t)blockIdx.x * blockDim.x * kFilterTile + threadIdx.x;
-  for (int i = 0; i < kFilterTile; ++i) {
-    const int64_t t = t0 + (int64_t)i * blockDim.x;
-    if (t >= job.n) break;
+  const int64_t n = job.n_dev ? (int64_t)*job.n_dev : job.n;
+  const int rows = job.rows > 0 ? job.rows : kFilterTile;
+  FilterTiles tiles{job.cursor, 256 * (int64_t)rows};
+  for (int64_t base = tiles.first(); base < n; base = tiles.after())
+  for (int i = 0; i < rows; ++i) {
+    const int64_t t = base + i * 256 + threadIdx.x;
+    if (t >= n) break;
     const int r = job.fr[t];
     const int L = job.lengths[r];
     job.flag[t] = sw_filter_dispatch_ext(job.W, job.genome, (int64_t)job.fd[t] - job.Is,
@@ -154,28 +181,36 @@ bool filter_dpx_ok(const ScoreParams& sp, int max_len) {
   return sp.fm <= 127 && sp.fx <= 128 && (int64_t)max_len * sp.fm < 32000 && sp.fe <= 32000 && sp.fo <= 32000;
 }
 
+// job.n: the candidates, or with job.n_dev an upper bound of them.  One tile per block, or with
+// job.cursor at most the resident grid.
 void launch_filter_flat_job(const FilterJob& job, const ScoreParams& sp, bool dpx, cudaStream_t st) {
   if (job.n <= 0) return;
-  const int64_t blocks = (job.n + 256 * kFilterTile - 1) / (256 * kFilterTile);  // one tile per block
+  const int64_t tile = 256 * (int64_t)(job.rows > 0 ? job.rows : kFilterTile);
+  const int64_t blocks = (job.n + tile - 1) / tile;
+  auto grid = [&](const void* k) {
+    return (unsigned)(job.cursor ? std::min<int64_t>(blocks, resident_grid_of(k, 256, 0)) : blocks);
+  };
+#define SG_FILTER(K, ...) K<<<grid(reinterpret_cast<const void*>(K)), 256, 0, st>>>(__VA_ARGS__)
   if (!dpx) {
-    filter_flat_scalar_kernel<<<(unsigned)blocks, 256, 0, st>>>(job, sp);
+    SG_FILTER(filter_flat_scalar_kernel, job, sp);
     return;
   }
   if (job.min_len >= job.W) {
     switch (job.W) {
-    case 2: filter_flat_dpx_kernel<2, false><<<(unsigned)blocks, 256, 0, st>>>(job); break;
-    case 4: filter_flat_dpx_kernel<4, false><<<(unsigned)blocks, 256, 0, st>>>(job); break;
-    case 8: filter_flat_dpx_kernel<8, false><<<(unsigned)blocks, 256, 0, st>>>(job); break;
-    default: filter_flat_dpx_kernel<16, false><<<(unsigned)blocks, 256, 0, st>>>(job); break;
+    case 2: SG_FILTER((filter_flat_dpx_kernel<2, false>), job); break;
+    case 4: SG_FILTER((filter_flat_dpx_kernel<4, false>), job); break;
+    case 8: SG_FILTER((filter_flat_dpx_kernel<8, false>), job); break;
+    default: SG_FILTER((filter_flat_dpx_kernel<16, false>), job); break;
     }
   } else {
     switch (job.W) {
-    case 2: filter_flat_dpx_kernel<2, true><<<(unsigned)blocks, 256, 0, st>>>(job); break;
-    case 4: filter_flat_dpx_kernel<4, true><<<(unsigned)blocks, 256, 0, st>>>(job); break;
-    case 8: filter_flat_dpx_kernel<8, true><<<(unsigned)blocks, 256, 0, st>>>(job); break;
-    default: filter_flat_dpx_kernel<16, true><<<(unsigned)blocks, 256, 0, st>>>(job); break;
+    case 2: SG_FILTER((filter_flat_dpx_kernel<2, true>), job); break;
+    case 4: SG_FILTER((filter_flat_dpx_kernel<4, true>), job); break;
+    case 8: SG_FILTER((filter_flat_dpx_kernel<8, true>), job); break;
+    default: SG_FILTER((filter_flat_dpx_kernel<16, true>), job); break;
     }
   }
+#undef SG_FILTER
 }
 
 // ------------------------------------------------------------------ compaction of passing candidates

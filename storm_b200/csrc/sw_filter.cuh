@@ -21,6 +21,13 @@ struct FilterJob {
   const uint8_t* rexp;          // read streams (bytes 0xC4 + c * 0x11), rstride bytes per read
   int64_t rstride;
   int min_len;                  // shortest read of the batch (reads shorter than W take another path)
+  // may be null; else the candidate count is read from here when the kernel starts (the hit
+  // gather's cursor), and n is only an upper bound for the grid
+  const unsigned long long* n_dev;
+  // may be null; else a zeroed work cursor: the grid is the resident set, and every block takes
+  // the next tile of 256 * kFilterTile candidates from it, in list order, until none is left
+  unsigned long long* cursor;
+  int rows;  // rows of 256 candidates in a block's tile; 0 = the default (8)
 };
 
 constexpr int64_t kGexpPad = 4096;   // bytes of padding around a byte-expanded sequence

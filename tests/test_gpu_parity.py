@@ -230,3 +230,43 @@ def test_map_is_invariant_to_read_order_in_a_mixed_length_batch():
         for k in live:
             nb = (int(got.hits["tb_len"][k]) + 1) // 2
             assert bytes(got.tb[k, :nb]) == bytes(base.tb[h4[k], :nb]), k
+
+
+def test_map_results_do_not_depend_on_the_launch_tuning():
+    """The launch parameters (hit bucket, reads per steal, filter tile rows, alignment run per
+    steal) and the autotuner that picks them change no result."""
+    from storm_b200 import synth
+    genome = synth.make_genome([80000], 41, gc=0.42, repeat_frac=0.4)
+    seqs, quals = synth.simulate_nucleotide_reads(genome, 2500, [35, 75, 150], 43)
+    codes, levels, lengths = _reads_arrays(seqs, quals)
+    prm = api.params(indels=15, min_score=100, min_score_filter=95)
+    m = api.Mapper(prm, "##-##-###-###;###--#-#--#--####")
+    for _, s in genome:
+        cp = ffi.pack2(s, PADB)
+        mk = ffi.pack2(np.zeros(len(s), np.uint8), PADB, fill=0x55)
+        m.add_reference(cp[PADB:], mk[PADB:], len(s))
+    m.build_index()
+    batch = api.ReadBatch(codes, lengths, levels)
+    tbs = ((150 + 15 + 1) // 2 + 7) & ~7
+    assert m.tuning() == {"gather_warp_cap": 768, "gather_reads_per_steal": 4, "filter_rows": 8, "align_steal": 32,
+                          "filter_cursor": 0}
+    base = m.map(batch, tbs)
+    st = m.stats()
+    assert base.mapped.sum() > len(seqs) // 4
+    settings = [dict(gather_warp_cap=256, gather_reads_per_steal=1, filter_rows=1, align_steal=1024, filter_cursor=1),
+                dict(gather_warp_cap=1536, gather_reads_per_steal=64, filter_rows=64, align_steal=32, filter_cursor=0),
+                dict(gather_warp_cap=1000, gather_reads_per_steal=3, filter_rows=5, align_steal=96, filter_cursor=1)]
+    for kw in settings:
+        m.set_tuning(**kw)
+        got = m.map(batch, tbs)
+        assert m.stats()["candidates"] == st["candidates"], kw
+        assert np.array_equal(got.mapped, base.mapped), kw
+        assert got.hits.tobytes() == base.hits.tobytes(), kw
+        assert got.tb.tobytes() == base.tb.tobytes(), kw
+    with pytest.raises(api.StormError, match="out of range"):
+        m.set_tuning(align_steal=48)
+    picked = m.autotune(batch, sample=1500)
+    assert m.tuning() == picked
+    got = m.map(batch, tbs)
+    assert got.hits.tobytes() == base.hits.tobytes() and got.tb.tobytes() == base.tb.tobytes()
+    m.close()
