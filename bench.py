@@ -401,6 +401,7 @@ def main():
     ap.add_argument("--cfg", type=int, default=1)
     ap.add_argument("--scale", type=float, default=1.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--tuning", default="", help="launch parameters name=value,... instead of the autotuner")
     ap.add_argument("--reads", type=int, default=0, help="map only the first N reads of the workload (profiling)")
     a = ap.parse_args()
 
@@ -421,6 +422,7 @@ def main():
             (batched_arm if a.cfg == 2 else serving_arm)(a, w, ref_path, reads_path, d)
         return
 
+    import numpy as np
     import torch
     dist = None
     if world > 1:
@@ -457,7 +459,11 @@ def main():
     # they change no result)
     t0 = time.perf_counter()
     mapper.build_index()
-    tuning = mapper.autotune(batch, sample=200000)
+    if a.tuning:  # fixed launch parameters (profiling runs that must launch the same kernels)
+        mapper.set_tuning(**{k: int(v) for k, v in (kv.split("=") for kv in a.tuning.split(","))})
+        tuning = mapper.tuning()
+    else:
+        tuning = mapper.autotune(batch, sample=200000)
     tune_s = time.perf_counter() - t0
     log("rank %d: autotuned %s in %.1f s" % (rank, tuning, tune_s))
     d_codes = torch.from_numpy(batch.codes).to(dev)
@@ -539,8 +545,13 @@ def main():
     h2d = pbatch.codes.nbytes + (pbatch.levels.nbytes if pbatch.levels is not None else 0) + pbatch.lengths.nbytes + \
         (pbatch.first_levels.nbytes if pbatch.first_levels is not None else 0)
     d2h = res.hits.nbytes + res.tb.nbytes + res.mapped.nbytes
+    # the host-buffer call (pipelined in chunks for large batches) gives the device-resident records
+    same = bool(np.array_equal(d_mapped.cpu().numpy(), res.mapped) and
+                d_hits.cpu().numpy().tobytes() == res.hits.tobytes() and
+                d_tb.cpu().numpy().tobytes() == res.tb.tobytes())
     e2e = {"value": world * n * len(e2e_ms) / (e2e_t / 1000.0), "unit": "reads/s", "h2d_bytes_per_step": int(h2d),
-           "d2h_bytes_per_step": int(d2h), "includes": "index build + reads H2D + map + results D2H, pinned host buffers"}
+           "d2h_bytes_per_step": int(d2h), "includes": "index build + reads H2D + map + results D2H, pinned host buffers",
+           "same_records_as_device": same}
 
     # roofline of the dominant kernel, from the last timed step's per-stage device times
     st = stage[-1]

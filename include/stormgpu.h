@@ -202,7 +202,8 @@ typedef struct stormgpu_tuning {
   int32_t gather_warp_cap;        /* index positions one gather warp holds in shared memory (the
                                      hit bucket), 256..1536; reads with more go to a block per read */
   int32_t gather_reads_per_steal; /* reads a gather warp takes from the work cursor at a time, 1..64 */
-  int32_t filter_rows;            /* rows of 256 candidates in a filter block's tile, 1..64 */
+  int32_t filter_rows;            /* rows of 256 candidates in a filter block's tile when
+                                     filter_cursor is 1 (else 8), 1..64 */
   int32_t align_steal;            /* passing candidates an alignment warp takes at a time, 32..1024,
                                      a multiple of 32 */
   int32_t filter_cursor;          /* 1: the filter runs as a persistent grid whose blocks take tiles

@@ -94,32 +94,37 @@ extern "C" int stormgpu_autotune(stormgpu_ctx* c, const stormgpu_reads* reads, i
     *ms = best;
     return 0;
   };
+  // one knob = the candidate settings of one or two fields (the filter's grid form and its tile
+  // rows go together: the rows only apply with a cursor)
   struct Knob {
-    int32_t stormgpu_tuning::*field;
+    int32_t stormgpu_tuning::*f1;
+    int32_t stormgpu_tuning::*f2;  // may be null
     double stormgpu_stats::*stage;
-    std::vector<int32_t> values;
+    std::vector<std::pair<int32_t, int32_t>> values;
   };
   const Knob knobs[] = {
-      {&stormgpu_tuning::gather_warp_cap, &stormgpu_stats::ms_gather, {512, 768, 1024, 1536}},
-      {&stormgpu_tuning::gather_reads_per_steal, &stormgpu_stats::ms_gather, {1, 2, 4, 8, 16}},
-      {&stormgpu_tuning::filter_cursor, &stormgpu_stats::ms_filter, {0, 1}},
-      {&stormgpu_tuning::filter_rows, &stormgpu_stats::ms_filter, {2, 4, 8, 16}},
-      {&stormgpu_tuning::align_steal, &stormgpu_stats::ms_align, {32, 64, 128}},
+      {&stormgpu_tuning::gather_warp_cap, nullptr, &stormgpu_stats::ms_gather, {{512, 0}, {768, 0}, {1024, 0}, {1536, 0}}},
+      {&stormgpu_tuning::gather_reads_per_steal, nullptr, &stormgpu_stats::ms_gather,
+       {{1, 0}, {2, 0}, {4, 0}, {8, 0}, {16, 0}}},
+      {&stormgpu_tuning::filter_cursor, &stormgpu_tuning::filter_rows, &stormgpu_stats::ms_filter,
+       {{0, 8}, {1, 2}, {1, 4}, {1, 8}, {1, 16}}},
+      {&stormgpu_tuning::align_steal, nullptr, &stormgpu_stats::ms_align, {{32, 0}, {64, 0}, {128, 0}}},
   };
   stormgpu_tuning best = c->tune;
   int rc = 0;
   for (const Knob& kn : knobs) {
     double best_ms = 1e300;
-    int32_t best_v = best.*kn.field;
-    for (int32_t v : kn.values) {
+    stormgpu_tuning pick = best;
+    for (const auto& v : kn.values) {
       stormgpu_tuning t = best;
-      t.*kn.field = v;
+      t.*kn.f1 = v.first;
+      if (kn.f2) t.*kn.f2 = v.second;
       double ms = 0;
       if ((rc = time_of(t, kn.stage, &ms))) break;
-      if (ms < best_ms) { best_ms = ms; best_v = v; }
+      if (ms < best_ms) { best_ms = ms; pick = t; }
     }
     if (rc) break;
-    best.*kn.field = best_v;
+    best = pick;
   }
   c->tune = best;
   c->stats = saved;

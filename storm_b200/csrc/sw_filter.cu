@@ -27,10 +27,10 @@
 namespace sg {
 
 // Candidates per thread: a block of 256 threads takes a tile of 256 * rows contiguous
-// candidates (rows of 256; FilterJob.rows, kFilterTile by default).  Tiles go out in list order -- from a work cursor to a persistent
-// grid (a block takes the next tile when all its warps are done with the last: uneven tiles
-// balance), or by block index to a grid of one tile per block -- so the warps resident at any
-// time work on neighbouring candidates: in a batch whose reads are grouped by length, an SM runs
+// candidates (rows of 256: kFilterTile, or FilterJob.rows with a cursor).  Tiles go out in
+// list order -- from a work cursor to a persistent grid (a block takes the next tile when all
+// its warps are done with the last: uneven tiles balance), or by block index to a grid of one
+// tile per block -- so the warps resident at any time work on neighbouring candidates: in a batch whose reads are grouped by length, an SM runs
 // warps of one read length.  A grid-stride loop over a grid larger than the resident set makes
 // every resident block walk the whole list instead, which mixes all lengths on every SM; on a
 // 35-150 bp batch that ran the same instructions 1.48x slower, stalled on instruction fetch.
@@ -81,10 +81,35 @@ __device__ __forceinline__ void add_filter_counters(unsigned long long* counters
   }
 }
 
+// Calls body(t) for the block's candidates t < n: with a cursor (CURSOR) tiles of `rows` rows
+// taken from it one after the other, else the one tile blockIdx.x of kFilterTile rows.  One
+// call site of body per instantiation (it is the long unrolled band code).  The one-tile form
+// has no barrier and a constant row count, which keeps the W = 8 kernel within 64 registers
+// without spilling; run through the cursor loop it measured 3 % slower.
+template <bool CURSOR, class Body>
+__device__ __forceinline__ void for_filter_tiles(const FilterJob& job, int64_t n, int rows, Body body) {
+  if constexpr (CURSOR) {
+    FilterTiles tiles{job.cursor, 256 * (int64_t)rows};
+    for (int64_t base = tiles.first(); base < n; base = tiles.after())
+      for (int i = 0; i < rows; ++i) {
+        const int64_t t = base + i * 256 + threadIdx.x;
+        if (t >= n) break;
+        body(t);
+      }
+  } else {
+    const int64_t t0 = (int64_t)blockIdx.x * blockDim.x * kFilterTile + threadIdx.x;
+    for (int i = 0; i < kFilterTile; ++i) {
+      const int64_t t = t0 + (int64_t)i * blockDim.x;
+      if (t >= n) break;
+      body(t);
+    }
+  }
+}
+
 // SHORT: the batch has reads shorter than W (band longer than the read), which take the
 // stream-decoding variant; without them the kernel holds only the split-layout core and
-// fits in 64 registers for W <= 8.
-template <int W, bool SHORT>
+// fits in 64 registers for W <= 8.  CURSOR: job.cursor is set (persistent grid).
+template <int W, bool SHORT, bool CURSOR>
 __global__ void __launch_bounds__(256, (W <= 8 ? 4 : 2)) filter_flat_dpx_kernel(FilterJob job) {
   const uint32_t T = (uint32_t)(job.fm & 0xff) | ((uint32_t)((256 - job.fx) & 0xff) << 8) |
                      ((uint32_t)((256 - job.fx) & 0xff) << 16) | ((uint32_t)((256 - job.fx) & 0xff) << 24);
@@ -93,12 +118,7 @@ __global__ void __launch_bounds__(256, (W <= 8 ? 4 : 2)) filter_flat_dpx_kernel(
   filter_split_consts(job.fm, job.fx, job.fo, job.fe, TLO, THI, NFE, CFO);
   unsigned long long cells = 0, cands = 0, band = 0;
   const int64_t n = job.n_dev ? (int64_t)*job.n_dev : job.n;
-  const int rows = job.rows > 0 ? job.rows : kFilterTile;
-  FilterTiles tiles{job.cursor, 256 * (int64_t)rows};
-  for (int64_t base = tiles.first(); base < n; base = tiles.after())
-  for (int i = 0; i < rows; ++i) {
-    const int64_t t = base + i * 256 + threadIdx.x;
-    if (t >= n) break;
+  for_filter_tiles<CURSOR>(job, n, job.rows > 0 ? job.rows : kFilterTile, [&](int64_t t) {
     const int r = job.fr[t];
     const int d = job.fd[t];
     const int L = job.lengths[r];
@@ -112,7 +132,7 @@ __global__ void __launch_bounds__(256, (W <= 8 ? 4 : 2)) filter_flat_dpx_kernel(
     cells += (unsigned long long)(2 * W) * (unsigned long long)(L + W - 1);
     band += (unsigned long long)L * (2 * job.Is + 1);
     cands++;
-  }
+  });
   if (job.counters) add_filter_counters(job.counters, cells, cands, band);
 }
 
@@ -157,15 +177,11 @@ void launch_expand_reads(const ReadsDev& rd, uint8_t* rexp, int64_t rstride, cud
 }
 
 // Plain 32-bit variant (any score values), the restatement in map_kernels.cu.
+template <bool CURSOR>
 __global__ void filter_flat_scalar_kernel(FilterJob job, ScoreParams sp) {
   unsigned long long cells = 0, cands = 0, band = 0;
   const int64_t n = job.n_dev ? (int64_t)*job.n_dev : job.n;
-  const int rows = job.rows > 0 ? job.rows : kFilterTile;
-  FilterTiles tiles{job.cursor, 256 * (int64_t)rows};
-  for (int64_t base = tiles.first(); base < n; base = tiles.after())
-  for (int i = 0; i < rows; ++i) {
-    const int64_t t = base + i * 256 + threadIdx.x;
-    if (t >= n) break;
+  for_filter_tiles<CURSOR>(job, n, job.rows > 0 ? job.rows : kFilterTile, [&](int64_t t) {
     const int r = job.fr[t];
     const int L = job.lengths[r];
     job.flag[t] = sw_filter_dispatch_ext(job.W, job.genome, (int64_t)job.fd[t] - job.Is,
@@ -173,7 +189,7 @@ __global__ void filter_flat_scalar_kernel(FilterJob job, ScoreParams sp) {
     cells += (unsigned long long)(2 * job.W) * (unsigned long long)(L + job.W - 1);
     band += (unsigned long long)L * (2 * job.Is + 1);
     cands++;
-  }
+  });
   if (job.counters) add_filter_counters(job.counters, cells, cands, band);
 }
 
@@ -185,31 +201,29 @@ bool filter_dpx_ok(const ScoreParams& sp, int max_len) {
 // job.cursor at most the resident grid.
 void launch_filter_flat_job(const FilterJob& job, const ScoreParams& sp, bool dpx, cudaStream_t st) {
   if (job.n <= 0) return;
-  const int64_t tile = 256 * (int64_t)(job.rows > 0 ? job.rows : kFilterTile);
+  const int64_t tile = 256 * (int64_t)(job.cursor && job.rows > 0 ? job.rows : kFilterTile);
   const int64_t blocks = (job.n + tile - 1) / tile;
   auto grid = [&](const void* k) {
     return (unsigned)(job.cursor ? std::min<int64_t>(blocks, resident_grid_of(k, 256, 0)) : blocks);
   };
 #define SG_FILTER(K, ...) K<<<grid(reinterpret_cast<const void*>(K)), 256, 0, st>>>(__VA_ARGS__)
+#define SG_FILTER_W(S, C)                                                \
+  switch (job.W) {                                                       \
+  case 2: SG_FILTER((filter_flat_dpx_kernel<2, S, C>), job); break;      \
+  case 4: SG_FILTER((filter_flat_dpx_kernel<4, S, C>), job); break;      \
+  case 8: SG_FILTER((filter_flat_dpx_kernel<8, S, C>), job); break;      \
+  default: SG_FILTER((filter_flat_dpx_kernel<16, S, C>), job); break;    \
+  }
+  const bool cur = job.cursor != nullptr, shrt = job.min_len < job.W;
   if (!dpx) {
-    SG_FILTER(filter_flat_scalar_kernel, job, sp);
-    return;
-  }
-  if (job.min_len >= job.W) {
-    switch (job.W) {
-    case 2: SG_FILTER((filter_flat_dpx_kernel<2, false>), job); break;
-    case 4: SG_FILTER((filter_flat_dpx_kernel<4, false>), job); break;
-    case 8: SG_FILTER((filter_flat_dpx_kernel<8, false>), job); break;
-    default: SG_FILTER((filter_flat_dpx_kernel<16, false>), job); break;
-    }
+    if (cur) SG_FILTER(filter_flat_scalar_kernel<true>, job, sp);
+    else SG_FILTER(filter_flat_scalar_kernel<false>, job, sp);
+  } else if (!shrt) {
+    if (cur) { SG_FILTER_W(false, true) } else { SG_FILTER_W(false, false) }
   } else {
-    switch (job.W) {
-    case 2: SG_FILTER((filter_flat_dpx_kernel<2, true>), job); break;
-    case 4: SG_FILTER((filter_flat_dpx_kernel<4, true>), job); break;
-    case 8: SG_FILTER((filter_flat_dpx_kernel<8, true>), job); break;
-    default: SG_FILTER((filter_flat_dpx_kernel<16, true>), job); break;
-    }
+    if (cur) { SG_FILTER_W(true, true) } else { SG_FILTER_W(true, false) }
   }
+#undef SG_FILTER_W
 #undef SG_FILTER
 }
 

@@ -27,7 +27,7 @@ struct FilterJob {
   // may be null; else a zeroed work cursor: the grid is the resident set, and every block takes
   // the next tile of 256 * kFilterTile candidates from it, in list order, until none is left
   unsigned long long* cursor;
-  int rows;  // rows of 256 candidates in a block's tile; 0 = the default (8)
+  int rows;  // with a cursor: rows of 256 candidates in a block's tile (0 = 8); without: 8
 };
 
 constexpr int64_t kGexpPad = 4096;   // bytes of padding around a byte-expanded sequence

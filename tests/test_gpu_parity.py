@@ -270,3 +270,30 @@ def test_map_results_do_not_depend_on_the_launch_tuning():
     got = m.map(batch, tbs)
     assert got.hits.tobytes() == base.hits.tobytes() and got.tb.tobytes() == base.tb.tobytes()
     m.close()
+
+
+def test_large_host_batch_is_pipelined_with_the_same_results():
+    """A host-buffer batch of a million reads or more is mapped in chunks whose copies overlap
+    the kernels; every read's result must be the one it gets in a small batch."""
+    from storm_b200 import synth
+    genome = synth.make_genome([50000], 51, gc=0.45, repeat_frac=0.2)
+    seqs, quals = synth.simulate_nucleotide_reads(genome, 3000, [50], 53)
+    codes, levels, lengths = _reads_arrays(seqs, quals)
+    prm = api.params(indels=3, min_score=100, min_score_filter=95)
+    m = api.Mapper(prm, "####--#-#--##--####;#####--###-#-###;###-##-#######")
+    for _, s in genome:
+        cp = ffi.pack2(s, PADB)
+        mk = ffi.pack2(np.zeros(len(s), np.uint8), PADB, fill=0x55)
+        m.add_reference(cp[PADB:], mk[PADB:], len(s))
+    m.build_index()
+    small = m.map(api.ReadBatch(codes, lengths, levels))
+    st_small = m.stats()
+    rep = 350  # 1,050,000 reads: two chunks of 2^19 and a remainder
+    big = m.map(api.ReadBatch(np.tile(codes, (rep, 1)), np.tile(lengths, rep), np.tile(levels, (rep, 1))))
+    st_big = m.stats()
+    m.close()
+    assert small.mapped.sum() > 1000
+    assert st_big["candidates"] == rep * st_small["candidates"]
+    assert np.array_equal(big.mapped, np.tile(small.mapped, rep))
+    assert big.hits.tobytes() == np.tile(small.hits, rep).tobytes()
+    assert big.tb.tobytes() == np.tile(small.tb, (rep, 1)).tobytes()
