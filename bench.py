@@ -296,6 +296,11 @@ def serving_arm(a, w, ref_path, reads_path, d):
         reference.add_to(m)
         m.build_index()
         mappers.append(m)
+    # launch parameters (no effect on results) picked on a sample with the first step's seeds,
+    # used by both arms
+    tuning = mappers[0].autotune(api.ReadBatch(reads.codes, reads.lengths, reads.levels), sample=200000)
+    for m in mappers[1:]:
+        m.set_tuning(**tuning)
 
     def plain(batch):
         n = batch.n
@@ -330,6 +335,7 @@ def serving_arm(a, w, ref_path, reads_path, d):
     # arrivals at 80 % of that capacity
     srv = api.Server(prm, chain, slots=3, budget_bytes=48 << 30)
     reference.add_to_server(srv)
+    srv.set_tuning(**tuning)
     srv.build()
     srv.poll(srv.submit(batches[0], tbs))  # warm-up
 
@@ -371,7 +377,7 @@ def serving_arm(a, w, ref_path, reads_path, d):
     line = {"metric": "served reads/sec (3-step -O chain, continuous batching)", "value": served_rate,
             "unit": "reads/s", "n_gpus": 1, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "u8/int32", "data": "synthetic",
-            "config": {"workload": workload_name(a.cfg, a.scale), "reads": total, "batches": len(batches),
+            "config": {"tuning": tuning, "workload": workload_name(a.cfg, a.scale), "reads": total, "batches": len(batches),
                        "batch_sizes": [b.n for b in batches], "chain": chain, "args": " ".join(w["args"]),
                        "arrivals": "capacity: all batches at once; latency: Poisson at 80 % of capacity",
                        "slots": 3},

@@ -162,6 +162,11 @@ int stormgpu_server_add_reference(stormgpu_server *s, const uint8_t *codes, cons
                                   const int32_t *region_ends, int32_t n_regions);
 /* Index every step, start the workers. */
 int stormgpu_server_build(stormgpu_server *s);
+/* Launch parameters of every worker slot (stormgpu_tuning, declared below; none changes a
+ * result).  Before stormgpu_server_build only (the slots take them when they are built), else
+ * STORMGPU_ESTATE.  No counterpart in the reference. */
+struct stormgpu_tuning;
+int stormgpu_server_set_tuning(stormgpu_server *s, const struct stormgpu_tuning *t);
 /* Queue a batch (host buffers, which must stay valid until stormgpu_poll reports it done).
  * step[r] (optional, n bytes) receives the chain step that mapped read r, 255 if none did. */
 int stormgpu_submit(stormgpu_server *s, const stormgpu_reads *reads, stormgpu_results *out,

@@ -64,6 +64,8 @@ class Tuning(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+DEFAULT_TUNING = dict(gather_warp_cap=768, gather_reads_per_steal=4, filter_rows=8, align_steal=32, filter_cursor=0)
+
 _lib = None
 
 
@@ -89,6 +91,7 @@ def lib():
         L.stormgpu_get_tuning.argtypes = [C.c_void_p, C.POINTER(Tuning)]
         L.stormgpu_set_tuning.argtypes = [C.c_void_p, C.POINTER(Tuning)]
         L.stormgpu_autotune.argtypes = [C.c_void_p, C.POINTER(Reads), C.c_int64, C.POINTER(Tuning)]
+        L.stormgpu_server_set_tuning.argtypes = [C.c_void_p, C.POINTER(Tuning)]
         L.stormgpu_sw_filter.argtypes = [C.c_int, C.c_int, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
                                          C.c_uint32, C.c_void_p, C.c_int64, C.c_int64, C.c_void_p,
                                          C.c_int64, C.c_void_p, C.c_void_p]
@@ -290,6 +293,13 @@ class Server:
         _check(lib().stormgpu_server_add_reference(self._h, C.c_void_p(codes) if isinstance(codes, int) else _p(codes),
                                                    C.c_void_p(mask) if isinstance(mask, int) else _p(mask), n_codes,
                                                    _p(rs), _p(re), len(regions)))
+
+    def set_tuning(self, **kw):
+        """Launch parameters of every slot (before build); unnamed ones keep their defaults."""
+        t = Tuning(**DEFAULT_TUNING)
+        for k, v in kw.items():
+            setattr(t, k, int(v))
+        _check(lib().stormgpu_server_set_tuning(self._h, C.byref(t)))
 
     def build(self):
         _check(lib().stormgpu_server_build(self._h))

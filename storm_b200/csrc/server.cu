@@ -128,6 +128,7 @@ struct stormgpu_server {
   std::map<int64_t, Request*> reqs;
   int64_t next_ticket = 1;
   bool built = false, stop = false;
+  stormgpu_tuning tune = {768, 4, 8, 32, 0};  // launch parameters of every slot
 };
 
 namespace {
@@ -288,6 +289,7 @@ extern "C" int stormgpu_server_build(stormgpu_server* s) {
     v->owns_refs = false;
     v->p = s->p;
     v->seeds = s->steps[0]->seeds;
+    v->tune = s->tune;
     memset(&v->stats, 0, sizeof(v->stats));
     if (cudaStreamCreateWithFlags(&v->st, cudaStreamNonBlocking) != cudaSuccess) {
       cudaGetLastError();
@@ -302,6 +304,14 @@ extern "C" int stormgpu_server_build(stormgpu_server* s) {
   }
   s->built = true;
   for (auto* sl : s->slots) sl->th = std::thread(worker, s, sl);
+  return 0;
+}
+
+extern "C" int stormgpu_server_set_tuning(stormgpu_server* s, const stormgpu_tuning* t) {
+  if (!s || !t) { sg_set_error("stormgpu_server_set_tuning: null argument"); return STORMGPU_EINVAL; }
+  if (s->built) { sg_set_error("stormgpu_server_set_tuning: call it before stormgpu_server_build"); return STORMGPU_ESTATE; }
+  if (const int rc = stormgpu_set_tuning(s->steps[0], t)) return rc;  // range check
+  s->tune = *t;
   return 0;
 }
 

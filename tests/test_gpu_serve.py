@@ -113,7 +113,11 @@ def test_served_chain_equals_plain_chain_alone_and_in_the_mix(world):
     assert {0, 1, 255} <= steps, steps  # reads mapped at several steps, and some at none
     srv = api.Server(api.params(**ARGS), CHAIN, slots=3, budget_bytes=2 << 30)
     _add(srv, refs)
+    # launch parameters other than the plain chain's: they must change no result
+    srv.set_tuning(gather_warp_cap=1536, gather_reads_per_steal=1, filter_cursor=1, filter_rows=2, align_steal=64)
     srv.build()
+    with pytest.raises(api.StormError, match="before"):
+        srv.set_tuning()
     for i, b in enumerate(batches):  # alone
         t = srv.submit(b, tbs)
         _same(srv.poll(t), plain[i], ("alone", i))
