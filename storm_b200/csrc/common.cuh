@@ -73,6 +73,21 @@ inline int64_t resident_grid_of(const void* k, int threads, size_t smem) {
   cache[key] = g;
   return g;
 }
+// Allows kernel k up to `bytes` of dynamic shared memory on the current device (the attribute
+// is per device: set once for each device a process launches on).
+inline void set_smem_attribute_once(const void* k, int bytes) {
+  static std::mutex mu;
+  static std::map<std::pair<const void*, int>, bool> done;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lock(mu);
+  bool& d = done[std::make_pair(k, dev)];
+  if (!d) {
+    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    d = true;
+  }
+}
+
 template <class K>
 inline int64_t resident_grid(K* k, int threads, size_t smem = 0) {
   return resident_grid_of(reinterpret_cast<const void*>(k), threads, smem);

@@ -496,10 +496,7 @@ __global__ void gather_block_kernel(ReadsDev rd, IndexView ix, int I, const int3
 void launch_gather_fused(const ReadsDev& rd, const IndexView& ix, int I, const GatherOut& go, const SeedSet& seeds,
                          cudaStream_t st) {
   if (rd.n <= 0) return;
-  static std::once_flag attr;
-  std::call_once(attr, [] {
-    cudaFuncSetAttribute(gather_fused_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kGWarps * 2 * kMaxWarpCap * 4);
-  });
+  set_smem_attribute_once(reinterpret_cast<const void*>(gather_fused_kernel), kGWarps * 2 * kMaxWarpCap * 4);
   const size_t smem = (size_t)kGWarps * 2 * go.warp_cap * sizeof(int32_t);
   const int64_t per_block = (int64_t)kGWarps * go.reads_per_steal;
   const int64_t blocks = std::min<int64_t>((rd.n + per_block - 1) / per_block,
@@ -512,10 +509,7 @@ void launch_gather_block(const ReadsDev& rd, const IndexView& ix, int I, const i
                          int32_t* huge_count, const SeedSet& seeds, cudaStream_t st) {
   if (nlist <= 0) return;
   const int smem_cap = kBlockGatherCap;
-  static std::once_flag attr;
-  std::call_once(attr, [] {
-    cudaFuncSetAttribute(gather_block_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kBlockGatherCap * 4);
-  });
+  set_smem_attribute_once(reinterpret_cast<const void*>(gather_block_kernel), kBlockGatherCap * 4);
   if (gbuf)
     gather_block_kernel<<<nlist, 1024, 0, st>>>(rd, ix, I, list, go, gcap, gbuf, huge_list, huge_h, huge_count,
                                                  seeds);
