@@ -75,6 +75,10 @@ extern "C" int stormgpu_autotune(stormgpu_ctx* c, const stormgpu_reads* reads, i
     r.first_levels = r.first_levels ? sf.data() : nullptr;
     r.lengths = slen.data();
   }
+  if (r.n == 0) {  // nothing to time: the parameters stay as they are
+    if (out) *out = c->tune;
+    return 0;
+  }
   int maxL = 0;
   for (int64_t k = 0; k < r.n; ++k) maxL = std::max<int>(maxL, r.lengths[k]);
   const int64_t tbs = ((maxL + c->p.allowed_indels + 1) / 2 + 7) & ~7LL;

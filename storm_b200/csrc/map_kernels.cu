@@ -87,7 +87,8 @@ constexpr int kMaxBand = 2 * STORMGPU_MAX_INDELS + 1;
 // machine :535-603 with the SNP adjustment :465-468), best cell on the last row (:621-630),
 // traceback :642-734.  The direction of every cell (2 bits) and, in colour space, whether its
 // pair score was made positive by the SNP adjustment (the `score > corner score` test of
-// :693) go to the scratch, slot-minor: word (row*wpr + k)*nslots + slot.
+// :693) go to the scratch, column-minor: word (row*wpr + k)*ns + sl for scratch column sl of
+// ns (the slot's index in a one-per-thread launch, the thread's index in a persistent one).
 // Genome and mask codes of the band of one row, 2 bits each in registers, for a constant band
 // width: row i + 1 is row i moved by one code, so each row loads one genome and one mask code
 // (instead of BW of each).
