@@ -303,7 +303,7 @@ __device__ __forceinline__ void align_one(const ReadsDev& rd, const ScoreParams&
 // count read from pb.npass_dev when it is given; scratch column = the thread's index in the
 // grid, so the scratch holds align_workers() columns).
 template <int BWT, int CM>
-__global__ void __launch_bounds__(128, (BWT > 0 && BWT <= 15 ? 5 : 1)) align_kernel(ReadsDev rd, ScoreParams sp, const uint8_t* __restrict__ genome,
+__global__ void __launch_bounds__(128, (BWT > 0 && BWT <= 15 ? 5 : BWT == 31 ? 4 : BWT == 41 ? 3 : 1)) align_kernel(ReadsDev rd, ScoreParams sp, const uint8_t* __restrict__ genome,
                                                     const uint8_t* __restrict__ mask, int64_t slot0, int64_t nslots,
                                                     PassBuffers pb) {
   // one call site of align_one (its band code is large and fully unrolled)
