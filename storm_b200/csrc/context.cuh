@@ -52,7 +52,6 @@ struct stormgpu_ctx {
   stormgpu_params p;
   sg::SeedSet seeds;
   cudaStream_t st = nullptr;
-  cudaStream_t cst = nullptr;  // copy stream of the pipelined host-buffer map (created on first use)
   std::vector<sg::RefSeq> refs;
   bool indexed = false;
   stormgpu_stats stats;

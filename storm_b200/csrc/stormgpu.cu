@@ -179,7 +179,6 @@ extern "C" void stormgpu_close(stormgpu_ctx* c) {
   c->gm_base.release();
   c->ord.release(); c->ord_tmp.release();
   for (auto& e : c->ev) cudaEventDestroy(e);
-  if (c->cst) { cudaStreamSynchronize(c->cst); cudaStreamDestroy(c->cst); }
   cudaStreamDestroy(c->st);
   delete c;
 }
@@ -248,9 +247,6 @@ extern "C" int stormgpu_build_index(stormgpu_ctx* c) {
 constexpr int64_t kMaxCandidatesPerPass = 1000000000;
 constexpr int64_t kMaxPassingPerPass = 100000000;  // their tracebacks are kept until the replay
 constexpr int kSplitBatch = 1;
-// Host-buffer batches of at least two chunks of this many reads are mapped chunk by chunk with
-// the copies overlapping the kernels (map_host_pipelined).
-constexpr int64_t kPipeChunk = 1 << 19;
 
 // S += s (everything but the index build time)
 static void add_stats(stormgpu_stats& S, const stormgpu_stats& s) {
@@ -528,102 +524,6 @@ extern "C" int stormgpu_sync(stormgpu_ctx* c) {
   return 0;
 }
 
-// Host-buffer mapping of a large batch, pipelined: chunks of `chunk` reads; every chunk's reads
-// go in on the copy stream up front, each chunk is mapped on the mapping stream once its reads
-// are in, and its results go out on the copy stream while the next chunk is mapped (reads are
-// independent, so the results are those of one call).  The copies overlap the kernels when the
-// host buffers are pinned.  The device buffers are already sized for the whole batch.
-static int map_host_pipelined(stormgpu_ctx* c, const stormgpu_reads* reads, stormgpu_results* out, int64_t chunk) {
-  const int64_t n = reads->n;
-  cudaStream_t st = c->st;
-  if (!c->cst && cudaStreamCreateWithFlags(&c->cst, cudaStreamNonBlocking) != cudaSuccess) {
-    cudaGetLastError();
-    sg_set_error("cudaStreamCreate failed");
-    return STORMGPU_ECUDA;
-  }
-  cudaStream_t cs = c->cst;
-  const int64_t nchunks = (n + chunk - 1) / chunk;
-  std::vector<cudaEvent_t> in((size_t)nchunks, nullptr), done((size_t)nchunks, nullptr);
-  int rc = 0;
-  for (int64_t k = 0; k < nchunks && !rc; ++k)
-    if (cudaEventCreateWithFlags(&in[k], cudaEventDisableTiming) != cudaSuccess ||
-        cudaEventCreateWithFlags(&done[k], cudaEventDisableTiming) != cudaSuccess) {
-      cudaGetLastError();
-      sg_set_error("cudaEventCreate failed");
-      rc = STORMGPU_ECUDA;
-    }
-  // chunk k of the batch: host (device = false) or device (device = true) buffers
-  auto piece = [&](int64_t k, bool device, stormgpu_reads& r, stormgpu_results& o) {
-    const int64_t k0 = k * chunk;
-    r = *reads;
-    o = *out;
-    r.n = std::min(chunk, n - k0);
-    r.codes = (device ? c->fcodes.p : reads->codes) + k0 * reads->code_stride;
-    if (reads->levels) r.levels = (device ? c->flevels.p : reads->levels) + k0 * reads->level_stride;
-    r.lengths = (device ? c->lengths.p : reads->lengths) + k0;
-    if (reads->first_levels) r.first_levels = (device ? c->first_levels.p : reads->first_levels) + k0;
-    o.hits = (device ? c->hits.p : out->hits) + 4 * k0;
-    o.tb = (device ? c->tb.p : out->tb) + 4 * k0 * out->tb_stride;
-    o.mapped = (device ? c->mapped.p : out->mapped) + k0;
-  };
-  for (int64_t k = 0; k < nchunks && !rc; ++k) {  // reads in
-    stormgpu_reads h, d;
-    stormgpu_results ho, dout;
-    piece(k, false, h, ho);
-    piece(k, true, d, dout);
-    if (cudaMemcpyAsync((void*)d.codes, h.codes, h.n * reads->code_stride, cudaMemcpyHostToDevice, cs) ||
-        cudaMemcpyAsync((void*)d.lengths, h.lengths, sizeof(int16_t) * h.n, cudaMemcpyHostToDevice, cs) ||
-        (reads->levels &&
-         cudaMemcpyAsync((void*)d.levels, h.levels, h.n * reads->level_stride, cudaMemcpyHostToDevice, cs)) ||
-        (reads->first_levels &&
-         cudaMemcpyAsync((void*)d.first_levels, h.first_levels, h.n, cudaMemcpyHostToDevice, cs)) ||
-        cudaEventRecord(in[k], cs)) {
-      cudaGetLastError();
-      sg_set_error("host to device copy failed");
-      rc = STORMGPU_ECUDA;
-    }
-  }
-  stormgpu_stats S;
-  memset(&S, 0, sizeof(S));
-  for (int64_t k = 0; k < nchunks && !rc; ++k) {  // map; results out
-    stormgpu_reads h, d;
-    stormgpu_results ho, dout;
-    piece(k, false, h, ho);
-    piece(k, true, d, dout);
-    if (cudaStreamWaitEvent(st, in[k], 0)) {
-      cudaGetLastError();
-      sg_set_error("stream wait failed");
-      rc = STORMGPU_ECUDA;
-      break;
-    }
-    if ((rc = map_device_impl(c, &d, &dout))) break;
-    add_stats(S, c->stats);
-    if (cudaEventRecord(done[k], st) || cudaStreamWaitEvent(cs, done[k], 0) ||
-        cudaMemcpyAsync(ho.hits, dout.hits, sizeof(stormgpu_hit) * h.n * 4, cudaMemcpyDeviceToHost, cs) ||
-        cudaMemcpyAsync(ho.tb, dout.tb, h.n * 4 * out->tb_stride, cudaMemcpyDeviceToHost, cs) ||
-        cudaMemcpyAsync(ho.mapped, dout.mapped, h.n, cudaMemcpyDeviceToHost, cs)) {
-      cudaGetLastError();
-      sg_set_error("device to host copy failed");
-      rc = STORMGPU_ECUDA;
-    }
-  }
-  if (cudaStreamSynchronize(cs) != cudaSuccess && !rc) {
-    cudaGetLastError();
-    sg_set_error("copy stream failed");
-    rc = STORMGPU_ECUDA;
-  }
-  cudaStreamSynchronize(st);
-  for (int64_t k = 0; k < nchunks; ++k) {
-    if (in[k]) cudaEventDestroy(in[k]);
-    if (done[k]) cudaEventDestroy(done[k]);
-  }
-  if (rc) return rc;
-  S.ms_index = c->stats.ms_index;
-  c->stats = S;
-  c->last_n = n;
-  return 0;
-}
-
 extern "C" int stormgpu_map(stormgpu_ctx* c, const stormgpu_reads* reads, stormgpu_results* out) {
   if (!c || !reads || !out || reads->n < 0) { sg_set_error("null argument"); return STORMGPU_EINVAL; }
   SG_CUDA(cudaSetDevice(c->p.device));
@@ -635,7 +535,6 @@ extern "C" int stormgpu_map(stormgpu_ctx* c, const stormgpu_reads* reads, stormg
     return STORMGPU_ENOMEM;
   if (reads->levels && c->flevels.grow(std::max<int64_t>(n * reads->level_stride, 1))) return STORMGPU_ENOMEM;
   if (reads->first_levels && c->first_levels.grow(std::max<int64_t>(n, 1))) return STORMGPU_ENOMEM;
-  if (n >= 2 * kPipeChunk) return map_host_pipelined(c, reads, out, kPipeChunk);
   if (n > 0) {
     SG_CUDA(cudaMemcpyAsync(c->fcodes.p, reads->codes, n * reads->code_stride, cudaMemcpyHostToDevice, st));
     SG_CUDA(cudaMemcpyAsync(c->lengths.p, reads->lengths, sizeof(int16_t) * n, cudaMemcpyHostToDevice, st));

@@ -272,9 +272,9 @@ def test_map_results_do_not_depend_on_the_launch_tuning():
     m.close()
 
 
-def test_large_host_batch_is_pipelined_with_the_same_results():
-    """A host-buffer batch of a million reads or more is mapped in chunks whose copies overlap
-    the kernels; every read's result must be the one it gets in a small batch."""
+def test_large_host_batch_gives_the_small_batch_results():
+    """A host-buffer batch of a million reads (3,000 distinct reads repeated): every read's
+    result must be the one it gets in a batch of its own 3,000."""
     from storm_b200 import synth
     genome = synth.make_genome([50000], 51, gc=0.45, repeat_frac=0.2)
     seqs, quals = synth.simulate_nucleotide_reads(genome, 3000, [50], 53)
@@ -288,7 +288,7 @@ def test_large_host_batch_is_pipelined_with_the_same_results():
     m.build_index()
     small = m.map(api.ReadBatch(codes, lengths, levels))
     st_small = m.stats()
-    rep = 350  # 1,050,000 reads: two chunks of 2^19 and a remainder
+    rep = 350  # 1,050,000 reads
     big = m.map(api.ReadBatch(np.tile(codes, (rep, 1)), np.tile(lengths, rep), np.tile(levels, (rep, 1))))
     st_big = m.stats()
     m.close()
