@@ -46,8 +46,7 @@ void launch_reverse_reads(const ReadsDev& in, const uint8_t* first_levels, int c
   reverse_reads_kernel<<<(unsigned)((in.n + 127) / 128), 128, 0, st>>>(in, first_levels, colour, rcodes, rlevels);
 }
 
-__global__ void init_results_kernel(int64_t n, stormgpu_hit* __restrict__ hits, uint8_t* __restrict__ mapped,
-                                    uint8_t* __restrict__ tb, int64_t tbs) {
+__global__ void init_results_kernel(int64_t n, stormgpu_hit* __restrict__ hits, uint8_t* __restrict__ mapped) {
   int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n * 4) return;
   stormgpu_hit h;
@@ -58,13 +57,13 @@ __global__ void init_results_kernel(int64_t n, stormgpu_hit* __restrict__ hits, 
   h.tb_len = 0;
   hits[t] = h;
   if ((t & 3) == 0) mapped[t >> 2] = 0;
-  for (int64_t b = 0; b < tbs; ++b) tb[t * tbs + b] = 0;
 }
 
 void launch_init_results(int64_t n, stormgpu_hit* hits, uint8_t* mapped, uint8_t* tb, int64_t tbs,
                          cudaStream_t st) {
   if (n <= 0) return;
-  init_results_kernel<<<(unsigned)((n * 4 + 255) / 256), 256, 0, st>>>(n, hits, mapped, tb, tbs);
+  init_results_kernel<<<(unsigned)((n * 4 + 255) / 256), 256, 0, st>>>(n, hits, mapped);
+  cudaMemsetAsync(tb, 0, (size_t)(n * 4 * tbs), st);  // the 4n traceback rows are contiguous
 }
 
 // ------------------------------------------------------------------------------ align
