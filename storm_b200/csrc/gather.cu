@@ -29,6 +29,21 @@ __device__ __forceinline__ uint32_t read_key(const SeedDev& s, const uint8_t* rd
   return key;
 }
 
+// The same key from a register window: codes rp .. rp + 31 of a read staged in shared memory
+// (4-byte aligned, readable for 12 bytes from word rp / 16), codes from L on masked to 0;
+// one shift and mask per care position instead of a shared-memory load.  Seeds of span <= 32.
+__device__ __forceinline__ uint32_t read_key_window(const SeedDev& s, const uint8_t* rd, int L, int rp) {
+  const uint32_t* w = reinterpret_cast<const uint32_t*>(rd) + (rp >> 4);
+  const uint64_t lo = (uint64_t)w[0] | ((uint64_t)w[1] << 32);
+  const int sh = 2 * (rp & 15);
+  uint64_t win = sh ? (lo >> sh) | ((uint64_t)w[2] << (64 - sh)) : lo;  // code rp + k at bits 2k
+  const int lim = L - rp;
+  if (lim < 32) win &= (1ull << (2 * lim)) - 1ull;
+  uint32_t key = 0;
+  for (int c = 0; c < s.n_care; ++c) key = (key << 2) | (uint32_t)((win >> (2 * s.care[c])) & 3u);
+  return key;
+}
+
 __device__ __forceinline__ int seed_npos(const SeedDev& s, int L) {
   return s.n_positions ? s.n_positions : (L - s.span + 1 > 0 ? L - s.span + 1 : 0);
 }
@@ -46,14 +61,15 @@ __device__ __forceinline__ void seed_item(const SeedSet& gs, const IndexView& ix
   cnt = __ldg(ix.first[si] + key + 1) - a;
 }
 
-// (index offset, count, read position) of position t of seed s, with that seed's key table
+// (index offset, count, read position) of position t of seed s, with that seed's key table;
+// `read` is staged in shared memory (see read_key_window)
 __device__ __forceinline__ void item_lookup(const int32_t* __restrict__ first, const SeedDev& s, int t,
                                             const uint8_t* read, int L, int& a, int& cnt, int& rp) {
   a = 0; cnt = 0; rp = 0;
   if (t >= seed_npos(s, L)) return;
   rp = s.n_positions ? s.positions[t] : t;
   if (rp < 0 || rp >= L) return;
-  const uint32_t key = read_key(s, read, L, rp);
+  const uint32_t key = s.span <= 32 ? read_key_window(s, read, L, rp) : read_key(s, read, L, rp);
   a = __ldg(first + key);
   cnt = __ldg(first + key + 1) - a;
 }
