@@ -238,6 +238,61 @@ static int header_name_len(const char *line, size_t ll) {
   return n - 1;
 }
 
+/* Read i of the batch (its raw record r) into out: name, codes, tag, qualities.  Returns 0, or
+ * STORMGPU_EINVAL for a negative quality value, with the message only when `report` is set.
+ * qv: scratch of maxl + 2 shorts. */
+static int fill_one(sh_reads *out, const char *buf, const rawread *r, int64_t i, int colour, int quality_base,
+                    int any_qual, int maxl, short *qv, int report) {
+  out->file_index[i] = i;
+  out->names[i] = malloc((size_t)r->name_len + 1);
+  memcpy(out->names[i], buf + r->name_off, (size_t)r->name_len);
+  out->names[i][r->name_len] = 0;
+  const char *sq = buf + r->seq_off;
+  int L = r->seq_len - (colour ? 2 : 0);
+  out->lengths[i] = (int16_t)L;
+  uint8_t *cd = out->codes + i * out->code_stride;
+  if (!colour) {
+    for (int k = 0; k < L; ++k) {
+      char c = sq[k];
+      put2(cd, k, c == 'A' ? 0 : c == 'C' ? 1 : c == 'G' ? 2 : c == 'T' ? 3 : 0);
+    }
+  } else {
+    /* reads_data.c:488-491: real first base = TRANSFORM(primer, first colour) */
+    int c0 = sq[0];
+    int b = ((c0 & 0x4) >> 1) | (((c0 & 0x4) >> 2) ^ ((c0 & 0x2) >> 1));
+    out->first_base[i] = (uint8_t)((b ^ (sq[1] & 3)) & 3);
+    for (int k = 0; k < L; ++k) put2(cd, k, sq[k + 2] & 3);
+  }
+  /* tag: maximum of the rolling 64-bit window, codes remapped to a,t,g,c order */
+  uint64_t tag = 0, ct = 0;
+  for (int k = 0; k < L; ++k) {
+    ct = (ct << 2) | (uint64_t)((((unsigned)get2(cd, k) + 1) & 3) ^ 1);
+    if (ct > tag) tag = ct;
+  }
+  out->tags[i] = tag;
+  if (any_qual && r->has_qual) {
+    const char *ql = buf + r->qual_off;
+    int qlen = r->qual_len;
+    memset(qv, 0, sizeof(short) * ((size_t)maxl + 2));
+    if (colour) {
+      int v = (int)(signed char)(qlen > 0 ? ql[0] : '\n') - quality_base;
+      if (v < 0) return report ? fail(STORMGPU_EINVAL, "Quality level char induces a negative value (read #%ld).", (long)i + 1) : STORMGPU_EINVAL;
+      out->first_level[i] = (uint8_t)quality_level(v > 93 ? 93 : v);
+    }
+    int lim = L < qlen ? L : qlen;
+    for (int k = colour ? 1 : 0; k < lim; ++k) {
+      int v = (int)(signed char)ql[k] - quality_base;
+      if (v < 0) return report ? fail(STORMGPU_EINVAL, "Quality level char \"%c\" induces a negative value (read #%ld).", ql[k], (long)i + 1) : STORMGPU_EINVAL;
+      qv[k] = (short)(v > 93 ? 93 : v);
+    }
+    uint8_t *lv = out->levels + i * out->level_stride;
+    /* colour: level of colour k is the quality of file colour k+1 (compress shift 1); the
+     * last one reads one past the parsed qualities, which is 0 (read_quality.c:31-41) */
+    for (int k = 0; k < L; ++k) put2(lv, k, quality_level(colour ? (k + 1 < L ? qv[k + 1] : 0) : qv[k]));
+  }
+  return 0;
+}
+
 static int fill_reads(sh_reads *out, const char *buf, rawread *rr, int64_t n, int colour,
                       int quality_base, int allow_mixed, int any_qual) {
   int minl = 1 << 30, maxl = 0;
@@ -265,58 +320,24 @@ static int fill_reads(sh_reads *out, const char *buf, rawread *rr, int64_t n, in
   out->first_base = calloc((size_t)(n ? n : 1), 1);
   out->first_level = calloc((size_t)(n ? n : 1), 1);
   out->file_index = calloc((size_t)(n ? n : 1), sizeof(int64_t));
-  short *qv = calloc((size_t)maxl + 2, sizeof(short));
-  for (int64_t i = 0; i < n; ++i) {
-    const rawread *r = &rr[i];
-    out->file_index[i] = i;
-    out->names[i] = malloc((size_t)r->name_len + 1);
-    memcpy(out->names[i], buf + r->name_off, (size_t)r->name_len);
-    out->names[i][r->name_len] = 0;
-    const char *sq = buf + r->seq_off;
-    int L = r->seq_len - (colour ? 2 : 0);
-    out->lengths[i] = (int16_t)L;
-    uint8_t *cd = out->codes + i * out->code_stride;
-    if (!colour) {
-      for (int k = 0; k < L; ++k) {
-        char c = sq[k];
-        put2(cd, k, c == 'A' ? 0 : c == 'C' ? 1 : c == 'G' ? 2 : c == 'T' ? 3 : 0);
-      }
-    } else {
-      /* reads_data.c:488-491: real first base = TRANSFORM(primer, first colour) */
-      int c0 = sq[0];
-      int b = ((c0 & 0x4) >> 1) | (((c0 & 0x4) >> 2) ^ ((c0 & 0x2) >> 1));
-      out->first_base[i] = (uint8_t)((b ^ (sq[1] & 3)) & 3);
-      for (int k = 0; k < L; ++k) put2(cd, k, sq[k + 2] & 3);
-    }
-    /* tag: maximum of the rolling 64-bit window, codes remapped to a,t,g,c order */
-    uint64_t tag = 0, ct = 0;
-    for (int k = 0; k < L; ++k) {
-      ct = (ct << 2) | (uint64_t)((((unsigned)get2(cd, k) + 1) & 3) ^ 1);
-      if (ct > tag) tag = ct;
-    }
-    out->tags[i] = tag;
-    if (any_qual && r->has_qual) {
-      const char *ql = buf + r->qual_off;
-      int qlen = r->qual_len;
-      memset(qv, 0, sizeof(short) * ((size_t)maxl + 2));
-      if (colour) {
-        int v = (int)(signed char)(qlen > 0 ? ql[0] : '\n') - quality_base;
-        if (v < 0) return fail(STORMGPU_EINVAL, "Quality level char induces a negative value (read #%ld).", (long)i + 1);
-        out->first_level[i] = (uint8_t)quality_level(v > 93 ? 93 : v);
-      }
-      int lim = L < qlen ? L : qlen;
-      for (int k = colour ? 1 : 0; k < lim; ++k) {
-        int v = (int)(signed char)ql[k] - quality_base;
-        if (v < 0) return fail(STORMGPU_EINVAL, "Quality level char \"%c\" induces a negative value (read #%ld).", ql[k], (long)i + 1);
-        qv[k] = (short)(v > 93 ? 93 : v);
-      }
-      uint8_t *lv = out->levels + i * out->level_stride;
-      /* colour: level of colour k is the quality of file colour k+1 (compress shift 1); the
-       * last one reads one past the parsed qualities, which is 0 (read_quality.c:31-41) */
-      for (int k = 0; k < L; ++k) put2(lv, k, quality_level(colour ? (k + 1 < L ? qv[k + 1] : 0) : qv[k]));
-    }
+  /* reads are independent: filled in parallel; the first failing read (in file order) is filled
+   * again alone to report its message, as a sequential pass would */
+  int64_t first_bad = n;
+#pragma omp parallel
+  {
+    short *qv = calloc((size_t)maxl + 2, sizeof(short));
+#pragma omp for schedule(static) reduction(min : first_bad)
+    for (int64_t i = 0; i < n; ++i)
+      if (fill_one(out, buf, &rr[i], i, colour, quality_base, any_qual, maxl, qv, 0)) first_bad = i < first_bad ? i : first_bad;
+    free(qv);
   }
-  free(qv);
+  if (first_bad < n) {
+    short *qv = calloc((size_t)maxl + 2, sizeof(short));
+    free(out->names[first_bad]);
+    const int rc = fill_one(out, buf, &rr[first_bad], first_bad, colour, quality_base, any_qual, maxl, qv, 1);
+    free(qv);
+    return rc;
+  }
   return 0;
 }
 
@@ -529,20 +550,28 @@ void sh_sort_reads(sh_reads *r) {
   int64_t n = r->n;
   sortkey *k = malloc(sizeof(sortkey) * (size_t)(n ? n : 1));
   for (int64_t i = 0; i < n; ++i) { k[i].len = r->lengths[i]; k[i].tag = r->tags[i]; k[i].idx = i; }
-  /* stable LSD radix sort on (length, tag), bytes of the tag first: from file order, equal keys
-   * keep file order */
-  {
-    sortkey *t = malloc(sizeof(sortkey) * (size_t)(n ? n : 1));
-    for (int pass = 0; pass < 10 && n > 0; ++pass) {
-      int64_t cnt[257] = {0};
-#define SK_BYTE(x) (pass < 8 ? (int)(((x).tag >> (8 * pass)) & 0xff) : (int)((((uint16_t)(x).len) >> (8 * (pass - 8))) & 0xff))
-      for (int64_t i = 0; i < n; ++i) cnt[SK_BYTE(k[i]) + 1]++;
-      if (cnt[SK_BYTE(k[0]) + 1] == n) continue;  /* one value of this byte: order unchanged */
-      for (int b = 0; b < 256; ++b) cnt[b + 1] += cnt[b];
-      for (int64_t i = 0; i < n; ++i) t[cnt[SK_BYTE(k[i])]++] = k[i];
-#undef SK_BYTE
+  /* stable LSD radix sort on (length, tag), 16-bit digits of the tag first: from file order,
+   * equal keys keep file order.  Digits that are the same for every read are skipped. */
+  if (n > 0) {
+    uint64_t vt = 0;
+    uint16_t vl = 0;
+    for (int64_t i = 0; i < n; ++i) {
+      vt |= k[i].tag ^ k[0].tag;
+      vl |= (uint16_t)(k[i].len ^ k[0].len);
+    }
+    sortkey *t = malloc(sizeof(sortkey) * (size_t)n);
+    int64_t *cnt = malloc(sizeof(int64_t) * 65537);
+    for (int pass = 0; pass < 5; ++pass) {
+      if (pass < 4 ? ((vt >> (16 * pass)) & 0xffff) == 0 : vl == 0) continue;
+#define SK_DIGIT(x) (pass < 4 ? (int)(((x).tag >> (16 * pass)) & 0xffff) : (int)(uint16_t)(x).len)
+      memset(cnt, 0, sizeof(int64_t) * 65537);
+      for (int64_t i = 0; i < n; ++i) cnt[SK_DIGIT(k[i]) + 1]++;
+      for (int b = 0; b < 65536; ++b) cnt[b + 1] += cnt[b];
+      for (int64_t i = 0; i < n; ++i) t[cnt[SK_DIGIT(k[i])]++] = k[i];
+#undef SK_DIGIT
       sortkey *sw = k; k = t; t = sw;
     }
+    free(cnt);
     free(t);
   }
   uint8_t *codes = malloc((size_t)(n ? n : 1) * (size_t)r->code_stride);
@@ -552,6 +581,7 @@ void sh_sort_reads(sh_reads *r) {
   char **names = malloc(sizeof(char *) * (size_t)(n ? n : 1));
   uint8_t *fb = malloc((size_t)(n ? n : 1)), *fl = malloc((size_t)(n ? n : 1));
   int64_t *fi = malloc(sizeof(int64_t) * (size_t)(n ? n : 1));
+#pragma omp parallel for schedule(static)
   for (int64_t i = 0; i < n; ++i) {
     int64_t s = k[i].idx;
     memcpy(codes + i * r->code_stride, r->codes + s * r->code_stride, (size_t)r->code_stride);
