@@ -730,13 +730,33 @@ static int symbol_at(const sh_refs *refs, uint8_t *const *chk, int s, int64_t po
   return b & 3;
 }
 
-/* the records of reads [first, first + count) (hit_map.c:197-504) */
+/* decimal text of v at p (as printf's %ld); returns the end */
+static inline char *put_long(char *p, long v) {
+  char t[24];
+  int k = 0;
+  unsigned long u = v < 0 ? 0ul - (unsigned long)v : (unsigned long)v;
+  do { t[k++] = (char)('0' + u % 10); u /= 10; } while (u);
+  if (v < 0) *p++ = '-';
+  while (k) *p++ = t[--k];
+  return p;
+}
+static inline char *put_str(char *p, const char *s) {
+  const size_t n = strlen(s);
+  memcpy(p, s, n);
+  return p + n;
+}
+
+/* the records of reads [first, first + count) (hit_map.c:197-504); a mapped record's line is
+ * formatted in a buffer (the fields of the reference's fprintf, hit_map.c:291-340) and written
+ * at once */
 static void write_sam_records(FILE *f, const sh_sam_opts *o, const sh_refs *refs, const sh_reads *reads,
                               const stormgpu_results *res, int64_t first, int64_t count, uint8_t *const *chk) {
   const int colour = o->colour;
   char cigar[4 * STORMGPU_MAX_READ_LEN + 64], seq[2 * STORMGPU_MAX_READ_LEN + 8];
   static const char B[4] = {'A', 'C', 'G', 'T'};
   char *qbuf = malloc((size_t)reads->max_len + 8);
+  size_t lcap = 4096;
+  char *line = malloc(lcap);
   for (int64_t r = first; r < first + count; ++r) {
     const stormgpu_hit *h = &res->hits[r * 4];
     int L = reads->lengths[r];
@@ -758,23 +778,35 @@ static void write_sam_records(FILE *f, const sh_sam_opts *o, const sh_refs *refs
         }
         int ed = sh_traceback_to_cigar(res->tb + (size_t)(r * 4 + k) * (size_t)res->tb_stride, h[k].tb_len,
                                        refs->codes[ref_id], ref_start, colour, sym, cigar, seq);
-        fprintf(f, "%s\t%d\t%s\t%ld\t%d\t%s\t*\t0\t0\t%s\t", reads->names[r], flag,
-                refs->names[ref_id] ? refs->names[ref_id] : "*", (long)(ref_start + 1), mapq, cigar, seq);
+        const char *rname = refs->names[ref_id] ? refs->names[ref_id] : "*";
+        const size_t need = strlen(reads->names[r]) + strlen(rname) + strlen(cigar) + strlen(seq) + (size_t)L + 160;
+        if (need > lcap) { lcap = 2 * need; line = realloc(line, lcap); }
+        char *p = line;
+        p = put_str(p, reads->names[r]); *p++ = '\t';
+        p = put_long(p, flag); *p++ = '\t';
+        p = put_str(p, rname); *p++ = '\t';
+        p = put_long(p, (long)(ref_start + 1)); *p++ = '\t';
+        p = put_long(p, mapq); *p++ = '\t';
+        p = put_str(p, cigar);
+        p = put_str(p, "\t*\t0\t0\t");
+        p = put_str(p, seq); *p++ = '\t';
         if (reads->levels) {
           const uint8_t *lv = reads->levels + r * reads->level_stride;
-          int qi = 0;
           if (rev) {
-            for (int q = L - 1; q >= 0; --q) { int c = o->quality_base + LEVEL_UB[get2(lv, q)]; qbuf[qi++] = (char)(c < 126 ? c : 126); }
-            if (colour) { int c = o->quality_base + LEVEL_UB[reads->first_level[r]]; qbuf[qi++] = (char)(c < 126 ? c : 126); }
+            for (int q = L - 1; q >= 0; --q) { int c = o->quality_base + LEVEL_UB[get2(lv, q)]; *p++ = (char)(c < 126 ? c : 126); }
+            if (colour) { int c = o->quality_base + LEVEL_UB[reads->first_level[r]]; *p++ = (char)(c < 126 ? c : 126); }
           } else {
-            if (colour) { int c = o->quality_base + LEVEL_UB[reads->first_level[r]]; qbuf[qi++] = (char)(c < 126 ? c : 126); }
-            for (int q = 0; q < L; ++q) { int c = o->quality_base + LEVEL_UB[get2(lv, q)]; qbuf[qi++] = (char)(c < 126 ? c : 126); }
+            if (colour) { int c = o->quality_base + LEVEL_UB[reads->first_level[r]]; *p++ = (char)(c < 126 ? c : 126); }
+            for (int q = 0; q < L; ++q) { int c = o->quality_base + LEVEL_UB[get2(lv, q)]; *p++ = (char)(c < 126 ? c : 126); }
           }
-          fwrite(qbuf, 1, (size_t)qi, f);
         } else {
-          fputc('*', f);
+          *p++ = '*';
         }
-        fprintf(f, "\tAS:i:%d\tNM:i:%d\tNH:i:%d\n", h[k].score, ed, nrep);
+        p = put_str(p, "\tAS:i:"); p = put_long(p, h[k].score);
+        p = put_str(p, "\tNM:i:"); p = put_long(p, ed);
+        p = put_str(p, "\tNH:i:"); p = put_long(p, nrep);
+        *p++ = '\n';
+        fwrite(line, 1, (size_t)(p - line), f);
       }
 #undef REPORTABLE
     } else if (o->print_all) {
@@ -795,6 +827,7 @@ static void write_sam_records(FILE *f, const sh_sam_opts *o, const sh_refs *refs
       }
     }
   }
+  free(line);
   free(qbuf);
 }
 
