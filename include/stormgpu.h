@@ -260,7 +260,8 @@ int stormgpu_align(const stormgpu_params *params, const uint8_t *read, const uin
  * current device, owned by the caller, and nothing is allocated: read / levels are packed as
  * for stormgpu_align (levels may be NULL); genome / mask hold n_codes codes with no padding,
  * and every window must lie inside them (0 <= win[k], win[k] + read_len + 2 * allowed_indels
- * <= n_codes; otherwise STORMGPU_EINVAL and unspecified outputs); win, score, bound, tb_len
+ * <= n_codes; otherwise STORMGPU_EINVAL, and every output buffer may have been overwritten,
+ * the results of the valid windows included); win, score, bound, tb_len
  * hold n entries, best 4n, tb n * tb_stride bytes (zero-filled, then the traceback).
  * params->device is not consulted.  Runs on `stream` (a cudaStream_t; NULL: the default
  * stream) and returns when the results are in place.
@@ -269,10 +270,11 @@ int stormgpu_align(const stormgpu_params *params, const uint8_t *read, const uin
  * library, which every GPU that loads the library holds until the process exits.  A call
  * needs 4 * read_len * words_per_row * n bytes of it plus at most 8n + 768 of bookkeeping
  * (words_per_row = ceil((4I + 2) / 32), plus ceil((2I + 1) / 32) in colour space,
- * I = allowed_indels); larger calls fail with STORMGPU_EINVAL: split the windows.  The first
- * call on a device looks up the array's device address (cudaGetSymbolAddress): make it before
- * any stream capture.  Every call on a device shares that device's array, so calls that
- * overlap on the GPU race: serialise them. */
+ * I = allowed_indels); larger calls fail with STORMGPU_EINVAL: split the windows.  Every call
+ * looks up the array's device address on the current device (cudaGetSymbolAddress, which
+ * allocates nothing); the first call on a device also loads the library's module there, so
+ * make it before any stream capture.  Every call on a device shares that device's array, so
+ * calls that overlap on the GPU race: serialise them. */
 #define STORMGPU_NOALLOC_SCRATCH_BYTES (8ll << 20)
 int stormgpu_align_noalloc(const stormgpu_params *params, const uint8_t *read, const uint8_t *levels,
                            int read_len, const uint8_t *genome, const uint8_t *mask, int64_t n_codes,

@@ -13,11 +13,11 @@
 // It comes from g_noalloc_scratch below: one file-scope device array of kNoAllocScratchBytes
 // (8 MiB) that every GPU which loads this library holds until the process exits.  In host
 // code the array's name is only a host-side stand-in for it; its device address is obtained
-// once per device with cudaGetSymbolAddress, with that device current, by the first call on
-// that device.  Every call shares the array and it keeps the last call's contents: what must
-// start at zero (the error count, the per-window read indices) is cleared by each call.
+// with cudaGetSymbolAddress, with that device current, at the start of every call (the first
+// call on a device also loads the module there).  Every call shares the array and it keeps
+// the last call's contents: what must start at zero (the error count, the per-window read
+// indices) is cleared by each call.
 #include <cstring>
-#include <mutex>
 
 #include "map_kernels.cuh"
 
@@ -38,25 +38,18 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratch
 constexpr int64_t kHeaderBytes = 256;
 inline int64_t round256(int64_t x) { return (x + 255) & ~255LL; }
 
-constexpr int kMaxDevices = 64;
-std::mutex g_setup_mutex;
-void* g_scratch_addr[kMaxDevices];  // device address of g_noalloc_scratch, per device
-
-// Device address of the scratch on `dev` (the current device); the first call on a device
-// looks it up.
+// Device address of the scratch on the current device.  cudaGetSymbolAddress allocates
+// nothing; it is asked on every call rather than cached, so that an address never outlives
+// the module it came from (a device reset or a primary-context release reloads the module).
 int scratch_address(int dev, unsigned char** out) {
-  std::lock_guard<std::mutex> lock(g_setup_mutex);
-  if (!g_scratch_addr[dev]) {
-    unsigned char* ptr = nullptr;
-    const cudaError_t e = cudaGetSymbolAddress((void**)&ptr, g_noalloc_scratch);
-    if (e != cudaSuccess || !ptr) {
-      sg_set_error("stormgpu_align_noalloc: cudaGetSymbolAddress of the scratch array failed on device %d: %s",
-                   dev, cudaGetErrorString(e));
-      return STORMGPU_ECUDA;
-    }
-    g_scratch_addr[dev] = ptr;
+  unsigned char* ptr = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress((void**)&ptr, g_noalloc_scratch);
+  if (e != cudaSuccess || !ptr) {
+    sg_set_error("stormgpu_align_noalloc: cudaGetSymbolAddress of the scratch array failed on device %d: %s",
+                 dev, cudaGetErrorString(e));
+    return STORMGPU_ECUDA;
   }
-  *out = static_cast<unsigned char*>(g_scratch_addr[dev]);
+  *out = ptr;
   return 0;
 }
 
@@ -116,10 +109,6 @@ extern "C" int stormgpu_align_noalloc(const stormgpu_params* params, const uint8
   if (n == 0) return 0;
   int dev = 0;
   SG_CUDA(cudaGetDevice(&dev));
-  if (dev < 0 || dev >= kMaxDevices) {
-    sg_set_error("stormgpu_align_noalloc: device %d beyond %d", dev, kMaxDevices);
-    return STORMGPU_EINVAL;
-  }
   unsigned char* scr = nullptr;
   if (const int rc = scratch_address(dev, &scr)) return rc;
   cudaStream_t st = static_cast<cudaStream_t>(stream);

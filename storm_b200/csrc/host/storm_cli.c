@@ -226,6 +226,10 @@ int storm_cli_main(int argc, char **argv, int colour, const storm_mapper *mapper
   res.hits = calloc((size_t)(reads.n ? reads.n : 1) * 4, sizeof(stormgpu_hit));
   res.tb = calloc((size_t)(reads.n ? reads.n : 1) * 4, (size_t)res.tb_stride);
   res.mapped = calloc((size_t)(reads.n ? reads.n : 1), 1);
+  if (!res.hits || !res.tb || !res.mapped) {
+    err("Not enough memory for the results of %ld reads.", (long)reads.n);
+    exit(1);
+  }
   char emsg[512] = {0};
   int rc = mapper->map(mapper->user, &p, seeds, &refs, &reads, &res, emsg, sizeof(emsg));
   if (rc == STORMGPU_EINVAL && strstr(emsg, "seed")) {
@@ -250,7 +254,10 @@ int storm_cli_main(int argc, char **argv, int colour, const storm_mapper *mapper
     if (output) {
       static char obuf[1 << 22];
       setvbuf(output, obuf, _IOFBF, sizeof(obuf));
-      sh_write_sam(output, &so, &refs, &reads, &res, 0, reads.n, 1);
+      if (sh_write_sam(output, &so, &refs, &reads, &res, 0, reads.n, 1) != 0) {
+        err("%s", sh_last_error());
+        exit(1);
+      }
       fflush(output);
     } else {
       err("No file name provided for SAM output.");
@@ -259,6 +266,10 @@ int storm_cli_main(int argc, char **argv, int colour, const storm_mapper *mapper
     /* the per-position map (genome_map, run.c:1025-1061) */
     msg(1, "\n\nReference mapping...\n");
     sh_placement *pl = malloc(sizeof(sh_placement) * (size_t)(reads.n ? reads.n : 1));
+    if (!pl) {
+      err("Not enough memory for the placement of %ld reads.", (long)reads.n);
+      exit(1);
+    }
     int64_t npl = 0;
     if (map_greedy) {
       if (!mapper->place_greedy ||

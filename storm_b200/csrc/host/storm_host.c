@@ -711,9 +711,15 @@ typedef struct colour_cursor { int seq; int64_t pos; int base; } colour_cursor;
 #define SYM_STEP 64
 static uint8_t **symbol_checkpoints(const sh_refs *refs) {
   uint8_t **chk = calloc((size_t)refs->n, sizeof(uint8_t *));
+  if (!chk) return NULL;
   for (int s = 0; s < refs->n; ++s) {
     const int64_t nck = refs->sizes[s] / SYM_STEP + 2;
     chk[s] = malloc((size_t)nck);
+    if (!chk[s]) {
+      for (int t = 0; t < s; ++t) free(chk[t]);
+      free(chk);
+      return NULL;
+    }
     int b = refs->first_base[s];
     for (int64_t p = 0, k = 0; k < nck; ++k) {
       chk[s][k] = (uint8_t)b;
@@ -748,8 +754,8 @@ static inline char *put_str(char *p, const char *s) {
 
 /* the records of reads [first, first + count) (hit_map.c:197-504); a mapped record's line is
  * formatted in a buffer (the fields of the reference's fprintf, hit_map.c:291-340) and written
- * at once */
-static void write_sam_records(FILE *f, const sh_sam_opts *o, const sh_refs *refs, const sh_reads *reads,
+ * at once.  Returns 0, or STORMGPU_ENOMEM when a line buffer cannot be allocated. */
+static int write_sam_records(FILE *f, const sh_sam_opts *o, const sh_refs *refs, const sh_reads *reads,
                               const stormgpu_results *res, int64_t first, int64_t count, uint8_t *const *chk) {
   const int colour = o->colour;
   char cigar[4 * STORMGPU_MAX_READ_LEN + 64], seq[2 * STORMGPU_MAX_READ_LEN + 8];
@@ -757,6 +763,7 @@ static void write_sam_records(FILE *f, const sh_sam_opts *o, const sh_refs *refs
   char *qbuf = malloc((size_t)reads->max_len + 8);
   size_t lcap = 4096;
   char *line = malloc(lcap);
+  if (!qbuf || !line) { free(qbuf); free(line); return STORMGPU_ENOMEM; }
   for (int64_t r = first; r < first + count; ++r) {
     const stormgpu_hit *h = &res->hits[r * 4];
     int L = reads->lengths[r];
@@ -780,7 +787,12 @@ static void write_sam_records(FILE *f, const sh_sam_opts *o, const sh_refs *refs
                                        refs->codes[ref_id], ref_start, colour, sym, cigar, seq);
         const char *rname = refs->names[ref_id] ? refs->names[ref_id] : "*";
         const size_t need = strlen(reads->names[r]) + strlen(rname) + strlen(cigar) + strlen(seq) + (size_t)L + 160;
-        if (need > lcap) { lcap = 2 * need; line = realloc(line, lcap); }
+        if (need > lcap) {
+          char *grown = realloc(line, 2 * need);
+          if (!grown) { free(line); free(qbuf); return STORMGPU_ENOMEM; }
+          line = grown;
+          lcap = 2 * need;
+        }
         char *p = line;
         p = put_str(p, reads->names[r]); *p++ = '\t';
         p = put_long(p, flag); *p++ = '\t';
@@ -829,6 +841,7 @@ static void write_sam_records(FILE *f, const sh_sam_opts *o, const sh_refs *refs
   }
   free(line);
   free(qbuf);
+  return 0;
 }
 
 int sh_write_sam(FILE *f, const sh_sam_opts *o, const sh_refs *refs, const sh_reads *reads,
@@ -856,18 +869,20 @@ int sh_write_sam(FILE *f, const sh_sam_opts *o, const sh_refs *refs, const sh_re
   const int64_t per_round = CH * nthreads * 2;
   char **bufs = calloc((size_t)nthreads * 2, sizeof(char *));
   size_t *lens = calloc((size_t)nthreads * 2, sizeof(size_t));
-  for (int64_t lo = first; lo < first + count; lo += per_round) {
+  int nomem = !bufs || !lens || (colour && !chk);
+  for (int64_t lo = first; !nomem && lo < first + count; lo += per_round) {
     const int64_t hi = lo + per_round < first + count ? lo + per_round : first + count;
     const int nchunks = (int)((hi - lo + CH - 1) / CH);
-#pragma omp parallel for schedule(dynamic, 1)
+#pragma omp parallel for schedule(dynamic, 1) reduction(|| : nomem)
     for (int c = 0; c < nchunks; ++c) {
       const int64_t a = lo + (int64_t)c * CH, e = a + CH < hi ? a + CH : hi;
       FILE *m = open_memstream(&bufs[c], &lens[c]);
-      write_sam_records(m, o, refs, reads, res, a, e - a, chk);
+      if (!m) { nomem = 1; continue; }
+      if (write_sam_records(m, o, refs, reads, res, a, e - a, chk)) nomem = 1;
       fclose(m);
     }
     for (int c = 0; c < nchunks; ++c) {
-      fwrite(bufs[c], 1, lens[c], f);
+      if (!nomem) fwrite(bufs[c], 1, lens[c], f);
       free(bufs[c]);
       bufs[c] = NULL;
     }
@@ -878,6 +893,7 @@ int sh_write_sam(FILE *f, const sh_sam_opts *o, const sh_refs *refs, const sh_re
     for (int s = 0; s < refs->n; ++s) free(chk[s]);
     free(chk);
   }
+  if (nomem) return fail(STORMGPU_ENOMEM, "Out of memory while writing the SAM output.");
   return 0;
 }
 

@@ -50,7 +50,8 @@ def _noalloc(prm, c, wins=None):
     wins = c["wins"] if wins is None else wins
     n, L, I = len(wins), c["L"], c["I"]
     tbs = ((L + I + 1) // 2 + 7) & ~7
-    d = {k: _dev(c[k]) for k in ("rp", "qp", "gp", "mp")}
+    d = {k: _dev(c[k]) for k in ("rp", "gp", "mp")}
+    qaddr = _dev(c["qp"]) if c["qp"] is not None else None
     dw = _dev(wins)
     score = torch.empty(n, dtype=torch.int32, device="cuda")
     bound = torch.empty(n, dtype=torch.int32, device="cuda")
@@ -58,7 +59,8 @@ def _noalloc(prm, c, wins=None):
     tbl = torch.empty(n, dtype=torch.int32, device="cuda")
     tb = torch.full((n, tbs), 0xAB, dtype=torch.uint8, device="cuda")
     torch.cuda.synchronize()
-    api.align_noalloc(prm, d["rp"].data_ptr(), d["qp"].data_ptr(), L, d["gp"].data_ptr(), d["mp"].data_ptr(),
+    levels = qaddr.data_ptr() if qaddr is not None else 0
+    api.align_noalloc(prm, d["rp"].data_ptr(), levels, L, d["gp"].data_ptr(), d["mp"].data_ptr(),
                       c["G"], dw.data_ptr(), n, score.data_ptr(), bound.data_ptr(), best.data_ptr(),
                       tbl.data_ptr(), tb.data_ptr(), tbs, torch.cuda.current_stream().cuda_stream)
     return score.cpu().numpy(), bound.cpu().numpy(), best.cpu().numpy(), tbl.cpu().numpy(), tb.cpu().numpy()
@@ -87,6 +89,14 @@ def test_noalloc_matches_align_on_calls_in_a_row():
     for c in cases:
         _check_same(c)
     _check_same(cases[1])  # the same small call again, after a larger one
+
+
+def test_noalloc_without_quality_levels():
+    """levels = NULL (every level 3) in both calls, nucleotide and colour."""
+    rng = np.random.default_rng(2025)
+    for c in (_case(rng, 0, 7, 75, 2000, 17), _case(rng, 1, 3, 50, 1200, 11)):
+        c["qp"] = None
+        _check_same(c)
 
 
 def test_noalloc_rejects_sizes_beyond_its_scratch():
