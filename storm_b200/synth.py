@@ -47,12 +47,26 @@ def random_bases(rng: np.random.Generator, n: int, gc: float = 0.5) -> np.ndarra
     return rng.choice(4, size=n, p=p).astype(np.uint8)
 
 
+def random_bases_fast(rng: np.random.Generator, n: int, gc: float = 0.5, chunk: int = 1 << 24) -> np.ndarray:
+    """Like random_bases, for genomes of billions of codes: 16-bit uniforms through a table of
+    the base probabilities (quantised to 1/65536), in chunks, without 64-bit temporaries."""
+    p = np.array([(1 - gc) / 2, gc / 2, gc / 2, (1 - gc) / 2])
+    edges = np.rint(np.cumsum(p) * 65536).astype(np.int64)
+    lut = np.searchsorted(edges, np.arange(65536), side="right").astype(np.uint8)
+    out = np.empty(n, np.uint8)
+    for a in range(0, n, chunk):
+        e = min(n, a + chunk)
+        out[a:e] = lut[rng.integers(0, 65536, size=e - a, dtype=np.uint16)]
+    return out
+
+
 def make_reference(size: int, seed: int, gc: float = 0.5, repeat_frac: float = 0.0,
                    seg_min: int = 300, seg_max: int = 6000, mut_min: float = 0.05,
-                   mut_max: float = 0.15) -> np.ndarray:
-    """One reference sequence of `size` codes; `repeat_frac` of it is made of mutated copies."""
+                   mut_max: float = 0.15, fast: bool = False) -> np.ndarray:
+    """One reference sequence of `size` codes; `repeat_frac` of it is made of mutated copies.
+    `fast` draws the bases with random_bases_fast (another sequence for the same seed)."""
     rng = np.random.default_rng(seed)
-    seq = random_bases(rng, size, gc)
+    seq = random_bases_fast(rng, size, gc) if fast else random_bases(rng, size, gc)
     if repeat_frac > 0 and size > 2 * seg_max:
         covered = 0
         target = int(repeat_frac * size)
@@ -69,9 +83,9 @@ def make_reference(size: int, seed: int, gc: float = 0.5, repeat_frac: float = 0
     return seq
 
 
-def make_genome(sizes, seed: int, gc: float = 0.5, repeat_frac: float = 0.0):
+def make_genome(sizes, seed: int, gc: float = 0.5, repeat_frac: float = 0.0, fast: bool = False):
     """Several named sequences ("chr1", ...) with independent seeds derived from `seed`."""
-    return [("chr%d" % (i + 1), make_reference(int(s), seed * 1000 + i, gc, repeat_frac))
+    return [("chr%d" % (i + 1), make_reference(int(s), seed * 1000 + i, gc, repeat_frac, fast=fast))
             for i, s in enumerate(sizes)]
 
 
@@ -226,15 +240,34 @@ def workload(cfg: int, scale: float = 1.0):
         sizes = (sizes * (3.1e9 / sizes.sum()) * scale).astype(np.int64)
         return dict(mode="nucleotide", ref_sizes=[int(s) for s in sizes], gc=0.41, repeat=0.50,
                     ref_seed=4, reads=int(100_000_000 * scale), lengths=100, read_seed=14,
-                    model=dict(indel_rate=0.002, indel_max=20),
+                    model=dict(indel_rate=0.002, indel_max=20), fast_genome=True,
                     args=["-i", "20", "-z", "85", "-t", "100", "-M", "1"])
     raise ValueError(cfg)
+
+
+def genome_of(w):
+    """The reference sequences of workload `w` (a workload() dict)."""
+    return make_genome(w["ref_sizes"], w["ref_seed"], w["gc"], w["repeat"], fast=w.get("fast_genome", False))
+
+
+CHUNK_READS = 100_000
+
+
+def reads_chunk(w, genome, chunk: int, n: int = CHUNK_READS):
+    """Reads [chunk * CHUNK_READS, chunk * CHUNK_READS + n) of workload `w`'s read set, when the
+    set is drawn in independent chunks of CHUNK_READS reads (so that any chunk can be made
+    without the others): chunk c draws from seed read_seed * 100003 + c.  Nucleotide workloads
+    only; returns (seqs, quals) as simulate_nucleotide_reads."""
+    if w["mode"] != "nucleotide":
+        raise ValueError("chunked reads are drawn for nucleotide workloads")
+    model = ReadModel(**w.get("model", {}))
+    return simulate_nucleotide_reads(genome, n, w["lengths"], w["read_seed"] * 100003 + chunk, model)
 
 
 def generate(cfg: int, scale: float, ref_path, reads_path):
     """Write the reference FASTA and the reads FASTQ of workload `cfg` at `scale`."""
     w = workload(cfg, scale)
-    genome = make_genome(w["ref_sizes"], w["ref_seed"], w["gc"], w["repeat"])
+    genome = genome_of(w)
     write_fasta(ref_path, genome)
     model = ReadModel(**w.get("model", {}))
     if w["mode"] == "colour":
