@@ -1,22 +1,32 @@
 #!/usr/bin/env python
 """Benchmark of the mapping hot path on B200.
 
-One step = the hot path over one batch: build the spaced-seed index of the resident
-reference (every seed), then map every read of the batch on both strands (hit gather,
-banded filter, full alignment with traceback, top-4 update) into device-resident results.
-The default workload is the colour-space one (10 Mbp, 41% GC, 20% mutated repeats, 2M reads
-of a primer + 50 colours, storm-color -M 1 -z 105 -t 120 -i 7 and its three w11 seeds),
-generated here from fixed seeds.
+Default workload (the metric's batched form): the mixed-length nucleotide workload at full
+size -- a 100 Mbp reference (41 % GC, 45 % of it mutated repeat copies) and a read set of 10M
+Illumina-like reads of 35, 50, 75, 100 and 150 bp, mapped with `storm-nucleotide -i 15 -M 1
+-z 100 -t 100` and three weight-10 spaced seeds.  The read set is drawn in independent chunks
+of 100,000 reads (storm_b200.synth.reads_chunk); one step maps one chunk, a different chunk
+every step, with the reference and its index resident in HBM.
 
     python bench.py [--gpus N --steps K --warmup W] [--impl reference] [--cfg 0..4 --scale s]
 
-value   reads/s with reads, reference and results resident in HBM (device-timed, CUDA events);
-e2e     the same through the host-buffer C ABI call (stormgpu_map: reads copied in, results
-        copied out inside the timed region) plus the index build;
-roofline the dominant kernel against its measured ceiling; cpu_baseline the reference's
-        OpenMP/AVX2 build (oracle/_ref) on this host's cores on a bounded read sample.
-Multi-GPU: one process per GPU (torchrun), each maps its own batch (weak scaling), no
-collective on the data path; time = max over ranks.
+value        reads/s, device-resident: the chunk's packed reads in HBM before the timed region,
+             results left in HBM; CUDA events on the mapping stream, max over ranks.
+e2e          reads/s through the resident front end (storm_b200.pipeline.ResidentMapper): the
+             chunk's FASTQ file in, its SAM file out -- parsing, tag sort, host->device copies,
+             mapping, device->host copies and SAM formatting inside the timed region.
+roofline     the dominant kernel against the chip (integer issue rate at the sampled clock, or
+             the measured HBM bandwidth); every stage's fraction is in `stages`.
+cpu_baseline the reference's own OpenMP/AVX2 build (oracle/_ref) on this host's cores, on a
+             bounded sample (the first reads of each length of a chunk), index resident.
+parity_vs_reference  chunk 0 mapped through the same front end, per read length, against the
+             digests of the reference's own SAM for that chunk (tests/golden/scale_digests.json).
+
+--impl reference times the reference (oracle/_ref/storm-nucleotide-resident: its stock command
+line run once per request with its reference and indexes kept in memory) on the same chunks,
+each step the first reads of each length of the step's chunk.
+Multi-GPU (torchrun): each rank maps its own chunks (weak scaling), no collective on the data
+path; time = max over ranks.
 """
 from __future__ import annotations
 
@@ -37,62 +47,33 @@ from storm_b200 import synth  # noqa: E402
 
 PEAKS_PATH = os.path.join(ROOT, "MEASURED_PEAKS.json")
 TRAFFIC_PATH = os.path.join(ROOT, "profiles", "traffic.json")
-REF_DIR = os.path.join(ROOT, "oracle", "_ref")
+DIGESTS_PATH = os.path.join(ROOT, "tests", "golden", "scale_digests.json")
+FALLBACK_HBM_GBS = 6650.0  # measured on this pool's B200s before MEASURED_PEAKS.json existed
+SMS = 148
+REF_SAMPLE_PER_LENGTH = 80  # reference arm: reads of each length per step
 
 
 def log(*a):
     print(*a, file=sys.stderr, flush=True)
 
 
-def workload_files(cfg: int, scale: float, rank: int, nreads: int | None = None):
-    """Generate (once) the FASTA + FASTQ of workload `cfg` for this rank; returns paths + spec."""
-    w = synth.workload(cfg, scale)
-    d = os.path.join(tempfile.gettempdir(), "storm_bench_c%d_s%g_r%d" % (cfg, scale, rank))
-    os.makedirs(d, exist_ok=True)
-    ref, reads = os.path.join(d, "ref.fa"), os.path.join(d, "reads.fq")
-    done = os.path.join(d, "done")
-    if not os.path.exists(done):
-        genome = synth.make_genome(w["ref_sizes"], w["ref_seed"], w["gc"], w["repeat"])
-        synth.write_fasta(ref, genome)
-        model = synth.ReadModel(**w.get("model", {}))
-        if w["mode"] == "colour":
-            pr, cols, q = synth.simulate_colour_reads(genome, w["reads"], w["lengths"], w["read_seed"] + 1000 * rank, model)
-            synth.write_colour_fastq(reads, pr, cols, q)
-        else:
-            seqs, quals = synth.simulate_nucleotide_reads(genome, w["reads"], w["lengths"], w["read_seed"] + 1000 * rank, model)
-            synth.write_fastq(reads, seqs, quals)
-        open(done, "w").write("ok")
-    return w, ref, reads, d
-
-
-def parse_cli_args(args):
-    """The mapping parameters of a storm command line (main.c semantics)."""
-    p = dict(match=5, mismatch=-4, gap_open=-9, gap_extend=-4, indels=3, min_score=115,
-             min_score_filter=100, stdev=100, senses=3)
-    seeds = None
-    it = iter(range(len(args)))
-    i = 0
-    while i < len(args):
-        a = args[i]
-        v = args[i + 1] if i + 1 < len(args) else None
-        key = {"-m": "match", "-x": "mismatch", "-d": "gap_open", "-e": "gap_extend", "-i": "indels",
-               "-t": "min_score", "-z": "min_score_filter", "-l": "stdev"}.get(a)
-        if key:
-            p[key] = int(v)
-            i += 2
-        elif a == "-s":
-            seeds = v
-            i += 2
-        elif a in ("-M", "-b", "-o", "-O"):
-            i += 2
-        else:
-            i += 1
-    del it
-    return p, seeds
-
-
 DEFAULT_SEEDS = {0: "####--#-#--##--####;#####--###-#-###;###-##-#######",
                  1: "####----##--##-####;####-###--#----####;####-####-####"}
+
+
+def workload_name(cfg, scale):
+    names = {0: "nucleotide 1 Mbp, 100k x 50 bp, -i 3", 1: "colour 10 Mbp (20 % repeats), 2M x 50 colours, -i 7",
+             2: "mixed-length nucleotide 100 Mbp (45 % repeats), 10M x 35-150 bp, -i 15, three w10 seeds",
+             3: "served -O chain, 100 Mbp (45 % repeats), 35-150 bp", 4: "large 3.1 Gbp in 24 sequences, 100 bp, -i 20"}
+    return names[cfg] + ("" if scale == 1.0 else " (scale %g)" % scale)
+
+
+def headline_config(a, w):
+    """The workload identity, the same in both arms (the per-step samples are reported apart)."""
+    return {"workload": workload_name(a.cfg, a.scale), "reference_codes": sum(w["ref_sizes"]),
+            "reads_total": w["reads"], "read_lengths": w["lengths"] if isinstance(w["lengths"], list) else [w["lengths"]],
+            "args": " ".join(w["args"]), "parallelism": "dp%d (reads)" % a.gpus,
+            "l2": "inputs larger than L2 (the index alone is 1.2 GB) and a 512 MB write between timed steps"}
 
 
 class ClockSampler:
@@ -141,142 +122,575 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.samples)}
 
 
-def reference_exe(colour: bool) -> str:
-    name = "storm-color" if colour else "storm-nucleotide"
-    flags = open("/proc/cpuinfo").read() if os.path.exists("/proc/cpuinfo") else ""
-    if " avx2" not in flags:
-        name += "-sse2"
-    return os.path.join(REF_DIR, name)
+# ------------------------------------------------------------------------------ inputs
+
+def work_dir(cfg, scale, rank=0):
+    d = os.path.join(tempfile.gettempdir(), "storm_bench_c%d_s%g_r%d" % (cfg, scale, rank))
+    os.makedirs(d, exist_ok=True)
+    return d
 
 
-def sample_fastq(reads: str, d: str, n: int) -> str:
-    path = os.path.join(d, "sample_%d.fq" % n)
-    if not os.path.exists(path):
-        with open(reads, "rb") as f, open(path, "wb") as o:
-            for k, line in enumerate(f):
-                if k >= 4 * n:
-                    break
-                o.write(line)
-    return path
+def chunked_inputs(a, w, chunks, rank=0):
+    """Reference FASTA and the FASTQ of each chunk index in `chunks` (made once, cached)."""
+    d = work_dir(a.cfg, a.scale, rank)
+    ref = os.path.join(d, "ref.fa")
+    genome = None
+    if not os.path.exists(ref + ".done"):
+        genome = synth.genome_of(w)
+        synth.write_fasta(ref, genome)
+        open(ref + ".done", "w").write("ok")
+    paths = {}
+    for c in chunks:
+        p = os.path.join(d, "chunk%d.fq" % c)
+        if not os.path.exists(p + ".done"):
+            if genome is None:
+                genome = synth.genome_of(w)
+            seqs, quals = synth.reads_chunk(w, genome, c)
+            synth.write_fastq(p, seqs, quals)
+            open(p + ".done", "w").write("ok")
+        paths[c] = p
+    return ref, paths, d
 
 
-def run_reference_once(w, ref, sample, d, threads):
-    exe = reference_exe(w["mode"] == "colour")
-    cmd = [exe, "-g", ref, "-r", sample, "-o", os.path.join(d, "ref_out.sam"), "-v", "0", "-N", str(threads)] + w["args"]
-    t0 = time.perf_counter()
-    p = subprocess.run(cmd, cwd=d, capture_output=True, env=dict(os.environ, MALLOC_PERTURB_="255"))
-    dt = time.perf_counter() - t0
-    if p.returncode != 0:
-        raise RuntimeError("reference run failed: %s" % p.stderr[-500:])
-    return dt
+def whole_inputs(a, w, rank=0):
+    """Reference FASTA + the whole read set (the workloads mapped whole per step)."""
+    d = work_dir(a.cfg, a.scale, rank)
+    ref, reads = os.path.join(d, "ref.fa"), os.path.join(d, "reads.fq")
+    if not os.path.exists(os.path.join(d, "done")):
+        genome = synth.genome_of(w)
+        synth.write_fasta(ref, genome)
+        model = synth.ReadModel(**w.get("model", {}))
+        if w["mode"] == "colour":
+            pr, cols, q = synth.simulate_colour_reads(genome, w["reads"], w["lengths"], w["read_seed"] + 1000 * rank,
+                                                      model)
+            synth.write_colour_fastq(reads, pr, cols, q)
+        else:
+            seqs, quals = synth.simulate_nucleotide_reads(genome, w["reads"], w["lengths"], w["read_seed"] + 1000 * rank,
+                                                          model)
+            synth.write_fastq(reads, seqs, quals)
+        open(os.path.join(d, "done"), "w").write("ok")
+    return ref, reads, d
 
 
-def cpu_sample_size(cfg):
-    return {0: 100000, 1: 1000000, 2: 20000, 3: 20000, 4: 20000}[cfg]
+def fastq_records(path):
+    with open(path, "rb") as f:
+        while True:
+            rec = [f.readline() for _ in range(4)]
+            if not rec[0]:
+                return
+            yield rec
 
 
-def reference_arm(a, w, ref, reads, d):
+def per_length_sample(path, d, per_length, tag):
+    """FASTQ files of the first `per_length` reads of each length of `path`, in file order
+    (None: all of them); returns [(length, file, count)]."""
+    out = {}
+    for rec in fastq_records(path):
+        L = len(rec[1].rstrip(b"\n"))
+        o = out.setdefault(L, [])
+        if per_length is None or len(o) < per_length:
+            o.append(b"".join(rec))
+    res = []
+    for L in sorted(out):
+        p = os.path.join(d, "%s_len%d.fq" % (tag, L))
+        with open(p, "wb") as f:
+            f.writelines(out[L])
+        res.append((L, p, len(out[L])))
+    return res
+
+
+# ------------------------------------------------------------------------------ peaks
+
+def hbm_peak():
+    if os.path.exists(PEAKS_PATH):
+        try:
+            return float(json.load(open(PEAKS_PATH))["hbm_gbs"]), "MEASURED_PEAKS.json hbm_gbs (measured)"
+        except Exception:
+            pass
+    return FALLBACK_HBM_GBS, "fallback 6.65 TB/s (earlier measurement on this pool)"
+
+
+def issue_ceiling(sm_mhz):
+    """32-bit integer lane instructions per second the chip can issue: SMs x 4 warp
+    instructions per clock x 32 lanes x the sampled SM clock."""
+    return SMS * 4 * 32 * sm_mhz * 1e6
+
+
+def stage_rooflines(st, n_reads, max_len, sm_mhz, index_info=None):
+    """Per-stage achieved work rates and fractions from (summed) step statistics.
+
+    sw_filter   10 integer operations per band cell (L * (2 min(I,15) + 1) cells per candidate),
+                two 16-bit cells per 32-bit lane instruction: peak = 2 x the issue ceiling.
+    full_align  GCUPS on the band cells it computed ((2I + 1) per row it ran), and the same
+                10-operation cell count against the 32-bit issue ceiling.
+    hit_gather  8 B per seed lookup + 4 B per index position read + L/4 B of read per strand +
+                4 B per candidate diagonal written, against the HBM peak.
+    index_build per seed N/4 + 4 (N - span + 1) + 4 (4^w + 1) + 4 * 4^w bytes, against HBM."""
+    hbm, hbm_src = hbm_peak()
+    ceil = issue_ceiling(sm_mhz)
+    out = {}
+    if st["ms_filter"] > 0:
+        ach = 10.0 * st["filter_band_cells"] / (st["ms_filter"] * 1e-3)
+        out["sw_filter"] = {"ms": st["ms_filter"], "bound": "int", "achieved": ach / 1e12, "peak": 2 * ceil / 1e12,
+                            "unit": "T int-ops/s", "frac": ach / (2 * ceil),
+                            "band_gcups": st["filter_band_cells"] / (st["ms_filter"] * 1e-3) / 1e9,
+                            "cell_updates_per_s": st["filter_cells"] / (st["ms_filter"] * 1e-3)}
+    if st["ms_align"] > 0:
+        ach = 10.0 * st["align_cells"] / (st["ms_align"] * 1e-3)
+        out["full_align"] = {"ms": st["ms_align"], "bound": "int", "achieved": ach / 1e12, "peak": ceil / 1e12,
+                             "unit": "T int-ops/s", "frac": ach / ceil, "aligned": st["aligned"],
+                             "gcups": st["align_cells"] / (st["ms_align"] * 1e-3) / 1e9}
+    if st["ms_gather"] > 0:
+        gb = st["seed_lookups"] * 8 + st["hit_positions"] * 4 + n_reads * 2 * (max_len / 4) + st["candidates"] * 4
+        ach = gb / (st["ms_gather"] * 1e-3) / 1e9
+        out["hit_gather"] = {"ms": st["ms_gather"], "bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s",
+                             "frac": ach / hbm, "bytes": gb}
+    out["replay"] = {"ms": st["ms_replay"]}
+    if index_info:
+        ms, nbytes = index_info
+        ach = nbytes / (ms * 1e-3) / 1e9 if ms > 0 else 0.0
+        out["index_build"] = {"ms": ms, "bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
+                              "bytes": nbytes}
+    out["_peak_sources"] = {"int": "issue ceiling: %d SMs x 4 warp-inst/clk x 32 lanes x %.0f MHz (sampled)" % (SMS, sm_mhz),
+                            "hbm": hbm_src}
+    return out
+
+
+def index_bytes(seeds, sizes):
+    """Algorithmic bytes of building every seed's index of every sequence."""
+    tot = 0
+    for s in seeds.split(";"):
+        pat = s.split(":")[0]
+        wgt = pat.count("#") + pat.count("1")
+        span = len(pat)
+        for n in sizes:
+            tot += n / 4 + 4 * (n - span + 1) + 4 * (4 ** wgt + 1) + 4 * 4 ** wgt
+    return tot
+
+
+# ------------------------------------------------------------------------------ reference arm
+
+def run_reference_resident(w, ref, plan, d, threads, warmup, log_setup=True):
+    """Setup (reference loads + index build, once per read length), then every step of `plan`
+    [(chunk, [(length, file, count)])] maps its per-length sample files, one stock run each.
+    Returns (setup seconds, [(reads, seconds)] of the timed steps, of the warm-up steps)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from resident import ResidentReference
+    colour = w["mode"] == "colour"
+    out = os.path.join(d, "ref_out")
+    os.makedirs(out, exist_ok=True)
+
+    def args(path, k):
+        return ["-g", ref, "-r", path, "-o", os.path.join(out, "s%d.sam" % k), "-v", "0"] + list(w["args"])
+
+    steps = []
+    with ResidentReference(colour, threads=threads, cwd=d) as rr:
+        t0 = time.perf_counter()
+        # one run per read length on one read: the loads (padding per length) and the index
+        # build, the work the resident process does once
+        for L, path, _ in plan[0][1]:
+            one = os.path.join(d, "one_len%d.fq" % L)
+            with open(path, "rb") as f, open(one, "wb") as o:
+                o.writelines([f.readline() for _ in range(4)])
+            rr.run(args(one, 0))
+        setup = time.perf_counter() - t0
+        if log_setup:
+            log("reference: setup (reference loads, index build) %.1f s" % setup)
+        for c, samples in plan:
+            secs = sum(rr.run(args(path, j)) for j, (L, path, _) in enumerate(samples))
+            steps.append((sum(n for _, _, n in samples), secs))
+    return setup, steps[warmup:], steps[:warmup]
+
+
+def reference_arm(a, w):
     threads = os.cpu_count() or 1
-    if not os.path.exists(reference_exe(w["mode"] == "colour")):
-        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref not built (reference sources absent)"}))
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from resident import binary
+    if not os.path.exists(binary(w["mode"] == "colour")):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref not built (the reference's sources were absent)"}))
         return
-    n = min(cpu_sample_size(a.cfg), w["reads"])
-    sample = sample_fastq(reads, d, n)
-    # warm-up steps (untimed) run a small sample: they load the binary and the files into the
-    # page cache; every timed step runs the whole sample
-    warm = sample_fastq(reads, d, min(n, 50000))
-    for _ in range(a.warmup):
-        run_reference_once(w, ref, warm, d, threads)
-    times = [run_reference_once(w, ref, sample, d, threads) for _ in range(a.steps)]
-    tot = sum(times)
-    value = n * a.steps / tot
-    line = {"metric": "mapped reads/sec", "value": value, "unit": "reads/s", "n_gpus": a.gpus,
-            "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1000 * tot / a.steps,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8/int32",
-            "data": "synthetic", "impl": "reference",
-            "config": {"workload": workload_name(a.cfg, a.scale), "reads_per_step": n,
-                       "reference_codes": sum(w["ref_sizes"]), "args": " ".join(w["args"])},
-            "cpu_baseline": {"value": value, "unit": "reads/s", "cores": threads, "kind": "reference",
-                             "sample": "%d of the workload's reads, full reference, index build included" % n},
-            "e2e": {"value": value, "unit": "reads/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    if a.cfg != 2:
+        print(json.dumps({"impl": "reference", "unavailable": "the reference arm is defined for the default workload"}))
+        return
+    chunks = list(range(a.warmup + a.steps))
+    ref, paths, d = chunked_inputs(a, w, chunks)
+    plan = [(c, per_length_sample(paths[c], d, REF_SAMPLE_PER_LENGTH, "refsample%d" % c)) for c in chunks]
+    setup, steps, _ = run_reference_resident(w, ref, plan, d, threads, a.warmup)
+    reads = sum(n for n, _ in steps)
+    secs = sum(s for _, s in steps)
+    value = reads / secs
+    sample = ("each step: the first %d reads of each length of the step's chunk (%d reads), the reference's "
+              "stock command line run once per length with its reference and index resident (setup %.1f s, "
+              "untimed)" % (REF_SAMPLE_PER_LENGTH, steps[0][0] if steps else 0, setup))
+    line = {"metric": "mapped reads/sec", "value": value, "unit": "reads/s", "n_gpus": a.gpus, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": 1000 * secs / max(1, a.steps), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u8/int16/int32", "data": "synthetic", "impl": "reference",
+            "config": headline_config(a, w), "sample": sample,
+            "cpu_baseline": {"value": value, "unit": "reads/s", "cores": threads, "kind": "reference", "sample": sample},
+            "e2e": {"value": value, "unit": "reads/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0,
+                    "includes": "read file in, SAM file out (the stock command line per length)"},
+            "reference_setup_s": setup}
     print(json.dumps(line))
 
 
-def batched_arm(a, w, ref_path, reads_path, d):
-    """Configuration 2 (reads of 35-150 bp in one file): the whole file as one batch -- one launch
-    per stage over reads of every length, candidate lists flat across reads -- against the plain
-    per-batch path the reference implies (it maps one read length per run, so one batch per
-    length, each through the same call).  Host buffers in and out for both; the index is built
-    once and stays resident.  Checks that both give the same records."""
-    import numpy as np
+# ------------------------------------------------------------------------------ headline arm
 
-    from storm_b200 import api, build, host
+def mixed_arm(a, w):
+    import ctypes
+
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=900))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+
+    from storm_b200 import api, build, host, pipeline
     build.build()
-    prm_d, seeds = parse_cli_args(w["args"])
-    prm = api.params(colour=0, **prm_d)
-    reads = host.ReadSet(reads_path, 0)  # sorted by length, then tag
+    per_rank = a.warmup + a.steps
+    chunks = [rank * per_rank + k for k in range(per_rank)]
+    t0 = time.perf_counter()
+    ref_path, paths, d = chunked_inputs(a, w, sorted(set(chunks + [0])), rank)
+    log("rank %d: inputs ready in %.1f s" % (rank, time.perf_counter() - t0))
+
+    p, seeds, *_ = pipeline.parse_options(w["args"])
+    prm = api.params(colour=0, device=local, **p)
     reference = host.Reference(ref_path, 0)
-    mapper = api.Mapper(prm, seeds or DEFAULT_SEEDS[0])
+    mapper = api.Mapper(prm, seeds)
     reference.add_to(mapper)
+    t0 = time.perf_counter()
     mapper.build_index()
+    mapper.sync()
+    index_ms = mapper.stats()["ms_index"]
+    log("rank %d: index built in %.1f ms (device), %.2f s wall" % (rank, index_ms, time.perf_counter() - t0))
+
+    sets = {c: host.ReadSet(paths[c], 0) for c in chunks}
+    max_len = max(s.max_len for s in sets.values())
+    tbs = ((max_len + prm.allowed_indels + 1) // 2 + 7) & ~7
+    t0 = time.perf_counter()
+    if a.tuning:
+        mapper.set_tuning(**{k: int(v) for k, v in (kv.split("=") for kv in a.tuning.split(","))})
+        tuning = mapper.tuning()
+    else:
+        tuning = mapper.autotune(sets[chunks[0]].batch(), sample=a.tune_sample)
+    tune_s = time.perf_counter() - t0
+    log("rank %d: tuning %s (%.1f s)" % (rank, tuning, tune_s))
+
+    # device-resident inputs of every step, uploaded before the timed region
+    dev_in = {}
+    for c in chunks:
+        b = sets[c].batch()
+        dc = torch.from_numpy(b.codes).to(dev)
+        dl = torch.from_numpy(b.levels).to(dev)
+        dn = torch.from_numpy(b.lengths.copy()).to(dev)
+        dev_in[c] = (dc, dl, dn, api.Reads(b.n, dc.data_ptr(), b.codes.shape[1], dl.data_ptr(), b.levels.shape[1],
+                                             dn.data_ptr(), None))
+    nmax = max(s.n for s in sets.values())
+    d_hits = torch.empty(nmax * 4 * ctypes.sizeof(api.Hit), dtype=torch.uint8, device=dev)
+    d_tb = torch.empty(nmax * 4 * tbs, dtype=torch.uint8, device=dev)
+    d_mapped = torch.empty(nmax, dtype=torch.uint8, device=dev)
+    ostruct = api.Results(d_hits.data_ptr(), d_tb.data_ptr(), tbs, d_mapped.data_ptr())
+    stream = torch.cuda.Stream(device=dev)
+    flush = torch.empty(512 << 20, dtype=torch.uint8, device=dev)  # > 126 MB L2
+
+    for c in chunks[:a.warmup]:
+        mapper.map_device(dev_in[c][3], ostruct, stream.cuda_stream)
+    torch.cuda.synchronize()
+
+    ms_steps, stats, mapped_total, reads_total = [], [], 0, 0
+    with ClockSampler(local) as clk:
+        for c in chunks[a.warmup:]:
+            flush.fill_(1)
+            torch.cuda.synchronize()
+            if dist:
+                dist.barrier()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            mapper.map_device(dev_in[c][3], ostruct, stream.cuda_stream)
+            e1.record(stream)
+            e1.synchronize()
+            ms_steps.append(e0.elapsed_time(e1))
+            stats.append(mapper.stats())
+            mapped_total += int(d_mapped[:sets[c].n].sum().item())
+            reads_total += sets[c].n
+    torch.cuda.synchronize()
+    t_local = sum(ms_steps)
+    t_max, reads_all = t_local, float(reads_total)
+    if dist:
+        t = torch.tensor([t_local], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_max = float(t.item())
+        n_all = torch.tensor([reads_total], dtype=torch.float64, device=dev)
+        dist.all_reduce(n_all)
+        reads_all = float(n_all.item())
+    value = reads_all / (t_max / 1000.0)
+    clocks = clk.summary()
+    del dev_in
+    mapper.close()
+
+    # end to end through the resident front end: FASTQ file in, SAM file out, per chunk
+    res_mapper = pipeline.ResidentMapper(ref_path, w["args"], colour=0, device=local)
+    res_mapper.mapper.set_tuning(**tuning)
+    e2e_chunks = chunks[a.warmup:a.warmup + max(1, min(a.steps, a.e2e_steps))]
+    res_mapper.map_file(paths[chunks[0]], os.path.join(d, "warm.sam"))  # warm-up (buffers, page cache)
+    e2e_s, h2d, d2h = [], 0, 0
+    for c in e2e_chunks:
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        t0 = time.perf_counter()
+        res_mapper.map_file(paths[c], os.path.join(d, "e2e_%d.sam" % c))
+        e2e_s.append(time.perf_counter() - t0)
+        s = sets[c]
+        h2d += s.codes.nbytes + s.levels.nbytes + s.lengths.nbytes
+        d2h += s.n * (4 * ctypes.sizeof(api.Hit) + 4 * tbs + 1)
+    e2e_t = sum(e2e_s)
+    if dist:
+        t = torch.tensor([e2e_t], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_t = float(t.item())
+    e2e_reads = sum(sets[c].n for c in e2e_chunks) * world
+    e2e = {"value": e2e_reads / e2e_t, "unit": "reads/s", "h2d_bytes_per_step": int(h2d / len(e2e_chunks)),
+           "d2h_bytes_per_step": int(d2h / len(e2e_chunks)), "steps": len(e2e_chunks),
+           "includes": "read FASTQ file -> parse + tag sort -> host-to-device -> map -> device-to-host -> SAM file",
+           "api": "storm_b200.pipeline.ResidentMapper.map_file"}
+
+    parity = batching = cpu = None
+    if rank == 0:
+        parity = check_parity(res_mapper, paths, d)
+        batching = batched_vs_plain(res_mapper, sets[chunks[a.warmup]], tbs, api)
+    res_mapper.close()
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        cpu = cpu_baseline_leg(a, w)
+
+    if rank == 0:
+        agg = {k: sum(s[k] for s in stats) for k in stats[0] if k != "ms_index"}
+        sm_mhz = clocks.get("sm_mhz") or 1965.0
+        stages = stage_rooflines(agg, reads_total, max_len, sm_mhz, (index_ms, index_bytes(seeds, w["ref_sizes"])))
+        per_step = {k: v for k, v in stages.items() if not k.startswith("_")}
+        dom = max(("sw_filter", "full_align", "hit_gather"), key=lambda k: per_step.get(k, {}).get("ms", 0))
+        traffic = None
+        if os.path.exists(TRAFFIC_PATH):
+            traffic = json.load(open(TRAFFIC_PATH)).get("mixed_100M", {}).get(dom, {}).get("bytes_per_launch")
+        roof = {"kernel": dom, "bound": per_step[dom]["bound"], "achieved": per_step[dom]["achieved"],
+                "peak": per_step[dom]["peak"], "unit": per_step[dom]["unit"], "frac": per_step[dom]["frac"],
+                "traffic": traffic,
+                "peak_source": stages["_peak_sources"]["int" if per_step[dom]["bound"] == "int" else "hbm"]}
+        for v in per_step.values():
+            if "ms" in v:
+                v["ms_per_step"] = v["ms"] / len(stats)
+        line = {"metric": "mapped reads/sec", "value": value, "unit": "reads/s", "n_gpus": world, "steps": a.steps,
+                "warmup": a.warmup, "ms_per_step": t_max / a.steps, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "u8/int16/int32", "data": "synthetic",
+                "config": headline_config(a, w),
+                "sample": "each step: one chunk of %d reads (chunk = step index + %d x rank), reference and index "
+                          "resident" % (synth.CHUNK_READS, per_rank),
+                "tuning": tuning, "tuning_s": round(tune_s, 2),
+                "mapped_fraction": mapped_total / max(1, reads_total),
+                "gpu_launches": int(sum(s["kernels"] for s in stats)),
+                "roofline": roof, "stages": stages, "clocks": clocks, "e2e": e2e, "cpu_baseline": cpu,
+                "parity_vs_reference": parity, "batching": batching,
+                "counts_per_step": {k: int(agg[k] / len(stats)) for k in
+                                    ("candidates", "filter_passed", "aligned", "seed_lookups", "hit_positions",
+                                     "filter_cells", "filter_band_cells", "align_cells")}}
+        print(json.dumps(line))
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def check_parity(res_mapper, paths, d):
+    """Chunk 0 through the resident front end, one run per read length, against the reference's
+    digests of the same runs; and the mixed run's records against the per-length ones."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import scale_cases
+    case = "mixed_100M_chunk0"
+    digests = json.load(open(DIGESTS_PATH)) if os.path.exists(DIGESTS_PATH) else {}
+    if case not in digests:
+        return {"case": case, "checked": False, "why": "no reference digests for the case"}
+    ref_d = digests[case]
+    pd = os.path.join(d, "parity")
+    os.makedirs(pd, exist_ok=True)
+    ok, runs, bodies = True, 0, []
+    for L, path, n in per_length_sample(paths[0], pd, None, "chunk0"):
+        sam = os.path.join(pd, "len%d.sam" % L)
+        un = os.path.join(pd, "len%d.un.fq" % L)
+        res_mapper.map_file(path, sam, un)
+        h, nrec = scale_cases.digest_sam(sam)
+        exp = ref_d["runs"].get("len%d" % L)
+        ok &= exp is not None and h == exp["sam_sha256"] and scale_cases.digest_file(un) == exp["unmapped_fastq_sha256"]
+        runs += 1
+        with open(sam, "rb") as f:
+            bodies.append(b"".join(x for x in f if not x.startswith(b"@")))
+    mixed = os.path.join(pd, "mixed.sam")
+    res_mapper.map_file(paths[0], mixed)
+    with open(mixed, "rb") as f:
+        mixed_body = b"".join(x for x in f if not x.startswith(b"@"))
+    return {"case": case, "checked": True, "runs": runs, "identical": bool(ok and runs == len(ref_d["runs"])),
+            "mixed_run_equals_per_length_runs": mixed_body == b"".join(bodies)}
+
+
+def batched_vs_plain(res_mapper, reads, tbs, api):
+    """One chunk: one mapping call over every read length (the batched form) against one call
+    per length (the plain per-batch path the reference implies), host buffers in and out for
+    both, best of two after a warm-up; and whether both give the same records."""
+    import numpy as np
+    m = res_mapper.mapper
     batch = reads.batch()
-    tuning = mapper.autotune(batch, sample=200000)  # launch parameters (no effect on results)
-    tbs = ((reads.max_len + prm.allowed_indels + 1) // 2 + 7) & ~7
     L = reads.lengths
     cuts = [0] + [int(i) for i in np.nonzero(np.diff(L))[0] + 1] + [reads.n]
     buckets = [api.ReadBatch(batch.codes[x:y], batch.lengths[x:y], batch.levels[x:y]) for x, y in zip(cuts, cuts[1:])]
-    mapper.map(batch, tbs)  # warm-up
-    plain_t, batched_t = [], []
-    plain_st = {}
-    for _ in range(max(1, a.steps)):
+    whole = m.map(batch, tbs)
+    for b in buckets:
+        m.map(b, tbs)
+    tb_, tp_ = [], []
+    for _ in range(2):
         t0 = time.perf_counter()
-        parts, plain_st = [], {}
-        for b in buckets:
-            parts.append(mapper.map(b, tbs))
-            for k, v in mapper.stats().items():
-                if k.startswith("ms_") or k in ("candidates", "filter_passed", "hit_positions"):
-                    plain_st[k] = plain_st.get(k, 0) + v
-        plain_t.append(time.perf_counter() - t0)
+        parts = [m.map(b, tbs) for b in buckets]
+        tp_.append(time.perf_counter() - t0)
         t0 = time.perf_counter()
-        whole = mapper.map(batch, tbs)
-        batched_t.append(time.perf_counter() - t0)
-    st = mapper.stats()
-    mapper.close()
+        whole = m.map(batch, tbs)
+        tb_.append(time.perf_counter() - t0)
     hits = np.concatenate([p.hits for p in parts])
     mapped = np.concatenate([p.mapped for p in parts])
     live = np.repeat(mapped != 0, 4)
     same = bool(np.array_equal(mapped != 0, whole.mapped != 0) and hits[live].tobytes() == whole.hits[live].tobytes())
+    return {"reads": int(reads.n), "batched_ms": 1000 * min(tb_), "plain_per_length_ms": 1000 * min(tp_),
+            "plain_calls": len(buckets), "batched_over_plain": min(tp_) / min(tb_), "same_records": same}
+
+
+def cpu_baseline_leg(a, w):
+    """The reference on this host's cores on a bounded sample: the first reads of each length
+    of one chunk, index resident (its setup is reported, not counted)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from resident import binary
+    if not os.path.exists(binary(False)):
+        return None
+    ref, paths, d = chunked_inputs(a, w, [a.warmup])
+    plan = [(a.warmup, per_length_sample(paths[a.warmup], d, REF_SAMPLE_PER_LENGTH, "cpusample"))]
+    setup, _, warm = run_reference_resident(w, ref, plan, d, os.cpu_count() or 1, 1, log_setup=False)
+    n, secs = warm[0]
+    return {"value": n / secs, "unit": "reads/s", "cores": os.cpu_count(), "kind": "reference",
+            "sample": "the first %d reads of each length of chunk %d (%d reads), stock command line per length, "
+                      "reference and index resident (setup %.1f s, not counted)" % (REF_SAMPLE_PER_LENGTH, a.warmup,
+                                                                                    n, setup)}
+
+
+# ------------------------------------------------------------------------------ other workloads
+
+def whole_set_arm(a, w):
+    """Workloads mapped whole per step (colour, small nucleotide, large): every read of the
+    set, both strands, index build included, device-resident results."""
+    import ctypes
+
+    import torch
+    from storm_b200 import api, build, host, pipeline
+    build.build()
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    ref_path, reads_path, d = whole_inputs(a, w)
+    colour = 1 if w["mode"] == "colour" else 0
+    p, seeds, *_ = pipeline.parse_options(w["args"])
+    seeds = seeds or DEFAULT_SEEDS[colour]
+    prm = api.params(colour=colour, device=local, **p)
+    reads = host.ReadSet(reads_path, colour)
+    reference = host.Reference(ref_path, colour)
     n = reads.n
-    line = {"metric": "mapped reads/sec (mixed-length batch)", "value": n / min(batched_t), "unit": "reads/s",
-            "n_gpus": 1, "steps": a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "u8/int32", "data": "synthetic",
-            "config": {"workload": workload_name(a.cfg, a.scale), "reads": n, "lengths": sorted(set(int(x) for x in L)),
-                       "reference_codes": sum(w["ref_sizes"]), "args": " ".join(w["args"]), "tuning": tuning},
-            "batched": {"reads_per_s": n / min(batched_t), "ms": 1000 * min(batched_t)},
-            "plain_per_length": {"reads_per_s": n / min(plain_t), "ms": 1000 * min(plain_t), "batches": len(buckets)},
-            "batched_over_plain": min(plain_t) / min(batched_t), "same_records": same,
-            "stages_last_batched": {k: v for k, v in st.items()
-                                    if k.startswith("ms_") or k in ("candidates", "filter_passed", "hit_positions")},
-            "stages_last_plain": plain_st,
-            "e2e": {"value": n / min(batched_t), "unit": "reads/s", "includes": "host buffers in and out"}}
+    tbs = ((reads.max_len + prm.allowed_indels + 1) // 2 + 7) & ~7
+    mapper = api.Mapper(prm, seeds)
+    reference.add_to(mapper)
+    mapper.build_index()
+    batch = reads.batch()
+    if a.tuning:
+        mapper.set_tuning(**{k: int(v) for k, v in (kv.split("=") for kv in a.tuning.split(","))})
+        tuning = mapper.tuning()
+    else:
+        tuning = mapper.autotune(batch, sample=a.tune_sample)
+    d_codes = torch.from_numpy(batch.codes).to(dev)
+    d_levels = torch.from_numpy(batch.levels).to(dev) if batch.levels is not None else None
+    d_len = torch.from_numpy(batch.lengths.copy()).to(dev)
+    d_fl = torch.from_numpy(batch.first_levels).to(dev) if batch.first_levels is not None else None
+    d_hits = torch.empty(n * 4 * ctypes.sizeof(api.Hit), dtype=torch.uint8, device=dev)
+    d_tb = torch.empty(n * 4 * tbs, dtype=torch.uint8, device=dev)
+    d_mapped = torch.empty(n, dtype=torch.uint8, device=dev)
+    rstruct = api.Reads(n, d_codes.data_ptr(), batch.codes.shape[1], d_levels.data_ptr() if d_levels is not None else None,
+                        batch.levels.shape[1] if batch.levels is not None else 0, d_len.data_ptr(),
+                        d_fl.data_ptr() if d_fl is not None else None)
+    ostruct = api.Results(d_hits.data_ptr(), d_tb.data_ptr(), tbs, d_mapped.data_ptr())
+    stream = torch.cuda.Stream(device=dev)
+    flush = torch.empty(512 << 20, dtype=torch.uint8, device=dev)
+
+    def step():
+        mapper.build_index()
+        mapper.map_device(rstruct, ostruct, stream.cuda_stream)
+
+    for _ in range(a.warmup):
+        step()
+    torch.cuda.synchronize()
+    ms, stats = [], []
+    with ClockSampler(local) as clk:
+        for _ in range(a.steps):
+            flush.fill_(1)
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            step()
+            e1.record(stream)
+            e1.synchronize()
+            ms.append(e0.elapsed_time(e1))
+            stats.append(mapper.stats())
+    clocks = clk.summary()
+    mapper.close()
+    value = n * a.steps / (sum(ms) / 1000.0)
+    res_mapper = pipeline.ResidentMapper(ref_path, w["args"], colour=colour, default_seeds=seeds, device=local)
+    res_mapper.mapper.set_tuning(**tuning)
+    res_mapper.map_file(reads_path, os.path.join(d, "warm.sam"))
+    t0 = time.perf_counter()
+    res_mapper.map_file(reads_path, os.path.join(d, "e2e.sam"))
+    e2e_s = time.perf_counter() - t0
+    res_mapper.close()
+    st = stats[-1]
+    stages = stage_rooflines(st, n, reads.max_len, clocks.get("sm_mhz") or 1965.0,
+                             (st["ms_index"], index_bytes(seeds, w["ref_sizes"])))
+    per = {k: v for k, v in stages.items() if not k.startswith("_")}
+    dom = max(("sw_filter", "full_align", "hit_gather"), key=lambda k: per.get(k, {}).get("ms", 0))
+    line = {"metric": "mapped reads/sec", "value": value, "unit": "reads/s", "n_gpus": 1, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": sum(ms) / a.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u8/int16/int32", "data": "synthetic",
+            "config": dict(headline_config(a, w), step="index build (all seeds) + map every read, both strands"),
+            "tuning": tuning, "gpu_launches": int(sum(s["kernels"] for s in stats)),
+            "roofline": {"kernel": dom, **{k: per[dom][k] for k in ("bound", "achieved", "peak", "unit", "frac")},
+                         "traffic": None},
+            "stages": stages, "clocks": clocks,
+            "e2e": {"value": n / e2e_s, "unit": "reads/s", "h2d_bytes_per_step": int(batch.codes.nbytes),
+                    "d2h_bytes_per_step": int(n * (4 * ctypes.sizeof(api.Hit) + 4 * tbs + 1)),
+                    "includes": "read FASTQ file -> SAM file through storm_b200.pipeline.ResidentMapper (index resident)"}}
     print(json.dumps(line))
 
 
-def serving_arm(a, w, ref_path, reads_path, d):
-    """The served -O chain (configuration 3): the workload's reads split into batches of
-    log-uniform sizes (1k to 1M reads, scaled), arriving as a Poisson process (seed 7).  The same
-    batches first go through the plain per-batch path (each chain step mapped with stormgpu_map,
-    the unmapped reads picked on the host, one batch at a time); then the server takes them as
-    they arrive (continuous batching over 3 worker streams).  Reports the served reads/s, the
-    plain reads/s, p50/p99 batch latency, and checks that both give the same records."""
-    import threading
-
+def serving_arm(a, w):
+    """The served -O chain: the workload's reads split into batches of log-uniform sizes (1k to
+    1M reads, scaled), arriving as a Poisson process (seed 7).  The same batches first go through
+    the plain per-batch path (each chain step mapped with stormgpu_map, the unmapped reads
+    picked on the host, one batch at a time); then the server takes them as they arrive
+    (continuous batching).  Reports the served reads/s, the plain reads/s, p50/p99 batch
+    latency, and checks that both give the same records."""
     import numpy as np
 
-    from storm_b200 import api, build, host
+    from storm_b200 import api, build, host, pipeline
     build.build()
-    prm_d, _ = parse_cli_args(w["args"])
-    prm = api.params(colour=0, **prm_d)
+    ref_path, reads_path, d = whole_inputs(a, w)
+    p, _, *_ = pipeline.parse_options(w["args"])
+    prm = api.params(colour=0, **p)
     chain = w["chain"]
     reads = host.ReadSet(reads_path, 0)
     reference = host.Reference(ref_path, 0)
@@ -291,17 +705,13 @@ def serving_arm(a, w, ref_path, reads_path, d):
         batches.append(api.ReadBatch(reads.codes[idx], reads.lengths[idx], reads.levels[idx]))
     tbs = ((reads.max_len + prm.allowed_indels + 1) // 2 + 7) & ~7
     total = sum(b.n for b in batches)
-
-    # plain per-batch path: one mapper (resident index) per chain step, batches one at a time
     mappers = []
     for seeds in chain:
         m = api.Mapper(prm, seeds)
         reference.add_to(m)
         m.build_index()
         mappers.append(m)
-    # launch parameters (no effect on results) picked on a sample with the first step's seeds,
-    # used by both arms
-    tuning = mappers[0].autotune(api.ReadBatch(reads.codes, reads.lengths, reads.levels), sample=200000)
+    tuning = mappers[0].autotune(api.ReadBatch(reads.codes, reads.lengths, reads.levels), sample=a.tune_sample)
     for m in mappers[1:]:
         m.set_tuning(**tuning)
 
@@ -326,21 +736,18 @@ def serving_arm(a, w, ref_path, reads_path, d):
             cur = api.ReadBatch(cur.codes[keep], cur.lengths[keep], cur.levels[keep])
         return out, step
 
-    plain(batches[0])  # warm-up
+    plain(batches[0])
     t0 = time.perf_counter()
     ref_out = [plain(b) for b in batches]
     t_plain = time.perf_counter() - t0
     for m in mappers:
         m.close()
     plain_rate = total / t_plain
-
-    # served: capacity with every batch waiting at once, then batch latency under Poisson
-    # arrivals at 80 % of that capacity
     srv = api.Server(prm, chain, slots=3, budget_bytes=48 << 30)
     reference.add_to_server(srv)
     srv.set_tuning(**tuning)
     srv.build()
-    srv.poll(srv.submit(batches[0], tbs))  # warm-up
+    srv.poll(srv.submit(batches[0], tbs))
 
     def serve(arrivals):
         tickets = [None] * len(batches)
@@ -379,11 +786,11 @@ def serving_arm(a, w, ref_path, reads_path, d):
     served_rate = total / t_served
     line = {"metric": "served reads/sec (3-step -O chain, continuous batching)", "value": served_rate,
             "unit": "reads/s", "n_gpus": 1, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "u8/int32", "data": "synthetic",
-            "config": {"tuning": tuning, "workload": workload_name(a.cfg, a.scale), "reads": total, "batches": len(batches),
-                       "batch_sizes": [b.n for b in batches], "chain": chain, "args": " ".join(w["args"]),
-                       "arrivals": "capacity: all batches at once; latency: Poisson at 80 % of capacity",
-                       "slots": 3},
+            "dtype": "u8/int16/int32", "data": "synthetic",
+            "config": {"tuning": tuning, "workload": workload_name(a.cfg, a.scale), "reads": total,
+                       "batches": len(batches), "batch_sizes": [b.n for b in batches], "chain": chain,
+                       "args": " ".join(w["args"]),
+                       "arrivals": "capacity: all batches at once; latency: Poisson at 80 % of capacity", "slots": 3},
             "serving": {"p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
                         "plain_reads_per_s": plain_rate, "served_over_plain": served_rate / plain_rate,
                         "same_records": same},
@@ -394,245 +801,32 @@ def serving_arm(a, w, ref_path, reads_path, d):
     print(json.dumps(line))
 
 
-def workload_name(cfg, scale):
-    names = {0: "cfg0 nucleotide 1 Mbp, 100k x 50 bp", 1: "cfg1 colour 10 Mbp, 2M x 50 colours",
-             2: "cfg2 nucleotide 100 Mbp, 10M x 35-150 bp, -i 15", 3: "cfg3 served -O chain",
-             4: "cfg4 3.1 Gbp, 100M x 100 bp"}
-    return names[cfg] + ("" if scale == 1.0 else " (scale %g)" % scale)
-
-
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--cfg", type=int, default=1)
+    ap.add_argument("--cfg", type=int, default=2)
     ap.add_argument("--scale", type=float, default=1.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--e2e-steps", type=int, default=5, help="chunks timed end to end")
+    ap.add_argument("--tune-sample", type=int, default=8000, help="reads the autotuner times each setting on")
     ap.add_argument("--tuning", default="", help="launch parameters name=value,... instead of the autotuner")
-    ap.add_argument("--reads", type=int, default=0, help="map only the first N reads of the workload (profiling)")
     a = ap.parse_args()
-
-    world = int(os.environ.get("WORLD_SIZE", "1"))
+    w = synth.workload(a.cfg, a.scale)
     rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-
     if a.impl == "reference":
-        if rank != 0:
-            return
-        w, ref, reads, d = workload_files(a.cfg, a.scale, 0)
-        reference_arm(a, w, ref, reads, d)
-        return
-
-    if a.cfg in (2, 3):
         if rank == 0:
-            w, ref_path, reads_path, d = workload_files(a.cfg, a.scale, 0)
-            (batched_arm if a.cfg == 2 else serving_arm)(a, w, ref_path, reads_path, d)
+            reference_arm(a, w)
         return
-
-    import numpy as np
-    import torch
-    dist = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
-    torch.cuda.set_device(local)
-    dev = torch.device("cuda", local)
-
-    from storm_b200 import api, build, host
-    build.build()
-    w, ref_path, reads_path, d = workload_files(a.cfg, a.scale, rank)
-    colour = 1 if w["mode"] == "colour" else 0
-    prm_d, seeds = parse_cli_args(w["args"])
-    seeds = seeds or DEFAULT_SEEDS[colour]
-    prm = api.params(colour=colour, device=local, **prm_d)
-    t0 = time.perf_counter()
-    if a.reads:
-        reads_path = sample_fastq(reads_path, d, a.reads)
-    reads = host.ReadSet(reads_path, colour)
-    reference = host.Reference(ref_path, colour)
-    log("rank %d: loaded %d reads, %d sequence(s) in %.1f s" % (rank, reads.n, reference.n, time.perf_counter() - t0))
-    n = reads.n
-    tbs = ((reads.max_len + prm.allowed_indels + 1) // 2 + 7) & ~7
-
-    mapper = api.Mapper(prm, seeds)
-    reference.add_to(mapper)
-
-    # device-resident inputs and outputs
-    batch = reads.batch()
-    # launch parameters picked by the autotuner on a sample of the workload (setup, untimed;
-    # they change no result)
-    t0 = time.perf_counter()
-    mapper.build_index()
-    if a.tuning:  # fixed launch parameters (profiling runs that must launch the same kernels)
-        mapper.set_tuning(**{k: int(v) for k, v in (kv.split("=") for kv in a.tuning.split(","))})
-        tuning = mapper.tuning()
-    else:
-        tuning = mapper.autotune(batch, sample=200000)
-    tune_s = time.perf_counter() - t0
-    log("rank %d: autotuned %s in %.1f s" % (rank, tuning, tune_s))
-    d_codes = torch.from_numpy(batch.codes).to(dev)
-    d_levels = torch.from_numpy(batch.levels).to(dev) if batch.levels is not None else None
-    d_len = torch.from_numpy(batch.lengths.copy()).to(dev)
-    d_fl = torch.from_numpy(batch.first_levels).to(dev) if batch.first_levels is not None else None
-    import ctypes
-    d_hits = torch.empty(n * 4 * ctypes.sizeof(api.Hit), dtype=torch.uint8, device=dev)
-    d_tb = torch.empty(n * 4 * tbs, dtype=torch.uint8, device=dev)
-    d_mapped = torch.empty(n, dtype=torch.uint8, device=dev)
-    rstruct = api.Reads(n, d_codes.data_ptr(), batch.codes.shape[1],
-                        d_levels.data_ptr() if d_levels is not None else None,
-                        batch.levels.shape[1] if batch.levels is not None else 0, d_len.data_ptr(),
-                        d_fl.data_ptr() if d_fl is not None else None)
-    ostruct = api.Results(d_hits.data_ptr(), d_tb.data_ptr(), tbs, d_mapped.data_ptr())
-    stream = torch.cuda.Stream(device=dev)
-    flush = torch.empty(512 << 20, dtype=torch.uint8, device=dev)  # > 126 MB L2
-
-    def step():
-        mapper.build_index()
-        mapper.map_device(rstruct, ostruct, stream.cuda_stream)
-
-    for _ in range(a.warmup):
-        step()
-    torch.cuda.synchronize()
-
-    ms_steps, stage = [], []
-    with ClockSampler(local) as clk:
-        for _ in range(a.steps):
-            flush.fill_(1)
-            torch.cuda.synchronize()
-            if dist:
-                dist.barrier()
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            step()
-            e1.record(stream)
-            e1.synchronize()
-            ms_steps.append(e0.elapsed_time(e1))
-            stage.append(mapper.stats())
-    torch.cuda.synchronize()
-    mapped = int(d_mapped.sum().item())
-    t_local = sum(ms_steps)
-    t_max = t_local
-    if dist:
-        t = torch.tensor([t_local], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_max = float(t.item())
-    value = world * n * a.steps / (t_max / 1000.0)
-
-    # end to end through the host-buffer ABI call: reads in pinned host memory, results read
-    # back into pinned host memory (both allocated once, outside the timed region)
-    def pinned(a):
-        t = torch.empty(a.nbytes, dtype=torch.uint8, pin_memory=True).numpy()
-        v = t.view(a.dtype).reshape(a.shape)
-        v[...] = a
-        return v
-
-    pbatch = api.ReadBatch(pinned(batch.codes), pinned(batch.lengths),
-                           None if batch.levels is None else pinned(batch.levels),
-                           None if batch.first_levels is None else pinned(batch.first_levels))
-    proto = api.MapResults(n, tbs)
-    res = api.MapResults(n, tbs, (pinned(proto.hits), pinned(proto.tb), pinned(proto.mapped)))
-    mapper.map(pbatch, out=res)  # warm-up
-    e2e_ms = []
-    for _ in range(max(1, min(a.steps, 3))):
-        torch.cuda.synchronize()
-        if dist:
-            dist.barrier()
-        t0 = time.perf_counter()
-        mapper.build_index()
-        mapper.map(pbatch, out=res)
-        e2e_ms.append(1000 * (time.perf_counter() - t0))
-    e2e_t = sum(e2e_ms)
-    if dist:
-        t = torch.tensor([e2e_t], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_t = float(t.item())
-    h2d = pbatch.codes.nbytes + (pbatch.levels.nbytes if pbatch.levels is not None else 0) + pbatch.lengths.nbytes + \
-        (pbatch.first_levels.nbytes if pbatch.first_levels is not None else 0)
-    d2h = res.hits.nbytes + res.tb.nbytes + res.mapped.nbytes
-    # the host-buffer call (pipelined in chunks for large batches) gives the device-resident records
-    same = bool(np.array_equal(d_mapped.cpu().numpy(), res.mapped) and
-                d_hits.cpu().numpy().tobytes() == res.hits.tobytes() and
-                d_tb.cpu().numpy().tobytes() == res.tb.tobytes())
-    e2e = {"value": world * n * len(e2e_ms) / (e2e_t / 1000.0), "unit": "reads/s", "h2d_bytes_per_step": int(h2d),
-           "d2h_bytes_per_step": int(d2h), "includes": "index build + reads H2D + map + results D2H, pinned host buffers",
-           "same_records_as_device": same}
-
-    # roofline of the dominant kernel, from the last timed step's per-stage device times
-    st = stage[-1]
-    peaks = json.load(open(PEAKS_PATH)) if os.path.exists(PEAKS_PATH) else {}
-    hbm = peaks.get("hbm_gbs", 6650.0)
-    # filter: algorithmic work = 3.25 lane instructions per cell update (6.5 per register of two
-    # packed 16-bit cells: gap subtraction, add-max, 3-way max, selector subtraction, permute,
-    # add-max, half a running max), over W * 2 * (L + W - 1) cell updates per candidate; peak =
-    # the measured rate of that instruction mix (stormgpu_filter_peak)
-    ops_s, ms_peak = _filter_peak(api, local)
-    filter_ops = st["filter_cells"] * 3.25
-    gather_bytes = st["seed_lookups"] * 8 + st["hit_positions"] * 4 + n * (reads.max_len / 4) * 2 + st["candidates"] * 4
-    stages = {
-        "sw_filter": {"ms": st["ms_filter"], "bound": "int", "achieved": filter_ops / (st["ms_filter"] * 1e-3) / 1e12,
-                      "peak": ops_s / 1e12, "unit": "T lane-inst/s", "gcups": st["filter_cells"] / (st["ms_filter"] * 1e-3) / 1e9,
-                      "band_gcups": st["filter_band_cells"] / (st["ms_filter"] * 1e-3) / 1e9},
-        "hit_gather": {"ms": st["ms_gather"], "bound": "hbm", "achieved": gather_bytes / (st["ms_gather"] * 1e-3) / 1e9,
-                       "peak": hbm, "unit": "GB/s"},
-        "full_align": {"ms": st["ms_align"], "aligned": st["aligned"]},
-        "replay": {"ms": st["ms_replay"]},
-        "index_build": {"ms": st["ms_index"]},
-    }
-    for v in stages.values():
-        if "achieved" in v:
-            v["frac"] = v["achieved"] / v["peak"]
-    dom = max(("sw_filter", "hit_gather"), key=lambda k: stages[k]["ms"])
-    traffic = None
-    if os.path.exists(TRAFFIC_PATH):
-        tr = json.load(open(TRAFFIC_PATH))
-        traffic = tr.get(dom, {}).get("bytes_per_launch")
-    roof = {"kernel": dom, "bound": stages[dom]["bound"], "achieved": stages[dom]["achieved"],
-            "peak": stages[dom]["peak"], "unit": stages[dom]["unit"], "frac": stages[dom]["frac"],
-            "traffic": traffic,
-            "peak_source": ("measured: stormgpu_filter_peak, the filter recurrence's instruction mix "
-                            "register-resident" if dom == "sw_filter" else "MEASURED_PEAKS.json hbm_gbs")}
-
-    cpu = None
-    if rank == 0 and world == 1 and not a.no_cpu_baseline and os.path.exists(reference_exe(colour)):
-        ns = min(cpu_sample_size(a.cfg), w["reads"])
-        sample = sample_fastq(reads_path, d, ns)
-        dt = run_reference_once(w, ref_path, sample, d, os.cpu_count() or 1)
-        cpu = {"value": ns / dt, "unit": "reads/s", "cores": os.cpu_count(), "kind": "reference",
-               "sample": "%d of the workload's reads, full reference, index build included, one run" % ns}
-
-    if rank == 0:
-        line = {"metric": "mapped reads/sec", "value": value, "unit": "reads/s", "n_gpus": world, "steps": a.steps,
-                "warmup": a.warmup, "ms_per_step": t_max / a.steps, "higher_is_better": True, "scaling": "weak",
-                "vs_baseline": None, "dtype": "u8/int32", "data": "synthetic",
-                "config": {"workload": workload_name(a.cfg, a.scale), "reads_per_gpu": n,
-                           "reference_codes": sum(w["ref_sizes"]), "args": " ".join(w["args"]),
-                           "step": "index build (all seeds) + map all reads, both strands",
-                           "l2": "flushed (512 MB write) between timed steps", "parallelism": "dp%d (reads)" % world,
-                           "tuning": tuning, "tuning_s": round(tune_s, 2)},
-                "mapped_fraction": mapped / n, "sw_filter_gcups": stages["sw_filter"]["gcups"],
-                "gpu_launches": int(st["kernels"]), "roofline": roof, "stages": stages,
-                "counts": {k: int(st[k]) for k in ("candidates", "filter_passed", "aligned", "seed_lookups",
-                                                   "hit_positions", "filter_cells", "filter_band_cells")},
-                "clocks": clk.summary(), "e2e": e2e, "cpu_baseline": cpu,
-                "filter_peak": {"lane_inst_per_s": ops_s, "ms": ms_peak}}
-        print(json.dumps(line))
-    mapper.close()
-    if dist:
-        dist.barrier()
-        dist.destroy_process_group()
-
-
-def _filter_peak(api, device):
-    import ctypes as C
-    ops, ms = C.c_double(0), C.c_double(0)
-    api.lib().stormgpu_filter_peak.argtypes = [C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)]
-    api._check(api.lib().stormgpu_filter_peak(device, C.byref(ops), C.byref(ms)))
-    return ops.value, ms.value
+    if a.cfg == 2:
+        mixed_arm(a, w)
+    elif a.cfg == 3:
+        if rank == 0:
+            serving_arm(a, w)
+    elif rank == 0:
+        whole_set_arm(a, w)
 
 
 if __name__ == "__main__":

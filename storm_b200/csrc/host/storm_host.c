@@ -1189,3 +1189,26 @@ int sh_write_unmapped_fastq(FILE *f, const sh_sam_opts *o, const sh_reads *reads
   }
   return 0;
 }
+
+/* writers into a named file, for callers without a FILE * (language bindings) */
+int sh_write_sam_path(const char *path, const sh_sam_opts *o, const sh_refs *refs, const sh_reads *reads,
+                      const stormgpu_results *res) {
+  FILE *f = fopen(path, "w");
+  if (!f) return fail(STORMGPU_EINVAL, "Cannot open %s for writing.", path);
+  char *obuf = malloc(1 << 22);
+  if (obuf) setvbuf(f, obuf, _IOFBF, 1 << 22);
+  const int rc = sh_write_sam(f, o, refs, reads, res, 0, reads->n, 1);
+  const int closed = fclose(f);
+  free(obuf);
+  if (closed != 0 && rc == 0) return fail(STORMGPU_EINVAL, "Cannot write %s.", path);
+  return rc;
+}
+
+int sh_write_unmapped_fastq_path(const char *path, const sh_sam_opts *o, const sh_reads *reads,
+                                 const stormgpu_results *res) {
+  FILE *f = fopen(path, "w");
+  if (!f) return fail(STORMGPU_EINVAL, "Cannot open %s for writing.", path);
+  const int rc = sh_write_unmapped_fastq(f, o, reads, res);
+  if (fclose(f) != 0 && rc == 0) return fail(STORMGPU_EINVAL, "Cannot write %s.", path);
+  return rc;
+}

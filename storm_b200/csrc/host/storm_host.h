@@ -90,6 +90,11 @@ int sh_write_sam(FILE *f, const sh_sam_opts *o, const sh_refs *refs, const sh_re
                  const stormgpu_results *res, int64_t first, int64_t count, int header);
 int sh_write_unmapped_fastq(FILE *f, const sh_sam_opts *o, const sh_reads *reads,
                             const stormgpu_results *res);
+/* The same into the file at `path` (created or truncated; the SAM with its header). */
+int sh_write_sam_path(const char *path, const sh_sam_opts *o, const sh_refs *refs, const sh_reads *reads,
+                      const stormgpu_results *res);
+int sh_write_unmapped_fastq_path(const char *path, const sh_sam_opts *o, const sh_reads *reads,
+                                 const stormgpu_results *res);
 
 /* genome_map (the mapping without -M): the reads placed on the references, in the order
  * genome_map__generate_SAM_output prints them (sequence, position, then placement order),

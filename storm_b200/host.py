@@ -88,9 +88,11 @@ class Reference:
 class ReadSet:
     """Loaded and tag-sorted reads, viewable as a stormgpu_reads batch (no copy)."""
 
-    def __init__(self, path: str, colour: int, quality_base: int = 33, allow_mixed: int = 1, sort: bool = True):
+    def __init__(self, path: str, colour: int, quality_base: int = 33, allow_mixed: int = 1, sort: bool = True,
+                 quality_path: str | None = None):
         self._s = ShReads()
-        rc = hostlib().sh_load_reads(path.encode(), None, colour, quality_base, allow_mixed, C.byref(self._s))
+        rc = hostlib().sh_load_reads(path.encode(), quality_path.encode() if quality_path else None, colour,
+                                     quality_base, allow_mixed, C.byref(self._s))
         if rc:
             raise api.StormError(hostlib().sh_last_error().decode())
         if sort:

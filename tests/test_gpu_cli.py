@@ -68,3 +68,36 @@ def _live(cfg, scale, extra, tmp_path, strip_m=False):
         outs[tag] = [l for l in lines if not l.startswith(b"@PG")], (tmp_path / (tag + ".fq")).read_bytes()
     assert outs["gpu"][0] == outs["ref"][0]
     assert outs["gpu"][1] == outs["ref"][1]
+
+
+@pytest.mark.parametrize("cfg,scale,extra", [(0, 0.05, []), (1, 0.01, []), (0, 0.05, ["-M", "3", "-A", "-i", "7"])])
+def test_resident_front_end_matches_cli(cfg, scale, extra, tmp_path):
+    """storm_b200.pipeline.ResidentMapper (reference and index resident, read file in, SAM out):
+    the same records and unmapped reads as the command line, on two read files in a row."""
+    from storm_b200 import pipeline
+    w = synth.generate(cfg, scale, str(tmp_path / "ref.fa"), str(tmp_path / "reads.fq"))
+    args = _without_m(w["args"]) + (extra if "-M" in extra else ["-M", "1"] + extra)
+    colour = w["mode"] == "colour"
+    seeds = None if "-s" in args else (synth_default_seeds(colour))
+    half = tmp_path / "half.fq"
+    with open(tmp_path / "reads.fq", "rb") as f, open(half, "wb") as o:
+        lines = f.readlines()
+        o.writelines(lines[:4 * (len(lines) // 8)])
+    rm = pipeline.ResidentMapper(str(tmp_path / "ref.fa"), args, colour=int(colour), default_seeds=seeds)
+    try:
+        for name in ("reads.fq", "half.fq"):
+            p = subprocess.run([_exe(w["mode"]), "-g", "ref.fa", "-r", name, "-o", "cli.sam", "-O", "cli.fq",
+                                "-v", "0"] + args, cwd=str(tmp_path), capture_output=True, timeout=600)
+            assert p.returncode == 0, p.stderr[-2000:]
+            rm.map_file(str(tmp_path / name), str(tmp_path / "res.sam"), str(tmp_path / "res.fq"))
+            body = [(tmp_path / x).read_bytes().split(b"\n") for x in ("cli.sam", "res.sam")]
+            assert [l for l in body[0] if not l.startswith(b"@PG")] == [l for l in body[1] if not l.startswith(b"@PG")]
+            assert (tmp_path / "cli.fq").read_bytes() == (tmp_path / "res.fq").read_bytes()
+    finally:
+        rm.close()
+
+
+def synth_default_seeds(colour):
+    """The command line's default seed family when no seeds file is found (seed.h:22-33)."""
+    return ("####----##--##-####;####-###--#----####;####-####-####" if colour
+            else "####--#-#--##--####;#####--###-#-###;###-##-#######")
