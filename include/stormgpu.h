@@ -193,7 +193,9 @@ typedef struct stormgpu_stats {
   int64_t seed_lookups;      /* (seed, read position) key lookups */
   int64_t hit_positions;     /* index positions read by the hit gather */
   int64_t filter_cells;      /* filter cell updates: W * 2 * (L + W - 1) per candidate, W = 2..16 */
-  int64_t align_cells;       /* L * (2*i+1) per full alignment */
+  int64_t align_cells;       /* band cells the full alignment computed: 2*i+1 per row, L rows for
+                                a candidate that runs to its last row, fewer for one that stops
+                                once it can no longer be accepted */
   int64_t kernels;           /* kernel launches */
   int64_t filter_band_cells; /* band cells of the filtered diagonals: L * (2*min(i,15)+1) each */
   double  ms_index, ms_gather, ms_filter, ms_align, ms_replay, ms_total;
@@ -213,8 +215,13 @@ typedef struct stormgpu_tuning {
                                      a multiple of 32 */
   int32_t filter_cursor;          /* 1: the filter runs as a persistent grid whose blocks take tiles
                                      from a work cursor; 0: one block per tile */
+  int32_t align_rounds;           /* 1..6: a read's passing candidates are aligned in this many
+                                     rounds of increasing rank (the first 8, then up to 32, 128,
+                                     512, 2048, then the rest), each followed by the replay of its
+                                     ranks; a later round's alignment stops as soon as it cannot
+                                     reach the read's running threshold.  1: one round */
 } stormgpu_tuning;
-/* The context's parameters (defaults 768, 4, 8, 32, 0). */
+/* The context's parameters (defaults 768, 4, 8, 32, 0, 4). */
 int stormgpu_get_tuning(stormgpu_ctx *ctx, stormgpu_tuning *out);
 /* Set them; STORMGPU_EINVAL (nothing changed) if one is outside its range. */
 int stormgpu_set_tuning(stormgpu_ctx *ctx, const stormgpu_tuning *t);

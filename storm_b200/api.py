@@ -58,13 +58,14 @@ class Stats(C.Structure):
 class Tuning(C.Structure):
     """stormgpu_tuning: launch parameters of the stages (none changes a result)."""
     _fields_ = [(n, C.c_int32) for n in ("gather_warp_cap", "gather_reads_per_steal", "filter_rows", "align_steal",
-                                         "filter_cursor")]
+                                         "filter_cursor", "align_rounds")]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
-DEFAULT_TUNING = dict(gather_warp_cap=768, gather_reads_per_steal=4, filter_rows=8, align_steal=32, filter_cursor=0)
+DEFAULT_TUNING = dict(gather_warp_cap=768, gather_reads_per_steal=4, filter_rows=8, align_steal=32, filter_cursor=0,
+                      align_rounds=4)
 
 _lib = None
 

@@ -17,6 +17,7 @@
 
 #include "common.cuh"
 #include "context.cuh"
+#include "map_kernels.cuh"
 #include "gather.cuh"
 
 namespace {
@@ -25,7 +26,8 @@ bool tuning_ok(const stormgpu_tuning& t) {
   return t.gather_warp_cap >= 256 && t.gather_warp_cap <= sg::kMaxWarpCap &&
          t.gather_reads_per_steal >= 1 && t.gather_reads_per_steal <= 64 && t.filter_rows >= 1 &&
          t.filter_rows <= 64 && t.align_steal >= 32 && t.align_steal <= 1024 && t.align_steal % 32 == 0 &&
-         (t.filter_cursor == 0 || t.filter_cursor == 1);
+         (t.filter_cursor == 0 || t.filter_cursor == 1) && t.align_rounds >= 1 &&
+         t.align_rounds <= sg::kMaxAlignRounds;
 }
 
 }  // namespace
@@ -113,6 +115,8 @@ extern "C" int stormgpu_autotune(stormgpu_ctx* c, const stormgpu_reads* reads, i
       {&stormgpu_tuning::filter_cursor, &stormgpu_tuning::filter_rows, &stormgpu_stats::ms_filter,
        {{0, 8}, {1, 2}, {1, 4}, {1, 8}, {1, 16}}},
       {&stormgpu_tuning::align_steal, nullptr, &stormgpu_stats::ms_align, {{32, 0}, {64, 0}, {128, 0}}},
+      // with rounds the replays run between the alignment launches: compare whole passes
+      {&stormgpu_tuning::align_rounds, nullptr, &stormgpu_stats::ms_total, {{1, 0}, {3, 0}, {4, 0}, {6, 0}}},
   };
   stormgpu_tuning best = c->tune;
   int rc = 0;

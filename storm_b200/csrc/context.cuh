@@ -55,7 +55,7 @@ struct stormgpu_ctx {
   std::vector<sg::RefSeq> refs;
   bool indexed = false;
   stormgpu_stats stats;
-  stormgpu_tuning tune = {768, 4, 8, 32, 0};  // launch parameters of the stages (no effect on results)
+  stormgpu_tuning tune = {768, 4, 8, 32, 0, 4};  // launch parameters of the stages (no effect on results)
   // per-batch read buffers
   sg::DevBuf<uint8_t> rcodes, rlevels, fcodes, flevels, first_levels;
   sg::DevBuf<int16_t> lengths;
@@ -72,9 +72,12 @@ struct stormgpu_ctx {
   sg::DevBuf<int16_t> a_pos;
   sg::DevBuf<uint8_t> a_tb;
   sg::DevBuf<uint32_t> scratch;
+  sg::DevBuf<int32_t> thr, round_slots;  // alignment rounds: per-read threshold, per-round slot lists
+  sg::DevBuf<int64_t> rounds;           // [0, 8): slots per round, [8, 16): the lists' fill cursors
   sg::DevBuf<unsigned long long> counters;
   sg::DevBuf<uint32_t> ord, ord_tmp;  // length order of a mixed-length batch: sort keys and values, sort scratch
   cudaEvent_t ev[8];
+  cudaEvent_t rev[2 * 6 + 1];  // alignment rounds: before the first, after each round's alignment and replay
   int64_t last_n = -1;  // reads of the last stormgpu_map call (its results stay in hits / mapped)
   // genome_map placement
   sg::DevBuf<uint32_t> gm_k0, gm_v0, gm_k1, gm_v1, gm_tmp, gm_base;

@@ -124,16 +124,18 @@ struct BandWindow {
 // BWT > 0: the band width 2I + 1 as a constant, so that the row arrays live in registers;
 // BWT = 0: any width up to kMaxBand (arrays in local memory).  CM: 0 nucleotide, 1 colour
 // space (the colour state machine compiled in), -1 either (sp.colour).
-// A candidate whose running abort bound falls below -t stops at that row: the replay
-// threshold never is below -t, so it is aborted whatever comes before it, and neither its score
-// nor its traceback is read.
-// One slot; its direction bits in scratch column sl of ns.
+// A candidate whose running abort bound falls below the replay's threshold stops at that row:
+// -t, or with rounds the running threshold its read had after the rounds before (the replay's
+// threshold only rises, so the candidate is aborted whatever comes before it), and neither its
+// score nor its traceback is read.
+// One slot; its direction bits in scratch column sl of ns.  Returns the rows it computed.
 template <int BWT, int CM>
-__device__ __forceinline__ void align_one(const ReadsDev& rd, const ScoreParams& sp, const uint8_t* __restrict__ genome,
-                                          const uint8_t* __restrict__ mask, int64_t slot, int64_t sl, int64_t ns,
-                                          const PassBuffers& pb) {
+__device__ __forceinline__ int align_one(const ReadsDev& rd, const ScoreParams& sp, const uint8_t* __restrict__ genome,
+                                         const uint8_t* __restrict__ mask, int64_t slot, int64_t sl, int64_t ns,
+                                         const PassBuffers& pb) {
   constexpr int NB = BWT > 0 ? BWT : kMaxBand;
   const int r = pb.p_read[slot];
+  const int thr = pb.thr ? max(sp.min_score, pb.thr[r]) : sp.min_score;
   const int d = pb.p_diag[slot];
   const int I = sp.I, BW = BWT > 0 ? BWT : 2 * I + 1, colour = CM >= 0 ? CM : sp.colour;
   const int L = rd.lengths[r];
@@ -167,6 +169,7 @@ __device__ __forceinline__ void align_one(const ReadsDev& rd, const ScoreParams&
   }
   int best_possible = (colour ? (L - 2) : L) * mbest;
   long long bound = 0x7fffffffLL;
+  int rows = L;
   for (int i = 1; i < L; ++i) {
     const int rc = code_at(rdc, i), q = rdq ? code_at(rdq, i) : 3;
     int max_on_line = kMinScore;
@@ -243,7 +246,10 @@ __device__ __forceinline__ void align_one(const ReadsDev& rd, const ScoreParams&
     for (int k = 0; k < wpr_dir; ++k) scr[((int64_t)i * wpr + k) * ns + sl] = wd[k];
     if (colour)
       for (int k = wpr_dir; k < wpr; ++k) scr[((int64_t)i * wpr + k) * ns + sl] = wc[k - wpr_dir];
-    if (bound < sp.min_score) break;  // aborted at any threshold
+    if (bound < thr) {  // aborted at any threshold it can meet
+      rows = i + 1;
+      break;
+    }
   }
   int best = kMinScore, bi = -1, bj = -1;
 #pragma unroll
@@ -254,7 +260,7 @@ __device__ __forceinline__ void align_one(const ReadsDev& rd, const ScoreParams&
   pb.a_bound[slot] = bnd;
   int i0 = bi, j0 = bj, tl = 0;
   uint8_t* tb = pb.a_tb + slot * pb.tbs;
-  if (bi >= 0 && bnd >= sp.min_score && best > sp.min_score) {
+  if (bi >= 0 && bnd >= thr && best > thr) {
     int i = bi, c = bj - bi, colr = 0;
     uint8_t cur = 0;
     while (i >= 0 && i < L && c >= 0 && c < BW) {
@@ -295,6 +301,7 @@ __device__ __forceinline__ void align_one(const ReadsDev& rd, const ScoreParams&
   pb.a_pos[slot * 4 + 1] = (int16_t)bj;
   pb.a_pos[slot * 4 + 2] = (int16_t)i0;
   pb.a_pos[slot * 4 + 3] = (int16_t)j0;
+  return rows;
 }
 
 // Slots slot0 .. slot0 + nslots: one per thread (scratch column = slot - slot0), or with
@@ -308,10 +315,16 @@ __global__ void __launch_bounds__(128, (BWT > 0 && BWT <= 15 ? 5 : BWT == 31 ? 4
   // one call site of align_one (its band code is large and fully unrolled)
   const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const bool steal = pb.cursor != nullptr;
-  const int64_t n = steal && pb.npass_dev ? *pb.npass_dev : nslots;
+  int64_t n = steal && pb.npass_dev ? *pb.npass_dev : nslots;
+  int64_t list0 = 0;  // with rounds: this round's slots are round_slots[list0 .. list0 + n)
+  if (pb.round_slots) {
+    n = pb.round_count[pb.round];
+    for (int k = 0; k < pb.round; ++k) list0 += pb.round_count[k];
+  }
   const int64_t ns = steal ? (int64_t)gridDim.x * blockDim.x : nslots;
   const int lane = threadIdx.x & 31;
   const int take = pb.steal >= 32 ? pb.steal & ~31 : 32;
+  unsigned long long rows = 0;
   int64_t s = tid, end = steal ? 0 : tid + 1;  // stealing: every lane takes the first run together
   for (;;) {
     if (steal && s >= end) {  // the warp's next run of `take` slots
@@ -322,9 +335,16 @@ __global__ void __launch_bounds__(128, (BWT > 0 && BWT <= 15 ? 5 : BWT == 31 ? 4
       end = s + take;
       s += lane;
     }
-    if (s < n) align_one<BWT, CM>(rd, sp, genome, mask, slot0 + s, steal ? tid : s, ns, pb);
+    if (s < n) {
+      const int64_t slot = pb.round_slots ? (int64_t)pb.round_slots[list0 + s] : slot0 + s;
+      rows += (unsigned long long)align_one<BWT, CM>(rd, sp, genome, mask, slot, steal ? tid : s, ns, pb);
+    }
     if (!steal) break;
     s += 32;
+  }
+  if (pb.cells) {
+    for (int o = 16; o > 0; o >>= 1) rows += __shfl_xor_sync(0xffffffffu, rows, o);
+    if (lane == 0 && rows) atomicAdd(pb.cells, rows * (unsigned long long)(2 * sp.I + 1));
   }
 }
 
@@ -364,17 +384,20 @@ __device__ __forceinline__ int tbget(const uint8_t* t, int i) { return (t[i >> 1
 // threshold starting at -t for every (sequence, strand, read): aborted iff the bound is
 // below the running threshold; accepted iff not aborted and score > threshold; then
 // hit_map__update (hit_map.c:50-144) and threshold = max(threshold, 4th score).
-__global__ void replay_kernel(int64_t n, ScoreParams sp, int ref_id, int sense, PassBuffers pb,
+// With rounds, the ranks [lo, hi) of each read, starting from the threshold the ranks before
+// left in pb.thr (the first round starts from -t), which it updates.
+__global__ void replay_kernel(int64_t n, ScoreParams sp, int ref_id, int sense, PassBuffers pb, int lo, int hi,
                               stormgpu_hit* __restrict__ hits, uint8_t* __restrict__ tbo, int64_t tbs,
                               uint8_t* __restrict__ mapped) {
   const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= n) return;
   const int P = pb.pcount[r];
-  if (P == 0) return;
+  if (P <= lo) return;
   const int64_t s0 = pb.pstart[r];
-  int T = sp.min_score;
+  int T = (pb.thr && lo > 0) ? pb.thr[r] : sp.min_score;
   stormgpu_hit* h = hits + r * 4;
-  for (int k = 0; k < P; ++k) {
+  const int kend = P < hi ? P : hi;
+  for (int k = lo; k < kend; ++k) {
     const int64_t slot = s0 + k;
     const int score = pb.a_score[slot];
     if (!(pb.a_bound[slot] >= T && score > T)) continue;
@@ -425,12 +448,80 @@ __global__ void replay_kernel(int64_t n, ScoreParams sp, int ref_id, int sense, 
     }
     if (h[3].score > T) T = h[3].score;
   }
+  if (pb.thr) pb.thr[r] = T;
 }
 
 void launch_replay(int64_t n, const ScoreParams& sp, int ref_id, int sense, PassBuffers& pb,
                    stormgpu_hit* hits, uint8_t* tb, int64_t tbs, uint8_t* mapped, cudaStream_t st) {
   if (n <= 0) return;
-  replay_kernel<<<(unsigned)((n + 127) / 128), 128, 0, st>>>(n, sp, ref_id, sense, pb, hits, tb, tbs, mapped);
+  replay_kernel<<<(unsigned)((n + 127) / 128), 128, 0, st>>>(n, sp, ref_id, sense, pb, 0, 0x7fffffff, hits, tb, tbs,
+                                                             mapped);
+}
+
+void launch_replay_round(int64_t n, const ScoreParams& sp, int ref_id, int sense, PassBuffers& pb, int rounds,
+                         stormgpu_hit* hits, uint8_t* tb, int64_t tbs, uint8_t* mapped, cudaStream_t st) {
+  if (n <= 0) return;
+  const int lo = align_round_bound(pb.round, rounds), hi = align_round_bound(pb.round + 1, rounds);
+  replay_kernel<<<(unsigned)((n + 127) / 128), 128, 0, st>>>(n, sp, ref_id, sense, pb, lo, hi, hits, tb, tbs, mapped);
+}
+
+// ------------------------------------------------------------------------------ rounds
+
+__device__ __forceinline__ int round_of_rank(int rank, int rounds) {
+  int k = 0;
+  while (k + 1 < rounds && rank >= align_round_bound(k + 1, rounds)) ++k;
+  return k;
+}
+
+// per round: slots whose rank falls in it (one atomic per warp and round)
+__global__ void round_count_kernel(int64_t npass, int rounds, const int32_t* __restrict__ p_read,
+                                   const int32_t* __restrict__ pstart, int64_t* __restrict__ count) {
+  const int lane = threadIdx.x & 31;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t base = (int64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < npass; base += stride) {
+    const int64_t s = base + lane;
+    const int k = s < npass ? round_of_rank((int)(s - pstart[p_read[s]]), rounds) : -1;
+    for (int j = 0; j < rounds; ++j) {
+      const unsigned m = __ballot_sync(0xffffffffu, k == j);
+      if (m && lane == 0) atomicAdd(reinterpret_cast<unsigned long long*>(&count[j]), (unsigned long long)__popc(m));
+    }
+  }
+}
+
+// the lists: a warp's slots of one round go out together, in slot order
+__global__ void round_scatter_kernel(int64_t npass, int rounds, const int32_t* __restrict__ p_read,
+                                     const int32_t* __restrict__ pstart, const int64_t* __restrict__ count,
+                                     unsigned long long* __restrict__ cursors, int32_t* __restrict__ slots) {
+  const int lane = threadIdx.x & 31;
+  int64_t start[kMaxAlignRounds];
+  int64_t acc = 0;
+  for (int j = 0; j < kMaxAlignRounds; ++j) {
+    start[j] = acc;
+    if (j < rounds) acc += count[j];
+  }
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t base = (int64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < npass; base += stride) {
+    const int64_t s = base + lane;
+    const int k = s < npass ? round_of_rank((int)(s - pstart[p_read[s]]), rounds) : -1;
+    for (int j = 0; j < rounds; ++j) {
+      const unsigned m = __ballot_sync(0xffffffffu, k == j);
+      if (!m) continue;
+      unsigned long long b = 0;
+      if (lane == 0) b = atomicAdd(&cursors[j], (unsigned long long)__popc(m));
+      b = __shfl_sync(0xffffffffu, b, 0);
+      if (k == j) slots[start[j] + (int64_t)b + __popc(m & ((1u << lane) - 1u))] = (int32_t)s;
+    }
+  }
+}
+
+void launch_round_lists(int64_t npass, int rounds, const int32_t* p_read, const int32_t* pstart, int64_t* round_count,
+                        unsigned long long* cursors, int32_t* round_slots, cudaStream_t st) {
+  if (npass <= 0) return;
+  int64_t blocks = (npass + 255) / 256;
+  if (blocks > 148 * 16) blocks = 148 * 16;
+  round_count_kernel<<<(unsigned)blocks, 256, 0, st>>>(npass, rounds, p_read, pstart, round_count);
+  round_scatter_kernel<<<(unsigned)blocks, 256, 0, st>>>(npass, rounds, p_read, pstart, round_count, cursors,
+                                                         round_slots);
 }
 
 }  // namespace sg

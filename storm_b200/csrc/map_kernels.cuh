@@ -61,7 +61,24 @@ struct PassBuffers {
   unsigned long long* cursor;
   const int64_t* npass_dev;  // may be null; else the slot count is read from here
   int steal;                 // with a cursor: slots a warp takes at a time, a multiple of 32 (0 = 32)
+  // Rounds (all null for one round over every slot).  The passing candidates of a read are
+  // aligned in rounds of increasing rank (rank = slot - pstart[read]): round k takes the ranks
+  // [align_round_bound(k), align_round_bound(k + 1)), listed in round_slots after the lists of
+  // the rounds before it (round_count[k] slots); thr[read] holds the replay's running threshold
+  // after the rounds before, below which a candidate can no longer be accepted, so that its
+  // alignment may stop there.
+  const int32_t* round_slots;
+  const int64_t* round_count;  // [kMaxAlignRounds]
+  int round;                   // the round of this launch
+  int32_t* thr;                // per read; written by the replay of each round
+  unsigned long long* cells;   // may be null; += band cells the alignment computed
 };
+
+constexpr int kMaxAlignRounds = 6;
+// first rank of each round: 0, 8, 32, 128, 512, 2048, then every rank left
+__host__ __device__ __forceinline__ int align_round_bound(int k, int rounds) {
+  return k <= 0 ? 0 : k >= rounds ? 0x7fffffff : 8 << (2 * (k - 1));
+}
 
 void launch_reverse_reads(const ReadsDev& in, const uint8_t* first_levels, int colour,
                           uint8_t* rcodes, uint8_t* rlevels, cudaStream_t st);
@@ -74,6 +91,14 @@ void launch_align(const ReadsDev& r, const ScoreParams& sp, const uint8_t* genom
 int64_t align_workers(int64_t nslots, const ScoreParams& sp);
 void launch_replay(int64_t n, const ScoreParams& sp, int ref_id, int sense, PassBuffers& pb,
                    stormgpu_hit* hits, uint8_t* tb, int64_t tbs, uint8_t* mapped, cudaStream_t st);
+// The slots of every round of a pass, in slot order within a warp's run: counts into
+// round_count (zeroed by the caller), then the lists into round_slots.  `cursors` holds
+// `rounds` zeroed counters.
+void launch_round_lists(int64_t npass, int rounds, const int32_t* p_read, const int32_t* pstart, int64_t* round_count,
+                        unsigned long long* cursors, int32_t* round_slots, cudaStream_t st);
+// Replay of round pb.round (the ranks of that round), continuing from pb.thr.
+void launch_replay_round(int64_t n, const ScoreParams& sp, int ref_id, int sense, PassBuffers& pb, int rounds,
+                         stormgpu_hit* hits, uint8_t* tb, int64_t tbs, uint8_t* mapped, cudaStream_t st);
 
 
 }  // namespace sg

@@ -128,7 +128,7 @@ struct stormgpu_server {
   std::map<int64_t, Request*> reqs;
   int64_t next_ticket = 1;
   bool built = false, stop = false;
-  stormgpu_tuning tune = {768, 4, 8, 32, 0};  // launch parameters of every slot
+  stormgpu_tuning tune = {768, 4, 8, 32, 0, 4};  // launch parameters of every slot
 };
 
 namespace {
@@ -299,6 +299,7 @@ extern "C" int stormgpu_server_build(stormgpu_server* s) {
       return STORMGPU_ECUDA;
     }
     for (auto& e : v->ev) cudaEventCreate(&e);
+    for (auto& e : v->rev) cudaEventCreate(&e);
     sl->ws = v;
     s->slots.push_back(sl);
   }

@@ -150,6 +150,7 @@ extern "C" int stormgpu_open(const stormgpu_params* params, const char* seeds, s
     return STORMGPU_ECUDA;
   }
   for (auto& e : c->ev) cudaEventCreate(&e);
+  for (auto& e : c->rev) cudaEventCreate(&e);
   *out = c;
   return 0;
 }
@@ -178,7 +179,9 @@ extern "C" void stormgpu_close(stormgpu_ctx* c) {
   c->gm_k0.release(); c->gm_v0.release(); c->gm_k1.release(); c->gm_v1.release(); c->gm_tmp.release();
   c->gm_base.release();
   c->ord.release(); c->ord_tmp.release();
+  c->thr.release(); c->round_slots.release(); c->rounds.release();
   for (auto& e : c->ev) cudaEventDestroy(e);
+  for (auto& e : c->rev) cudaEventDestroy(e);
   cudaStreamDestroy(c->st);
   delete c;
 }
@@ -316,7 +319,7 @@ static int map_device_once(stormgpu_ctx* c, const stormgpu_reads* reads, stormgp
   }
   if (c->pstart.grow(n) || c->pcount.grow(n) || c->scan_tmp64.grow(scan_tmp_elems(n) + 8) ||
       c->big_list.grow(n) || c->huge_list.grow(n) || c->huge_h.grow(n) || c->big_count.grow(2) ||
-      c->counters.grow(16) || c->fr.grow(std::max<int64_t>(n * 64, 1 << 20)) ||
+      c->counters.grow(32) || c->fr.grow(std::max<int64_t>(n * 64, 1 << 20)) ||
       c->fd.grow(std::max<int64_t>(n * 64, 1 << 20)))
     return STORMGPU_ENOMEM;
   const int BW = 2 * sp.I + 1;
@@ -337,7 +340,7 @@ static int map_device_once(stormgpu_ctx* c, const stormgpu_reads* reads, stormgp
       for (int attempt = 0;; ++attempt) {
         // fused hit gather: sorted, de-duplicated diagonals of every read, appended to the flat
         // candidate list (fr, fd); reads with many index positions go to the block kernel
-        SG_CUDA(cudaMemsetAsync(c->counters.p, 0, sizeof(unsigned long long) * 16, st));
+        SG_CUDA(cudaMemsetAsync(c->counters.p, 0, sizeof(unsigned long long) * 32, st));
         SG_CUDA(cudaMemsetAsync(c->big_count.p, 0, sizeof(int32_t) * 2, st));
         GatherOut go;
         go.fr = c->fr.p; go.fd = c->fd.p; go.cap = c->fr.cap; go.counters = c->counters.p;
@@ -390,6 +393,7 @@ static int map_device_once(stormgpu_ctx* c, const stormgpu_reads* reads, stormgp
       memset(&job, 0, sizeof(job));
       if (c->tune.filter_cursor) job.cursor = c->counters.p + 10;  // zeroed with the counters of the pass
       job.rows = c->tune.filter_rows;
+      job.one = 1;
       job.n = utot; job.fr = c->fr.p; job.fd = c->fd.p; job.flag = c->flag.p; job.codes = rd.codes;
       job.cstride = rd.cstride; job.lengths = rd.lengths; job.genome = R.d_codes; job.W = sp.W; job.Is = sp.Is;
       job.fm = sp.fm; job.fx = sp.fx; job.fo = sp.fo; job.fe = sp.fe; job.fthr = sp.fthr;
@@ -422,6 +426,7 @@ static int map_device_once(stormgpu_ctx* c, const stormgpu_reads* reads, stormgp
       pb.pstart = c->pstart.p; pb.pcount = c->pcount.p;
       pb.counters = c->counters.p;
       SG_CUDA(cudaMemsetAsync(c->pcount.p, 0, sizeof(int32_t) * n, st));
+      const int rounds = std::max(1, std::min<int>(c->tune.align_rounds, kMaxAlignRounds));
       if (npass > 0) {
         if (c->p_read.grow(npass) || c->p_diag.grow(npass) || c->a_score.grow(npass) || c->a_bound.grow(npass) ||
             c->a_tblen.grow(npass) || c->a_pos.grow(npass * 4) || c->a_tb.grow(npass * tbs))
@@ -438,13 +443,37 @@ static int map_device_once(stormgpu_ctx* c, const stormgpu_reads* reads, stormgp
         const int64_t per_slot = (int64_t)maxL * wpr;
         if (c->scratch.grow(align_workers(npass, sp) * per_slot)) return STORMGPU_ENOMEM;
         pb.a_scratch = c->scratch.p;
-        launch_align(rd, sp, R.d_codes, R.d_mask, 0, npass, pb, st);
-        launches++;
+        pb.cells = c->counters.p + 13;
+        if (rounds == 1) {
+          launch_align(rd, sp, R.d_codes, R.d_mask, 0, npass, pb, st);
+          launches++;
+        } else {
+          // rounds of increasing rank, each aligned with the thresholds the replay of the rounds
+          // before left, then replayed
+          if (c->thr.grow(n) || c->round_slots.grow(npass) || c->rounds.grow(16)) return STORMGPU_ENOMEM;
+          SG_CUDA(cudaMemsetAsync(c->rounds.p, 0, sizeof(int64_t) * 16, st));
+          launch_round_lists(npass, rounds, c->p_read.p, c->pstart.p, c->rounds.p,
+                             reinterpret_cast<unsigned long long*>(c->rounds.p + 8), c->round_slots.p, st);
+          launches += 2;
+          pb.round_slots = c->round_slots.p;
+          pb.round_count = c->rounds.p;
+          pb.thr = c->thr.p;
+          SG_CUDA(cudaEventRecord(c->rev[0], st));
+          for (int k = 0; k < rounds; ++k) {
+            pb.round = k;
+            pb.cursor = c->counters.p + 16 + k;  // zeroed with the counters of the pass
+            launch_align(rd, sp, R.d_codes, R.d_mask, 0, npass, pb, st);
+            SG_CUDA(cudaEventRecord(c->rev[2 * k + 1], st));
+            launch_replay_round(n, sp, (int)ref_id, strand ? -1 : 1, pb, rounds, out->hits, out->tb, out->tb_stride,
+                                out->mapped, st);
+            SG_CUDA(cudaEventRecord(c->rev[2 * k + 2], st));
+            launches += 2;
+          }
+        }
         S.aligned += npass;
-        S.align_cells += npass * (int64_t)maxL * BW;
       }
       SG_CUDA(cudaEventRecord(c->ev[3], st));
-      if (npass > 0) {
+      if (npass > 0 && rounds == 1) {
         launch_replay(n, sp, (int)ref_id, strand ? -1 : 1, pb, out->hits, out->tb, out->tb_stride, out->mapped, st);
         launches++;
       }
@@ -455,7 +484,21 @@ static int map_device_once(stormgpu_ctx* c, const stormgpu_reads* reads, stormgp
       cudaEventElapsedTime(&b, c->ev[1], c->ev[2]);
       cudaEventElapsedTime(&d, c->ev[2], c->ev[3]);
       cudaEventElapsedTime(&e, c->ev[3], c->ev[4]);
+      if (npass > 0 && rounds > 1) {  // the rounds' replays count as replay time
+        for (int k = 0; k < rounds; ++k) {
+          float x = 0;
+          cudaEventElapsedTime(&x, c->rev[2 * k + 1], c->rev[2 * k + 2]);
+          d -= x;
+          e += x;
+        }
+      }
       tg += a; tf += b; ta += d; tr += e;
+      if (npass > 0) {
+        unsigned long long cells = 0;
+        SG_CUDA(cudaMemcpyAsync(&cells, c->counters.p + 13, sizeof(cells), cudaMemcpyDeviceToHost, st));
+        SG_CUDA(cudaStreamSynchronize(st));
+        S.align_cells += (int64_t)cells;
+      }
     }
   }
   SG_CUDA(cudaEventRecord(c->ev[7], st));
@@ -638,6 +681,7 @@ extern "C" int stormgpu_sw_filter(int W, int read_len, uint32_t match, uint32_t 
     launch_expand_reads(one, rx, rstride, 0);
     FilterJob job;
     memset(&job, 0, sizeof(job));
+    job.one = 1;
     job.n = n; job.fr = dzero; job.fd = dpos; job.flag = dp; job.codes = dr; job.cstride = rb;
     job.lengths = dl; job.genome = gb; job.W = W; job.Is = 0;
     job.gexp = gx + kGexpPad; job.rexp = rx; job.rstride = rstride; job.min_len = read_len;
