@@ -101,3 +101,70 @@ def synth_default_seeds(colour):
     """The command line's default seed family when no seeds file is found (seed.h:22-33)."""
     return ("####----##--##-####;####-###--#----####;####-####-####" if colour
             else "####--#-#--##--####;#####--###-#-###;###-##-#######")
+
+
+def _write_csfasta(tmp_path, n=1500):
+    genome = synth.make_genome([40000], 19)
+    synth.write_fasta(str(tmp_path / "ref.fa"), genome)
+    pr, cols, q = synth.simulate_colour_reads(genome, n, 50, 20)
+    with open(tmp_path / "reads.csfasta", "wb") as f:
+        f.write(b"# Title: solid set\n")
+        for k in range(len(cols)):
+            f.write(b">r%d_F3\n%c%s\n" % (k, synth.BASES[pr[k]], synth.COLOURS[cols[k]].tobytes()))
+    with open(tmp_path / "reads.qual", "wb") as f:
+        f.write(b"# qualities\n")
+        for k in range(len(cols)):
+            v = [int(x) for x in q[k]]
+            if k % 50 == 3:
+                v[5] = -1
+            if k == 77:
+                v = v[:30]  # short line: the rest keeps the previous read's values
+            f.write(b">r%d_F3\n%s\n" % (k, b" ".join(b"%d" % x for x in v)))
+
+
+def _both(tmp_path, colour, args, tags=("ref", "gpu")):
+    """Run the reference binary and the GPU binary with the same arguments in tmp_path; returns
+    {tag: (SAM lines without @PG, -O FASTQ bytes)}."""
+    outs = {}
+    for tag in tags:
+        exe = (os.path.join(ffi.REF_DIR, "storm-color" if colour else "storm-nucleotide") if tag == "ref"
+               else _exe("colour" if colour else "nucleotide"))
+        p = subprocess.run([exe, "-o", tag + ".sam", "-O", tag + ".fq", "-v", "0"] + args, cwd=str(tmp_path),
+                           env=dict(os.environ, MALLOC_PERTURB_="255"), capture_output=True, timeout=1800)
+        assert p.returncode == 0, (tag, p.stderr[-3000:])
+        lines = (tmp_path / (tag + ".sam")).read_bytes().split(b"\n")
+        outs[tag] = [l for l in lines if not l.startswith(b"@PG")], (tmp_path / (tag + ".fq")).read_bytes()
+    return outs
+
+
+@pytest.mark.skipif(not ffi.ref_available(), reason="oracle/_ref not built")
+@pytest.mark.parametrize("with_qual", [True, False])
+def test_gpu_cli_csfasta_matches_reference(with_qual, tmp_path):
+    """Colour reads as CSFASTA with an integer .qual file (-q; a negative value, a short line)
+    or without qualities (reads_data.c:73-345), through the GPU binary and the reference."""
+    _write_csfasta(tmp_path)
+    args = ["-g", "ref.fa", "-r", "reads.csfasta", "-M", "2", "-z", "90", "-t", "100", "-i", "5"] + \
+        (["-q", "reads.qual"] if with_qual else [])
+    outs = _both(tmp_path, True, args)
+    assert outs["gpu"] == outs["ref"]
+    assert sum(1 for l in outs["ref"][0] if l and not l.startswith(b"@")) > 500
+
+
+@pytest.mark.skipif(not ffi.ref_available(), reason="oracle/_ref not built")
+def test_gpu_cli_colour_chain_matches_reference(tmp_path):
+    """Colour -O chain: each step maps the previous step's unmapped FASTQ, which has lost one
+    colour (hit_map.c:541-547), with a stricter seed family; GPU and reference, step by step."""
+    synth.generate(1, 0.01, str(tmp_path / "ref.fa"), str(tmp_path / "reads.fq"))
+    src = "reads.fq"
+    # a contiguous w15 seed at read position 0 only, then w14 at positions 0 and 5, then a
+    # spaced w11 seed: about half the reads, then a third of the rest, stay unmapped
+    for k, seeds in enumerate(["###############:0", "##############:0 5", "####-##-#-####"]):
+        args = ["-g", "ref.fa", "-r", src, "-M", "1", "-z", "100", "-t", "115", "-i", "7", "-s", seeds]
+        outs = _both(tmp_path, True, args)
+        assert outs["gpu"] == outs["ref"], k
+        assert sum(1 for l in outs["ref"][0] if l and not l.startswith(b"@")) > 1000, k
+        if k < 2:
+            assert outs["ref"][1].count(b"\n") > 4000, k
+        nxt = "step%d.fq" % k
+        (tmp_path / nxt).write_bytes(outs["ref"][1])
+        src = nxt
