@@ -11,6 +11,7 @@
 #include "storm_cli.h"
 
 #include <getopt.h>
+#include <pthread.h>
 #include <stdarg.h>
 #include <stdlib.h>
 #include <string.h>
@@ -41,6 +42,46 @@ static void err(const char *fmt, ...) {
   fprintf(stderr, "\033[0m\n");
   va_end(ap);
   fflush(stderr);
+}
+
+static double now_s(void) {
+  struct timespec t;
+  clock_gettime(CLOCK_MONOTONIC, &t);
+  return (double)t.tv_sec + 1e-9 * (double)t.tv_nsec;
+}
+
+/* the reference load, run beside the reads load */
+typedef struct ref_job {
+  const char *path;
+  int colour, ignore_lower, rc;
+  sh_refs refs;
+  char msg[512];
+  double seconds;
+} ref_job;
+
+static void *ref_job_run(void *arg) {
+  ref_job *j = (ref_job *)arg;
+  const double t = now_s();
+  j->rc = sh_load_reference(j->path, j->colour, j->ignore_lower, &j->refs);
+  if (j->rc) snprintf(j->msg, sizeof(j->msg), "%s", sh_last_error());
+  j->seconds = now_s() - t;
+  return NULL;
+}
+
+/* the mapper's device set-up, run beside the loads */
+typedef struct prep_job {
+  const storm_mapper *m;
+  const stormgpu_params *p;
+  const char *seeds;
+  double seconds;
+} prep_job;
+
+static void *prep_job_run(void *arg) {
+  prep_job *j = (prep_job *)arg;
+  const double t = now_s();
+  j->m->prepare(j->m->user, j->p, j->seeds);
+  j->seconds = now_s() - t;
+  return NULL;
 }
 
 /* seed.c:140-179: one seed per line, '%' lines ignored, trailing blanks removed, ';' added */
@@ -203,23 +244,48 @@ int storm_cli_main(int argc, char **argv, int colour, const storm_mapper *mapper
   p.stdev_distance = stdev; p.senses = senses; p.device = 0;
   if (allowed_indels > STORMGPU_MAX_INDELS) { err("-i above %d is not supported.", STORMGPU_MAX_INDELS); exit(1); }
 
+  /* the mapper's device set-up and the reference load run beside the reads load and sort;
+   * errors are reported in the reference's order (reads first, run.c:812-835) */
+  const double t_start = now_s();
+  prep_job prep = {mapper, &p, seeds, 0.0};
+  pthread_t prep_th, ref_th;
+  const int prep_started = mapper->prepare && pthread_create(&prep_th, NULL, prep_job_run, &prep) == 0;
+  ref_job rj;
+  memset(&rj, 0, sizeof(rj));
+  rj.path = genome_file;
+  rj.colour = colour;
+  rj.ignore_lower = ignore_lower;
+  const int ref_started = pthread_create(&ref_th, NULL, ref_job_run, &rj) == 0;
   msg(1, "Loading reads database...\n");
   sh_reads reads;
-  if (sh_load_reads(reads_file, qual_file, colour, quality_base, 1, &reads) != 0) {
-    err("%s", sh_last_error());
+  const int reads_rc = sh_load_reads(reads_file, qual_file, colour, quality_base, 1, &reads);
+  char reads_msg[512];
+  snprintf(reads_msg, sizeof(reads_msg), "%s", sh_last_error());
+  const double t_reads = now_s();
+  const int sort_rc = reads_rc == 0 ? sh_sort_reads(&reads) : 0;
+  if (sort_rc != 0) snprintf(reads_msg, sizeof(reads_msg), "%s", sh_last_error());
+  const double t_sort = now_s();
+  if (ref_started) pthread_join(ref_th, NULL);
+  else ref_job_run(&rj);
+  if (reads_rc != 0 || sort_rc != 0) {
+    err("%s", reads_msg);
+    if (reads_rc == STORMGPU_ENOMEM || sort_rc == STORMGPU_ENOMEM) exit(1);  /* SAFE_FAILURE__ALLOC, util.h:70-80 */
     err("Reads could not be loaded. Exiting.");
     exit(-1);
   }
   msg(1, "Loaded %ld reads (read length %d..%d).\n", (long)reads.n, reads.min_len, reads.max_len);
-  sh_sort_reads(&reads);
   msg(1, "Loading reference database...\n");
-  sh_refs refs;
-  if (sh_load_reference(genome_file, colour, ignore_lower, &refs) != 0) {
-    err("%s", sh_last_error());
+  sh_refs refs = rj.refs;
+  if (rj.rc != 0) {
+    err("%s", rj.msg);
+    if (rj.rc == STORMGPU_ENOMEM) exit(1);
     err("Reference could not be loaded. Exiting.");
     exit(-1);
   }
   msg(1, "Loaded %d reference sequence%s.\n", refs.n, refs.n == 1 ? "" : "s");
+  if (prep_started) pthread_join(prep_th, NULL);
+  msg(2, "Times: reads %.3f s, sort %.3f s, reference %.3f s (beside), device set-up %.3f s (beside).\n",
+      t_reads - t_start, t_sort - t_reads, rj.seconds, prep.seconds);
 
   stormgpu_results res;
   res.tb_stride = ((reads.max_len + allowed_indels + 1) / 2 + 7) & ~7;
@@ -231,7 +297,9 @@ int storm_cli_main(int argc, char **argv, int colour, const storm_mapper *mapper
     exit(1);
   }
   char emsg[512] = {0};
+  const double t_map = now_s();
   int rc = mapper->map(mapper->user, &p, seeds, &refs, &reads, &res, emsg, sizeof(emsg));
+  msg(2, "Times: index build and mapping %.3f s.\n", now_s() - t_map);
   if (rc == STORMGPU_EINVAL && strstr(emsg, "seed")) {
     err("The seed pattern is invalid: \"%s\".\nExpected: {0,1}+ or {-,#}+ with at least one '1'/'#' (seed separator ';').", seeds);
     exit(-1);
@@ -254,11 +322,13 @@ int storm_cli_main(int argc, char **argv, int colour, const storm_mapper *mapper
     if (output) {
       static char obuf[1 << 22];
       setvbuf(output, obuf, _IOFBF, sizeof(obuf));
+      const double t_sam = now_s();
       if (sh_write_sam(output, &so, &refs, &reads, &res, 0, reads.n, 1) != 0) {
         err("%s", sh_last_error());
         exit(1);
       }
       fflush(output);
+      msg(2, "Times: SAM output %.3f s.\n", now_s() - t_sam);
     } else {
       err("No file name provided for SAM output.");
     }

@@ -25,6 +25,10 @@ typedef struct storm_mapper {
   /* release what map kept (may be NULL) */
   void (*finish)(void *user);
   void *user;
+  /* may be NULL; else called once at start-up, from another thread, while the inputs load:
+   * device set-up that needs only the parameters and the seeds (map must still work, and report
+   * the error, if it failed) */
+  void (*prepare)(void *user, const stormgpu_params *p, const char *seeds);
 } storm_mapper;
 
 int storm_cli_main(int argc, char **argv, int colour, const storm_mapper *mapper);

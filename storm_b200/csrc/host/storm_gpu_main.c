@@ -12,11 +12,18 @@ typedef struct gpu_state {
   stormgpu_ctx *ctx;
 } gpu_state;
 
+/* context creation (the device's start-up) while the command line loads its inputs */
+static void gpu_prepare(void *user, const stormgpu_params *p, const char *seeds) {
+  gpu_state *gs = (gpu_state *)user;
+  if (stormgpu_open(p, seeds, &gs->ctx) != 0) gs->ctx = NULL;  /* gpu_map opens again and reports */
+}
+
 static int gpu_map(void *user, const stormgpu_params *p, const char *seeds, const sh_refs *refs,
                    const sh_reads *reads, stormgpu_results *out, char *err, int errlen) {
   gpu_state *gs = (gpu_state *)user;
-  stormgpu_ctx *ctx = NULL;
-  int rc = stormgpu_open(p, seeds, &ctx);
+  stormgpu_ctx *ctx = gs->ctx;
+  gs->ctx = NULL;
+  int rc = ctx ? 0 : stormgpu_open(p, seeds, &ctx);
   if (rc) goto fail;
   for (int s = 0; s < refs->n; ++s) {
     rc = stormgpu_add_reference(ctx, refs->codes[s], refs->masks[s], refs->sizes[s], refs->rs[s],
@@ -59,6 +66,6 @@ static void gpu_finish(void *user) {
 
 int main(int argc, char **argv) {
   gpu_state gs = {NULL};
-  storm_mapper m = {"cuda", gpu_map, gpu_place_greedy, gpu_finish, &gs};
+  storm_mapper m = {"cuda", gpu_map, gpu_place_greedy, gpu_finish, &gs, gpu_prepare};
   return storm_cli_main(argc, argv, STORM_COLOUR, &m);
 }

@@ -9,11 +9,13 @@
 
 #include <ctype.h>
 #include <math.h>
+#include <stdio.h>
+#include <sys/stat.h>
 #include <stdarg.h>
 #include <stdlib.h>
 #include <string.h>
 
-static char g_err[512];
+static __thread char g_err[512];  /* per thread: loads may run in parallel threads */
 const char *sh_last_error(void) { return g_err; }
 static int fail(int code, const char *fmt, ...) {
   va_list ap;
@@ -36,14 +38,24 @@ static inline void put2(uint8_t *p, int64_t i, int v) {
 }
 static inline int get2(const uint8_t *p, int64_t i) { return (p[i >> 2] >> ((i & 3) << 1)) & 3; }
 
-/* whole file in memory, NUL-terminated */
-static char *slurp(const char *path, size_t *len) {
+/* whole file in memory, NUL-terminated; one allocation of the file's size when it has one.
+ * NULL when the file cannot be read; *oom is set when memory ran out. */
+static char *slurp(const char *path, size_t *len, int *oom) {
+  *oom = 0;
   FILE *f = fopen(path, "rb");
   if (!f) return NULL;
+  struct stat st;
   size_t cap = 1 << 20, n = 0;
+  if (fstat(fileno(f), &st) == 0 && S_ISREG(st.st_mode) && st.st_size > 0) cap = (size_t)st.st_size;
   char *buf = malloc(cap + 1);
+  if (!buf) { fclose(f); *oom = 1; return NULL; }
   for (;;) {
-    if (n == cap) { cap *= 2; buf = realloc(buf, cap + 1); }
+    if (n == cap) {
+      char *grown = realloc(buf, 2 * cap + 1);
+      if (!grown) { free(buf); fclose(f); *oom = 1; return NULL; }
+      buf = grown;
+      cap *= 2;
+    }
     size_t got = fread(buf + n, 1, cap - n, f);
     if (!got) break;
     n += got;
@@ -54,7 +66,24 @@ static char *slurp(const char *path, size_t *len) {
   return buf;
 }
 
+static int read_failed(int oom, const char *path, const char *what) {
+  if (oom) return fail(STORMGPU_ENOMEM, "Not enough memory to read %s (%s).", path, what);
+  return fail(STORMGPU_EINVAL, "Failed to read input file %s (%s).", path, what);
+}
+
 /* ---------------------------------------------------------------------------- reference */
+
+/* doubles the masked-region arrays; non-zero (arrays unchanged) when memory runs out */
+static int grow_regions(int32_t **rs, int32_t **re, int32_t *cap) {
+  int32_t *a = realloc(*rs, sizeof(int32_t) * (size_t)(2 * *cap));
+  if (!a) return 1;
+  *rs = a;
+  int32_t *b = realloc(*re, sizeof(int32_t) * (size_t)(2 * *cap));
+  if (!b) return 1;
+  *re = b;
+  *cap *= 2;
+  return 0;
+}
 
 /* reference_data.c:14-190: one FASTA chunk per '>' header; whitespace skipped; letters
  * upper-cased unless -j; non-ACGT letters are masked and coded rand()&3 (nucleotide) or as
@@ -63,8 +92,9 @@ static char *slurp(const char *path, size_t *len) {
 int sh_load_reference(const char *path, int colour, int ignore_lowercase, sh_refs *out) {
   memset(out, 0, sizeof(*out));
   size_t len;
-  char *buf = slurp(path, &len);
-  if (!buf) return fail(STORMGPU_EINVAL, "Failed to read input file %s (reference sequence).", path);
+  int oom;
+  char *buf = slurp(path, &len, &oom);
+  if (!buf) return read_failed(oom, path, "reference sequence");
   /* count chunks: lines starting with '>' (reference_data.c:210-220) */
   int nseq = 0;
   for (size_t i = 0; i < len; ++i)
@@ -81,6 +111,12 @@ int sh_load_reference(const char *path, int colour, int ignore_lowercase, sh_ref
   out->re = calloc((size_t)nseq, sizeof(int32_t *));
   out->nreg = calloc((size_t)nseq, sizeof(int32_t));
   out->first_base = calloc((size_t)nseq, 1);
+  if (!out->names || !out->sizes || !out->codes || !out->masks || !out->alloc_codes || !out->alloc_masks ||
+      !out->rs || !out->re || !out->nreg || !out->first_base) {
+    free(buf);
+    sh_free_reference(out);
+    return fail(STORMGPU_ENOMEM, "Not enough memory for the reference sequences.");
+  }
   size_t p = 0;
   int s;
   for (s = 0; s < nseq; ++s) {
@@ -93,6 +129,7 @@ int sh_load_reference(const char *path, int colour, int ignore_lowercase, sh_ref
       if (nl > e - p - 1) nl = e - p - 1;
       if (nl == 0) { free(buf); return fail(STORMGPU_EINVAL, "Empty fasta header line in the reference sequence."); }
       out->names[s] = malloc(nl + 1);
+      if (!out->names[s]) { free(buf); out->n = s; sh_free_reference(out); return fail(STORMGPU_ENOMEM, "Not enough memory for the reference sequences."); }
       memcpy(out->names[s], buf + p + 1, nl);
       out->names[s][nl] = 0;
       if (out->names[s][0] == '=' || out->names[s][0] == '*') out->names[s][0] = '-';
@@ -112,11 +149,17 @@ int sh_load_reference(const char *path, int colour, int ignore_lowercase, sh_ref
     int64_t nbytes = (size + 3) / 4 + 1;
     int64_t tot = nbytes + 2 * SH_PAD_BYTES;
     uint8_t *ca = calloc((size_t)tot, 1), *ma = calloc((size_t)tot, 1);
+    int32_t rcap = 16, nr = 0;
+    int32_t *rs = malloc(sizeof(int32_t) * (size_t)rcap), *re = malloc(sizeof(int32_t) * (size_t)rcap);
+    if (!ca || !ma || !rs || !re) {
+      free(ca); free(ma); free(rs); free(re); free(buf);
+      out->n = s + 1;  /* the name of this sequence is freed with the others */
+      sh_free_reference(out);
+      return fail(STORMGPU_ENOMEM, "Not enough memory for the reference sequences.");
+    }
     memset(ma, 0x55, SH_PAD_BYTES);
     uint8_t *cd = ca + SH_PAD_BYTES, *mk = ma + SH_PAD_BYTES;
     int64_t i = 0, mstart = -1;
-    int32_t rcap = 16, nr = 0;
-    int32_t *rs = malloc(sizeof(int32_t) * (size_t)rcap), *re = malloc(sizeof(int32_t) * (size_t)rcap);
     int code_prev = 0, have_first = 0;
     while (p < len) {
       int c = ignore_lowercase ? (unsigned char)buf[p] : toupper((unsigned char)buf[p]);
@@ -131,7 +174,12 @@ int sh_load_reference(const char *path, int colour, int ignore_lowercase, sh_ref
       } else {
         code = (c == 'A') ? 0 : (c == 'C') ? 1 : (c == 'G') ? 2 : 3;
         if (mstart != -1) {
-          if (nr == rcap) { rcap *= 2; rs = realloc(rs, sizeof(int32_t) * (size_t)rcap); re = realloc(re, sizeof(int32_t) * (size_t)rcap); }
+          if (nr == rcap && grow_regions(&rs, &re, &rcap)) {
+            free(ca); free(ma); free(rs); free(re); free(buf);
+            out->n = s + 1;
+            sh_free_reference(out);
+            return fail(STORMGPU_ENOMEM, "Not enough memory for the masked regions of the reference.");
+          }
           rs[nr] = (int32_t)mstart; re[nr] = (int32_t)i; nr++;
           mstart = -1;
         }
@@ -150,7 +198,12 @@ int sh_load_reference(const char *path, int colour, int ignore_lowercase, sh_ref
       }
     }
     if (mstart != -1) {
-      if (nr == rcap) { rcap *= 2; rs = realloc(rs, sizeof(int32_t) * (size_t)rcap); re = realloc(re, sizeof(int32_t) * (size_t)rcap); }
+      if (nr == rcap && grow_regions(&rs, &re, &rcap)) {
+        free(ca); free(ma); free(rs); free(re); free(buf);
+        out->n = s + 1;
+        sh_free_reference(out);
+        return fail(STORMGPU_ENOMEM, "Not enough memory for the masked regions of the reference.");
+      }
       rs[nr] = (int32_t)mstart; re[nr] = (int32_t)i; nr++;
     }
     out->sizes[s] = i;
@@ -174,8 +227,10 @@ int sh_load_reference(const char *path, int colour, int ignore_lowercase, sh_ref
 void sh_free_reference(sh_refs *r) {
   for (int s = 0; s < r->n; ++s) {
     free(r->names ? r->names[s] : NULL);
-    free(r->alloc_codes[s]); free(r->alloc_masks[s]);
-    free(r->rs[s]); free(r->re[s]);
+    if (r->alloc_codes) free(r->alloc_codes[s]);
+    if (r->alloc_masks) free(r->alloc_masks[s]);
+    if (r->rs) free(r->rs[s]);
+    if (r->re) free(r->re[s]);
   }
   free(r->names); free(r->sizes); free(r->codes); free(r->masks); free(r->alloc_codes);
   free(r->alloc_masks); free(r->rs); free(r->re); free(r->nreg); free(r->first_base);
@@ -184,11 +239,15 @@ void sh_free_reference(sh_refs *r) {
 
 /* ---------------------------------------------------------------------------- reads */
 
-typedef struct growbuf { char *p; size_t n, cap; } growbuf;
+typedef struct growbuf { char *p; size_t n, cap; int oom; } growbuf;
 static void gb_put(growbuf *g, const void *src, size_t n) {
+  if (g->oom) return;
   if (g->n + n > g->cap) {
-    g->cap = (g->n + n) * 2 + 4096;
-    g->p = realloc(g->p, g->cap);
+    const size_t cap = (g->n + n) * 2 + 4096;
+    char *p = realloc(g->p, cap);
+    if (!p) { g->oom = 1; return; }
+    g->p = p;
+    g->cap = cap;
   }
   memcpy(g->p + g->n, src, n);
   g->n += n;
@@ -199,6 +258,15 @@ typedef struct rawread {
   int name_len, seq_len, qual_len;
   int has_qual;
 } rawread;
+
+/* doubles the raw-record array; non-zero (array unchanged) when memory runs out */
+static int grow_raw(rawread **rr, int64_t *cap) {
+  rawread *p = realloc(*rr, sizeof(rawread) * (size_t)(2 * *cap));
+  if (!p) return 1;
+  *rr = p;
+  *cap *= 2;
+  return 0;
+}
 
 /* reads_data.c:538-564: printable common prefix of the first and last read names */
 static char *common_name(const char *a, const char *b) {
@@ -219,8 +287,9 @@ static char *common_name(const char *a, const char *b) {
 
 static int next_line(const char *buf, size_t len, size_t *pos, const char **line, size_t *ll) {
   if (*pos >= len) return 0;
-  size_t s = *pos, e = s;
-  while (e < len && buf[e] != '\n') e++;
+  size_t s = *pos;
+  const char *nl = memchr(buf + s, '\n', len - s);
+  size_t e = nl ? (size_t)(nl - buf) : len;
   *line = buf + s;
   *ll = e - s;  /* without '\n' */
   *pos = (e < len) ? e + 1 : e;
@@ -244,9 +313,7 @@ static int header_name_len(const char *line, size_t ll) {
 static int fill_one(sh_reads *out, const char *buf, const rawread *r, int64_t i, int colour, int quality_base,
                     int any_qual, int maxl, short *qv, int report) {
   out->file_index[i] = i;
-  out->names[i] = malloc((size_t)r->name_len + 1);
-  memcpy(out->names[i], buf + r->name_off, (size_t)r->name_len);
-  out->names[i][r->name_len] = 0;
+  out->names[i] = out->arena + r->name_off;  /* NUL-terminated in the arena by fill_reads */
   const char *sq = buf + r->seq_off;
   int L = r->seq_len - (colour ? 2 : 0);
   out->lengths[i] = (int16_t)L;
@@ -293,7 +360,9 @@ static int fill_one(sh_reads *out, const char *buf, const rawread *r, int64_t i,
   return 0;
 }
 
-static int fill_reads(sh_reads *out, const char *buf, rawread *rr, int64_t n, int colour,
+/* buf: the loaded text, which becomes the reads' name arena (each name is NUL-terminated in
+ * place: the byte after a name is a separator of its header line, read by nothing later). */
+static int fill_reads(sh_reads *out, char *buf, rawread *rr, int64_t n, int colour,
                       int quality_base, int allow_mixed, int any_qual) {
   int minl = 1 << 30, maxl = 0;
   for (int64_t i = 0; i < n; ++i) {
@@ -320,20 +389,28 @@ static int fill_reads(sh_reads *out, const char *buf, rawread *rr, int64_t n, in
   out->first_base = calloc((size_t)(n ? n : 1), 1);
   out->first_level = calloc((size_t)(n ? n : 1), 1);
   out->file_index = calloc((size_t)(n ? n : 1), sizeof(int64_t));
+  out->arena = buf;
+  if (!out->codes || (any_qual && !out->levels) || !out->lengths || !out->tags || !out->names || !out->first_base ||
+      !out->first_level || !out->file_index)
+    return fail(STORMGPU_ENOMEM, "Not enough memory for %ld reads.", (long)n);
+  for (int64_t i = 0; i < n; ++i) buf[rr[i].name_off + (size_t)rr[i].name_len] = 0;
   /* reads are independent: filled in parallel; the first failing read (in file order) is filled
    * again alone to report its message, as a sequential pass would */
   int64_t first_bad = n;
-#pragma omp parallel
+  int nomem = 0;
+#pragma omp parallel reduction(|| : nomem)
   {
     short *qv = calloc((size_t)maxl + 2, sizeof(short));
+    if (!qv) nomem = 1;
 #pragma omp for schedule(static) reduction(min : first_bad)
     for (int64_t i = 0; i < n; ++i)
-      if (fill_one(out, buf, &rr[i], i, colour, quality_base, any_qual, maxl, qv, 0)) first_bad = i < first_bad ? i : first_bad;
+      if (qv && fill_one(out, buf, &rr[i], i, colour, quality_base, any_qual, maxl, qv, 0)) first_bad = i < first_bad ? i : first_bad;
     free(qv);
   }
+  if (nomem) return fail(STORMGPU_ENOMEM, "Not enough memory for %ld reads.", (long)n);
   if (first_bad < n) {
     short *qv = calloc((size_t)maxl + 2, sizeof(short));
-    free(out->names[first_bad]);
+    if (!qv) return fail(STORMGPU_ENOMEM, "Not enough memory for %ld reads.", (long)n);
     const int rc = fill_one(out, buf, &rr[first_bad], first_bad, colour, quality_base, any_qual, maxl, qv, 1);
     free(qv);
     return rc;
@@ -343,8 +420,10 @@ static int fill_reads(sh_reads *out, const char *buf, rawread *rr, int64_t n, in
 
 static int load_fastq(const char *path, int colour, int quality_base, int allow_mixed, sh_reads *out) {
   size_t len;
-  char *buf = slurp(path, &len);
-  if (!buf) return fail(STORMGPU_EINVAL, "Failed to read input file %s (read sequences).", path);
+  int oom;
+  memset(out, 0, sizeof(*out));
+  char *buf = slurp(path, &len, &oom);
+  if (!buf) return read_failed(oom, path, "read sequences");
   size_t pos = 0;
   const char *line;
   size_t ll;
@@ -359,6 +438,7 @@ static int load_fastq(const char *path, int colour, int quality_base, int allow_
       size_t nl = strcspn(line + 9, "\r\n");
       if (nl > ll - 9) nl = ll - 9;
       title = malloc(nl + 1);
+      if (!title) { free(buf); return fail(STORMGPU_ENOMEM, "Not enough memory to read %s.", path); }
       memcpy(title, line + 9, nl);
       title[nl] = 0;
     }
@@ -368,6 +448,7 @@ static int load_fastq(const char *path, int colour, int quality_base, int allow_
   pos = rec_start;
   int64_t cap = 1 << 16, n = 0;
   rawread *rr = malloc(sizeof(rawread) * (size_t)cap);
+  if (!rr) { free(buf); free(title); return fail(STORMGPU_ENOMEM, "Not enough memory to read %s.", path); }
   int any_qual = 0;
   int state = 0; /* 0 header, 1 seq, 2 plus, 3 qual */
   while (next_line(buf, len, &pos, &line, &ll)) {
@@ -375,7 +456,7 @@ static int load_fastq(const char *path, int colour, int quality_base, int allow_
     while (l2 > 0 && (line[l2 - 1] == '\r' || line[l2 - 1] == '\n')) l2--;
     if (state == 0) {
       if (ll == 0 || line[0] != '@') { free(rr); free(buf); free(title); return fail(STORMGPU_EINVAL, "Reads file seams corrupt at line %d.", lineno + 1); }
-      if (n == cap) { cap *= 2; rr = realloc(rr, sizeof(rawread) * (size_t)cap); }
+      if (n == cap && grow_raw(&rr, &cap)) { free(rr); free(buf); free(title); return fail(STORMGPU_ENOMEM, "Not enough memory to read %s.", path); }
       rr[n].name_off = (size_t)(line - buf) + 1;
       rr[n].name_len = header_name_len(line, l2);
       rr[n].has_qual = 0;
@@ -401,14 +482,16 @@ static int load_fastq(const char *path, int colour, int quality_base, int allow_
     lineno++;
   }
   if (n == 0) { free(rr); free(buf); free(title); return fail(STORMGPU_EINVAL, "Reads could not be loaded."); }
-  memset(out, 0, sizeof(*out));
   int rc = fill_reads(out, buf, rr, n, colour, quality_base, allow_mixed, any_qual);
   if (rc == 0) {
     if (title) out->db_name = title;
     else out->db_name = common_name(out->names[0], out->names[n - 1]);
-  } else free(title);
+  } else {
+    free(title);
+    if (!out->arena) free(buf);
+    sh_free_reads(out);
+  }
   free(rr);
-  free(buf);
   return rc;
 }
 
@@ -421,8 +504,10 @@ static int load_fastq(const char *path, int colour, int quality_base, int allow_
  * reference parses into one buffer reused across reads, load_data.c:15-33). */
 static int load_fasta(const char *path, const char *qual_path, int colour, int allow_mixed, sh_reads *out) {
   size_t len;
-  char *buf = slurp(path, &len);
-  if (!buf) return fail(STORMGPU_EINVAL, "Failed to read input file %s (read sequences).", path);
+  int oom;
+  memset(out, 0, sizeof(*out));
+  char *buf = slurp(path, &len, &oom);
+  if (!buf) return read_failed(oom, path, "read sequences");
   size_t pos = 0;
   const char *line;
   size_t ll;
@@ -435,6 +520,7 @@ static int load_fasta(const char *path, const char *qual_path, int colour, int a
       size_t nl = strcspn(line + 9, "\r\n");
       if (nl > ll - 9) nl = ll - 9;
       title = malloc(nl + 1);
+      if (!title) { free(buf); return fail(STORMGPU_ENOMEM, "Not enough memory to read %s.", path); }
       memcpy(title, line + 9, nl);
       title[nl] = 0;
     }
@@ -446,6 +532,7 @@ static int load_fasta(const char *path, const char *qual_path, int colour, int a
   growbuf seq = {0};
   int64_t cap = 1 << 16, n = 0;
   rawread *rr = malloc(sizeof(rawread) * (size_t)cap);
+  if (!rr) { free(buf); free(title); return fail(STORMGPU_ENOMEM, "Not enough memory to read %s.", path); }
   size_t name_off = 0;
   int name_len = -1;
   int in_seq = 0;
@@ -455,7 +542,10 @@ static int load_fasta(const char *path, const char *qual_path, int colour, int a
     const int type = ll == 0 || line[0] == '\r' ? 0 : line[0] == '#' ? 0 : line[0] == '>' ? 1 : 2;
     if (type == 2 && name_len >= 0) {
       if (!in_seq) {
-        if (n == cap) { cap *= 2; rr = realloc(rr, sizeof(rawread) * (size_t)cap); }
+        if (n == cap && grow_raw(&rr, &cap)) {
+          free(rr); free(buf); free(seq.p); free(title);
+          return fail(STORMGPU_ENOMEM, "Not enough memory to read %s.", path);
+        }
         rr[n].name_off = name_off;
         rr[n].name_len = name_len;
         rr[n].seq_off = seq.n;
@@ -476,20 +566,24 @@ static int load_fasta(const char *path, const char *qual_path, int colour, int a
     }
   }
   if (n == 0) { free(rr); free(buf); free(seq.p); free(title); return fail(STORMGPU_EINVAL, "Reads could not be loaded."); }
-  /* names live in buf, sequences in seq: copy the names next to the sequences */
-  const size_t names_at = seq.n;
+  /* names live in buf, sequences in seq: copy the names next to the sequences, each followed by
+   * a byte for its terminating NUL */
   for (int64_t i = 0; i < n; ++i) {
     const size_t o = seq.n;
-    gb_put(&seq, buf + rr[i].name_off, (size_t)rr[i].name_len);
+    gb_put(&seq, buf + rr[i].name_off, (size_t)rr[i].name_len + 1);
     rr[i].name_off = o;
   }
-  (void)names_at;
-  memset(out, 0, sizeof(*out));
+  if (seq.oom) {
+    free(rr); free(buf); free(seq.p); free(title);
+    return fail(STORMGPU_ENOMEM, "Not enough memory to read %s.", path);
+  }
   int rc = fill_reads(out, seq.p, rr, n, colour, 33, allow_mixed, 0);
+  if (rc && !out->arena) free(seq.p);
+  seq.p = NULL;
   if (rc == 0 && qual_path) {
     size_t qlen;
-    char *qb = slurp(qual_path, &qlen);
-    if (!qb) rc = fail(STORMGPU_EINVAL, "Failed to read input file %s (quality of read sequences).", qual_path);
+    char *qb = slurp(qual_path, &qlen, &oom);
+    if (!qb) rc = read_failed(oom, qual_path, "quality of read sequences");
     else {
       out->has_quality = 1;
       out->levels = calloc((size_t)n, (size_t)out->level_stride);
@@ -498,6 +592,10 @@ static int load_fasta(const char *path, const char *qual_path, int colour, int a
       size_t qp = 0;
       int64_t i = 0;
       char *tmp = malloc(qlen + 1);
+      if (!out->levels || !qv || !tmp) {
+        rc = fail(STORMGPU_ENOMEM, "Not enough memory to read %s.", qual_path);
+        i = n;  /* nothing is parsed */
+      }
       while (i < n && next_line(qb, qlen, &qp, &line, &ll)) {
         if (ll == 0 || line[0] == '\r' || line[0] == '#' || line[0] == '>') continue;
         memcpy(tmp, line, ll);
@@ -519,9 +617,11 @@ static int load_fasta(const char *path, const char *qual_path, int colour, int a
   if (rc == 0) {
     if (title) out->db_name = title;
     else out->db_name = common_name(out->names[0], out->names[n - 1]);
-  } else free(title);
+  } else {
+    free(title);
+    sh_free_reads(out);
+  }
   free(rr);
-  free(seq.p);
   free(buf);
   return rc;
 }
@@ -535,7 +635,7 @@ int sh_load_reads(const char *path, const char *qual_path, int colour, int quali
 }
 
 void sh_free_reads(sh_reads *r) {
-  for (int64_t i = 0; i < r->n; ++i) free(r->names[i]);
+  free(r->arena);
   free(r->names); free(r->codes); free(r->levels); free(r->lengths); free(r->tags);
   free(r->first_base); free(r->first_level); free(r->file_index); free(r->db_name);
   memset(r, 0, sizeof(*r));
@@ -544,46 +644,83 @@ void sh_free_reads(sh_reads *r) {
 /* ---------------------------------------------------------------------------- ordering */
 
 /* order: length, then tag, then file position */
-typedef struct sortkey { int16_t len; uint64_t tag; int64_t idx; } sortkey;
+typedef struct sortkey { uint64_t tag; uint32_t idx; uint16_t len; } sortkey;
 
-void sh_sort_reads(sh_reads *r) {
-  int64_t n = r->n;
-  sortkey *k = malloc(sizeof(sortkey) * (size_t)(n ? n : 1));
-  for (int64_t i = 0; i < n; ++i) { k[i].len = r->lengths[i]; k[i].tag = r->tags[i]; k[i].idx = i; }
-  /* stable LSD radix sort on (length, tag), 16-bit digits of the tag first: from file order,
-   * equal keys keep file order.  Digits that are the same for every read are skipped. */
-  if (n > 0) {
-    uint64_t vt = 0;
-    uint16_t vl = 0;
-    for (int64_t i = 0; i < n; ++i) {
-      vt |= k[i].tag ^ k[0].tag;
-      vl |= (uint16_t)(k[i].len ^ k[0].len);
+/* One stable counting pass on digit d (8 bits) of every key, from `a` into `b`: each thread
+ * counts its contiguous block, the counts are laid out bucket-major (bucket, thread), and every
+ * thread scatters its block in order, so equal digits keep their order. */
+static void radix_pass(const sortkey *a, sortkey *b, int64_t n, int d, int nt, int64_t *cnt) {
+#define SK_DIGIT(x) (d < 8 ? (int)(((x).tag >> (8 * d)) & 0xff) : (int)(((x).len >> (8 * (d - 8))) & 0xff))
+  memset(cnt, 0, sizeof(int64_t) * 256 * (size_t)nt);
+#pragma omp parallel num_threads(nt)
+  {
+    const int t = omp_get_thread_num();
+    const int64_t lo = n * t / nt, hi = n * (t + 1) / nt;
+    int64_t *c = cnt + 256 * t;
+    for (int64_t i = lo; i < hi; ++i) c[SK_DIGIT(a[i])]++;
+#pragma omp barrier
+#pragma omp single
+    {
+      int64_t acc = 0;
+      for (int v = 0; v < 256; ++v)
+        for (int u = 0; u < nt; ++u) {
+          const int64_t x = cnt[256 * u + v];
+          cnt[256 * u + v] = acc;
+          acc += x;
+        }
     }
-    sortkey *t = malloc(sizeof(sortkey) * (size_t)n);
-    int64_t *cnt = malloc(sizeof(int64_t) * 65537);
-    for (int pass = 0; pass < 5; ++pass) {
-      if (pass < 4 ? ((vt >> (16 * pass)) & 0xffff) == 0 : vl == 0) continue;
-#define SK_DIGIT(x) (pass < 4 ? (int)(((x).tag >> (16 * pass)) & 0xffff) : (int)(uint16_t)(x).len)
-      memset(cnt, 0, sizeof(int64_t) * 65537);
-      for (int64_t i = 0; i < n; ++i) cnt[SK_DIGIT(k[i]) + 1]++;
-      for (int b = 0; b < 65536; ++b) cnt[b + 1] += cnt[b];
-      for (int64_t i = 0; i < n; ++i) t[cnt[SK_DIGIT(k[i])]++] = k[i];
-#undef SK_DIGIT
-      sortkey *sw = k; k = t; t = sw;
-    }
-    free(cnt);
-    free(t);
+    for (int64_t i = lo; i < hi; ++i) b[c[SK_DIGIT(a[i])]++] = a[i];
   }
-  uint8_t *codes = malloc((size_t)(n ? n : 1) * (size_t)r->code_stride);
-  uint8_t *levels = r->levels ? malloc((size_t)(n ? n : 1) * (size_t)r->level_stride) : NULL;
-  int16_t *lengths = malloc(sizeof(int16_t) * (size_t)(n ? n : 1));
-  uint64_t *tags = malloc(sizeof(uint64_t) * (size_t)(n ? n : 1));
-  char **names = malloc(sizeof(char *) * (size_t)(n ? n : 1));
-  uint8_t *fb = malloc((size_t)(n ? n : 1)), *fl = malloc((size_t)(n ? n : 1));
-  int64_t *fi = malloc(sizeof(int64_t) * (size_t)(n ? n : 1));
-#pragma omp parallel for schedule(static)
+#undef SK_DIGIT
+}
+
+/* reads_data.c:59-67 (a stable sort by tag) per read length, lengths ascending: a stable LSD
+ * radix sort on (length, tag) from file order, 8-bit digits, parallel passes; digits that are
+ * the same for every read are skipped.  The read arrays are then permuted in parallel.
+ * Returns 0, or STORMGPU_ENOMEM (reads unchanged). */
+int sh_sort_reads(sh_reads *r) {
+  const int64_t n = r->n;
+  if (n <= 1) return 0;
+  if (n > (int64_t)UINT32_MAX) return fail(STORMGPU_EINVAL, "More than %u reads in one file.", UINT32_MAX);
+  int nt = 1;
+#ifdef _OPENMP
+  nt = omp_get_max_threads();
+#endif
+  if (nt > 64) nt = 64;
+  if (n < 65536) nt = 1;
+  sortkey *k = malloc(sizeof(sortkey) * (size_t)n), *t = malloc(sizeof(sortkey) * (size_t)n);
+  int64_t *cnt = malloc(sizeof(int64_t) * 256 * (size_t)nt);
+  uint8_t *codes = malloc((size_t)n * (size_t)r->code_stride);
+  uint8_t *levels = r->levels ? malloc((size_t)n * (size_t)r->level_stride) : NULL;
+  int16_t *lengths = malloc(sizeof(int16_t) * (size_t)n);
+  uint64_t *tags = malloc(sizeof(uint64_t) * (size_t)n);
+  char **names = malloc(sizeof(char *) * (size_t)n);
+  uint8_t *fb = malloc((size_t)n), *fl = malloc((size_t)n);
+  int64_t *fi = malloc(sizeof(int64_t) * (size_t)n);
+  if (!k || !t || !cnt || !codes || (r->levels && !levels) || !lengths || !tags || !names || !fb || !fl || !fi) {
+    free(k); free(t); free(cnt); free(codes); free(levels); free(lengths); free(tags); free(names);
+    free(fb); free(fl); free(fi);
+    return fail(STORMGPU_ENOMEM, "Not enough memory to sort %ld reads.", (long)n);
+  }
+  uint64_t vt = 0;
+  uint16_t vl = 0;
+#pragma omp parallel for schedule(static) reduction(| : vt, vl) num_threads(nt)
   for (int64_t i = 0; i < n; ++i) {
-    int64_t s = k[i].idx;
+    k[i].tag = r->tags[i];
+    k[i].len = (uint16_t)r->lengths[i];
+    k[i].idx = (uint32_t)i;
+    vt |= r->tags[i] ^ r->tags[0];
+    vl |= (uint16_t)(r->lengths[i] ^ r->lengths[0]);
+  }
+  for (int d = 0; d < 10; ++d) {
+    const int varies = d < 8 ? ((vt >> (8 * d)) & 0xff) != 0 : ((vl >> (8 * (d - 8))) & 0xff) != 0;
+    if (!varies) continue;
+    radix_pass(k, t, n, d, nt, cnt);
+    sortkey *sw = k; k = t; t = sw;
+  }
+#pragma omp parallel for schedule(static) num_threads(nt)
+  for (int64_t i = 0; i < n; ++i) {
+    const int64_t s = k[i].idx;
     memcpy(codes + i * r->code_stride, r->codes + s * r->code_stride, (size_t)r->code_stride);
     if (levels) memcpy(levels + i * r->level_stride, r->levels + s * r->level_stride, (size_t)r->level_stride);
     lengths[i] = r->lengths[s]; tags[i] = r->tags[s]; names[i] = r->names[s];
@@ -593,7 +730,8 @@ void sh_sort_reads(sh_reads *r) {
   free(r->first_base); free(r->first_level); free(r->file_index);
   r->codes = codes; r->levels = levels; r->lengths = lengths; r->tags = tags; r->names = names;
   r->first_base = fb; r->first_level = fl; r->file_index = fi;
-  free(k);
+  free(k); free(t); free(cnt);
+  return 0;
 }
 
 void sh_reads_view(const sh_reads *r, stormgpu_reads *v) {

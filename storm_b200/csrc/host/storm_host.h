@@ -52,6 +52,7 @@ typedef struct sh_reads {
   uint8_t  *first_base;    /* colour: real first base (TRANSFORM(primer, colour 1)) */
   uint8_t  *first_level;   /* colour: level of the first colour's quality */
   int64_t  *file_index;    /* original position in the file */
+  char     *arena;         /* the names[] strings live here (one allocation) */
 } sh_reads;
 
 /* Status: 0 ok, negative on error (message in sh_last_error()). */
@@ -67,8 +68,8 @@ int  sh_load_reads(const char *path, const char *qual_path, int colour, int qual
 void sh_free_reads(sh_reads *r);
 
 /* Stable sort by (length, tag): within one length, the order of the reference's qsort by tag
- * with ties in file order (reads_data.c:41-67). */
-void sh_sort_reads(sh_reads *r);
+ * with ties in file order (reads_data.c:41-67).  0, or STORMGPU_ENOMEM (reads unchanged). */
+int sh_sort_reads(sh_reads *r);
 
 /* The reads as the C ABI expects them. */
 void sh_reads_view(const sh_reads *r, stormgpu_reads *view);

@@ -25,7 +25,8 @@ class ShReads(C.Structure):
                 ("has_quality", C.c_int), ("db_name", C.c_char_p), ("names", C.c_void_p),
                 ("codes", C.c_void_p), ("code_stride", C.c_int64), ("levels", C.c_void_p),
                 ("level_stride", C.c_int64), ("lengths", C.c_void_p), ("tags", C.c_void_p),
-                ("first_base", C.c_void_p), ("first_level", C.c_void_p), ("file_index", C.c_void_p)]
+                ("first_base", C.c_void_p), ("first_level", C.c_void_p), ("file_index", C.c_void_p),
+                ("arena", C.c_void_p)]
 
 
 _h = None
@@ -96,7 +97,9 @@ class ReadSet:
         if rc:
             raise api.StormError(hostlib().sh_last_error().decode())
         if sort:
-            hostlib().sh_sort_reads(C.byref(self._s))
+            rc = hostlib().sh_sort_reads(C.byref(self._s))
+            if rc:
+                raise api.StormError(hostlib().sh_last_error().decode())
         s = self._s
         self.n = s.n
         self.max_len = s.max_len
