@@ -46,7 +46,8 @@ static char *slurp(const char *path, size_t *len, int *oom) {
   if (!f) return NULL;
   struct stat st;
   size_t cap = 1 << 20, n = 0;
-  if (fstat(fileno(f), &st) == 0 && S_ISREG(st.st_mode) && st.st_size > 0) cap = (size_t)st.st_size;
+  /* one byte more than the file: the read that finds the end needs no larger buffer */
+  if (fstat(fileno(f), &st) == 0 && S_ISREG(st.st_mode) && st.st_size > 0) cap = (size_t)st.st_size + 1;
   char *buf = malloc(cap + 1);
   if (!buf) { fclose(f); *oom = 1; return NULL; }
   for (;;) {
