@@ -345,7 +345,9 @@ __global__ void __launch_bounds__(kGWarps * 32, 8) gather_fused_kernel(ReadsDev 
     const uint8_t* read = rs;
     const int T = so[nseeds];
     int H = 0;
-    for (int r0 = 0; r0 < T; r0 += 32 * kItems) {
+    // a read with more positions than the warp holds stops here and goes to the block kernel,
+    // which looks it up again (its lookups and positions are counted there)
+    for (int r0 = 0; r0 < T && H <= cap; r0 += 32 * kItems) {
       // every lane looks up its items (all key-table loads in flight together) ...
       int a[kItems], cnt[kItems], rp[kItems], sid[kItems];
 #pragma unroll
@@ -356,7 +358,6 @@ __global__ void __launch_bounds__(kGWarps * 32, 8) gather_fused_kernel(ReadsDev 
           while (it >= so[si + 1]) ++si;
         sid[m] = si;
         item_lookup(s_first[si], gs.s[si], it < T ? it - so[si] : 0x40000000, read, L, a[m], cnt[m], rp[m]);
-        lookups += it < T ? 1 : 0;
       }
       // ... then one scan places all of them, and the position loads go out together
       int tot = 0;
@@ -368,6 +369,7 @@ __global__ void __launch_bounds__(kGWarps * 32, 8) gather_fused_kernel(ReadsDev 
 #pragma unroll
       for (int m = 1; m < kItems; ++m) dst[m] = dst[m - 1] + cnt[m - 1];
       H += __shfl_sync(0xffffffffu, incl, 31);
+      if (H > cap) break;  // uniform over the warp
 #pragma unroll
       for (int m = 0; m < kItems; ++m) {
         if (cnt[m] <= 8) {
@@ -395,12 +397,13 @@ __global__ void __launch_bounds__(kGWarps * 32, 8) gather_fused_kernel(ReadsDev 
         }
       }
     }
-    positions += (unsigned long long)H;
     if (H > cap) {
       if (lane == 0) go.big_list[atomicAdd(go.big_count, 1)] = (int32_t)r;
       __syncwarp();
       continue;
     }
+    positions += (unsigned long long)H;
+    lookups += (unsigned long long)T;
     __syncwarp();
     if (H <= 32) {
       sort_emit_regs<1>(s, H, I, (int)r, go);
@@ -412,100 +415,212 @@ __global__ void __launch_bounds__(kGWarps * 32, 8) gather_fused_kernel(ReadsDev 
     __syncwarp();
   }
   }
-  for (int o = 16; o > 0; o >>= 1) lookups += __shfl_xor_sync(0xffffffffu, lookups, o);
-  if (lane == 0) {
+  if (lane == 0) {  // both counts are the same in every lane of the warp
     atomicAdd(&go.counters[3], lookups);
     atomicAdd(&go.counters[4], positions);
   }
 }
 
-// One block per read: the same steps with a block-wide scan, in dynamic shared memory (`cap`
-// positions) or, when gbuf is given, in that global buffer.  Reads with more than `cap`
-// positions are recorded in the huge list with their count.
-__global__ void gather_block_kernel(ReadsDev rd, IndexView ix, int I, const int32_t* __restrict__ list, GatherOut go,
-                                    int cap, int32_t* gbuf, int32_t* huge_list, int32_t* huge_h, int32_t* huge_count,
-                                    const __grid_constant__ SeedSet gs) {
-  extern __shared__ int32_t dsm[];
-  __shared__ int wtot[32];
-  __shared__ int s_H;
-  int32_t* s = gbuf ? gbuf : dsm;
-  const int r = list[blockIdx.x];
-  const int L = rd.lengths[r];
-  const uint8_t* read = rd.codes + (int64_t)r * rd.cstride;
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  if (threadIdx.x == 0) s_H = 0;
+// One block per read of the list, for reads with more index positions than a warp holds: the
+// positions go to a block-private slice of a global buffer (scratch: 2 * cap words per block,
+// its working set small enough to stay in L2), then a bucket sort without comparisons across
+// buckets: min / max, buckets of equal power-of-two width over [min, max] (about 8 values each,
+// so that bucket order is value order), counted and scattered with shared atomics, then every
+// thread insertion-sorts its buckets, dropping repeated values on the way.  The surviving
+// diagonals are appended in order; the smallest is dropped when it is not above -I
+// (run.c:617, :648).  Reads with more than `cap` positions are appended to (huge_list,
+// huge_h) for a second launch with a larger cap.  The grid is persistent: blocks take the next
+// read of the list from `cursor` (zeroed), list_count read on the device when given.
+constexpr int kBT = 512;              // threads of a block-gather block
+constexpr int kMaxBuckets = 4096;
+
+// exclusive scan of a[0..n) in place (n <= kMaxBuckets, every thread of the block); the total
+__device__ __forceinline__ int block_excl_scan(int32_t* a, int n, int* wtot) {
+  constexpr int per = kMaxBuckets / kBT;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int b0 = threadIdx.x * per;
+  int loc = 0;
+#pragma unroll
+  for (int k = 0; k < per; ++k)
+    if (b0 + k < n) loc += a[b0 + k];
+  const int incl = warp_incl_scan(loc);
+  if (lane == 31) wtot[w] = incl;
   __syncthreads();
-  for (int si = 0; si < gs.n; ++si) {
-    const int np = seed_npos(gs.s[si], L);
-    const int32_t* mp = ix.map[si];
-    for (int t0 = 0; t0 < np; t0 += blockDim.x) {
-      int a, cnt, rp;
-      seed_item(gs, ix, si, t0 + threadIdx.x, read, L, a, cnt, rp);
-      const int incl = warp_incl_scan(cnt);
-      if (lane == 31) wtot[w] = incl;
-      __syncthreads();
-      int before = 0, tot = 0;
-      for (int q = 0; q < nw; ++q) { if (q < w) before += wtot[q]; tot += wtot[q]; }
-      const int dst = s_H + before + incl - cnt;
-      for (int u = 0; u < cnt; ++u)
-        if (dst + u < cap) s[dst + u] = __ldg(mp + a + u) - rp;
-      __syncthreads();
-      if (threadIdx.x == 0) s_H += tot;
-      __syncthreads();
-    }
+  int before = 0, tot = 0;
+  for (int q = 0; q < kBT / 32; ++q) {
+    if (q < w) before += wtot[q];
+    tot += wtot[q];
   }
-  const int H = s_H;
-  if (H > cap) {
+  int run = before + incl - loc;
+#pragma unroll
+  for (int k = 0; k < per; ++k)
+    if (b0 + k < n) {
+      const int v = a[b0 + k];
+      a[b0 + k] = run;
+      run += v;
+    }
+  __syncthreads();
+  return tot;
+}
+
+__global__ void __launch_bounds__(kBT) gather_block_kernel(ReadsDev rd, IndexView ix, int I, const int32_t* __restrict__ list,
+                                                           const int32_t* __restrict__ list_count, int64_t nlist,
+                                                           GatherOut go, int32_t* __restrict__ scratch, int cap,
+                                                           unsigned long long* cursor, int32_t* huge_list, int32_t* huge_h,
+                                                           int32_t* huge_count, const __grid_constant__ SeedSet gs) {
+  __shared__ int32_t cnt[kMaxBuckets];   // per bucket: count, start, then end
+  __shared__ int32_t uoff[kMaxBuckets];  // per bucket: distinct values, then their offset
+  __shared__ int wtot[kBT / 32];
+  __shared__ int s_read, s_H;
+  __shared__ int32_t s_min, s_max;
+  __shared__ unsigned long long s_base;
+  __shared__ __align__(16) uint8_t srd[kReadBytes];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  int32_t* A = scratch + (int64_t)blockIdx.x * 2 * cap;
+  int32_t* B = A + cap;
+  const int64_t n = list_count ? (int64_t)*list_count : nlist;
+  unsigned long long lookups = 0, positions = 0;
+  for (;;) {
     if (threadIdx.x == 0) {
-      const int k = atomicAdd(huge_count, 1);
-      huge_list[k] = r;
-      huge_h[k] = H;
+      const unsigned long long k = atomicAdd(cursor, 1ull);
+      s_read = (int64_t)k < n ? list[k] : -1;
+      s_H = 0;
+      s_min = 0x7fffffff;
+      s_max = (int32_t)0x80000000;
     }
-    return;
-  }
-  int P = 1;
-  while (P < H) P <<= 1;
-  for (int i = H + threadIdx.x; i < P; i += blockDim.x) s[i] = 0x7fffffff;
-  __syncthreads();
-  for (int k = 2; k <= P; k <<= 1)
-    for (int j = k >> 1; j > 0; j >>= 1) {
-      for (int i = threadIdx.x; i < P; i += blockDim.x) {
-        const int ixj = i ^ j;
-        if (ixj > i) {
-          const int32_t x = s[i], y = s[ixj];
-          if ((x > y) == ((i & k) == 0)) { s[i] = y; s[ixj] = x; }
+    __syncthreads();
+    const int r = s_read;
+    if (r < 0) break;
+    const int L = rd.lengths[r];
+    {
+      const uint8_t* src = rd.codes + (int64_t)r * rd.cstride;
+      const int nbytes = (L + 3) >> 2;
+      for (int b = threadIdx.x; b < kReadBytes; b += kBT) srd[b] = b < nbytes ? src[b] : 0;
+    }
+    __syncthreads();
+    // gather: every (seed, read position) item's CSR range, placed by a block scan
+    int T = 0;
+    for (int si = 0; si < gs.n; ++si) {
+      const int np = seed_npos(gs.s[si], L);
+      T += np;
+      const int32_t* first = ix.first[si];
+      const int32_t* mp = ix.map[si];
+      for (int t0 = 0; t0 < np; t0 += kBT) {
+        int a, c, rp;
+        item_lookup(first, gs.s[si], t0 + threadIdx.x, srd, L, a, c, rp);
+        const int incl = warp_incl_scan(c);
+        if (lane == 31) wtot[w] = incl;
+        __syncthreads();
+        int before = 0, tot = 0;
+        for (int q = 0; q < kBT / 32; ++q) {
+          if (q < w) before += wtot[q];
+          tot += wtot[q];
         }
+        const int dst = s_H + before + incl - c;
+        if (c <= 8) {
+          for (int u = 0; u < c; ++u)
+            if (dst + u < cap) A[dst + u] = __ldg(mp + a + u) - rp;
+        }
+        unsigned bm = __ballot_sync(0xffffffffu, c > 8);  // long lists: the warp copies each
+        while (bm) {
+          const int j = __ffs(bm) - 1;
+          bm &= bm - 1;
+          const int aj = __shfl_sync(0xffffffffu, a, j), cj = __shfl_sync(0xffffffffu, c, j);
+          const int dj = __shfl_sync(0xffffffffu, dst, j), rj = __shfl_sync(0xffffffffu, rp, j);
+          for (int u = lane; u < cj; u += 32)
+            if (dj + u < cap) A[dj + u] = __ldg(mp + aj + u) - rj;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) s_H += tot;
+        __syncthreads();
+      }
+    }
+    const int H = s_H;
+    lookups += (unsigned long long)T;
+    positions += (unsigned long long)H;
+    if (H > cap) {
+      if (threadIdx.x == 0) {
+        const int k = atomicAdd(huge_count, 1);
+        huge_list[k] = r;
+        huge_h[k] = H;
       }
       __syncthreads();
+      continue;
     }
-  // de-duplicate in chunks of blockDim, appending in order
-  const unsigned lt = (1u << lane) - 1u;
-  int U = 0;
-  for (int t0 = 0; t0 < H; t0 += blockDim.x) {
-    const int t = t0 + threadIdx.x;
-    const int32_t v = t < H ? s[t] : 0;
-    const int32_t prev = t == 0 ? -I : (t < H ? s[t - 1] : 0);
-    const bool keep = t < H && v > prev;
-    const unsigned m = __ballot_sync(0xffffffffu, keep);
-    if (lane == 0) wtot[w] = __popc(m);
+    if (H == 0) {
+      __syncthreads();
+      continue;
+    }
+    // range
+    int32_t vmin = 0x7fffffff, vmax = (int32_t)0x80000000;
+    for (int i = threadIdx.x; i < H; i += kBT) {
+      const int32_t v = A[i];
+      vmin = min(vmin, v);
+      vmax = max(vmax, v);
+    }
+    vmin = __reduce_min_sync(0xffffffffu, vmin);
+    vmax = __reduce_max_sync(0xffffffffu, vmax);
+    if (lane == 0) {
+      atomicMin(&s_min, vmin);
+      atomicMax(&s_max, vmax);
+    }
     __syncthreads();
-    int before = 0, tot = 0;
-    for (int q = 0; q < nw; ++q) { if (q < w) before += wtot[q]; tot += wtot[q]; }
-    if (keep) s[U + before + __popc(m & lt)] = v;
-    U += tot;
+    vmin = s_min;
+    const uint32_t range = (uint32_t)s_max - (uint32_t)vmin;
+    int nb = 1;
+    while (nb < kMaxBuckets && nb * 8 < H) nb <<= 1;
+    int shift = 0;
+    while ((range >> shift) >= (uint32_t)nb) ++shift;
+    for (int b = threadIdx.x; b < nb; b += kBT) cnt[b] = 0;
+    __syncthreads();
+    for (int i = threadIdx.x; i < H; i += kBT) atomicAdd(&cnt[((uint32_t)A[i] - (uint32_t)vmin) >> shift], 1);
+    __syncthreads();
+    block_excl_scan(cnt, nb, wtot);
+    for (int i = threadIdx.x; i < H; i += kBT) {
+      const int32_t v = A[i];
+      B[atomicAdd(&cnt[((uint32_t)v - (uint32_t)vmin) >> shift], 1)] = v;
+    }
+    __syncthreads();  // cnt[b] is now the end of bucket b
+    for (int b = threadIdx.x; b < nb; b += kBT) {
+      const int s0 = b ? cnt[b - 1] : 0, e = cnt[b];
+      int u = 0;
+      for (int x = s0; x < e; ++x) {  // insertion into the sorted distinct prefix B[s0, s0 + u)
+        const int32_t t = B[x];
+        int y = u - 1;
+        while (y >= 0 && B[s0 + y] > t) --y;
+        if (y >= 0 && B[s0 + y] == t) continue;
+        for (int z = u - 1; z > y; --z) B[s0 + z + 1] = B[s0 + z];
+        B[s0 + y + 1] = t;
+        ++u;
+      }
+      uoff[b] = u;
+    }
+    __syncthreads();
+    const int U = block_excl_scan(uoff, nb, wtot);
+    for (int b = threadIdx.x; b < nb; b += kBT) {
+      const int s0 = b ? cnt[b - 1] : 0, o = uoff[b];
+      const int u = (b + 1 < nb ? uoff[b + 1] : U) - o;
+      for (int k = 0; k < u; ++k) A[o + k] = B[s0 + k];
+    }
+    __syncthreads();
+    const int drop = A[0] <= -I ? 1 : 0;  // the first diagonal must exceed -I (run.c:617, :648)
+    const int Uo = U - drop;
+    if (threadIdx.x == 0) s_base = Uo ? atomicAdd(&go.counters[7], (unsigned long long)Uo) : 0ull;
+    __syncthreads();
+    const unsigned long long base = s_base;
+    if ((int64_t)(base + Uo) > go.cap) {
+      if (threadIdx.x == 0) atomicExch(&go.counters[8], 1ull);
+    } else {
+      for (int k = threadIdx.x; k < Uo; k += kBT) {
+        go.fr[base + k] = r;
+        go.fd[base + k] = A[k + drop];
+      }
+    }
     __syncthreads();
   }
-  __shared__ unsigned long long s_base;
-  if (threadIdx.x == 0) s_base = U ? atomicAdd(&go.counters[7], (unsigned long long)U) : 0ull;
-  __syncthreads();
-  const unsigned long long base = s_base;
-  if ((int64_t)(base + U) > go.cap) {
-    if (threadIdx.x == 0) atomicExch(&go.counters[8], 1ull);
-    return;
-  }
-  for (int k = threadIdx.x; k < U; k += blockDim.x) {
-    go.fr[base + k] = r;
-    go.fd[base + k] = s[k];
+  if (threadIdx.x == 0) {
+    atomicAdd(&go.counters[3], lookups);
+    atomicAdd(&go.counters[4], positions);
   }
 }
 
@@ -520,18 +635,15 @@ void launch_gather_fused(const ReadsDev& rd, const IndexView& ix, int I, const G
   gather_fused_kernel<<<(unsigned)blocks, kGWarps * 32, smem, st>>>(rd, ix, I, go, seeds);
 }
 
-void launch_gather_block(const ReadsDev& rd, const IndexView& ix, int I, const int32_t* list, int nlist,
-                         const GatherOut& go, int32_t* gbuf, int gcap, int32_t* huge_list, int32_t* huge_h,
-                         int32_t* huge_count, const SeedSet& seeds, cudaStream_t st) {
-  if (nlist <= 0) return;
-  const int smem_cap = kBlockGatherCap;
-  set_smem_attribute_once(reinterpret_cast<const void*>(gather_block_kernel), kBlockGatherCap * 4);
-  if (gbuf)
-    gather_block_kernel<<<nlist, 1024, 0, st>>>(rd, ix, I, list, go, gcap, gbuf, huge_list, huge_h, huge_count,
-                                                 seeds);
-  else
-    gather_block_kernel<<<nlist, 1024, smem_cap * 4, st>>>(rd, ix, I, list, go, smem_cap, nullptr, huge_list,
-                                                              huge_h, huge_count, seeds);
+int64_t gather_block_grid() { return resident_grid(gather_block_kernel, kBT, 0); }
+
+void launch_gather_block(const ReadsDev& rd, const IndexView& ix, int I, const int32_t* list, int64_t nlist,
+                         const GatherOut& go, int32_t* scratch, int cap, int64_t grid, unsigned long long* cursor,
+                         int32_t* huge_list, int32_t* huge_h, int32_t* huge_count, const SeedSet& seeds,
+                         cudaStream_t st) {
+  if (nlist <= 0 || grid <= 0) return;
+  gather_block_kernel<<<(unsigned)grid, kBT, 0, st>>>(rd, ix, I, list, nullptr, nlist, go, scratch, cap, cursor,
+                                                      huge_list, huge_h, huge_count, seeds);
 }
 
 }  // namespace sg

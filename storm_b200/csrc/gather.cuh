@@ -20,16 +20,19 @@ struct GatherOut {
 
 constexpr int kMaxWarpCap = 1536;
 
-constexpr int kBlockGatherCap = 32768;
+constexpr int kBlockGatherCap = 65536;
 
 // The seed family travels with every launch (a kernel parameter), so that mapping calls with
 // different seed families can run concurrently on different streams.
 void launch_gather_fused(const ReadsDev& rd, const IndexView& ix, int I, const GatherOut& go, const SeedSet& seeds,
                          cudaStream_t st);
-// one block per listed read; gbuf == nullptr: shared memory (kBlockGatherCap positions),
-// reads beyond it are appended to (huge_list, huge_h); else the global buffer gbuf of gcap.
-void launch_gather_block(const ReadsDev& rd, const IndexView& ix, int I, const int32_t* list, int nlist,
-                         const GatherOut& go, int32_t* gbuf, int gcap, int32_t* huge_list, int32_t* huge_h,
-                         int32_t* huge_count, const SeedSet& seeds, cudaStream_t st);
+// The nlist reads of `list`, a persistent grid of `grid` blocks (at most gather_block_grid()
+// useful) taking reads from the zeroed `cursor`; scratch holds 2 * cap words per block.  Reads
+// with more than `cap` positions are appended to (huge_list, huge_h) with their count.
+void launch_gather_block(const ReadsDev& rd, const IndexView& ix, int I, const int32_t* list, int64_t nlist,
+                         const GatherOut& go, int32_t* scratch, int cap, int64_t grid, unsigned long long* cursor,
+                         int32_t* huge_list, int32_t* huge_h, int32_t* huge_count, const SeedSet& seeds,
+                         cudaStream_t st);
+int64_t gather_block_grid();
 
 }  // namespace sg

@@ -318,7 +318,7 @@ static int map_device_once(stormgpu_ctx* c, const stormgpu_reads* reads, stormgp
     rev.levels = reads->levels ? c->rlevels.p : nullptr;
   }
   if (c->pstart.grow(n) || c->pcount.grow(n) || c->scan_tmp64.grow(scan_tmp_elems(n) + 8) ||
-      c->big_list.grow(n) || c->huge_list.grow(n) || c->huge_h.grow(n) || c->big_count.grow(2) ||
+      c->big_list.grow(n) || c->huge_list.grow(2 * n) || c->huge_h.grow(2 * n) || c->big_count.grow(2) ||
       c->counters.grow(32) || c->fr.grow(std::max<int64_t>(n * 64, 1 << 20)) ||
       c->fd.grow(std::max<int64_t>(n * 64, 1 << 20)))
     return STORMGPU_ENOMEM;
@@ -353,25 +353,29 @@ static int map_device_once(stormgpu_ctx* c, const stormgpu_reads* reads, stormgp
         int32_t nbig[2] = {0, 0};
         SG_CUDA(cudaMemcpyAsync(nbig, c->big_count.p, sizeof(nbig), cudaMemcpyDeviceToHost, st));
         SG_CUDA(cudaStreamSynchronize(st));
-        if (nbig[0] > 0) {
-          launch_gather_block(rd, ix, sp.I, c->big_list.p, nbig[0], go, nullptr, 0, c->huge_list.p, c->huge_h.p,
-                              c->big_count.p + 1, c->seeds, st);
+        if (nbig[0] > 0) {  // reads with more positions than a warp holds: a block each
+          const int64_t grid = std::min<int64_t>(nbig[0], gather_block_grid());
+          if (c->big_tmp.grow(grid * 2 * (int64_t)kBlockGatherCap)) return STORMGPU_ENOMEM;
+          launch_gather_block(rd, ix, sp.I, c->big_list.p, nbig[0], go, c->big_tmp.p, kBlockGatherCap, grid,
+                              c->counters.p + 14, c->huge_list.p, c->huge_h.p, c->big_count.p + 1, c->seeds, st);
           launches++;
           SG_CUDA(cudaMemcpyAsync(nbig, c->big_count.p, sizeof(nbig), cudaMemcpyDeviceToHost, st));
           SG_CUDA(cudaStreamSynchronize(st));
-          if (nbig[1] > 0) {
-            std::vector<int32_t> hl(nbig[1]), hh(nbig[1]);
-            SG_CUDA(cudaMemcpyAsync(hl.data(), c->huge_list.p, sizeof(int32_t) * nbig[1], cudaMemcpyDeviceToHost, st));
+          if (nbig[1] > 0) {  // beyond kBlockGatherCap: the same with a slice of the largest read's size
+            std::vector<int32_t> hh(nbig[1]);
             SG_CUDA(cudaMemcpyAsync(hh.data(), c->huge_h.p, sizeof(int32_t) * nbig[1], cudaMemcpyDeviceToHost, st));
             SG_CUDA(cudaStreamSynchronize(st));
-            for (int k = 0; k < nbig[1]; ++k) {
-              int64_t P = 1;
-              while (P < hh[k]) P <<= 1;
-              if (c->big_tmp.grow(P)) return STORMGPU_ENOMEM;
-              launch_gather_block(rd, ix, sp.I, c->huge_list.p + k, 1, go, c->big_tmp.p, (int)P, c->huge_list.p,
-                                  c->huge_h.p, c->big_count.p + 1, c->seeds, st);
-              launches++;
-            }
+            int64_t cap2 = kBlockGatherCap;
+            for (int k = 0; k < nbig[1]; ++k) while (cap2 < hh[k]) cap2 <<= 1;
+            if (cap2 > (int64_t)1 << 30) { sg_set_error("a read has %lld index positions", (long long)cap2); return STORMGPU_EINVAL; }
+            // at most 1 GiB of slices
+            const int64_t grid2 = std::max<int64_t>(1, std::min<int64_t>({(int64_t)nbig[1], gather_block_grid(),
+                                                                           ((int64_t)1 << 27) / cap2}));
+            if (c->big_tmp.grow(grid2 * 2 * cap2)) return STORMGPU_ENOMEM;
+            launch_gather_block(rd, ix, sp.I, c->huge_list.p, nbig[1], go, c->big_tmp.p, (int)cap2, grid2,
+                                c->counters.p + 15, c->huge_list.p + n, c->huge_h.p + n, c->big_count.p + 1, c->seeds,
+                                st);
+            launches++;
           }
         }
         unsigned long long g[9];

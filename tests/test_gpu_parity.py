@@ -249,13 +249,16 @@ def test_map_results_do_not_depend_on_the_launch_tuning():
     batch = api.ReadBatch(codes, lengths, levels)
     tbs = ((150 + 15 + 1) // 2 + 7) & ~7
     assert m.tuning() == {"gather_warp_cap": 768, "gather_reads_per_steal": 4, "filter_rows": 8, "align_steal": 32,
-                          "filter_cursor": 0}
+                          "filter_cursor": 0, "align_rounds": 4}
     base = m.map(batch, tbs)
     st = m.stats()
     assert base.mapped.sum() > len(seqs) // 4
-    settings = [dict(gather_warp_cap=256, gather_reads_per_steal=1, filter_rows=1, align_steal=1024, filter_cursor=1),
-                dict(gather_warp_cap=1536, gather_reads_per_steal=64, filter_rows=64, align_steal=32, filter_cursor=0),
-                dict(gather_warp_cap=1000, gather_reads_per_steal=3, filter_rows=5, align_steal=96, filter_cursor=1)]
+    settings = [dict(gather_warp_cap=256, gather_reads_per_steal=1, filter_rows=1, align_steal=1024, filter_cursor=1,
+                     align_rounds=1),
+                dict(gather_warp_cap=1536, gather_reads_per_steal=64, filter_rows=64, align_steal=32, filter_cursor=0,
+                     align_rounds=6),
+                dict(gather_warp_cap=1000, gather_reads_per_steal=3, filter_rows=5, align_steal=96, filter_cursor=1,
+                     align_rounds=2)]
     for kw in settings:
         m.set_tuning(**kw)
         got = m.map(batch, tbs)
@@ -297,3 +300,62 @@ def test_large_host_batch_gives_the_small_batch_results():
     assert np.array_equal(big.mapped, np.tile(small.mapped, rep))
     assert big.hits.tobytes() == np.tile(small.hits, rep).tobytes()
     assert big.tb.tobytes() == np.tile(small.tb, (rep, 1)).tobytes()
+
+
+def _oracle_map(packed, seeds, codes, levels, lengths, tbs, indels, min_score, min_score_filter):
+    orc = ffi.oracle()
+    R = (ffi.OrRef * len(packed))()
+    keep = []
+    for k, (cp, mk, n) in enumerate(packed):
+        zr = np.zeros(1, np.int32)
+        keep.append(zr)
+        R[k] = ffi.OrRef(cp.ctypes.data + PADB, mk.ctypes.data + PADB, n, zr.ctypes.data, zr.ctypes.data, 0)
+    n = len(lengths)
+    rd = ffi.ReadsT(n, codes.ctypes.data, codes.shape[1], levels.ctypes.data, levels.shape[1], lengths.ctypes.data,
+                    None)
+    hits = np.zeros(n * 4, dtype=api.HIT_DTYPE)
+    tb = np.zeros((n * 4, tbs), np.uint8)
+    mapped = np.zeros(n, np.uint8)
+    out = ffi.ResultsT(hits.ctypes.data, tb.ctypes.data, tbs, mapped.ctypes.data)
+    p = ffi.make_params(colour=0, indels=indels, min_score=min_score, min_score_filter=min_score_filter)
+    assert orc.or_map(C.byref(p), seeds.encode(), R, len(packed), C.byref(rd), C.byref(out), None) == 0
+    return hits, tb, mapped
+
+
+def test_map_of_tandem_repeats_vs_oracle():
+    """Reads from 300 mutated copies of one 1,000-bp unit: every seed key of such a read occurs
+    about 250 times, so a 150-bp read-strand gathers about 100,000 index positions -- the
+    block-per-read gather and its large-slice second launch -- and every read has hundreds of
+    passing candidates, aligned in several rounds whose later ones stop early."""
+    from storm_b200 import synth
+    rng = np.random.default_rng(77)
+    unit = synth.random_bases(rng, 1000, 0.45)
+    copies = [_mutate(rng, unit, 0.02) for _ in range(300)]
+    g = np.concatenate([synth.random_bases(rng, 20000, 0.45)] + copies + [synth.random_bases(rng, 20000, 0.45)])
+    genome = [("chr1", g)]
+    seqs, quals = synth.simulate_nucleotide_reads(genome, 600, [50, 150], 78)
+    codes, levels, lengths = _reads_arrays(seqs, quals)
+    seeds = "##-##-###-###;###--#-#--#--####;####--#--#---#---###"
+    prm = api.params(indels=15, min_score=100, min_score_filter=100)
+    m = api.Mapper(prm, seeds)
+    cp = ffi.pack2(g, PADB)
+    mk = ffi.pack2(np.zeros(len(g), np.uint8), PADB, fill=0x55)
+    m.add_reference(cp[PADB:], mk[PADB:], len(g))
+    m.build_index()
+    tbs = ((150 + 15 + 1) // 2 + 7) & ~7
+    batch = api.ReadBatch(codes, lengths, levels)
+    results = []
+    for rounds in (1, 4, 6):
+        m.set_tuning(align_rounds=rounds)
+        results.append(m.map(batch, tbs))
+        st = m.stats()
+        assert st["hit_positions"] / len(seqs) > 20000, st  # the strand a read came from gathers ~50,000
+    m.close()
+    hits, tb, mapped = _oracle_map([(cp, mk, len(g))], seeds, codes, levels, lengths, tbs, 15, 100, 100)
+    assert mapped.sum() > len(seqs) // 2
+    for res in results:
+        assert np.array_equal(res.mapped, mapped)
+        assert res.hits.tobytes() == hits.tobytes()
+        for k in np.nonzero(hits["ref_id"] >= 0)[0]:
+            nb = (int(hits["tb_len"][k]) + 1) // 2
+            assert bytes(res.tb[k, :nb]) == bytes(tb[k, :nb]), k
