@@ -148,9 +148,14 @@ int stormgpu_sync(stormgpu_ctx *ctx);
 /* Served mapping ----------------------------------------------------------------------------
  * The reference and the index of every step of an -O seed chain stay resident on the GPU;
  * batches are submitted from any thread and run concurrently on `slots` workers (own stream and
- * buffers each).  A batch is admitted, in arrival order, when a worker is free and the device
- * memory its reads need (stormgpu_submit estimates it) fits what the batches in flight leave of
- * `budget_bytes`.  Step k of a batch maps, with chain[k], the reads no earlier step mapped, in
+ * buffers each).  `budget_bytes` bounds the device memory of the batches besides the resident
+ * sequences and indexes: half of it is the workers' mapping buffers (an equal share each, never
+ * exceeded: a pass that would need more maps its reads in halves), the other half the chain
+ * buffers of the batches in flight (reads, results; exactly sized, taken when a batch starts and
+ * returned when it ends).  A batch is admitted, in arrival order, when a worker is free and its
+ * chain buffers fit what the batches in flight leave of that half; a batch whose chain buffers
+ * alone exceed it is refused by stormgpu_submit.  Host copies go through a pinned staging area
+ * per worker.  Step k of a batch maps, with chain[k], the reads no earlier step mapped, in
  * their order: the reference run again on its own -O FASTQ output (README:97-101,
  * hit_map.c:514-579); every read gets the results of the step that mapped it.
  * No counterpart in the reference (one read file per process there). */

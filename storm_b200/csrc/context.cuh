@@ -23,22 +23,45 @@ struct RefSeq {
   std::vector<DevIndex> idx;
 };
 
+// Working memory of one mapping context (its DevBufs grown while it maps), with an optional
+// limit: a growth past it fails with STORMGPU_ENOMEM and sets `over`, and the mapping call then
+// maps the batch in halves instead (the reads are independent).  Set for the thread that maps
+// (g_work_budget) around the context's mapping.
+struct WorkBudget {
+  int64_t used = 0;   // bytes of the DevBufs grown while it was set
+  int64_t limit = 0;  // 0: none
+  bool over = false;
+};
+extern thread_local WorkBudget* g_work_budget;
+
 template <typename T>
 struct DevBuf {
   T* p = nullptr;
   int64_t cap = 0;
   int grow(int64_t n) {
     if (n <= cap) return 0;
+    WorkBudget* b = g_work_budget;
+    int64_t c = std::max<int64_t>(n, cap + cap / 2);
+    if (b && b->limit > 0 && b->used + (c - cap) * (int64_t)sizeof(T) > b->limit) {
+      c = n;  // the exact size, when the usual headroom does not fit
+      if (b->used + (c - cap) * (int64_t)sizeof(T) > b->limit) {
+        b->over = true;
+        sg_set_error("working memory limit of %lld bytes reached", (long long)b->limit);
+        return STORMGPU_ENOMEM;
+      }
+    }
     if (p) cudaFree(p);
     p = nullptr;
-    int64_t c = std::max<int64_t>(n, cap + cap / 2);
+    if (b) b->used -= cap * (int64_t)sizeof(T);
+    cap = 0;
     if (cudaMalloc(&p, sizeof(T) * (size_t)std::max<int64_t>(c, 1)) != cudaSuccess) {
       cudaGetLastError();
-      cap = 0;
+      p = nullptr;
       sg_set_error("device allocation of %lld bytes failed", (long long)(sizeof(T) * c));
       return STORMGPU_ENOMEM;
     }
     cap = c;
+    if (b) b->used += cap * (int64_t)sizeof(T);
     return 0;
   }
   void release() { if (p) cudaFree(p); p = nullptr; cap = 0; }
@@ -79,6 +102,7 @@ struct stormgpu_ctx {
   cudaEvent_t ev[8];
   cudaEvent_t rev[2 * 6 + 1];  // alignment rounds: before the first, after each round's alignment and replay
   int64_t last_n = -1;  // reads of the last stormgpu_map call (its results stay in hits / mapped)
+  sg::WorkBudget work;  // working memory of the mapping buffers; work.limit 0 = no limit
   // genome_map placement
   sg::DevBuf<uint32_t> gm_k0, gm_v0, gm_k1, gm_v1, gm_tmp, gm_base;
 };

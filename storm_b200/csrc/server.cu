@@ -87,31 +87,58 @@ struct Request {
   std::string err;
 };
 
-// One worker: a view context (stream + mapping buffers) and the chain's own buffers.
+// One worker: a view context (stream + mapping buffers, whose working memory is capped) and a
+// pinned host staging area for the batch's copies.
 struct Slot {
   stormgpu_ctx* ws = nullptr;
-  DevBuf<uint8_t> codes[2], levels[2], first_levels[2];
-  DevBuf<int16_t> lengths[2];
-  DevBuf<int32_t> ids[2];
-  DevBuf<stormgpu_hit> hits, hits_all;
-  DevBuf<uint8_t> tb, tb_all, mapped, mapped_all, step_all, unmapped;
-  DevBuf<int64_t> off, scan_tmp;
+  uint8_t* staging = nullptr;  // pinned host memory
+  int64_t staging_cap = 0;
   std::thread th;
   void release() {
-    for (int k = 0; k < 2; ++k) {
-      codes[k].release(); levels[k].release(); first_levels[k].release(); lengths[k].release(); ids[k].release();
-    }
-    hits.release(); hits_all.release(); tb.release(); tb_all.release(); mapped.release(); mapped_all.release();
-    step_all.release(); unmapped.release(); off.release(); scan_tmp.release();
+    if (staging) cudaFreeHost(staging);
+    staging = nullptr;
+    staging_cap = 0;
   }
 };
 
-// Device memory a batch holds while it runs: two chain copies of its reads, its results, and
-// the mapping buffers (candidate lists and the rest), counted per read.
-constexpr int64_t kWorkBytesPerRead = 4096;
-int64_t footprint(const stormgpu_reads* r, int64_t tbs) {
-  return r->n * (2 * (r->code_stride + r->level_stride + 2 + 1 + 4) + 4 * (int64_t)sizeof(stormgpu_hit) * 2 +
-                 8 * tbs + 4 + 9 + kWorkBytesPerRead);
+// The device memory of one batch's chain, besides the slot's mapping buffers: two copies of its
+// reads (the reads of the current step and the compacted unmapped ones), their indices, the
+// results of a step and of the batch, and the bookkeeping of the compaction; one stream-ordered
+// allocation of exactly this size per batch, returned when the batch ends.
+struct ChainLayout {
+  int64_t codes[2], levels[2], first_levels[2], lengths[2], ids[2];
+  int64_t hits, hits_all, tb, tb_all, mapped, mapped_all, step_all, unmapped, off, scan_tmp;
+  int64_t bytes;
+};
+
+ChainLayout chain_layout(const stormgpu_reads* r, int64_t tbs) {
+  const int64_t n = std::max<int64_t>(r->n, 1);
+  ChainLayout L;
+  int64_t at = 0;
+  auto take = [&](int64_t bytes) {
+    const int64_t o = at;
+    at += (bytes + 255) & ~255LL;
+    return o;
+  };
+  for (int k = 0; k < 2; ++k) {
+    L.codes[k] = take(n * r->code_stride);
+    L.levels[k] = take(r->levels ? n * r->level_stride : 0);
+    L.first_levels[k] = take(r->first_levels ? n : 0);
+    L.lengths[k] = take(n * (int64_t)sizeof(int16_t));
+    L.ids[k] = take(n * (int64_t)sizeof(int32_t));
+  }
+  L.hits = take((n * 4 + 4) * (int64_t)sizeof(stormgpu_hit));
+  L.hits_all = take((n * 4 + 4) * (int64_t)sizeof(stormgpu_hit));
+  L.tb = take(n * 4 * tbs + 4);
+  L.tb_all = take(n * 4 * tbs + 4);
+  L.mapped = take(n + 1);
+  L.mapped_all = take(n + 1);
+  L.step_all = take(n + 1);
+  L.unmapped = take(n + 1);
+  L.off = take((n + 2) * (int64_t)sizeof(int64_t));
+  L.scan_tmp = take((scan_tmp_elems(n + 1) + 8) * (int64_t)sizeof(int64_t));
+  L.bytes = at;
+  return L;
 }
 
 }  // namespace
@@ -121,7 +148,11 @@ struct stormgpu_server {
   std::vector<stormgpu_ctx*> steps;
   std::vector<Slot*> slots;
   int nslots = 1;
-  int64_t budget = 0, in_use = 0;
+  // budget: device memory for the batches, besides the resident sequences and indexes.  Half
+  // of it is the slots' mapping buffers (work_cap each, never exceeded: a pass that would need
+  // more maps its reads in halves); the other half, chain_budget, is shared by the chains of the
+  // batches in flight, each charged its exact chain size when admitted.
+  int64_t budget = 0, work_cap = 0, chain_budget = 0, in_use = 0;
   std::mutex mu;
   std::condition_variable cv_work, cv_done;
   std::deque<Request*> queue;
@@ -140,16 +171,47 @@ int run_chain(stormgpu_server* s, Slot* sl, Request* q, std::string& err) {
   const int64_t n = R.n, cs = R.code_stride, ls = R.levels ? R.level_stride : 0, tbs = q->out.tb_stride;
   const bool lv = R.levels != nullptr, fl = R.first_levels != nullptr;
   auto fail = [&](int rc) { err = stormgpu_last_error(); return rc; };
-  for (int k = 0; k < 2; ++k)
-    if (sl->codes[k].grow(std::max<int64_t>(n * cs, 1)) || sl->lengths[k].grow(std::max<int64_t>(n, 1)) ||
-        sl->ids[k].grow(std::max<int64_t>(n, 1)) || (lv && sl->levels[k].grow(std::max<int64_t>(n * ls, 1))) ||
-        (fl && sl->first_levels[k].grow(std::max<int64_t>(n, 1))))
-      return fail(STORMGPU_ENOMEM);
-  if (sl->hits.grow(n * 4 + 4) || sl->hits_all.grow(n * 4 + 4) || sl->tb.grow(n * 4 * tbs + 4) ||
-      sl->tb_all.grow(n * 4 * tbs + 4) || sl->mapped.grow(n + 1) || sl->mapped_all.grow(n + 1) ||
-      sl->step_all.grow(n + 1) || sl->unmapped.grow(n + 1) || sl->off.grow(n + 2) ||
-      sl->scan_tmp.grow(scan_tmp_elems(n + 1) + 8))
-    return fail(STORMGPU_ENOMEM);
+  const ChainLayout lay = chain_layout(&R, tbs);
+  uint8_t* blk = nullptr;
+  if (cudaMallocAsync(reinterpret_cast<void**>(&blk), (size_t)lay.bytes, st) != cudaSuccess) {
+    cudaGetLastError();
+    err = "stormgpu_submit: the chain buffers of the batch (" + std::to_string(lay.bytes) + " bytes) could not be allocated";
+    return STORMGPU_ENOMEM;
+  }
+  struct ChainView {
+    uint8_t *codes[2], *levels[2], *first_levels[2];
+    int16_t* lengths[2];
+    int32_t* ids[2];
+    stormgpu_hit *hits, *hits_all;
+    uint8_t *tb, *tb_all, *mapped, *mapped_all, *step_all, *unmapped;
+    int64_t *off, *scan_tmp;
+  } cv;
+  for (int k = 0; k < 2; ++k) {
+    cv.codes[k] = blk + lay.codes[k];
+    cv.levels[k] = blk + lay.levels[k];
+    cv.first_levels[k] = blk + lay.first_levels[k];
+    cv.lengths[k] = reinterpret_cast<int16_t*>(blk + lay.lengths[k]);
+    cv.ids[k] = reinterpret_cast<int32_t*>(blk + lay.ids[k]);
+  }
+  cv.hits = reinterpret_cast<stormgpu_hit*>(blk + lay.hits);
+  cv.hits_all = reinterpret_cast<stormgpu_hit*>(blk + lay.hits_all);
+  cv.tb = blk + lay.tb;
+  cv.tb_all = blk + lay.tb_all;
+  cv.mapped = blk + lay.mapped;
+  cv.mapped_all = blk + lay.mapped_all;
+  cv.step_all = blk + lay.step_all;
+  cv.unmapped = blk + lay.unmapped;
+  cv.off = reinterpret_cast<int64_t*>(blk + lay.off);
+  cv.scan_tmp = reinterpret_cast<int64_t*>(blk + lay.scan_tmp);
+  // the chain block goes back to the pool on every way out (stream-ordered, no device sync)
+  struct FreeAtEnd {
+    uint8_t* p;
+    cudaStream_t st;
+    ~FreeAtEnd() {
+      cudaFreeAsync(p, st);
+      cudaStreamSynchronize(st);
+    }
+  } free_at_end{blk, st};
 #define SGS(call)                                                        \
   do {                                                                   \
     cudaError_t e_ = (call);                                             \
@@ -158,15 +220,44 @@ int run_chain(stormgpu_server* s, Slot* sl, Request* q, std::string& err) {
       return STORMGPU_ECUDA;                                             \
     }                                                                    \
   } while (0)
-  if (n > 0) {
-    SGS(cudaMemcpyAsync(sl->codes[0].p, R.codes, n * cs, cudaMemcpyHostToDevice, st));
-    SGS(cudaMemcpyAsync(sl->lengths[0].p, R.lengths, n * sizeof(int16_t), cudaMemcpyHostToDevice, st));
-    if (lv) SGS(cudaMemcpyAsync(sl->levels[0].p, R.levels, n * ls, cudaMemcpyHostToDevice, st));
-    if (fl) SGS(cudaMemcpyAsync(sl->first_levels[0].p, R.first_levels, n, cudaMemcpyHostToDevice, st));
+  // host copies through the slot's pinned staging: the transfers then overlap the other slots'
+  // kernels; results come back the same way
+  const int64_t in_bytes = n * cs + n * (int64_t)sizeof(int16_t) + (lv ? n * ls : 0) + (fl ? n : 0);
+  const int64_t out_bytes = n * 4 * (int64_t)sizeof(stormgpu_hit) + n * 4 * tbs + 2 * n;
+  const int64_t stage = std::max(in_bytes, out_bytes) + 64;
+  if (sl->staging_cap < stage) {
+    if (sl->staging) cudaFreeHost(sl->staging);
+    sl->staging = nullptr;
+    sl->staging_cap = 0;
+    if (cudaMallocHost(reinterpret_cast<void**>(&sl->staging), (size_t)stage) != cudaSuccess) {
+      cudaGetLastError();
+      err = "stormgpu_submit: pinned host staging of " + std::to_string(stage) + " bytes could not be allocated";
+      return STORMGPU_ENOMEM;
+    }
+    sl->staging_cap = stage;
   }
-  launch_init_results(n, sl->hits_all.p, sl->mapped_all.p, sl->tb_all.p, tbs, st);
-  SGS(cudaMemsetAsync(sl->step_all.p, 0xff, std::max<int64_t>(n, 1), st));
-  iota_kernel<<<grid_for(n), 256, 0, st>>>(sl->ids[0].p, n);
+  if (n > 0) {
+    uint8_t* h = sl->staging;
+    int64_t o = 0;
+    memcpy(h + o, R.codes, (size_t)(n * cs));
+    SGS(cudaMemcpyAsync(cv.codes[0], h + o, n * cs, cudaMemcpyHostToDevice, st));
+    o += n * cs;
+    memcpy(h + o, R.lengths, (size_t)n * sizeof(int16_t));
+    SGS(cudaMemcpyAsync(cv.lengths[0], h + o, n * sizeof(int16_t), cudaMemcpyHostToDevice, st));
+    o += n * (int64_t)sizeof(int16_t);
+    if (lv) {
+      memcpy(h + o, R.levels, (size_t)(n * ls));
+      SGS(cudaMemcpyAsync(cv.levels[0], h + o, n * ls, cudaMemcpyHostToDevice, st));
+      o += n * ls;
+    }
+    if (fl) {
+      memcpy(h + o, R.first_levels, (size_t)n);
+      SGS(cudaMemcpyAsync(cv.first_levels[0], h + o, n, cudaMemcpyHostToDevice, st));
+    }
+  }
+  launch_init_results(n, cv.hits_all, cv.mapped_all, cv.tb_all, tbs, st);
+  SGS(cudaMemsetAsync(cv.step_all, 0xff, std::max<int64_t>(n, 1), st));
+  iota_kernel<<<grid_for(n), 256, 0, st>>>(cv.ids[0], n);
   int cur = 0;
   int64_t m = n;
   const int nsteps = (int)s->steps.size();
@@ -175,32 +266,39 @@ int run_chain(stormgpu_server* s, Slot* sl, Request* q, std::string& err) {
     ws->refs = src->refs;
     ws->seeds = src->seeds;
     ws->indexed = true;
-    stormgpu_reads r{m, sl->codes[cur].p, cs, lv ? sl->levels[cur].p : nullptr, ls, sl->lengths[cur].p,
-                     fl ? sl->first_levels[cur].p : nullptr};
-    stormgpu_results o{sl->hits.p, sl->tb.p, tbs, sl->mapped.p};
+    stormgpu_reads r{m, cv.codes[cur], cs, lv ? cv.levels[cur] : nullptr, ls, cv.lengths[cur],
+                     fl ? cv.first_levels[cur] : nullptr};
+    stormgpu_results o{cv.hits, cv.tb, tbs, cv.mapped};
     if (const int rc = map_device_impl(ws, &r, &o)) return fail(rc);
-    chain_scatter_kernel<<<grid_for(m), 256, 0, st>>>(m, sl->ids[cur].p, sl->hits.p, sl->tb.p, sl->mapped.p, tbs, k,
-                                                      sl->hits_all.p, sl->tb_all.p, sl->mapped_all.p,
-                                                      sl->step_all.p, sl->unmapped.p);
+    chain_scatter_kernel<<<grid_for(m), 256, 0, st>>>(m, cv.ids[cur], cv.hits, cv.tb, cv.mapped, tbs, k,
+                                                      cv.hits_all, cv.tb_all, cv.mapped_all,
+                                                      cv.step_all, cv.unmapped);
     if (k + 1 == nsteps) break;
-    exclusive_scan<uint8_t, int64_t>(sl->unmapped.p, sl->off.p, m, sl->off.p + m, sl->scan_tmp.p, st);
+    exclusive_scan<uint8_t, int64_t>(cv.unmapped, cv.off, m, cv.off + m, cv.scan_tmp, st);
     const int nx = 1 - cur;
     chain_compact_kernel<<<grid_for(m), 256, 0, st>>>(
-        m, sl->unmapped.p, sl->off.p, sl->codes[cur].p, cs, lv ? sl->levels[cur].p : nullptr, ls,
-        sl->lengths[cur].p, fl ? sl->first_levels[cur].p : nullptr, sl->ids[cur].p, sl->codes[nx].p,
-        lv ? sl->levels[nx].p : nullptr, sl->lengths[nx].p, fl ? sl->first_levels[nx].p : nullptr, sl->ids[nx].p);
+        m, cv.unmapped, cv.off, cv.codes[cur], cs, lv ? cv.levels[cur] : nullptr, ls,
+        cv.lengths[cur], fl ? cv.first_levels[cur] : nullptr, cv.ids[cur], cv.codes[nx],
+        lv ? cv.levels[nx] : nullptr, cv.lengths[nx], fl ? cv.first_levels[nx] : nullptr, cv.ids[nx]);
     int64_t next = 0;
-    SGS(cudaMemcpyAsync(&next, sl->off.p + m, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+    SGS(cudaMemcpyAsync(&next, cv.off + m, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
     SGS(cudaStreamSynchronize(st));
     m = next;
     cur = nx;
   }
   SGS(cudaGetLastError());
   if (n > 0) {
-    SGS(cudaMemcpyAsync(q->out.hits, sl->hits_all.p, n * 4 * sizeof(stormgpu_hit), cudaMemcpyDeviceToHost, st));
-    SGS(cudaMemcpyAsync(q->out.tb, sl->tb_all.p, n * 4 * tbs, cudaMemcpyDeviceToHost, st));
-    SGS(cudaMemcpyAsync(q->out.mapped, sl->mapped_all.p, n, cudaMemcpyDeviceToHost, st));
-    if (q->step) SGS(cudaMemcpyAsync(q->step, sl->step_all.p, n, cudaMemcpyDeviceToHost, st));
+    uint8_t* h = sl->staging;
+    const int64_t oh = 0, ot = oh + n * 4 * (int64_t)sizeof(stormgpu_hit), om = ot + n * 4 * tbs, os = om + n;
+    SGS(cudaMemcpyAsync(h + oh, cv.hits_all, n * 4 * sizeof(stormgpu_hit), cudaMemcpyDeviceToHost, st));
+    SGS(cudaMemcpyAsync(h + ot, cv.tb_all, n * 4 * tbs, cudaMemcpyDeviceToHost, st));
+    SGS(cudaMemcpyAsync(h + om, cv.mapped_all, n, cudaMemcpyDeviceToHost, st));
+    if (q->step) SGS(cudaMemcpyAsync(h + os, cv.step_all, n, cudaMemcpyDeviceToHost, st));
+    SGS(cudaStreamSynchronize(st));
+    memcpy(q->out.hits, h + oh, (size_t)n * 4 * sizeof(stormgpu_hit));
+    memcpy(q->out.tb, h + ot, (size_t)(n * 4 * tbs));
+    memcpy(q->out.mapped, h + om, (size_t)n);
+    if (q->step) memcpy(q->step, h + os, (size_t)n);
   }
   SGS(cudaStreamSynchronize(st));
 #undef SGS
@@ -214,7 +312,9 @@ void worker(stormgpu_server* s, Slot* sl) {
     {
       std::unique_lock<std::mutex> lk(s->mu);
       // arrival order; the first waiting batch goes as soon as its memory fits
-      s->cv_work.wait(lk, [&] { return s->stop || (!s->queue.empty() && s->in_use + s->queue.front()->bytes <= s->budget); });
+      s->cv_work.wait(lk, [&] {
+        return s->stop || (!s->queue.empty() && s->in_use + s->queue.front()->bytes <= s->chain_budget);
+      });
       if (s->stop) return;
       q = s->queue.front();
       s->queue.pop_front();
@@ -247,6 +347,8 @@ extern "C" int stormgpu_server_open(const stormgpu_params* params, const char* c
   s->p = *params;
   s->nslots = slots;
   s->budget = budget_bytes;
+  s->work_cap = budget_bytes / (2 * slots);
+  s->chain_budget = budget_bytes - s->work_cap * slots;
   for (int k = 0; k < nsteps; ++k) {
     stormgpu_ctx* c = nullptr;
     const int rc = stormgpu_open(params, chain[k], &c);
@@ -290,6 +392,7 @@ extern "C" int stormgpu_server_build(stormgpu_server* s) {
     v->p = s->p;
     v->seeds = s->steps[0]->seeds;
     v->tune = s->tune;
+    v->work.limit = s->work_cap;
     memset(&v->stats, 0, sizeof(v->stats));
     if (cudaStreamCreateWithFlags(&v->st, cudaStreamNonBlocking) != cudaSuccess) {
       cudaGetLastError();
@@ -334,11 +437,11 @@ extern "C" int stormgpu_submit(stormgpu_server* s, const stormgpu_reads* reads, 
   q->reads = *reads;
   q->out = *out;
   q->step = step;
-  q->bytes = footprint(reads, out->tb_stride);
-  if (q->bytes > s->budget) {
-    sg_set_error("stormgpu_submit: a batch of %lld reads needs about %lld bytes of device memory, more than the "
-                 "server's budget of %lld; split it",
-                 (long long)reads->n, (long long)q->bytes, (long long)s->budget);
+  q->bytes = chain_layout(reads, out->tb_stride).bytes;
+  if (q->bytes > s->chain_budget) {
+    sg_set_error("stormgpu_submit: the chain buffers of a batch of %lld reads take %lld bytes of device memory, "
+                 "more than the %lld the server's budget leaves for batches in flight; split it",
+                 (long long)reads->n, (long long)q->bytes, (long long)s->chain_budget);
     delete q;
     return STORMGPU_EINVAL;
   }

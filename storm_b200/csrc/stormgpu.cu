@@ -18,6 +18,7 @@
 #include "context.cuh"
 
 static thread_local char g_err[1024];
+thread_local sg::WorkBudget* sg::g_work_budget = nullptr;
 
 void sg_set_error(const char* fmt, ...) {
   va_list ap;
@@ -516,9 +517,20 @@ static int map_device_once(stormgpu_ctx* c, const stormgpu_reads* reads, stormgp
 }
 
 int sg::map_device_impl(stormgpu_ctx* c, const stormgpu_reads* reads, stormgpu_results* out) {
-  const int rc = map_device_once(c, reads, out);
-  if (rc != kSplitBatch) return rc;
+  WorkBudget* saved = g_work_budget;
+  g_work_budget = &c->work;
+  c->work.over = false;
+  int rc = map_device_once(c, reads, out);
+  g_work_budget = saved;
   const int64_t n = reads->n;
+  if (rc == STORMGPU_ENOMEM && c->work.over) {
+    if (n <= 1) {
+      sg_set_error("one read needs more than the working memory limit of %lld bytes", (long long)c->work.limit);
+      return STORMGPU_ENOMEM;
+    }
+    rc = kSplitBatch;
+  }
+  if (rc != kSplitBatch) return rc;
   if (n <= 1) {
     sg_set_error("one read has more than %lld candidate diagonals", (long long)kMaxCandidatesPerPass);
     return STORMGPU_ENOMEM;

@@ -145,3 +145,51 @@ def test_server_rejects_a_batch_beyond_its_budget(world):
     with pytest.raises(api.StormError, match="budget"):
         srv.submit(batches[2])
     srv.close()
+
+
+def test_tight_budget_bounds_device_memory_and_every_batch_completes(world):
+    """Under a budget far below what the batches would take at full speed, batches submitted
+    together from several threads all complete (no out-of-memory): a pass that would need more
+    than a slot's share of working memory maps its reads in halves, and a batch waits until the
+    chains in flight leave room for its own.  Device memory in use, sampled while they run,
+    never exceeds what the resident indexes took plus the budget (and a little for lazily loaded
+    kernel code); every batch still gets the plain chain's results."""
+    torch = pytest.importorskip("torch")
+    _, refs, batches = world
+    tbs = ((100 + ARGS["indels"] + 1) // 2 + 7) & ~7
+    plain = [_plain_chain(refs, b, tbs) for b in batches]
+    budget = 96 << 20
+    torch.cuda.synchronize()
+    free0, total = torch.cuda.mem_get_info()
+    srv = api.Server(api.params(**ARGS), CHAIN, slots=3, budget_bytes=budget)
+    _add(srv, refs)
+    srv.build()
+    _same(srv.poll(srv.submit(batches[0], tbs)), plain[0], "warm-up")
+    free1, _ = torch.cuda.mem_get_info()
+    resident = free0 - free1
+    samples, stop = [], threading.Event()
+
+    def sample():
+        while not stop.is_set():
+            samples.append(torch.cuda.mem_get_info()[0])
+            stop.wait(0.002)
+    th = threading.Thread(target=sample)
+    th.start()
+    tickets = [None] * len(batches)
+
+    def go(i):
+        tickets[i] = srv.submit(batches[i], tbs)
+    ths = [threading.Thread(target=go, args=(i,)) for i in range(len(batches))]
+    for t in ths:
+        t.start()
+    for t in ths:
+        t.join()
+    outs = [srv.poll(t) for t in tickets]
+    stop.set()
+    th.join()
+    srv.close()
+    for i, out in enumerate(outs):
+        _same(out, plain[i], ("tight", i))
+    peak = max(free0 - f for f in samples) if samples else 0
+    assert len(samples) > 10
+    assert peak <= resident + budget + (32 << 20), (peak >> 20, resident >> 20, budget >> 20)
