@@ -135,7 +135,9 @@ __device__ __forceinline__ int align_one(const ReadsDev& rd, const ScoreParams& 
                                          const PassBuffers& pb) {
   constexpr int NB = BWT > 0 ? BWT : kMaxBand;
   const int r = pb.p_read[slot];
-  const int thr = pb.thr ? max(sp.min_score, pb.thr[r]) : sp.min_score;
+  // the first round, and a launch without rounds, stop at -t only: pb.thr holds the read's
+  // threshold after the rounds before this one (in the first round, a previous pass's value)
+  const int thr = (pb.thr && pb.round > 0) ? max(sp.min_score, pb.thr[r]) : sp.min_score;
   const int d = pb.p_diag[slot];
   const int I = sp.I, BW = BWT > 0 ? BWT : 2 * I + 1, colour = CM >= 0 ? CM : sp.colour;
   const int L = rd.lengths[r];
