@@ -467,6 +467,7 @@ def mixed_arm(a, w):
     if rank == 0:
         parity = check_parity(res_mapper, paths, d)
         batching = batched_vs_plain(res_mapper, sets[chunks[a.warmup]], tbs, api)
+        batching["command_line"] = cli_batching(ref_path, paths[chunks[a.warmup]], d, w)
     res_mapper.close()
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         cpu = cpu_baseline_leg(a, w)
@@ -565,6 +566,31 @@ def batched_vs_plain(res_mapper, reads, tbs, api):
     same = bool(np.array_equal(mapped != 0, whole.mapped != 0) and hits[live].tobytes() == whole.hits[live].tobytes())
     return {"reads": int(reads.n), "batched_ms": 1000 * min(tb_), "plain_per_length_ms": 1000 * min(tp_),
             "plain_calls": len(buckets), "batched_over_plain": min(tp_) / min(tb_), "same_records": same}
+
+
+def cli_batching(ref_path, reads_path, d, w):
+    """The drop-in command line on one chunk, wall clock, file in and SAM out: one run over the
+    mixed-length file, against one run per read length (what the reference needs: it maps one
+    read length per run, reads_data.c:418-426); every run loads the reference, builds the index
+    and starts the device."""
+    from storm_b200 import build
+    exe = os.path.join(build.BIN_DIR, "storm-nucleotide")
+    cd = os.path.join(d, "cli")
+    os.makedirs(cd, exist_ok=True)
+
+    def run(path, tag):
+        t0 = time.perf_counter()
+        p = subprocess.run([exe, "-g", ref_path, "-r", path, "-o", os.path.join(cd, tag + ".sam"), "-v", "0"]
+                           + list(w["args"]), capture_output=True)
+        if p.returncode:
+            raise RuntimeError("command line failed: %s" % p.stderr[-500:])
+        return time.perf_counter() - t0
+
+    run(reads_path, "warm")
+    mixed = run(reads_path, "mixed")
+    per = [run(path, "len%d" % L) for L, path, _ in per_length_sample(reads_path, cd, None, "cli")]
+    return {"mixed_run_s": mixed, "per_length_runs_s": sum(per), "runs": len(per),
+            "mixed_over_per_length": sum(per) / mixed}
 
 
 def cpu_baseline_leg(a, w):
