@@ -336,6 +336,8 @@ def reference_arm(a, w):
 # ------------------------------------------------------------------------------ headline arm
 
 def mixed_arm(a, w):
+    """The workloads whose read set is drawn in chunks (mixed-length, large): one chunk per
+    step, reference and index resident."""
     import ctypes
 
     import torch
@@ -465,11 +467,12 @@ def mixed_arm(a, w):
 
     parity = batching = cpu = None
     if rank == 0:
-        parity = check_parity(res_mapper, paths, d)
-        batching = batched_vs_plain(res_mapper, sets[chunks[a.warmup]], tbs, api)
-        batching["command_line"] = cli_batching(ref_path, paths[chunks[a.warmup]], d, w)
+        parity = check_parity(a, res_mapper, paths, d)
+        if a.cfg == 2:  # reads of several lengths
+            batching = batched_vs_plain(res_mapper, sets[chunks[a.warmup]], tbs, api)
+            batching["command_line"] = cli_batching(ref_path, paths[chunks[a.warmup]], d, w)
     res_mapper.close()
-    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+    if rank == 0 and world == 1 and not a.no_cpu_baseline and a.cfg == 2:
         cpu = cpu_baseline_leg(a, w)
 
     if rank == 0:
@@ -508,18 +511,31 @@ def mixed_arm(a, w):
         dist.destroy_process_group()
 
 
-def check_parity(res_mapper, paths, d):
-    """Chunk 0 through the resident front end, one run per read length, against the reference's
-    digests of the same runs; and the mixed run's records against the per-length ones."""
+PARITY_CASE = {2: "mixed_100M_chunk0", 4: "large_3G_10k"}
+
+
+def check_parity(a, res_mapper, paths, d):
+    """The workload's at-scale parity case through the resident front end against the digests
+    of the reference's own runs: for the mixed-length workload chunk 0, one run per read length,
+    and the mixed run's records against the per-length ones; for the large one its 10k-read
+    sample, one run."""
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     import scale_cases
-    case = "mixed_100M_chunk0"
+    case = PARITY_CASE.get(a.cfg)
     digests = json.load(open(DIGESTS_PATH)) if os.path.exists(DIGESTS_PATH) else {}
     if case not in digests:
         return {"case": case, "checked": False, "why": "no reference digests for the case"}
     ref_d = digests[case]
     pd = os.path.join(d, "parity")
     os.makedirs(pd, exist_ok=True)
+    if scale_cases.CASES[case]["kind"] == "single":
+        w, _, reads = scale_cases.make_inputs(case, pd)
+        sam, un = os.path.join(pd, "all.sam"), os.path.join(pd, "all.un.fq")
+        res_mapper.map_file(reads, sam, un)
+        h, nrec = scale_cases.digest_sam(sam)
+        exp = ref_d["runs"]["all"]
+        return {"case": case, "checked": True, "runs": 1, "records": nrec,
+                "identical": h == exp["sam_sha256"] and scale_cases.digest_file(un) == exp["unmapped_fastq_sha256"]}
     ok, runs, bodies = True, 0, []
     for L, path, n in per_length_sample(paths[0], pd, None, "chunk0"):
         sam = os.path.join(pd, "len%d.sam" % L)
@@ -846,7 +862,7 @@ def main():
         if rank == 0:
             reference_arm(a, w)
         return
-    if a.cfg == 2:
+    if a.cfg in (2, 4):
         mixed_arm(a, w)
     elif a.cfg == 3:
         if rank == 0:
