@@ -364,6 +364,7 @@ def mixed_arm(a, w):
     log("rank %d: inputs ready in %.1f s" % (rank, time.perf_counter() - t0))
 
     p, seeds, *_ = pipeline.parse_options(w["args"])
+    seeds = seeds or DEFAULT_SEEDS[0]
     prm = api.params(colour=0, device=local, **p)
     reference = host.Reference(ref_path, 0)
     mapper = api.Mapper(prm, seeds)
@@ -439,7 +440,7 @@ def mixed_arm(a, w):
     mapper.close()
 
     # end to end through the resident front end: FASTQ file in, SAM file out, per chunk
-    res_mapper = pipeline.ResidentMapper(ref_path, w["args"], colour=0, device=local)
+    res_mapper = pipeline.ResidentMapper(ref_path, w["args"], colour=0, default_seeds=seeds, device=local)
     res_mapper.mapper.set_tuning(**tuning)
     e2e_chunks = chunks[a.warmup:a.warmup + max(1, min(a.steps, a.e2e_steps))]
     res_mapper.map_file(paths[chunks[0]], os.path.join(d, "warm.sam"))  # warm-up (buffers, page cache)
