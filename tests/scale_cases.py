@@ -10,7 +10,8 @@ tests/golden/make_scale_digests.py).  A case runs as one or more runs of the com
   buckets one run per read length, the reads of that length in file order (the reference maps
           one read length per run, reads_data.c:418-426);
   chain   per read length, the runs of an -O chain: run k maps the -O FASTQ of run k - 1 with
-          the k-th seed family (README:97-101, hit_map.c:514-579).
+          the k-th seed family (README:97-101, hit_map.c:514-579); a chain stops when a run
+          leaves no read unmapped (the reference refuses an empty read file).
 """
 from __future__ import annotations
 
@@ -92,6 +93,11 @@ def runs(name: str, w, reads: str, d: str):
                 out.append((lab, src, seeds, os.path.join(d, lab + ".sam"), os.path.join(d, lab + ".un.fq")))
                 src = os.path.join(d, lab + ".un.fq")
     return out
+
+
+def skip_run(path: str) -> bool:
+    """A chain's run whose input, the previous run's -O FASTQ, is empty does not run."""
+    return os.path.exists(path) and os.path.getsize(path) == 0
 
 
 def command_args(w, seeds, reads: str, sam: str, unmapped: str, ref: str):
