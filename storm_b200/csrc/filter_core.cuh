@@ -39,22 +39,6 @@ SG_HD uint32_t prmt(uint32_t a, uint32_t b, uint32_t s) {
 #endif
 }
 
-// a * b + c as one IMAD.  With b a value the compiler cannot see (a kernel argument that is 1,
-// or its negation), a 32-bit add or subtraction issues on the FMA pipe instead of the integer
-// ALU, which the filter's DPX max operations and byte permutes keep busy.
-#ifndef SG_FILTER_IMAD
-#define SG_FILTER_IMAD 1
-#endif
-SG_HD uint32_t imad(uint32_t a, uint32_t b, uint32_t c) {
-#if defined(__CUDA_ARCH__)
-  uint32_t d;
-  asm("mad.lo.u32 %0, %1, %2, %3;" : "=r"(d) : "r"(a), "r"(b), "r"(c));
-  return d;
-#else
-  return a * b + c;
-#endif
-}
-
 // per-register 0xFFFF/0 masks of cells (2j, 2j+1) from the W-bit cell mask
 SG_HD uint32_t mask_word(uint32_t m, int j) {
   return (((m >> (2 * j)) & 1u) ? 0x0000FFFFu : 0u) | (((m >> (2 * j + 1)) & 1u) ? 0xFFFF0000u : 0u);
@@ -252,7 +236,7 @@ template <int W, int MODE, int K> __host__ __device__ constexpr uint32_t split_p
 template <int W, bool ODD, int T, int Q, uint32_t MB>
 SG_HD void fstep_split(uint32_t (&A)[W / 2], uint32_t (&B)[W / 2], uint32_t (&M1)[W / 2], uint32_t (&M2)[W / 2],
                        uint32_t (&I1)[W / 2], uint32_t& Max, uint32_t rcur, uint32_t gcur, uint32_t TLO,
-                       uint32_t THI, uint32_t NFE, uint32_t CFO, uint32_t ONE) {
+                       uint32_t THI, uint32_t NFE, uint32_t CFO) {
   constexpr int H = W / 2;
   constexpr int RA = (Q + 1) % H;                // read steps done (mod H), this one included
   constexpr int RB = (ODD ? Q + 1 : Q) % H;      // genome steps done (mod H)
@@ -267,13 +251,7 @@ SG_HD void fstep_split(uint32_t (&A)[W / 2], uint32_t (&B)[W / 2], uint32_t (&M1
 #pragma unroll
   // P = max(I1 - ext, M1 - open) as one add-max: NFE holds -ext in both halves, and every half
   // stays positive (cells are biased by 256, ext and open are below 256)
-  for (int j = 0; j < H; ++j) {
-#if SG_FILTER_IMAD
-    P[j] = __viaddmax_s16x2(I1[j], NFE, imad(M1[j], ONE, 0u - CFO));
-#else
-    P[j] = __viaddmax_s16x2(I1[j], NFE, M1[j] - CFO);
-#endif
-  }
+  for (int j = 0; j < H; ++j) P[j] = __viaddmax_s16x2(I1[j], NFE, M1[j] - CFO);
 #pragma unroll
   for (int j = 0; j < H; ++j) {
     uint32_t nbr;
@@ -284,11 +262,7 @@ SG_HD void fstep_split(uint32_t (&A)[W / 2], uint32_t (&B)[W / 2], uint32_t (&M1
     if (!lo && !hi) {
       Mn[j] = kFBB;  // M of cells outside the read is 0; their I still propagates
     } else {
-#if SG_FILTER_IMAD
-      const uint32_t sc = prmt(TLO, THI, imad(B[(j - RB + H) % H], 0u - ONE, A[(j + RA) % H]));
-#else
       const uint32_t sc = prmt(TLO, THI, A[(j + RA) % H] - B[(j - RB + H) % H]);
-#endif
       const uint32_t mv = __viaddmax_s16x2(M2[j], sc, In[j]);
       Mn[j] = (lo && hi) ? mv : lo ? ((mv & 0x0000FFFFu) | (kFBB & 0xFFFF0000u))
                                    : ((mv & 0xFFFF0000u) | (kFBB & 0x0000FFFFu));
@@ -314,13 +288,12 @@ SG_HD void fstep_split(uint32_t (&A)[W / 2], uint32_t (&B)[W / 2], uint32_t (&M1
 template <int W, int MODE, int QB, int K, int NP, int NWD>
 SG_HD void run_pairs_split(uint32_t (&A)[W / 2], uint32_t (&B)[W / 2], uint32_t (&M1)[W / 2], uint32_t (&M2)[W / 2],
                            uint32_t (&I1)[W / 2], uint32_t& Max, const uint32_t (&rc)[NWD],
-                           const uint32_t (&gc)[NWD], uint32_t TLO, uint32_t THI, uint32_t NFE, uint32_t CFO,
-                           uint32_t ONE) {
+                           const uint32_t (&gc)[NWD], uint32_t TLO, uint32_t THI, uint32_t NFE, uint32_t CFO) {
   if constexpr (K < NP) {
     constexpr uint32_t MB = split_pair_mask<W, MODE, K>();
-    fstep_split<W, false, K % 4, QB + K, MB>(A, B, M1, M2, I1, Max, rc[K / 4], gc[K / 4], TLO, THI, NFE, CFO, ONE);
-    fstep_split<W, true, K % 4, QB + K, MB>(A, B, M1, M2, I1, Max, rc[K / 4], gc[K / 4], TLO, THI, NFE, CFO, ONE);
-    run_pairs_split<W, MODE, QB, K + 1, NP, NWD>(A, B, M1, M2, I1, Max, rc, gc, TLO, THI, NFE, CFO, ONE);
+    fstep_split<W, false, K % 4, QB + K, MB>(A, B, M1, M2, I1, Max, rc[K / 4], gc[K / 4], TLO, THI, NFE, CFO);
+    fstep_split<W, true, K % 4, QB + K, MB>(A, B, M1, M2, I1, Max, rc[K / 4], gc[K / 4], TLO, THI, NFE, CFO);
+    run_pairs_split<W, MODE, QB, K + 1, NP, NWD>(A, B, M1, M2, I1, Max, rc, gc, TLO, THI, NFE, CFO);
   }
 }
 
@@ -328,12 +301,11 @@ SG_HD void run_pairs_split(uint32_t (&A)[W / 2], uint32_t (&B)[W / 2], uint32_t 
 template <int W, int QB, int K, int NP, int NWD>
 SG_HD void run_rest_split(int r, uint32_t (&A)[W / 2], uint32_t (&B)[W / 2], uint32_t (&M1)[W / 2],
                           uint32_t (&M2)[W / 2], uint32_t (&I1)[W / 2], uint32_t& Max, const uint32_t (&rc)[NWD],
-                          const uint32_t (&gc)[NWD], uint32_t TLO, uint32_t THI, uint32_t NFE, uint32_t CFO,
-                          uint32_t ONE) {
+                          const uint32_t (&gc)[NWD], uint32_t TLO, uint32_t THI, uint32_t NFE, uint32_t CFO) {
   if constexpr (K < NP) {
     if (K < r) {
-      run_pairs_split<W, 0, QB, K, K + 1, NWD>(A, B, M1, M2, I1, Max, rc, gc, TLO, THI, NFE, CFO, ONE);
-      run_rest_split<W, QB, K + 1, NP, NWD>(r, A, B, M1, M2, I1, Max, rc, gc, TLO, THI, NFE, CFO, ONE);
+      run_pairs_split<W, 0, QB, K, K + 1, NWD>(A, B, M1, M2, I1, Max, rc, gc, TLO, THI, NFE, CFO);
+      run_rest_split<W, QB, K + 1, NP, NWD>(r, A, B, M1, M2, I1, Max, rc, gc, TLO, THI, NFE, CFO);
     }
   }
 }
@@ -349,10 +321,9 @@ SG_HD uint32_t funnel_sel(uint32_t s) { return s | ((s + 1) << 4) | ((s + 2) << 
 // W-1..L-1 (main) unmasked in blocks of BP pairs; the main remainder (fewer than BP pairs)
 // keeps constant rotations, and the registers are rotated back to rotation 0 once, before
 // the epilogue.
-// ONE: 1, from a value the compiler cannot see (see imad).
 template <int W>
 SG_HD int filter_split(const uint8_t* __restrict__ gexp, int64_t pos, const uint8_t* __restrict__ rexp, int L,
-                       uint32_t TLO, uint32_t THI, uint32_t NFE, uint32_t CFO, uint32_t ONE) {
+                       uint32_t TLO, uint32_t THI, uint32_t NFE, uint32_t CFO) {
   constexpr int H = W / 2;
   constexpr int BP = H > 4 ? H : 4;
   constexpr int NPRO = W - 1;
@@ -382,7 +353,7 @@ SG_HD int filter_split(const uint8_t* __restrict__ gexp, int64_t pos, const uint
       gc[k] = prmt(wp, wn, sel);
       wp = wn;
     }
-    run_pairs_split<W, 1, 0, 0, NPRO, NWP>(A, B, M1, M2, I1, Max, rc, gc, TLO, THI, NFE, CFO, ONE);
+    run_pairs_split<W, 1, 0, 0, NPRO, NWP>(A, B, M1, M2, I1, Max, rc, gc, TLO, THI, NFE, CFO);
   }
   {  // main: pairs W-1..L-1, index W-1 = H-1 mod H at every block start
     const int nmain = L - W + 1;
@@ -405,7 +376,7 @@ SG_HD int filter_split(const uint8_t* __restrict__ gexp, int64_t pos, const uint
         gp = gn;
         rp = rn;
       }
-      run_pairs_split<W, 0, H - 1, 0, BP, NWB>(A, B, M1, M2, I1, Max, rc, gc, TLO, THI, NFE, CFO, ONE);
+      run_pairs_split<W, 0, H - 1, 0, BP, NWB>(A, B, M1, M2, I1, Max, rc, gc, TLO, THI, NFE, CFO);
     }
     const int r = nmain - pm;
     if (r > 0) {
@@ -419,7 +390,7 @@ SG_HD int filter_split(const uint8_t* __restrict__ gexp, int64_t pos, const uint
         gp = gn;
         rp = rn;
       }
-      run_rest_split<W, H - 1, 0, BP, NWB>(r, A, B, M1, M2, I1, Max, rc, gc, TLO, THI, NFE, CFO, ONE);
+      run_rest_split<W, H - 1, 0, BP, NWB>(r, A, B, M1, M2, I1, Max, rc, gc, TLO, THI, NFE, CFO);
     }
   }
   if (H > 1) {  // back to rotation 0: logical read register j = A[(j + L) mod H], genome B[(j - L) mod H]
@@ -453,7 +424,7 @@ SG_HD int filter_split(const uint8_t* __restrict__ gexp, int64_t pos, const uint
       gc[k] = prmt(wp, wn, sel);
       wp = wn;
     }
-    run_pairs_split<W, 2, 0, 0, NPRO, NWP>(A, B, M1, M2, I1, Max, rc, gc, TLO, THI, NFE, CFO, ONE);
+    run_pairs_split<W, 2, 0, 0, NPRO, NWP>(A, B, M1, M2, I1, Max, rc, gc, TLO, THI, NFE, CFO);
   }
   const int lo = (int)(int16_t)(Max & 0xffffu), hi = (int)(int16_t)(Max >> 16);
   return (lo > hi ? lo : hi) - (int)kFB;

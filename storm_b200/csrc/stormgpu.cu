@@ -398,7 +398,6 @@ static int map_device_once(stormgpu_ctx* c, const stormgpu_reads* reads, stormgp
       memset(&job, 0, sizeof(job));
       if (c->tune.filter_cursor) job.cursor = c->counters.p + 10;  // zeroed with the counters of the pass
       job.rows = c->tune.filter_rows;
-      job.one = 1;
       job.n = utot; job.fr = c->fr.p; job.fd = c->fd.p; job.flag = c->flag.p; job.codes = rd.codes;
       job.cstride = rd.cstride; job.lengths = rd.lengths; job.genome = R.d_codes; job.W = sp.W; job.Is = sp.Is;
       job.fm = sp.fm; job.fx = sp.fx; job.fo = sp.fo; job.fe = sp.fe; job.fthr = sp.fthr;
@@ -697,7 +696,6 @@ extern "C" int stormgpu_sw_filter(int W, int read_len, uint32_t match, uint32_t 
     launch_expand_reads(one, rx, rstride, 0);
     FilterJob job;
     memset(&job, 0, sizeof(job));
-    job.one = 1;
     job.n = n; job.fr = dzero; job.fd = dpos; job.flag = dp; job.codes = dr; job.cstride = rb;
     job.lengths = dl; job.genome = gb; job.W = W; job.Is = 0;
     job.gexp = gx + kGexpPad; job.rexp = rx; job.rstride = rstride; job.min_len = read_len;

@@ -125,7 +125,7 @@ __global__ void __launch_bounds__(256, (W <= 8 ? 4 : 2)) filter_flat_dpx_kernel(
     const int64_t pos = (int64_t)d - job.Is;
     int mx;
     if (!SHORT || L >= W)
-      mx = filter_split<W>(job.gexp, pos, job.rexp + (int64_t)r * job.rstride, L, TLO, THI, NFE, CFO, job.one);
+      mx = filter_split<W>(job.gexp, pos, job.rexp + (int64_t)r * job.rstride, L, TLO, THI, NFE, CFO);
     else
       mx = filter_dpx<W>(job.genome, pos, job.codes + (int64_t)r * job.cstride, job.cstride, L, T, NFE, NFO);
     job.flag[t] = mx > job.fthr ? 1 : 0;

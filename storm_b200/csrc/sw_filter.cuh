@@ -28,7 +28,6 @@ struct FilterJob {
   // the next tile of 256 * kFilterTile candidates from it, in list order, until none is left
   unsigned long long* cursor;
   int rows;  // with a cursor: rows of 256 candidates in a block's tile (0 = 8); without: 8
-  uint32_t one;  // 1: a multiplier the compiler cannot fold (moves adds to the FMA pipe)
 };
 
 constexpr int64_t kGexpPad = 4096;   // bytes of padding around a byte-expanded sequence

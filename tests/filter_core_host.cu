@@ -21,7 +21,7 @@ template <int W>
 static int filter_ws(const uint8_t* gexp, int64_t pos, const uint8_t* rexp, int L, int fm, int fx, int fo, int fe) {
   uint32_t TLO, THI, NFE, CFO;
   sg::filter_split_consts(fm, fx, fo, fe, TLO, THI, NFE, CFO);
-  return sg::filter_split<W>(gexp, pos, rexp, L, TLO, THI, NFE, CFO, 1u);
+  return sg::filter_split<W>(gexp, pos, rexp, L, TLO, THI, NFE, CFO);
 }
 
 template <int W>
