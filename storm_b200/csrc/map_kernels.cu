@@ -306,12 +306,137 @@ __device__ __forceinline__ int align_one(const ReadsDev& rd, const ScoreParams& 
   return rows;
 }
 
+// Nucleotide space with a constant band: the same DP as align_one, each cell kept in one
+// register as score * 2048 + from * 512 + indels (from: 3 corner, 2 top, 1 left).  The largest of
+// the three candidate values is the reference's choice (alignment.c:521-532: the higher score,
+// and on equal scores corner before top before left), carrying its direction and indel count,
+// so a cell costs one three-way max instead of compares and selects on separate score and state
+// arrays.  Cells are floored at kCellFloor (score -2^19): a cell below it cannot lie on the path
+// of an alignment whose score exceeds any threshold (a path gains at most the match score per
+// row), it can only lower the candidates of its neighbours, and a row whose maximum is below it
+// bounds every threshold out (bound below -t); so every score, bound and traceback the replay
+// reads is the reference's, and the packed value never overflows.
+constexpr int kCellShift = 11;
+constexpr int kCellFloor = -(1 << 30);
+
+template <int BW>
+__device__ __forceinline__ int align_one_nuc(const ReadsDev& rd, const ScoreParams& sp,
+                                             const uint8_t* __restrict__ genome, const uint8_t* __restrict__ mask,
+                                             int64_t slot, int64_t sl, int64_t ns, const PassBuffers& pb) {
+  const int r = pb.p_read[slot];
+  const int thr = (pb.thr && pb.round > 0) ? max(sp.min_score, pb.thr[r]) : sp.min_score;
+  const int d = pb.p_diag[slot];
+  const int I = sp.I;
+  const int L = rd.lengths[r];
+  const uint8_t* rdc = rd.codes + (int64_t)r * rd.cstride;
+  const uint8_t* rdq = rd.levels ? rd.levels + (int64_t)r * rd.lstride : nullptr;
+  const int win = max(d - I, -sp.Is);  // run.c:667
+  constexpr int wpr = (2 * BW + 31) / 32;
+  uint32_t* scr = pb.a_scratch;
+  const int OPEN = sp.gap_open * (1 << kCellShift), EXT = sp.gap_ext * (1 << kCellShift);
+  const int MINS = kMinScore * (1 << kCellShift);
+  constexpr int FROM = 0x600, TOP = 0x400, LEFT = 0x200, IND = 0x1ff;
+  int v[BW];
+  const int mbest = sp.pair[0][3];
+  BandWindow<BW> bwin;
+  bwin.load(genome, mask, win);
+  {  // row 0: pair scores only (alignment.c:326-360)
+    const int rc = code_at(rdc, 0), q = rdq ? code_at(rdq, 0) : 3;
+    const int SM = sp.pair[0][q] * (1 << kCellShift), SX = sp.pair[1][q] * (1 << kCellShift);
+    uint32_t wd[wpr] = {};
+#pragma unroll
+    for (int c = 0; c < BW; ++c) {
+      v[c] = (bwin.mcode(c) == 0 ? (rc != bwin.gcode(c) ? SX : SM) : MINS) | FROM;
+      wd[(2 * c) >> 5] |= 3u << ((2 * c) & 31);
+    }
+#pragma unroll
+    for (int k = 0; k < wpr; ++k) scr[(int64_t)k * ns + sl] = wd[k];
+  }
+  int best_possible = L * mbest;
+  long long bound = 0x7fffffffLL;
+  int rows = L;
+  for (int i = 1; i < L; ++i) {
+    const int rc = code_at(rdc, i), q = rdq ? code_at(rdq, i) : 3;
+    const int SM = sp.pair[0][q] * (1 << kCellShift), SX = sp.pair[1][q] * (1 << kCellShift);
+    bwin.advance(genome, mask, (int64_t)win + i + BW - 1);
+    int mol = MINS, left = kCellFloor;  // the row maximum starts at MIN_SCORE (alignment.c:500)
+    bool lok = false;  // the left border (alignment.c:504-509): no gap from outside the band
+    uint32_t wd[wpr] = {};
+#pragma unroll
+    for (int c = 0; c < BW; ++c) {
+      const int s0 = bwin.mcode(c) == 0 ? (rc != bwin.gcode(c) ? SX : SM) : MINS;
+      const int corner = (v[c] | FROM) + s0;
+      int top = kCellFloor, lft = kCellFloor;
+      if (c + 1 < BW) {
+        const int t = v[c + 1];
+        if ((t & IND) < I) top = ((t & ~FROM) | TOP) + (((t & FROM) == TOP) ? EXT : OPEN) + 1;
+      }
+      if (lok && (left & IND) < I) lft = ((left & ~FROM) | LEFT) + (((left & FROM) == LEFT) ? EXT : OPEN) + 1;
+      const int nv = max(max(max(corner, top), lft), kCellFloor);
+      v[c] = nv;
+      left = nv;
+      lok = true;
+      mol = max(mol, nv);
+      wd[(2 * c) >> 5] |= (uint32_t)((nv >> 9) & 3) << ((2 * c) & 31);
+    }
+    const long long ml = (long long)(mol >> kCellShift) + best_possible;
+    if (ml < bound) bound = ml;
+    best_possible -= mbest;
+#pragma unroll
+    for (int k = 0; k < wpr; ++k) scr[((int64_t)i * wpr + k) * ns + sl] = wd[k];
+    if (bound < thr) {
+      rows = i + 1;
+      break;
+    }
+  }
+  int best = kMinScore, bi = -1, bj = -1;
+#pragma unroll
+  for (int c = 0; c < BW; ++c) {
+    const int s = v[c] >> kCellShift;
+    if (best < s) { best = s; bi = L - 1; bj = L - 1 + c; }
+  }
+  const int32_t bnd = bound > 0x7fffffffLL ? 0x7fffffff : (int32_t)bound;
+  pb.a_score[slot] = best;
+  pb.a_bound[slot] = bnd;
+  int i0 = bi, j0 = bj, tl = 0;
+  uint8_t* tb = pb.a_tb + slot * pb.tbs;
+  if (bi >= 0 && bnd >= thr && best > thr) {  // alignment.c:642-734
+    int i = bi, c = bj - bi;
+    uint8_t cur = 0;
+    while (i >= 0 && i < L && c >= 0 && c < BW) {
+      const int j = i + c;
+      i0 = i;
+      j0 = j;
+      const uint32_t wdir = scr[((int64_t)i * wpr + ((2 * c) >> 5)) * ns + sl];
+      const int from = (wdir >> ((2 * c) & 31)) & 3;
+      const int rc = code_at(rdc, i);
+      int op;
+      if (from == 2) op = 0xC | rc;
+      else if (from == 1) op = 0x1;
+      else op = rc != code_at(genome, (int64_t)win + j) ? 0x4 | rc : 0x3;
+      if (tl & 1) { cur |= (uint8_t)op; tb[tl >> 1] = cur; }
+      else { cur = (uint8_t)(op << 4); tb[tl >> 1] = cur; }
+      tl++;
+      if (from == 2) { i--; c++; }
+      else if (from == 1) { c--; }
+      else { i--; }
+    }
+  }
+  pb.a_tblen[slot] = tl;
+  pb.a_pos[slot * 4 + 0] = (int16_t)bi;
+  pb.a_pos[slot * 4 + 1] = (int16_t)bj;
+  pb.a_pos[slot * 4 + 2] = (int16_t)i0;
+  pb.a_pos[slot * 4 + 3] = (int16_t)j0;
+  return rows;
+}
+
 // Slots slot0 .. slot0 + nslots: one per thread (scratch column = slot - slot0), or with
 // pb.cursor a persistent grid whose warps take the next 32 slots from the cursor (the slot
 // count read from pb.npass_dev when it is given; scratch column = the thread's index in the
 // grid, so the scratch holds align_workers() columns).
 template <int BWT, int CM>
-__global__ void __launch_bounds__(128, (BWT > 0 && BWT <= 15 ? 5 : BWT == 31 ? 4 : BWT == 41 ? 3 : 1)) align_kernel(ReadsDev rd, ScoreParams sp, const uint8_t* __restrict__ genome,
+__global__ void __launch_bounds__(128, CM == 0 ? (BWT > 0 && BWT <= 15 ? 7 : BWT == 31 ? 5 : BWT == 41 ? 4 : 1)
+                                              : (BWT > 0 && BWT <= 15 ? 5 : BWT == 31 ? 4 : BWT == 41 ? 3 : 1)) align_kernel(ReadsDev rd, ScoreParams sp, const uint8_t* __restrict__ genome,
                                                     const uint8_t* __restrict__ mask, int64_t slot0, int64_t nslots,
                                                     PassBuffers pb) {
   // one call site of align_one (its band code is large and fully unrolled)
@@ -339,7 +464,10 @@ __global__ void __launch_bounds__(128, (BWT > 0 && BWT <= 15 ? 5 : BWT == 31 ? 4
     }
     if (s < n) {
       const int64_t slot = pb.round_slots ? (int64_t)pb.round_slots[list0 + s] : slot0 + s;
-      rows += (unsigned long long)align_one<BWT, CM>(rd, sp, genome, mask, slot, steal ? tid : s, ns, pb);
+      if constexpr (CM == 0 && BWT > 0)
+        rows += (unsigned long long)align_one_nuc<BWT>(rd, sp, genome, mask, slot, steal ? tid : s, ns, pb);
+      else
+        rows += (unsigned long long)align_one<BWT, CM>(rd, sp, genome, mask, slot, steal ? tid : s, ns, pb);
     }
     if (!steal) break;
     s += 32;
