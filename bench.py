@@ -372,8 +372,12 @@ def mixed_arm(a, w):
     t0 = time.perf_counter()
     mapper.build_index()
     mapper.sync()
+    index_cold_ms = mapper.stats()["ms_index"]
+    mapper.build_index()  # again: the first build also grows the memory pool
+    mapper.sync()
     index_ms = mapper.stats()["ms_index"]
-    log("rank %d: index built in %.1f ms (device), %.2f s wall" % (rank, index_ms, time.perf_counter() - t0))
+    log("rank %d: index built in %.1f ms (device; first build %.1f ms), %.2f s wall"
+        % (rank, index_ms, index_cold_ms, time.perf_counter() - t0))
 
     sets = {c: host.ReadSet(paths[c], 0) for c in chunks}
     max_len = max(s.max_len for s in sets.values())
@@ -480,6 +484,7 @@ def mixed_arm(a, w):
         agg = {k: sum(s[k] for s in stats) for k in stats[0] if k != "ms_index"}
         sm_mhz = clocks.get("sm_mhz") or 1965.0
         stages = stage_rooflines(agg, reads_total, max_len, sm_mhz, (index_ms, index_bytes(seeds, w["ref_sizes"])))
+        stages["index_build"]["first_build_ms"] = index_cold_ms
         per_step = {k: v for k, v in stages.items() if not k.startswith("_")}
         dom = max(("sw_filter", "full_align", "hit_gather"), key=lambda k: per_step.get(k, {}).get("ms", 0))
         traffic = None
@@ -489,8 +494,8 @@ def mixed_arm(a, w):
                 "peak": per_step[dom]["peak"], "unit": per_step[dom]["unit"], "frac": per_step[dom]["frac"],
                 "traffic": traffic,
                 "peak_source": stages["_peak_sources"]["int" if per_step[dom]["bound"] == "int" else "hbm"]}
-        for v in per_step.values():
-            if "ms" in v:
+        for k, v in per_step.items():
+            if "ms" in v and k != "index_build":  # the index is built once, before the steps
                 v["ms_per_step"] = v["ms"] / len(stats)
         line = {"metric": "mapped reads/sec", "value": value, "unit": "reads/s", "n_gpus": world, "steps": a.steps,
                 "warmup": a.warmup, "ms_per_step": t_max / a.steps, "higher_is_better": True, "scaling": "weak",

@@ -90,8 +90,22 @@ static int grow_regions(int32_t **rs, int32_t **re, int32_t *cap) {
  * upper-cased unless -j; non-ACGT letters are masked and coded rand()&3 (nucleotide) or as
  * the previous base (colour); colour space stores the XOR of consecutive bases and keeps
  * the first base apart; masked regions are the maximal runs of masked codes. */
+enum { REF_SPACE = 4, REF_HEADER = 5, REF_OTHER = 6 };
+
+/* Class of each input byte: 0-3 the base (upper-cased first unless -j), REF_SPACE (isspace),
+ * REF_HEADER ('>'), REF_OTHER (masked). */
+static void reference_classes(int ignore_lowercase, uint8_t cls[256]) {
+  for (int c = 0; c < 256; ++c) {
+    const int u = ignore_lowercase ? c : toupper(c);
+    cls[c] = (uint8_t)(u == 'A' ? 0 : u == 'C' ? 1 : u == 'G' ? 2 : u == 'T' ? 3 : isspace(u) ? REF_SPACE
+                       : u == '>' ? REF_HEADER : REF_OTHER);
+  }
+}
+
 int sh_load_reference(const char *path, int colour, int ignore_lowercase, sh_refs *out) {
   memset(out, 0, sizeof(*out));
+  uint8_t cls[256];
+  reference_classes(ignore_lowercase, cls);
   size_t len;
   int oom;
   char *buf = slurp(path, &len, &oom);
@@ -140,11 +154,10 @@ int sh_load_reference(const char *path, int colour, int ignore_lowercase, sh_ref
     size_t q = p;
     int64_t size = 0;
     while (q < len) {
-      int c = ignore_lowercase ? (unsigned char)buf[q] : toupper((unsigned char)buf[q]);
-      if (c == '>') break;
+      const int k = cls[(unsigned char)buf[q]];
+      if (k == REF_HEADER) break;
       q++;
-      if (isspace(c)) continue;
-      size++;
+      size += k != REF_SPACE;
     }
     if (size == 0) break; /* reference_data.c:67-70, load_reference_db:241-246 */
     int64_t nbytes = (size + 3) / 4 + 1;
@@ -162,18 +175,19 @@ int sh_load_reference(const char *path, int colour, int ignore_lowercase, sh_ref
     uint8_t *cd = ca + SH_PAD_BYTES, *mk = ma + SH_PAD_BYTES;
     int64_t i = 0, mstart = -1;
     int code_prev = 0, have_first = 0;
+    unsigned cacc = 0; /* the codes of the byte being filled */
     while (p < len) {
-      int c = ignore_lowercase ? (unsigned char)buf[p] : toupper((unsigned char)buf[p]);
-      if (c == '>') break;
+      const int k = cls[(unsigned char)buf[p]];
+      if (k == REF_HEADER) break;
       p++;
-      if (isspace(c)) continue;
+      if (k == REF_SPACE) continue;
       int code;
-      if (!(c == 'A' || c == 'C' || c == 'G' || c == 'T')) {
+      if (k == REF_OTHER) {
         code = colour ? code_prev : (rand() & 3);
         if (mstart == -1) mstart = i;
         put2(mk, i, 1);
       } else {
-        code = (c == 'A') ? 0 : (c == 'C') ? 1 : (c == 'G') ? 2 : 3;
+        code = k;
         if (mstart != -1) {
           if (nr == rcap && grow_regions(&rs, &re, &rcap)) {
             free(ca); free(ma); free(rs); free(re); free(buf);
@@ -185,19 +199,18 @@ int sh_load_reference(const char *path, int colour, int ignore_lowercase, sh_ref
           mstart = -1;
         }
       }
-      if (!colour) {
-        put2(cd, i, code);
-        i++;
-      } else if (!have_first) {
+      if (colour && !have_first) {
         have_first = 1;
         code_prev = code;
         out->first_base[s] = (uint8_t)code;
-      } else {
-        put2(cd, i, code_prev ^ code);
-        i++;
-        code_prev = code;
+        continue;
       }
+      cacc |= (unsigned)(colour ? code_prev ^ code : code) << ((i & 3) << 1);
+      if ((i & 3) == 3) { cd[i >> 2] = (uint8_t)cacc; cacc = 0; }
+      i++;
+      code_prev = code;
     }
+    if (i & 3) cd[i >> 2] = (uint8_t)cacc;
     if (mstart != -1) {
       if (nr == rcap && grow_regions(&rs, &re, &rcap)) {
         free(ca); free(ma); free(rs); free(re); free(buf);

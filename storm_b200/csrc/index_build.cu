@@ -4,7 +4,7 @@
 // index.c:212-241).
 //
 // Build = seed keys of every indexed position (kernel) -> stable LSD radix sort of (key, pos)
-// -> per-key counts -> repeat filter (exact integer moments; the host turns them into the
+// -> per-key runs of the sorted list (start, count) -> repeat filter (exact integer moments; the host turns them into the
 // largest admissible count) -> two scans -> compaction into the CSR.  HBM-streaming work.
 #include <cmath>
 #include <vector>
@@ -32,9 +32,20 @@ __global__ void seed_keys_kernel(const uint8_t* __restrict__ codes, const int64_
   pos[t] = (uint32_t)p;
 }
 
-__global__ void count_keys_kernel(const uint32_t* __restrict__ keys, int64_t n, int32_t* __restrict__ counts) {
-  int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t < n) atomicAdd(&counts[keys[t]], 1);
+// Runs of equal keys in the sorted list: start[k] = first index of key k, end[k] = one past its
+// last (both left at 0 for absent keys), so that count = end - start with no atomics.
+__global__ void key_runs_kernel(const uint32_t* __restrict__ skeys, int64_t n, int32_t* __restrict__ start,
+                                int32_t* __restrict__ end) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const uint32_t k = skeys[t];
+  if (t == 0 || skeys[t - 1] != k) start[k] = (int32_t)t;
+  if (t == n - 1 || skeys[t + 1] != k) end[k] = (int32_t)(t + 1);
+}
+
+__global__ void run_counts_kernel(const int32_t* __restrict__ start, int64_t nkeys, int32_t* __restrict__ counts) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < nkeys) counts[k] -= start[k];
 }
 
 __global__ void moments_kernel(const int32_t* __restrict__ counts, int64_t nkeys,
@@ -164,18 +175,19 @@ int build_one_index(const uint8_t* d_codes, int64_t n_codes, const int32_t* rs, 
   uint32_t* sk = which ? k1 : k0;
   uint32_t* sv = which ? v1 : v0;
   SG_CUDA(cudaMemsetAsync(counts, 0, sizeof(int32_t) * nkeys, st));
-  count_keys_kernel<<<(unsigned)((total + TB - 1) / TB), TB, 0, st>>>(sk, total, counts);
+  SG_CUDA(cudaMemsetAsync(allstart, 0, sizeof(int32_t) * nkeys, st));
+  key_runs_kernel<<<(unsigned)((total + TB - 1) / TB), TB, 0, st>>>(sk, total, allstart, counts);
+  run_counts_kernel<<<(unsigned)((nkeys + TB - 1) / TB), TB, 0, st>>>(allstart, nkeys, counts);
   SG_CUDA(cudaMemsetAsync(mom, 0, sizeof(unsigned long long) * 2, st));
   moments_kernel<<<592, TB, 0, st>>>(counts, nkeys, mom);
-  L += 2;
+  L += 3;
   unsigned long long hm[2];
   SG_CUDA(cudaMemcpyAsync(hm, mom, sizeof(hm), cudaMemcpyDeviceToHost, st));
   SG_CUDA(cudaStreamSynchronize(st));
   int32_t cmax = repeat_cutoff(stdev_distance, total, hm[0], hm[1]);
   kept_kernel<<<(unsigned)((nkeys + TB - 1) / TB), TB, 0, st>>>(counts, nkeys, cmax, kept);
   exclusive_scan<int32_t, int32_t>(kept, out->first, nkeys, out->first + nkeys, (int32_t*)tmp, st);
-  exclusive_scan<int32_t, int32_t>(counts, allstart, nkeys, (int32_t*)nullptr, (int32_t*)tmp, st);
-  L += 1 + 6;
+  L += 1 + 3;
   int32_t nmap = 0;
   SG_CUDA(cudaMemcpyAsync(&nmap, out->first + nkeys, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
   SG_CUDA(cudaStreamSynchronize(st));

@@ -3,7 +3,7 @@
 // Per pass: (1) per-tile digit histograms, stored digit-major so that (2) one exclusive scan
 // gives every (digit, tile) its output offset, then (3) each tile re-reads its items and
 // scatters them, ranking equal digits in input order with __match_any_sync inside a warp and
-// a per-digit running count across the warps and rounds of the tile.  Stability is what the
+// per-(warp, digit) offsets across the warps of the tile.  Stability is what the
 // seed index needs: positions are generated in increasing order and must stay so per key.
 #pragma once
 
@@ -32,45 +32,63 @@ static __global__ void radix_hist_kernel(const uint32_t* __restrict__ keys, int6
     hist[(int64_t)d * ntiles + blockIdx.x] = h[d];
 }
 
+// Each warp owns a contiguous eighth of the tile: 16 rounds of 32 items, held in
+// registers.  The warps count their digits apart (per-warp counters in shared memory), one
+// block-wide pass turns the counts into per-(warp, digit) output offsets, and each warp then
+// scatters its items in input order: two block barriers per tile.
 static __global__ void radix_scatter_kernel(const uint32_t* __restrict__ keys_in,
                                      const uint32_t* __restrict__ vals_in, int64_t n, int shift,
                                      const uint32_t* __restrict__ offs, int ntiles,
                                      uint32_t* __restrict__ keys_out, uint32_t* __restrict__ vals_out) {
   constexpr int NW = kSortThreads / 32;
-  __shared__ uint32_t run[kRadixBins];
+  constexpr int PER_WARP = kSortTile / NW;  // = 32 * kSortRounds
   __shared__ uint32_t wc[NW][kRadixBins];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (int d = threadIdx.x; d < kRadixBins; d += blockDim.x) run[d] = offs[(int64_t)d * ntiles + blockIdx.x];
-  const int64_t base = (int64_t)blockIdx.x * kSortTile;
   const unsigned lt = (1u << lane) - 1u;
-  for (int r = 0; r < kSortRounds; ++r) {
-    const int64_t i = base + (int64_t)r * kSortThreads + threadIdx.x;
-    const bool valid = i < n;
-    uint32_t k = valid ? keys_in[i] : 0u, v = valid ? vals_in[i] : 0u;
-    int d = valid ? (int)((k >> shift) & (kRadixBins - 1)) : kRadixBins;  // invalid: own group
-    for (int t = threadIdx.x; t < NW * kRadixBins; t += blockDim.x) (&wc[0][0])[t] = 0;
-    __syncthreads();
-    unsigned peers = __match_any_sync(0xffffffffu, d);
-    int rank = __popc(peers & lt);
-    if (valid && rank == 0) wc[warp][d] = (uint32_t)__popc(peers);
-    __syncthreads();
-    for (int dd = threadIdx.x; dd < kRadixBins; dd += blockDim.x) {
-      uint32_t o = run[dd];
+  const int64_t base = (int64_t)blockIdx.x * kSortTile + (int64_t)warp * PER_WARP + lane;
+  uint32_t k[kSortRounds], v[kSortRounds];
 #pragma unroll
-      for (int w = 0; w < NW; ++w) {
-        uint32_t c = wc[w][dd];
-        wc[w][dd] = o;
-        o += c;
-      }
-      run[dd] = o;
+  for (int r = 0; r < kSortRounds; ++r) {
+    const int64_t i = base + 32 * r;
+    k[r] = i < n ? keys_in[i] : 0u;
+    v[r] = i < n ? vals_in[i] : 0u;
+  }
+  for (int d = lane; d < kRadixBins; d += 32) wc[warp][d] = 0;
+  __syncwarp();
+#pragma unroll
+  for (int r = 0; r < kSortRounds; ++r) {  // the warp's digit counts
+    const bool valid = base + 32 * r < n;
+    const int d = valid ? (int)((k[r] >> shift) & (kRadixBins - 1)) : kRadixBins;
+    const unsigned peers = __match_any_sync(0xffffffffu, d);
+    if (valid && __popc(peers & lt) == 0) wc[warp][d] += (uint32_t)__popc(peers);
+    __syncwarp();
+  }
+  __syncthreads();
+  for (int d = threadIdx.x; d < kRadixBins; d += blockDim.x) {  // counts -> offsets, warps in order
+    uint32_t o = offs[(int64_t)d * ntiles + blockIdx.x];
+#pragma unroll
+    for (int w = 0; w < NW; ++w) {
+      const uint32_t c = wc[w][d];
+      wc[w][d] = o;
+      o += c;
     }
-    __syncthreads();
+  }
+  __syncthreads();
+#pragma unroll
+  for (int r = 0; r < kSortRounds; ++r) {
+    const bool valid = base + 32 * r < n;
+    const int d = valid ? (int)((k[r] >> shift) & (kRadixBins - 1)) : kRadixBins;
+    const unsigned peers = __match_any_sync(0xffffffffu, d);
+    const int rank = __popc(peers & lt);
+    uint32_t at = 0;
+    if (valid) at = wc[warp][d];
+    __syncwarp();
     if (valid) {
-      uint32_t dst = wc[warp][d] + (uint32_t)rank;
-      keys_out[dst] = k;
-      vals_out[dst] = v;
+      keys_out[at + rank] = k[r];
+      vals_out[at + rank] = v[r];
+      if (rank == 0) wc[warp][d] = at + (uint32_t)__popc(peers);
     }
-    __syncthreads();
+    __syncwarp();
   }
 }
 

@@ -37,6 +37,10 @@ def run_case(name: str, work: str):
     w, ref, reads = scale_cases.make_inputs(name, d)
     colour = w["mode"] == "colour"
     plan = scale_cases.runs(name, w, reads, d)
+    for _, _, _, sam, un in plan:          # outputs of an earlier attempt must not feed a chain
+        for p in (sam, un):
+            if os.path.exists(p):
+                os.remove(p)
     entry = {"case": c, "inputs_sha256_16": scale_cases.inputs_digest(ref, reads),
              "reads_per_length": scale_cases.sample_sizes(reads), "threads": os.cpu_count(), "runs": {}}
     t0 = time.time()

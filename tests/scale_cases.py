@@ -96,8 +96,9 @@ def runs(name: str, w, reads: str, d: str):
 
 
 def skip_run(path: str) -> bool:
-    """A chain's run whose input, the previous run's -O FASTQ, is empty does not run."""
-    return os.path.exists(path) and os.path.getsize(path) == 0
+    """A chain's run whose input, the previous run's -O FASTQ, is empty or was never written
+    (the chain stopped earlier) does not run."""
+    return not os.path.exists(path) or os.path.getsize(path) == 0
 
 
 def command_args(w, seeds, reads: str, sam: str, unmapped: str, ref: str):
