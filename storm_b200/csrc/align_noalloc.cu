@@ -127,6 +127,7 @@ extern "C" int stormgpu_align_noalloc(const stormgpu_params* params, const uint8
   ScoreParams sp = make_score_params(*params);
   sp.Is = 1 << 28;            // window = diag - I exactly
   sp.min_score = -(1 << 29);  // always trace back
+  sp.packed = 0;                // every cell exact: no floor
   const int64_t rb = (read_len + 3) / 4;
   ReadsDev rd{1, read, rb, levels, rb, len};
   PassBuffers pb;

@@ -123,7 +123,8 @@ struct BandWindow {
 
 // BWT > 0: the band width 2I + 1 as a constant, so that the row arrays live in registers;
 // BWT = 0: any width up to kMaxBand (arrays in local memory).  CM: 0 nucleotide, 1 colour
-// space (the colour state machine compiled in), -1 either (sp.colour).
+// space (the colour state machine compiled in), -1 either (sp.colour); the kernel's CM = 2 runs
+// the packed nucleotide form below (align_one_nuc).
 // A candidate whose running abort bound falls below the replay's threshold stops at that row:
 // -t, or with rounds the running threshold its read had after the rounds before (the replay's
 // threshold only rises, so the candidate is aborted whatever comes before it), and neither its
@@ -306,23 +307,82 @@ __device__ __forceinline__ int align_one(const ReadsDev& rd, const ScoreParams& 
   return rows;
 }
 
-// Nucleotide space with a constant band: the same DP as align_one, each cell kept in one
-// register as score * 2048 + from * 512 + indels (from: 3 corner, 2 top, 1 left).  The largest of
-// the three candidate values is the reference's choice (alignment.c:521-532: the higher score,
-// and on equal scores corner before top before left), carrying its direction and indel count,
-// so a cell costs one three-way max instead of compares and selects on separate score and state
-// arrays.  Cells are floored at kCellFloor (score -2^19): a cell below it cannot lie on the path
-// of an alignment whose score exceeds any threshold (a path gains at most the match score per
-// row), it can only lower the candidates of its neighbours, and a row whose maximum is below it
-// bounds every threshold out (bound below -t); so every score, bound and traceback the replay
-// reads is the reference's, and the packed value never overflows.
-constexpr int kCellShift = 11;
-constexpr int kCellFloor = -(1 << 30);
+// Nucleotide space with a constant band: the DP of align_one with each cell in one register,
+//   score << 13 | from << 10 (one-hot: corner 4, top 2, left 1) | guard << 8 | ind',
+// ind' = indels + 256 - I in 8 bits, whose carry into the guard bit marks indels == I (no gap
+// may leave such a cell).  The largest candidate value is the reference's choice
+// (alignment.c:521-532: the higher score, on equal scores corner before top before left) and
+// carries its direction and indel count, so a cell is one three-way max.  The gap candidates
+// are formed with integer multiply-adds, which issue on the FMA pipe beside the ALU's logic and
+// max operations: t + (open << 13 | 1) relabelled as a gap, plus (t & (its from bit | guard))
+// times a constant K chosen modulo 2^32 so that the from bit adds (ext - open) << 13 (an
+// extension) and the guard about -2^30, which puts a gap the reference does not allow below
+// every cell.  Direction bits are moved into the row's words by multiply-adds too.
+// Cells are floored at score -2^16: a cell below it cannot lie on the path of an alignment the
+// replay keeps (sp.packed holds only when -t - L * match stays above it), it only lowers its
+// neighbours' candidates, and the row maximum starts at MIN_SCORE, above it; so every score,
+// bound and traceback the replay reads is the reference's, and no packed value overflows.
+constexpr int kCellShift = 13;
+constexpr int kCellFloor = -(1 << 29);
+constexpr uint32_t kFromC = 1u << 12, kFromT = 1u << 11, kFromL = 1u << 10, kFromAll = kFromC | kFromT | kFromL;
+constexpr uint32_t kGuard = 1u << 8;
+
+__device__ __forceinline__ uint32_t mad_lo(uint32_t a, uint32_t b, uint32_t c) {
+  uint32_t d;
+  asm("mad.lo.u32 %0, %1, %2, %3;" : "=r"(d) : "r"(a), "r"(b), "r"(c));
+  return d;
+}
+__device__ __forceinline__ uint32_t mad_hi(uint32_t a, uint32_t b, uint32_t c) {
+  uint32_t d;
+  asm("mad.hi.u32 %0, %1, %2, %3;" : "=r"(d) : "r"(a), "r"(b), "r"(c));
+  return d;
+}
+
+// One row of the packed DP: v[] holds the previous row and becomes this one; mis / msk hold a
+// bit at 2c for a mismatching / masked cell c (word c >> 4); returns the row maximum.
+template <int BW, bool MASKED>
+__device__ __forceinline__ int packed_row(int (&v)[BW], uint32_t (&wd)[(2 * BW + 31) / 32], const uint32_t* mis,
+                                          const uint32_t* msk, int SM, int SX, int MINS, const ScoreParams& sp) {
+  int mol = MINS, left = 0, pend = MINS;
+#pragma unroll
+  for (int c = 0; c < BW; ++c) {
+    const uint32_t bit = 1u << (2 * (c & 15));
+    int s0 = (mis[c >> 4] & bit) ? SX : SM;
+    if (MASKED && (msk[c >> 4] & bit)) s0 = MINS;
+    const uint32_t cv = ((uint32_t)v[c] & ~kFromAll) | kFromC;
+    int nv = max((int)mad_lo((uint32_t)s0, sp.one, cv), kCellFloor);
+    int top = 0, lft = 0;
+    if (c + 1 < BW) {
+      const uint32_t t = (uint32_t)v[c + 1];
+      const uint32_t b = (mad_lo(t, sp.one, sp.open1) & ~kFromAll) | kFromT;
+      top = (int)mad_lo(t & (kFromT | kGuard), sp.kt, b);
+    }
+    if (c > 0) {
+      const uint32_t l = (uint32_t)left;
+      const uint32_t b = (mad_lo(l, sp.one, sp.open1) & ~kFromAll) | kFromL;
+      lft = (int)mad_lo(l & (kFromL | kGuard), sp.kl, b);
+    }
+    if (c > 0 && c + 1 < BW) nv = __vimax3_s32(nv, top, lft);
+    else if (c + 1 < BW) nv = max(nv, top);
+    else if (c > 0) nv = max(nv, lft);
+    v[c] = nv;
+    left = nv;
+    if (c & 1) mol = __vimax3_s32(mol, pend, nv);
+    else if (c + 1 == BW) mol = max(mol, nv);
+    else pend = nv;
+    const uint32_t x = (uint32_t)nv & (kFromC | kFromT);  // direction: 2 corner, 1 top, 0 left
+    const int p = 2 * (c & 15);
+    if (p <= 10) wd[c >> 4] = mad_hi(x, sp.pw[21 + p], wd[c >> 4]);
+    else wd[c >> 4] = mad_lo(x, sp.pw[p - 11], wd[c >> 4]);
+  }
+  return mol;
+}
 
 template <int BW>
 __device__ __forceinline__ int align_one_nuc(const ReadsDev& rd, const ScoreParams& sp,
                                              const uint8_t* __restrict__ genome, const uint8_t* __restrict__ mask,
                                              int64_t slot, int64_t sl, int64_t ns, const PassBuffers& pb) {
+  static_assert(BW <= 48, "three direction words per row at most");
   const int r = pb.p_read[slot];
   const int thr = (pb.thr && pb.round > 0) ? max(sp.min_score, pb.thr[r]) : sp.min_score;
   const int d = pb.p_diag[slot];
@@ -332,22 +392,22 @@ __device__ __forceinline__ int align_one_nuc(const ReadsDev& rd, const ScorePara
   const uint8_t* rdq = rd.levels ? rd.levels + (int64_t)r * rd.lstride : nullptr;
   const int win = max(d - I, -sp.Is);  // run.c:667
   constexpr int wpr = (2 * BW + 31) / 32;
+  constexpr int NW64 = (BW + 31) / 32;
   uint32_t* scr = pb.a_scratch;
-  const int OPEN = sp.gap_open * (1 << kCellShift), EXT = sp.gap_ext * (1 << kCellShift);
   const int MINS = kMinScore * (1 << kCellShift);
-  constexpr int FROM = 0x600, TOP = 0x400, LEFT = 0x200, IND = 0x1ff;
   int v[BW];
   const int mbest = sp.pair[0][3];
   BandWindow<BW> bwin;
   bwin.load(genome, mask, win);
-  {  // row 0: pair scores only (alignment.c:326-360)
+  {  // row 0: pair scores only (alignment.c:326-360); indels 0
     const int rc = code_at(rdc, 0), q = rdq ? code_at(rdq, 0) : 3;
     const int SM = sp.pair[0][q] * (1 << kCellShift), SX = sp.pair[1][q] * (1 << kCellShift);
+    const int init = (int)kFromC | (256 - I);
     uint32_t wd[wpr] = {};
 #pragma unroll
     for (int c = 0; c < BW; ++c) {
-      v[c] = (bwin.mcode(c) == 0 ? (rc != bwin.gcode(c) ? SX : SM) : MINS) | FROM;
-      wd[(2 * c) >> 5] |= 3u << ((2 * c) & 31);
+      v[c] = (bwin.mcode(c) == 0 ? (rc != bwin.gcode(c) ? SX : SM) : MINS) | init;
+      wd[(2 * c) >> 5] |= 2u << ((2 * c) & 31);
     }
 #pragma unroll
     for (int k = 0; k < wpr; ++k) scr[(int64_t)k * ns + sl] = wd[k];
@@ -359,26 +419,23 @@ __device__ __forceinline__ int align_one_nuc(const ReadsDev& rd, const ScorePara
     const int rc = code_at(rdc, i), q = rdq ? code_at(rdq, i) : 3;
     const int SM = sp.pair[0][q] * (1 << kCellShift), SX = sp.pair[1][q] * (1 << kCellShift);
     bwin.advance(genome, mask, (int64_t)win + i + BW - 1);
-    int mol = MINS, left = kCellFloor;  // the row maximum starts at MIN_SCORE (alignment.c:500)
-    bool lok = false;  // the left border (alignment.c:504-509): no gap from outside the band
-    uint32_t wd[wpr] = {};
+    uint32_t mis[2 * NW64], msk[2 * NW64];
+    bool masked = false;
+    const uint64_t rrep = (uint64_t)rc * 0x5555555555555555ull;
 #pragma unroll
-    for (int c = 0; c < BW; ++c) {
-      const int s0 = bwin.mcode(c) == 0 ? (rc != bwin.gcode(c) ? SX : SM) : MINS;
-      const int corner = (v[c] | FROM) + s0;
-      int top = kCellFloor, lft = kCellFloor;
-      if (c + 1 < BW) {
-        const int t = v[c + 1];
-        if ((t & IND) < I) top = ((t & ~FROM) | TOP) + (((t & FROM) == TOP) ? EXT : OPEN) + 1;
-      }
-      if (lok && (left & IND) < I) lft = ((left & ~FROM) | LEFT) + (((left & FROM) == LEFT) ? EXT : OPEN) + 1;
-      const int nv = max(max(max(corner, top), lft), kCellFloor);
-      v[c] = nv;
-      left = nv;
-      lok = true;
-      mol = max(mol, nv);
-      wd[(2 * c) >> 5] |= (uint32_t)((nv >> 9) & 3) << ((2 * c) & 31);
+    for (int k = 0; k < NW64; ++k) {
+      const uint64_t x = bwin.g[k] ^ rrep;
+      const uint64_t mm = (x | (x >> 1)) & 0x5555555555555555ull;
+      const uint64_t mk = (bwin.m[k] | (bwin.m[k] >> 1)) & 0x5555555555555555ull;
+      mis[2 * k] = (uint32_t)mm;
+      mis[2 * k + 1] = (uint32_t)(mm >> 32);
+      msk[2 * k] = (uint32_t)mk;
+      msk[2 * k + 1] = (uint32_t)(mk >> 32);
+      masked |= mk != 0;
     }
+    uint32_t wd[wpr] = {};
+    const int mol = masked ? packed_row<BW, true>(v, wd, mis, msk, SM, SX, MINS, sp)
+                           : packed_row<BW, false>(v, wd, mis, msk, SM, SX, MINS, sp);
     const long long ml = (long long)(mol >> kCellShift) + best_possible;
     if (ml < bound) bound = ml;
     best_possible -= mbest;
@@ -408,17 +465,17 @@ __device__ __forceinline__ int align_one_nuc(const ReadsDev& rd, const ScorePara
       i0 = i;
       j0 = j;
       const uint32_t wdir = scr[((int64_t)i * wpr + ((2 * c) >> 5)) * ns + sl];
-      const int from = (wdir >> ((2 * c) & 31)) & 3;
+      const int from = (wdir >> ((2 * c) & 31)) & 3;  // 2 corner, 1 top, 0 left
       const int rc = code_at(rdc, i);
       int op;
-      if (from == 2) op = 0xC | rc;
-      else if (from == 1) op = 0x1;
+      if (from == 1) op = 0xC | rc;
+      else if (from == 0) op = 0x1;
       else op = rc != code_at(genome, (int64_t)win + j) ? 0x4 | rc : 0x3;
       if (tl & 1) { cur |= (uint8_t)op; tb[tl >> 1] = cur; }
       else { cur = (uint8_t)(op << 4); tb[tl >> 1] = cur; }
       tl++;
-      if (from == 2) { i--; c++; }
-      else if (from == 1) { c--; }
+      if (from == 1) { i--; c++; }
+      else if (from == 0) { c--; }
       else { i--; }
     }
   }
@@ -435,7 +492,7 @@ __device__ __forceinline__ int align_one_nuc(const ReadsDev& rd, const ScorePara
 // count read from pb.npass_dev when it is given; scratch column = the thread's index in the
 // grid, so the scratch holds align_workers() columns).
 template <int BWT, int CM>
-__global__ void __launch_bounds__(128, CM == 0 ? (BWT > 0 && BWT <= 15 ? 7 : BWT == 31 ? 5 : BWT == 41 ? 4 : 1)
+__global__ void __launch_bounds__(128, CM == 2 ? (BWT > 0 && BWT <= 15 ? 7 : BWT == 31 ? 5 : BWT == 41 ? 4 : 1)
                                               : (BWT > 0 && BWT <= 15 ? 5 : BWT == 31 ? 4 : BWT == 41 ? 3 : 1)) align_kernel(ReadsDev rd, ScoreParams sp, const uint8_t* __restrict__ genome,
                                                     const uint8_t* __restrict__ mask, int64_t slot0, int64_t nslots,
                                                     PassBuffers pb) {
@@ -464,7 +521,7 @@ __global__ void __launch_bounds__(128, CM == 0 ? (BWT > 0 && BWT <= 15 ? 7 : BWT
     }
     if (s < n) {
       const int64_t slot = pb.round_slots ? (int64_t)pb.round_slots[list0 + s] : slot0 + s;
-      if constexpr (CM == 0 && BWT > 0)
+      if constexpr (CM == 2)
         rows += (unsigned long long)align_one_nuc<BWT>(rd, sp, genome, mask, slot, steal ? tid : s, ns, pb);
       else
         rows += (unsigned long long)align_one<BWT, CM>(rd, sp, genome, mask, slot, steal ? tid : s, ns, pb);
@@ -480,7 +537,8 @@ __global__ void __launch_bounds__(128, CM == 0 ? (BWT > 0 && BWT <= 15 ? 7 : BWT
 
 static const void* align_kernel_of(const ScoreParams& sp) {
 #define SG_ALIGN(BW) \
-  case BW: return sp.colour ? (const void*)align_kernel<BW, 1> : (const void*)align_kernel<BW, 0>;
+  case BW: return sp.colour ? (const void*)align_kernel<BW, 1> \
+                  : sp.packed ? (const void*)align_kernel<BW, 2> : (const void*)align_kernel<BW, 0>;
   switch (2 * sp.I + 1) {
     SG_ALIGN(7)
     SG_ALIGN(15)

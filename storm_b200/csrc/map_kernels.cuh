@@ -16,6 +16,13 @@ struct ScoreParams {
   int pair[2][4];     // SCALE_SCORE(match|mismatch, level) (alignment.h:30, alignment.c:275-278)
   int gap_open, gap_ext;
   int min_score;      // -t
+  // the packed nucleotide alignment (align_one_nuc): used when `packed`; its constants come
+  // through the kernel parameters so that the multiply-adds stay multiply-adds
+  int packed;
+  uint32_t one;       // 1
+  uint32_t open1;     // (gap_open << 13) + 1
+  uint32_t kt, kl;    // 4 (ext - open) - 2^22, 8 (ext - open) - 2^22 (modulo 2^32)
+  uint32_t pw[32];    // 2^k
 };
 
 // filter width W for the SIMD half-width Is (run.c:64-101), and the scoring of a parameter set

@@ -111,6 +111,19 @@ ScoreParams make_score_params(const stormgpu_params& p) {
   sp.gap_open = p.gap_open;
   sp.gap_ext = p.gap_extend;
   sp.min_score = p.min_score;
+  // packed cells: scores and penalties below 256 in magnitude, at most 200 indels, and -t
+  // minus the most a read can gain above the floor's score -2^16 (align_one_nuc)
+  int maxpair = 0;
+  for (int l = 0; l < 4; ++l) maxpair = std::max({maxpair, std::abs(sp.pair[0][l]), std::abs(sp.pair[1][l])});
+  sp.packed = !p.colour && p.allowed_indels >= 0 && p.allowed_indels <= 200 && maxpair <= 255 &&
+              std::abs(p.gap_open) <= 255 && std::abs(p.gap_extend) <= 255 &&
+              (int64_t)p.min_score - (int64_t)STORMGPU_MAX_READ_LEN * maxpair > -60000;
+  sp.one = 1u;
+  sp.open1 = (uint32_t)p.gap_open * 8192u + 1u;
+  const uint32_t dx = (uint32_t)(p.gap_extend - p.gap_open);
+  sp.kt = 4u * dx - (1u << 22);
+  sp.kl = 8u * dx - (1u << 22);
+  for (int k = 0; k < 32; ++k) sp.pw[k] = 1u << k;
   return sp;
 }
 
@@ -734,6 +747,7 @@ extern "C" int stormgpu_align(const stormgpu_params* params, const uint8_t* read
   ScoreParams sp = make_score_params(*params);
   sp.Is = 1 << 28;              // window = diag - I exactly
   sp.min_score = -(1 << 29);    // always trace back
+  sp.packed = 0;                // every cell exact: no floor
   uint8_t *ga, *gb, *ma, *mb;
   if (upload_padded(genome, n_codes, pad, 0, &ga, &gb)) return STORMGPU_ECUDA;
   if (upload_padded(mask, n_codes, pad, 0x55, &ma, &mb)) return STORMGPU_ECUDA;

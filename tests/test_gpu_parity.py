@@ -141,14 +141,36 @@ def _reads_arrays(seqs, quals, colour_first_levels=None):
     return codes, levels, np.array([len(s) for s in seqs], np.int16)
 
 
-@pytest.mark.parametrize("colour,indels,seeds", [
-    (0, 3, "####--#-#--##--####;#####--###-#-###;###-##-#######"),
-    (0, 15, "##-##-###-###;###--#-#--#--####"),
-    (1, 7, "####-##-#-####;###-#--##-##--###;####-#---#----#--####"),
+def _masked_runs(n, rng, frac=0.004):
+    """Masked runs (start, end) of 1-30 codes covering about `frac` of n codes, and the 0/1 mask."""
+    m = np.zeros(n, np.uint8)
+    runs = []
+    pos = int(rng.integers(0, 400))
+    while True:
+        pos += int(rng.integers(1, int(30 / frac)))
+        if pos >= n - 40:
+            break
+        ln = int(rng.integers(1, 31))
+        m[pos:pos + ln] = 1
+        runs.append((pos, pos + ln))
+        pos += ln
+    return runs, m
+
+
+@pytest.mark.parametrize("colour,indels,seeds,masked,min_score", [
+    (0, 3, "####--#-#--##--####;#####--###-#-###;###-##-#######", False, 100),
+    (0, 15, "##-##-###-###;###--#-#--#--####", False, 100),
+    (1, 7, "####-##-#-####;###-#--##-##--###;####-#---#----#--####", False, 110),
+    # masked reference runs (alignment rows with masked cells), every constant band width
+    (0, 7, "####--#-#--##--####;#####--###-#-###;###-##-#######", True, 100),
+    (0, 15, "##-##-###-###;###--#-#--#--####", True, 60),
+    (0, 20, "##-##-###-###;###--#-#--#--####", True, 100),
 ])
-def test_map_api_vs_oracle(colour, indels, seeds):
+def test_map_api_vs_oracle(colour, indels, seeds, masked, min_score):
     from storm_b200 import synth
     genome = synth.make_genome([40000, 15000], 21, gc=0.45, repeat_frac=0.2)
+    rng = np.random.default_rng(77)
+    masks = [_masked_runs(len(s), rng) if masked else ([], np.zeros(len(s), np.uint8)) for _, s in genome]
     if colour:
         pr, cols, q = synth.simulate_colour_reads(genome, 1500, 40, 22)
         seqs = [c for c in cols]
@@ -160,15 +182,14 @@ def test_map_api_vs_oracle(colour, indels, seeds):
         refs = genome
     codes, levels, lengths = _reads_arrays(seqs, quals)
     first_levels = np.full(len(seqs), 2, np.uint8) if colour else None
-    prm = api.params(colour=colour, indels=indels, min_score=100 if not colour else 110,
-                     min_score_filter=95)
+    prm = api.params(colour=colour, indels=indels, min_score=min_score, min_score_filter=95)
     m = api.Mapper(prm, seeds)
     packed = []
-    for name, s in refs:
+    for (name, s), (runs, mask) in zip(refs, masks):
         cp = ffi.pack2(s, PADB)
-        mk = ffi.pack2(np.zeros(len(s), np.uint8), PADB, fill=0x55)
-        packed.append((cp, mk, len(s)))
-        m.add_reference(cp[PADB:], mk[PADB:], len(s))
+        mk = ffi.pack2(mask[:len(s)], PADB, fill=0x55)
+        packed.append((cp, mk, len(s), runs))
+        m.add_reference(cp[PADB:], mk[PADB:], len(s), regions=runs)
     m.build_index()
     batch = api.ReadBatch(codes, lengths, levels, first_levels)
     res = m.map(batch)
@@ -178,17 +199,18 @@ def test_map_api_vs_oracle(colour, indels, seeds):
     orc = ffi.oracle()
     R = (ffi.OrRef * len(packed))()
     keep = []
-    for k, (cp, mk, n) in enumerate(packed):
-        zr = np.zeros(1, np.int32)
-        keep.append(zr)
-        R[k] = ffi.OrRef(cp.ctypes.data + PADB, mk.ctypes.data + PADB, n, zr.ctypes.data, zr.ctypes.data, 0)
+    for k, (cp, mk, n, runs) in enumerate(packed):
+        rs = np.array([a for a, _ in runs] or [0], np.int32)
+        re = np.array([b for _, b in runs] or [0], np.int32)
+        keep += [rs, re]
+        R[k] = ffi.OrRef(cp.ctypes.data + PADB, mk.ctypes.data + PADB, n, rs.ctypes.data, re.ctypes.data, len(runs))
     rd = ffi.ReadsT(len(seqs), codes.ctypes.data, codes.shape[1], levels.ctypes.data, levels.shape[1],
                     lengths.ctypes.data, first_levels.ctypes.data if colour else None)
     hits = np.zeros(len(seqs) * 4, dtype=api.HIT_DTYPE)
     tb = np.zeros((len(seqs) * 4, res.tb_stride), np.uint8)
     mapped = np.zeros(len(seqs), np.uint8)
     out = ffi.ResultsT(hits.ctypes.data, tb.ctypes.data, res.tb_stride, mapped.ctypes.data)
-    p = ffi.make_params(colour=colour, indels=indels, min_score=prm.min_score, min_score_filter=95)
+    p = ffi.make_params(colour=colour, indels=indels, min_score=min_score, min_score_filter=95)
     cnt = np.zeros(3, np.int64)
     assert orc.or_map(C.byref(p), seeds.encode(), R, len(packed), C.byref(rd), C.byref(out), cnt.ctypes.data) == 0
     assert np.array_equal(res.mapped, mapped)
@@ -306,10 +328,11 @@ def _oracle_map(packed, seeds, codes, levels, lengths, tbs, indels, min_score, m
     orc = ffi.oracle()
     R = (ffi.OrRef * len(packed))()
     keep = []
-    for k, (cp, mk, n) in enumerate(packed):
-        zr = np.zeros(1, np.int32)
-        keep.append(zr)
-        R[k] = ffi.OrRef(cp.ctypes.data + PADB, mk.ctypes.data + PADB, n, zr.ctypes.data, zr.ctypes.data, 0)
+    for k, (cp, mk, n, runs) in enumerate(packed):
+        rs = np.array([a for a, _ in runs] or [0], np.int32)
+        re = np.array([b for _, b in runs] or [0], np.int32)
+        keep += [rs, re]
+        R[k] = ffi.OrRef(cp.ctypes.data + PADB, mk.ctypes.data + PADB, n, rs.ctypes.data, re.ctypes.data, len(runs))
     n = len(lengths)
     rd = ffi.ReadsT(n, codes.ctypes.data, codes.shape[1], levels.ctypes.data, levels.shape[1], lengths.ctypes.data,
                     None)
@@ -351,7 +374,7 @@ def test_map_of_tandem_repeats_vs_oracle():
         st = m.stats()
         assert st["hit_positions"] / len(seqs) > 20000, st  # the strand a read came from gathers ~50,000
     m.close()
-    hits, tb, mapped = _oracle_map([(cp, mk, len(g))], seeds, codes, levels, lengths, tbs, 15, 100, 100)
+    hits, tb, mapped = _oracle_map([(cp, mk, len(g), [])], seeds, codes, levels, lengths, tbs, 15, 100, 100)
     assert mapped.sum() > len(seqs) // 2
     for res in results:
         assert np.array_equal(res.mapped, mapped)
