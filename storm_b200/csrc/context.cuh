@@ -103,6 +103,10 @@ struct stormgpu_ctx {
   cudaEvent_t rev[2 * 6 + 1];  // alignment rounds: before the first, after each round's alignment and replay
   int64_t last_n = -1;  // reads of the last stormgpu_map call (its results stay in hits / mapped)
   sg::WorkBudget work;  // working memory of the mapping buffers; work.limit 0 = no limit
+  // candidates and passing candidates per read of the densest strand pass of the last mapping
+  // call: a batch that would exceed a pass's bounds at that density is cut up front instead of
+  // after its gather
+  double dens_cand = 0, dens_pass = 0;
   // genome_map placement
   sg::DevBuf<uint32_t> gm_k0, gm_v0, gm_k1, gm_v1, gm_tmp, gm_base;
 };

@@ -318,10 +318,11 @@ __device__ __forceinline__ int align_one(const ReadsDev& rd, const ScoreParams& 
 // times a constant K chosen modulo 2^32 so that the from bit adds (ext - open) << 13 (an
 // extension) and the guard about -2^30, which puts a gap the reference does not allow below
 // every cell.  Direction bits are moved into the row's words by multiply-adds too.
-// Cells are floored at score -2^16: a cell below it cannot lie on the path of an alignment the
-// replay keeps (sp.packed holds only when -t - L * match stays above it), it only lowers its
-// neighbours' candidates, and the row maximum starts at MIN_SCORE, above it; so every score,
-// bound and traceback the replay reads is the reference's, and no packed value overflows.
+// Cells are floored at score -2^16 (every 16 rows, and in rows with masked cells): a floored
+// cell, and any cell whose value derives from one, stays below -2^16 + L * (largest pair score),
+// under the row maximum's start MIN_SCORE and below every cell of a path the replay can keep
+// (sp.packed holds only when -t - L * match stays above it); so every score, bound and traceback
+// the replay reads is the reference's, and no packed value overflows.
 constexpr int kCellShift = 13;
 constexpr int kCellFloor = -(1 << 29);
 constexpr uint32_t kFromC = 1u << 12, kFromT = 1u << 11, kFromL = 1u << 10, kFromAll = kFromC | kFromT | kFromL;
@@ -339,23 +340,29 @@ __device__ __forceinline__ uint32_t mad_hi(uint32_t a, uint32_t b, uint32_t c) {
 }
 
 // One row of the packed DP: v[] holds the previous row and becomes this one; mis / msk hold a
-// bit at 2c for a mismatching / masked cell c (word c >> 4); returns the row maximum.
+// bit at 2c for a mismatching / masked cell c (word c >> 4); returns the row maximum.  The
+// corner relabelling of v[c + 1] serves both this cell's top candidate and the next cell's
+// corner.  Rows without masked cells skip the floor (align_one_nuc floors every cell every 16
+// rows: between those a cell falls by at most 16 * 255 << 13, so nothing overflows and a gap
+// the reference forbids still lands below every cell); rows with masked cells (MIN_SCORE)
+// floor every cell.
 template <int BW, bool MASKED>
 __device__ __forceinline__ int packed_row(int (&v)[BW], uint32_t (&wd)[(2 * BW + 31) / 32], const uint32_t* mis,
                                           const uint32_t* msk, int SM, int SX, int MINS, const ScoreParams& sp) {
   int mol = MINS, left = 0, pend = MINS;
+  uint32_t cv = ((uint32_t)v[0] & ~kFromAll) | kFromC;  // v[c] relabelled as a corner source
 #pragma unroll
   for (int c = 0; c < BW; ++c) {
     const uint32_t bit = 1u << (2 * (c & 15));
     int s0 = (mis[c >> 4] & bit) ? SX : SM;
     if (MASKED && (msk[c >> 4] & bit)) s0 = MINS;
-    const uint32_t cv = ((uint32_t)v[c] & ~kFromAll) | kFromC;
-    int nv = max((int)mad_lo((uint32_t)s0, sp.one, cv), kCellFloor);
+    int nv = (int)mad_lo((uint32_t)s0, sp.one, cv);
+    if (MASKED) nv = max(nv, kCellFloor);
     int top = 0, lft = 0;
     if (c + 1 < BW) {
       const uint32_t t = (uint32_t)v[c + 1];
-      const uint32_t b = (mad_lo(t, sp.one, sp.open1) & ~kFromAll) | kFromT;
-      top = (int)mad_lo(t & (kFromT | kGuard), sp.kt, b);
+      cv = (t & ~kFromAll) | kFromC;
+      top = (int)mad_lo(t & (kFromT | kGuard), sp.kt, mad_lo(cv, sp.one, sp.open1_tc));
     }
     if (c > 0) {
       const uint32_t l = (uint32_t)left;
@@ -434,6 +441,10 @@ __device__ __forceinline__ int align_one_nuc(const ReadsDev& rd, const ScorePara
       masked |= mk != 0;
     }
     uint32_t wd[wpr] = {};
+    if ((i & 15) == 0) {
+#pragma unroll
+      for (int c = 0; c < BW; ++c) v[c] = max(v[c], kCellFloor);
+    }
     const int mol = masked ? packed_row<BW, true>(v, wd, mis, msk, SM, SX, MINS, sp)
                            : packed_row<BW, false>(v, wd, mis, msk, SM, SX, MINS, sp);
     const long long ml = (long long)(mol >> kCellShift) + best_possible;

@@ -21,6 +21,7 @@ struct ScoreParams {
   int packed;
   uint32_t one;       // 1
   uint32_t open1;     // (gap_open << 13) + 1
+  uint32_t open1_tc;  // open1 + (1 << 11) - (1 << 12): a corner-labelled cell as a top gap source
   uint32_t kt, kl;    // 4 (ext - open) - 2^22, 8 (ext - open) - 2^22 (modulo 2^32)
   uint32_t pw[32];    // 2^k
 };

@@ -2,6 +2,7 @@
 // and the mapping pipeline (per reference sequence, per strand: hit gather -> filter ->
 // full alignment -> top-4 replay), plus the unit-level entry points used by the tests.
 #include <algorithm>
+#include <cmath>
 #include <cstdarg>
 #include <cstdlib>
 #include <cstring>
@@ -111,15 +112,18 @@ ScoreParams make_score_params(const stormgpu_params& p) {
   sp.gap_open = p.gap_open;
   sp.gap_ext = p.gap_extend;
   sp.min_score = p.min_score;
-  // packed cells: scores and penalties below 256 in magnitude, at most 200 indels, and -t
-  // minus the most a read can gain above the floor's score -2^16 (align_one_nuc)
+  // packed cells (align_one_nuc): scores and penalties below 256 in magnitude, at most 200
+  // indels, a read's largest gain below 48000 (a floored cell stays under MIN_SCORE) and -t
+  // minus that gain above the floor's score -2^16
   int maxpair = 0;
   for (int l = 0; l < 4; ++l) maxpair = std::max({maxpair, std::abs(sp.pair[0][l]), std::abs(sp.pair[1][l])});
   sp.packed = !p.colour && p.allowed_indels >= 0 && p.allowed_indels <= 200 && maxpair <= 255 &&
               std::abs(p.gap_open) <= 255 && std::abs(p.gap_extend) <= 255 &&
+              (int64_t)STORMGPU_MAX_READ_LEN * maxpair < 48000 &&
               (int64_t)p.min_score - (int64_t)STORMGPU_MAX_READ_LEN * maxpair > -60000;
   sp.one = 1u;
   sp.open1 = (uint32_t)p.gap_open * 8192u + 1u;
+  sp.open1_tc = sp.open1 + (1u << 11) - (1u << 12);
   const uint32_t dx = (uint32_t)(p.gap_extend - p.gap_open);
   sp.kt = 4u * dx - (1u << 22);
   sp.kl = 8u * dx - (1u << 22);
@@ -340,6 +344,7 @@ static int map_device_once(stormgpu_ctx* c, const stormgpu_reads* reads, stormgp
   const int wpr = (2 * BW + 31) / 32 + (sp.colour ? (BW + 31) / 32 : 0);
   const int64_t tbs = ((maxL + sp.I + 1) / 2 + 7) & ~7LL;
   float tg = 0, tf = 0, ta = 0, tr = 0;
+  int64_t max_cand = 0, max_pass = 0;  // densest strand pass of this call
   SG_CUDA(cudaEventRecord(c->ev[6], st));
   for (size_t ref_id = 0; ref_id < c->refs.size(); ++ref_id) {
     RefSeq& R = c->refs[ref_id];
@@ -396,6 +401,7 @@ static int map_device_once(stormgpu_ctx* c, const stormgpu_reads* reads, stormgp
         SG_CUDA(cudaMemcpyAsync(g, c->counters.p, sizeof(g), cudaMemcpyDeviceToHost, st));
         SG_CUDA(cudaStreamSynchronize(st));
         utot = (int64_t)g[7];
+        max_cand = std::max(max_cand, utot);
         if (utot > kMaxCandidatesPerPass) return kSplitBatch;
         if (!g[8]) break;
         if (attempt > 2) { sg_set_error("internal: candidate list overflow"); return STORMGPU_EINVAL; }
@@ -437,6 +443,7 @@ static int map_device_once(stormgpu_ctx* c, const stormgpu_reads* reads, stormgp
       S.seed_lookups += (int64_t)cnt[3];
       S.hit_positions += (int64_t)cnt[4];
       S.filter_passed += npass;
+      max_pass = std::max(max_pass, npass);
       if (npass > kMaxPassingPerPass && n > 1) return kSplitBatch;
       PassBuffers pb;
       memset(&pb, 0, sizeof(pb));
@@ -525,10 +532,49 @@ static int map_device_once(stormgpu_ctx* c, const stormgpu_reads* reads, stormgp
   cudaEventElapsedTime(&tt, c->ev[6], c->ev[7]);
   S.ms_gather = tg; S.ms_filter = tf; S.ms_align = ta; S.ms_replay = tr; S.ms_total = tt;
   S.kernels = launches;
+  if (n > 0) {
+    c->dens_cand = (double)max_cand / (double)n;
+    c->dens_pass = (double)max_pass / (double)n;
+  }
+  return 0;
+}
+
+// Maps reads[lo, hi) into the matching part of out.
+static int map_range(stormgpu_ctx* c, const stormgpu_reads* reads, stormgpu_results* out, int64_t lo, int64_t hi) {
+  stormgpu_reads r = *reads;
+  stormgpu_results o = *out;
+  r.n = hi - lo;
+  r.codes += lo * reads->code_stride;
+  if (r.levels) r.levels += lo * reads->level_stride;
+  r.lengths += lo;
+  if (r.first_levels) r.first_levels += lo;
+  o.hits += 4 * lo;
+  o.tb += 4 * lo * out->tb_stride;
+  o.mapped += lo;
+  return sg::map_device_impl(c, &r, &o);
+}
+
+// Maps the batch as k consecutive pieces of (nearly) equal size, the stats summed.
+static int map_pieces(stormgpu_ctx* c, const stormgpu_reads* reads, stormgpu_results* out, int64_t k) {
+  const int64_t n = reads->n;
+  stormgpu_stats acc;
+  memset(&acc, 0, sizeof(acc));
+  for (int64_t q = 0; q < k; ++q) {
+    if (const int e = map_range(c, reads, out, n * q / k, n * (q + 1) / k)) return e;
+    add_stats(acc, c->stats);
+  }
+  acc.ms_index = c->stats.ms_index;
+  c->stats = acc;
   return 0;
 }
 
 int sg::map_device_impl(stormgpu_ctx* c, const stormgpu_reads* reads, stormgpu_results* out) {
+  {  // at the last call's density the batch would be cut after its gather: cut it now
+    const int64_t n = reads->n;
+    const double need = std::max(c->dens_cand * (double)n / (0.9 * (double)kMaxCandidatesPerPass),
+                                 c->dens_pass * (double)n / (0.9 * (double)kMaxPassingPerPass));
+    if (n > 1 && need > 1.0) return map_pieces(c, reads, out, std::min<int64_t>(n, (int64_t)std::ceil(need)));
+  }
   WorkBudget* saved = g_work_budget;
   g_work_budget = &c->work;
   c->work.over = false;
@@ -547,23 +593,7 @@ int sg::map_device_impl(stormgpu_ctx* c, const stormgpu_reads* reads, stormgpu_r
     sg_set_error("one read has more than %lld candidate diagonals", (long long)kMaxCandidatesPerPass);
     return STORMGPU_ENOMEM;
   }
-  const int64_t h = n / 2;
-  stormgpu_reads r1 = *reads, r2 = *reads;
-  stormgpu_results o1 = *out, o2 = *out;
-  r1.n = h;
-  r2.n = n - h;
-  r2.codes += h * reads->code_stride;
-  if (r2.levels) r2.levels += h * reads->level_stride;
-  r2.lengths += h;
-  if (r2.first_levels) r2.first_levels += h;
-  o2.hits += 4 * h;
-  o2.tb += 4 * h * out->tb_stride;
-  o2.mapped += h;
-  if (const int e = map_device_impl(c, &r1, &o1)) return e;
-  const stormgpu_stats s1 = c->stats;
-  if (const int e = map_device_impl(c, &r2, &o2)) return e;
-  add_stats(c->stats, s1);
-  return 0;
+  return map_pieces(c, reads, out, 2);
 }
 
 extern "C" int stormgpu_map_device(stormgpu_ctx* c, const stormgpu_reads* reads, stormgpu_results* out,
