@@ -488,8 +488,10 @@ def mixed_arm(a, w):
         per_step = {k: v for k, v in stages.items() if not k.startswith("_")}
         dom = max(("sw_filter", "full_align", "hit_gather"), key=lambda k: per_step.get(k, {}).get("ms", 0))
         traffic = None
-        if os.path.exists(TRAFFIC_PATH):
-            traffic = json.load(open(TRAFFIC_PATH)).get("mixed_100M", {}).get(dom, {}).get("bytes_per_launch")
+        if os.path.exists(TRAFFIC_PATH) and dom == "sw_filter" and agg.get("passes"):
+            per_cell = json.load(open(TRAFFIC_PATH)).get("mixed_100M", {}).get(dom, {}).get("bytes_per_cell_update")
+            if per_cell:  # measured on a small case, scaled to the mean launch of the timed steps
+                traffic = per_cell * agg["filter_cells"] / agg["passes"]
         roof = {"kernel": dom, "bound": per_step[dom]["bound"], "achieved": per_step[dom]["achieved"],
                 "peak": per_step[dom]["peak"], "unit": per_step[dom]["unit"], "frac": per_step[dom]["frac"],
                 "traffic": traffic,

@@ -204,6 +204,8 @@ typedef struct stormgpu_stats {
   int64_t kernels;           /* kernel launches */
   int64_t filter_band_cells; /* band cells of the filtered diagonals: L * (2*min(i,15)+1) each */
   double  ms_index, ms_gather, ms_filter, ms_align, ms_replay, ms_total;
+  int64_t passes;            /* strand passes run (one filter launch each; a batch cut into pieces
+                                runs one per piece, sequence and strand) */
 } stormgpu_stats;
 int stormgpu_get_stats(stormgpu_ctx *ctx, stormgpu_stats *out);
 

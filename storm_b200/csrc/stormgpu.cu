@@ -274,7 +274,7 @@ static void add_stats(stormgpu_stats& S, const stormgpu_stats& s) {
   S.candidates += s.candidates; S.filter_passed += s.filter_passed; S.aligned += s.aligned;
   S.seed_lookups += s.seed_lookups; S.hit_positions += s.hit_positions; S.filter_cells += s.filter_cells;
   S.align_cells += s.align_cells; S.kernels += s.kernels; S.filter_band_cells += s.filter_band_cells;
-  S.ms_gather += s.ms_gather; S.ms_filter += s.ms_filter; S.ms_align += s.ms_align;
+  S.ms_gather += s.ms_gather; S.ms_filter += s.ms_filter; S.ms_align += s.ms_align; S.passes += s.passes;
   S.ms_replay += s.ms_replay; S.ms_total += s.ms_total;
 }
 
@@ -427,6 +427,7 @@ static int map_device_once(stormgpu_ctx* c, const stormgpu_reads* reads, stormgp
       job.gexp = R.d_gexp; job.rexp = c->rexp.p; job.rstride = rstride; job.min_len = minL;
       launch_filter_flat_job(job, sp, filter_dpx_ok(sp, maxL), st);
       launches += 2;
+      S.passes++;
       SG_CUDA(cudaEventRecord(c->ev[2], st));
       launch_pack_flags(utot, c->flag.p, c->flagw.p, st);
       exclusive_scan<PassWord, int64_t>(reinterpret_cast<const PassWord*>(c->flagw.p), c->foff.p, nwords,
