@@ -488,7 +488,7 @@ def mixed_arm(a, w):
         per_step = {k: v for k, v in stages.items() if not k.startswith("_")}
         dom = max(("sw_filter", "full_align", "hit_gather"), key=lambda k: per_step.get(k, {}).get("ms", 0))
         traffic = None
-        if os.path.exists(TRAFFIC_PATH) and dom == "sw_filter" and agg.get("passes"):
+        if os.path.exists(TRAFFIC_PATH) and dom == "sw_filter" and agg.get("passes") and (a.cfg, a.scale) == (2, 1.0):
             per_cell = json.load(open(TRAFFIC_PATH)).get("mixed_100M", {}).get(dom, {}).get("bytes_per_cell_update")
             if per_cell:  # measured on a small case, scaled to the mean launch of the timed steps
                 traffic = per_cell * agg["filter_cells"] / agg["passes"]
