@@ -353,18 +353,11 @@ __device__ __forceinline__ int packed_row(int (&v)[BW], uint32_t (&wd)[(2 * BW +
   uint32_t cv = ((uint32_t)v[0] & ~kFromAll) | kFromC;  // v[c] relabelled as a corner source
 #pragma unroll
   for (int c = 0; c < BW; ++c) {
-    int nv;
-    if (MASKED) {
-      const uint32_t bit = 1u << (2 * (c & 15));
-      int s0 = (mis[c >> 4] & bit) ? SX : SM;
-      if (msk[c >> 4] & bit) s0 = MINS;
-      nv = max((int)mad_lo((uint32_t)s0, sp.one, cv), kCellFloor);
-    } else {  // corner = cv + SM + mismatch * (SX - SM), the mismatch bit moved to bit 31 and read
-              // off the top by multiplies: no compare or select on the ALU pipe
-      const uint32_t top_bit = mad_lo(mis[c >> 4], sp.pw[31 - 2 * (c & 15)], 0u);
-      const uint32_t mb = mad_hi(top_bit, sp.pw[1], 0u);
-      nv = (int)mad_lo(mb, (uint32_t)(SX - SM), mad_lo(cv, sp.one, (uint32_t)SM));
-    }
+    const uint32_t bit = 1u << (2 * (c & 15));
+    int s0 = (mis[c >> 4] & bit) ? SX : SM;
+    if (MASKED && (msk[c >> 4] & bit)) s0 = MINS;
+    int nv = (int)mad_lo((uint32_t)s0, sp.one, cv);
+    if (MASKED) nv = max(nv, kCellFloor);
     int top = 0, lft = 0;
     if (c + 1 < BW) {
       const uint32_t t = (uint32_t)v[c + 1];

@@ -572,8 +572,10 @@ static int map_pieces(stormgpu_ctx* c, const stormgpu_reads* reads, stormgpu_res
 int sg::map_device_impl(stormgpu_ctx* c, const stormgpu_reads* reads, stormgpu_results* out) {
   {  // at the last call's density the batch would be cut after its gather: cut it now
     const int64_t n = reads->n;
-    const double need = std::max(c->dens_cand * (double)n / (0.9 * (double)kMaxCandidatesPerPass),
-                                 c->dens_pass * (double)n / (0.9 * (double)kMaxPassingPerPass));
+    // 0.7: the pieces of one batch differ in density (read lengths, repeats), and a piece that
+    // still overflows is cut after its gather
+    const double need = std::max(c->dens_cand * (double)n / (0.7 * (double)kMaxCandidatesPerPass),
+                                 c->dens_pass * (double)n / (0.7 * (double)kMaxPassingPerPass));
     if (n > 1 && need > 1.0) return map_pieces(c, reads, out, std::min<int64_t>(n, (int64_t)std::ceil(need)));
   }
   WorkBudget* saved = g_work_budget;
