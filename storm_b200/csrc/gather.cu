@@ -14,6 +14,8 @@
 // (bucket_sort_emit).  Reads with more index positions than a warp can hold go to a
 // block-per-read kernel (shared memory up to 32768 positions) and, beyond that, to a
 // global-memory variant run one read at a time.
+#include <type_traits>
+
 #include "gather.cuh"
 
 namespace sg {
@@ -433,6 +435,7 @@ __global__ void __launch_bounds__(kGWarps * 32, 8) gather_fused_kernel(ReadsDev 
 // read of the list from `cursor` (zeroed), list_count read on the device when given.
 constexpr int kBT = 512;              // threads of a block-gather block
 constexpr int kMaxBuckets = 4096;
+constexpr int kSmallCap = kSmallGatherCap;  // a read with at most this many positions sorts in shared memory
 
 // exclusive scan of a[0..n) in place (n <= kMaxBuckets, every thread of the block); the total
 __device__ __forceinline__ int block_excl_scan(int32_t* a, int n, int* wtot) {
@@ -463,11 +466,17 @@ __device__ __forceinline__ int block_excl_scan(int32_t* a, int n, int* wtot) {
   return tot;
 }
 
+// SMEM: the slices in dynamic shared memory (every read of the list has at most kSmallCap
+// positions).  Without it a launch keeps its shared memory small (the L1 cache shares that
+// storage, and the global slices of reads with many positions live off it); when small_list
+// is given it hands its reads of at most kSmallCap positions on to a SMEM launch there.
+template <bool SMEM>
 __global__ void __launch_bounds__(kBT) gather_block_kernel(ReadsDev rd, IndexView ix, int I, const int32_t* __restrict__ list,
                                                            const int32_t* __restrict__ list_count, int64_t nlist,
                                                            GatherOut go, int32_t* __restrict__ scratch, int cap,
                                                            unsigned long long* cursor, int32_t* huge_list, int32_t* huge_h,
-                                                           int32_t* huge_count, const __grid_constant__ SeedSet gs) {
+                                                           int32_t* huge_count, int32_t* small_list,
+                                                           int32_t* small_count, const __grid_constant__ SeedSet gs) {
   __shared__ int32_t cnt[kMaxBuckets];   // per bucket: count, start, then end
   __shared__ int32_t uoff[kMaxBuckets];  // per bucket: distinct values, then their offset
   __shared__ int wtot[kBT / 32];
@@ -475,9 +484,10 @@ __global__ void __launch_bounds__(kBT) gather_block_kernel(ReadsDev rd, IndexVie
   __shared__ int32_t s_min, s_max;
   __shared__ unsigned long long s_base;
   __shared__ __align__(16) uint8_t srd[kReadBytes];
+  extern __shared__ int32_t dsm[];  // 2 * kSmallCap: the slices of a read with few positions
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  int32_t* A = scratch + (int64_t)blockIdx.x * 2 * cap;
-  int32_t* B = A + cap;
+  int32_t* const Ag = scratch + (int64_t)blockIdx.x * 2 * cap;  // the block's slices in global memory
+  int32_t* const Bg = Ag + cap;
   const int64_t n = list_count ? (int64_t)*list_count : nlist;
   unsigned long long lookups = 0, positions = 0;
   for (;;) {
@@ -498,11 +508,65 @@ __global__ void __launch_bounds__(kBT) gather_block_kernel(ReadsDev rd, IndexVie
       for (int b = threadIdx.x; b < kReadBytes; b += kBT) srd[b] = b < nbytes ? src[b] : 0;
     }
     __syncthreads();
-    // gather: every (seed, read position) item's CSR range, placed by a block scan
+    // the read's positions first counted (two key-table loads per item against one load per
+    // position), so that they go straight to shared memory when few, else to the global slice,
+    // and a read above `cap` loads none of them here
     int T = 0;
+    {
+      int part = 0;
+      for (int si = 0; si < gs.n; ++si) {
+        const int np = seed_npos(gs.s[si], L);
+        T += np;
+        for (int t = threadIdx.x; t < np; t += kBT) {
+          int a, c, rp;
+          item_lookup(ix.first[si], gs.s[si], t, srd, L, a, c, rp);
+          part += c;
+        }
+      }
+      part = __reduce_add_sync(0xffffffffu, part);
+      if (lane == 0 && part) atomicAdd(&s_H, part);
+      __syncthreads();
+    }
+    const int H = s_H;
+    if (H > cap) {
+      if (threadIdx.x == 0) {
+        const int k = atomicAdd(huge_count, 1);
+        huge_list[k] = r;
+        huge_h[k] = H;
+      }
+      __syncthreads();
+      continue;
+    }
+    if (!SMEM && small_list && H <= kSmallCap) {
+      if (threadIdx.x == 0) small_list[atomicAdd(small_count, 1)] = r;
+      __syncthreads();
+      continue;
+    }
+    lookups += (unsigned long long)T;
+    positions += (unsigned long long)H;
+    if (H == 0) {
+      __syncthreads();
+      continue;
+    }
+    __syncthreads();  // every thread has read s_H
+    if (threadIdx.x == 0) s_H = 0;
+    __syncthreads();
+    // the rest of the read, compiled twice: slices in shared memory (a read with few positions)
+    // or in the block's global slices, each with plain shared or global memory operations
+    auto per_read = [&](auto in_shared) {
+    constexpr bool SMALL = decltype(in_shared)::value;
+    int32_t* const A = SMALL ? dsm : Ag;
+    int32_t* const B = SMALL ? dsm + kSmallCap : Bg;
+    // gather: every (seed, read position) item's CSR range, placed by a block scan; the range
+    // of the values is taken on the way
+    int32_t vmin = 0x7fffffff, vmax = (int32_t)0x80000000;
+    auto put = [&](int k, int32_t v) {
+      vmin = min(vmin, v);
+      vmax = max(vmax, v);
+      A[k] = v;
+    };
     for (int si = 0; si < gs.n; ++si) {
       const int np = seed_npos(gs.s[si], L);
-      T += np;
       const int32_t* first = ix.first[si];
       const int32_t* mp = ix.map[si];
       for (int t0 = 0; t0 < np; t0 += kBT) {
@@ -518,8 +582,7 @@ __global__ void __launch_bounds__(kBT) gather_block_kernel(ReadsDev rd, IndexVie
         }
         const int dst = s_H + before + incl - c;
         if (c <= 8) {
-          for (int u = 0; u < c; ++u)
-            if (dst + u < cap) A[dst + u] = __ldg(mp + a + u) - rp;
+          for (int u = 0; u < c; ++u) put(dst + u, __ldg(mp + a + u) - rp);
         }
         unsigned bm = __ballot_sync(0xffffffffu, c > 8);  // long lists: the warp copies each
         while (bm) {
@@ -527,37 +590,14 @@ __global__ void __launch_bounds__(kBT) gather_block_kernel(ReadsDev rd, IndexVie
           bm &= bm - 1;
           const int aj = __shfl_sync(0xffffffffu, a, j), cj = __shfl_sync(0xffffffffu, c, j);
           const int dj = __shfl_sync(0xffffffffu, dst, j), rj = __shfl_sync(0xffffffffu, rp, j);
-          for (int u = lane; u < cj; u += 32)
-            if (dj + u < cap) A[dj + u] = __ldg(mp + aj + u) - rj;
+          for (int u = lane; u < cj; u += 32) put(dj + u, __ldg(mp + aj + u) - rj);
         }
         __syncthreads();
         if (threadIdx.x == 0) s_H += tot;
         __syncthreads();
       }
     }
-    const int H = s_H;
-    lookups += (unsigned long long)T;
-    positions += (unsigned long long)H;
-    if (H > cap) {
-      if (threadIdx.x == 0) {
-        const int k = atomicAdd(huge_count, 1);
-        huge_list[k] = r;
-        huge_h[k] = H;
-      }
-      __syncthreads();
-      continue;
-    }
-    if (H == 0) {
-      __syncthreads();
-      continue;
-    }
     // range
-    int32_t vmin = 0x7fffffff, vmax = (int32_t)0x80000000;
-    for (int i = threadIdx.x; i < H; i += kBT) {
-      const int32_t v = A[i];
-      vmin = min(vmin, v);
-      vmax = max(vmax, v);
-    }
     vmin = __reduce_min_sync(0xffffffffu, vmin);
     vmax = __reduce_max_sync(0xffffffffu, vmax);
     if (lane == 0) {
@@ -616,6 +656,9 @@ __global__ void __launch_bounds__(kBT) gather_block_kernel(ReadsDev rd, IndexVie
         go.fd[base + k] = A[k + drop];
       }
     }
+    };
+    if constexpr (SMEM) per_read(std::true_type{});
+    else per_read(std::false_type{});
     __syncthreads();
   }
   if (threadIdx.x == 0) {
@@ -635,15 +678,28 @@ void launch_gather_fused(const ReadsDev& rd, const IndexView& ix, int I, const G
   gather_fused_kernel<<<(unsigned)blocks, kGWarps * 32, smem, st>>>(rd, ix, I, go, seeds);
 }
 
-int64_t gather_block_grid() { return resident_grid(gather_block_kernel, kBT, 0); }
+constexpr size_t kBlockGatherSmem = 2 * kSmallCap * sizeof(int32_t);
+
+int64_t gather_block_grid(bool smem) {
+  if (!smem) return resident_grid(gather_block_kernel<false>, kBT, 0);
+  set_smem_attribute_once(reinterpret_cast<const void*>(gather_block_kernel<true>), (int)kBlockGatherSmem);
+  return resident_grid(gather_block_kernel<true>, kBT, kBlockGatherSmem);
+}
 
 void launch_gather_block(const ReadsDev& rd, const IndexView& ix, int I, const int32_t* list, int64_t nlist,
                          const GatherOut& go, int32_t* scratch, int cap, int64_t grid, unsigned long long* cursor,
-                         int32_t* huge_list, int32_t* huge_h, int32_t* huge_count, const SeedSet& seeds,
-                         cudaStream_t st) {
+                         int32_t* huge_list, int32_t* huge_h, int32_t* huge_count, int32_t* small_list,
+                         int32_t* small_count, bool smem, const SeedSet& seeds, cudaStream_t st) {
   if (nlist <= 0 || grid <= 0) return;
-  gather_block_kernel<<<(unsigned)grid, kBT, 0, st>>>(rd, ix, I, list, nullptr, nlist, go, scratch, cap, cursor,
-                                                      huge_list, huge_h, huge_count, seeds);
+  if (smem) {
+    set_smem_attribute_once(reinterpret_cast<const void*>(gather_block_kernel<true>), (int)kBlockGatherSmem);
+    gather_block_kernel<true><<<(unsigned)grid, kBT, kBlockGatherSmem, st>>>(
+        rd, ix, I, list, nullptr, nlist, go, scratch, cap, cursor, huge_list, huge_h, huge_count, nullptr, nullptr, seeds);
+  } else {
+    gather_block_kernel<false><<<(unsigned)grid, kBT, 0, st>>>(rd, ix, I, list, nullptr, nlist, go, scratch, cap, cursor,
+                                                               huge_list, huge_h, huge_count, small_list, small_count,
+                                                               seeds);
+  }
 }
 
 }  // namespace sg

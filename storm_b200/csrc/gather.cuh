@@ -26,13 +26,17 @@ constexpr int kBlockGatherCap = 65536;
 // different seed families can run concurrently on different streams.
 void launch_gather_fused(const ReadsDev& rd, const IndexView& ix, int I, const GatherOut& go, const SeedSet& seeds,
                          cudaStream_t st);
-// The nlist reads of `list`, a persistent grid of `grid` blocks (at most gather_block_grid()
+// The nlist reads of `list`, a persistent grid of `grid` blocks (at most gather_block_grid(smem)
 // useful) taking reads from the zeroed `cursor`; scratch holds 2 * cap words per block.  Reads
-// with more than `cap` positions are appended to (huge_list, huge_h) with their count.
+// with more than `cap` positions are appended to (huge_list, huge_h) with their count.  Without
+// smem, reads with at most kSmallGatherCap positions are appended to small_list when it is
+// given (for a launch with smem, which sorts them in shared memory); with smem every read of
+// the list must have at most that many.
+constexpr int kSmallGatherCap = 4096;
 void launch_gather_block(const ReadsDev& rd, const IndexView& ix, int I, const int32_t* list, int64_t nlist,
                          const GatherOut& go, int32_t* scratch, int cap, int64_t grid, unsigned long long* cursor,
-                         int32_t* huge_list, int32_t* huge_h, int32_t* huge_count, const SeedSet& seeds,
-                         cudaStream_t st);
-int64_t gather_block_grid();
+                         int32_t* huge_list, int32_t* huge_h, int32_t* huge_count, int32_t* small_list,
+                         int32_t* small_count, bool smem, const SeedSet& seeds, cudaStream_t st);
+int64_t gather_block_grid(bool smem);
 
 }  // namespace sg

@@ -287,6 +287,9 @@ static __global__ void length_keys_kernel(const int16_t* __restrict__ lengths, i
   }
 }
 
+// Work weight of a read: its seed positions, about L - 15 (candidates grow with them).
+static inline double read_weight(int L) { return L > 16 ? (double)(L - 15) : 1.0; }
+
 static int map_device_once(stormgpu_ctx* c, const stormgpu_reads* reads, stormgpu_results* out) {
   if (!c->indexed) { sg_set_error("stormgpu_build_index must be called before mapping"); return STORMGPU_ESTATE; }
   cudaStream_t st = c->st;
@@ -298,6 +301,7 @@ static int map_device_once(stormgpu_ctx* c, const stormgpu_reads* reads, stormgp
   S.ms_index = ms_index;
   int64_t launches = 0;
   int maxL = 0, minL = STORMGPU_MAX_READ_LEN;
+  double wsum = 0;  // the batch's work weight (read_weight)
   {
     std::vector<int16_t> hl(n > 0 ? n : 1);
     if (n > 0) SG_CUDA(cudaMemcpyAsync(hl.data(), reads->lengths, sizeof(int16_t) * n, cudaMemcpyDeviceToHost, st));
@@ -305,6 +309,7 @@ static int map_device_once(stormgpu_ctx* c, const stormgpu_reads* reads, stormgp
     for (int64_t r = 0; r < n; ++r) {
       maxL = std::max<int>(maxL, hl[r]);
       minL = std::min<int>(minL, hl[r]);
+      wsum += read_weight(hl[r]);
     }
     if (maxL > STORMGPU_MAX_READ_LEN) { sg_set_error("read longer than %d", STORMGPU_MAX_READ_LEN); return STORMGPU_EINVAL; }
   }
@@ -336,7 +341,8 @@ static int map_device_once(stormgpu_ctx* c, const stormgpu_reads* reads, stormgp
     rev.levels = reads->levels ? c->rlevels.p : nullptr;
   }
   if (c->pstart.grow(n) || c->pcount.grow(n) || c->scan_tmp64.grow(scan_tmp_elems(n) + 8) ||
-      c->big_list.grow(n) || c->huge_list.grow(2 * n) || c->huge_h.grow(2 * n) || c->big_count.grow(2) ||
+      c->big_list.grow(n) || c->small_list.grow(n) || c->huge_list.grow(2 * n) || c->huge_h.grow(2 * n) ||
+      c->big_count.grow(3) ||
       c->counters.grow(32) || c->fr.grow(std::max<int64_t>(n * 64, 1 << 20)) ||
       c->fd.grow(std::max<int64_t>(n * 64, 1 << 20)))
     return STORMGPU_ENOMEM;
@@ -360,7 +366,7 @@ static int map_device_once(stormgpu_ctx* c, const stormgpu_reads* reads, stormgp
         // fused hit gather: sorted, de-duplicated diagonals of every read, appended to the flat
         // candidate list (fr, fd); reads with many index positions go to the block kernel
         SG_CUDA(cudaMemsetAsync(c->counters.p, 0, sizeof(unsigned long long) * 32, st));
-        SG_CUDA(cudaMemsetAsync(c->big_count.p, 0, sizeof(int32_t) * 2, st));
+        SG_CUDA(cudaMemsetAsync(c->big_count.p, 0, sizeof(int32_t) * 3, st));
         GatherOut go;
         go.fr = c->fr.p; go.fd = c->fd.p; go.cap = c->fr.cap; go.counters = c->counters.p;
         go.big_list = c->big_list.p; go.big_count = c->big_count.p;
@@ -369,17 +375,25 @@ static int map_device_once(stormgpu_ctx* c, const stormgpu_reads* reads, stormgp
         go.warp_cap = c->tune.gather_warp_cap;
         launch_gather_fused(rd, ix, sp.I, go, c->seeds, st);
         launches++;
-        int32_t nbig[2] = {0, 0};
-        SG_CUDA(cudaMemcpyAsync(nbig, c->big_count.p, sizeof(nbig), cudaMemcpyDeviceToHost, st));
+        int32_t nbig[3] = {0, 0, 0};  // handed to the block gather, above its slice, with few positions
+        SG_CUDA(cudaMemcpyAsync(nbig, c->big_count.p, sizeof(int32_t) * 2, cudaMemcpyDeviceToHost, st));
         SG_CUDA(cudaStreamSynchronize(st));
         if (nbig[0] > 0) {  // reads with more positions than a warp holds: a block each
-          const int64_t grid = std::min<int64_t>(nbig[0], gather_block_grid());
+          const int64_t grid = std::min<int64_t>(nbig[0], gather_block_grid(false));
           if (c->big_tmp.grow(grid * 2 * (int64_t)kBlockGatherCap)) return STORMGPU_ENOMEM;
           launch_gather_block(rd, ix, sp.I, c->big_list.p, nbig[0], go, c->big_tmp.p, kBlockGatherCap, grid,
-                              c->counters.p + 14, c->huge_list.p, c->huge_h.p, c->big_count.p + 1, c->seeds, st);
+                              c->counters.p + 14, c->huge_list.p, c->huge_h.p, c->big_count.p + 1, c->small_list.p,
+                              c->big_count.p + 2, false, c->seeds, st);
           launches++;
           SG_CUDA(cudaMemcpyAsync(nbig, c->big_count.p, sizeof(nbig), cudaMemcpyDeviceToHost, st));
           SG_CUDA(cudaStreamSynchronize(st));
+          if (nbig[2] > 0) {  // the ones with few positions: sorted in shared memory
+            const int64_t grid_s = std::min<int64_t>(nbig[2], gather_block_grid(true));
+            launch_gather_block(rd, ix, sp.I, c->small_list.p, nbig[2], go, c->big_tmp.p, kBlockGatherCap, grid_s,
+                                c->counters.p + 9, c->huge_list.p, c->huge_h.p, c->big_count.p + 1, nullptr, nullptr,
+                                true, c->seeds, st);
+            launches++;
+          }
           if (nbig[1] > 0) {  // beyond kBlockGatherCap: the same with a slice of the largest read's size
             std::vector<int32_t> hh(nbig[1]);
             SG_CUDA(cudaMemcpyAsync(hh.data(), c->huge_h.p, sizeof(int32_t) * nbig[1], cudaMemcpyDeviceToHost, st));
@@ -388,12 +402,12 @@ static int map_device_once(stormgpu_ctx* c, const stormgpu_reads* reads, stormgp
             for (int k = 0; k < nbig[1]; ++k) while (cap2 < hh[k]) cap2 <<= 1;
             if (cap2 > (int64_t)1 << 30) { sg_set_error("a read has %lld index positions", (long long)cap2); return STORMGPU_EINVAL; }
             // at most 1 GiB of slices
-            const int64_t grid2 = std::max<int64_t>(1, std::min<int64_t>({(int64_t)nbig[1], gather_block_grid(),
+            const int64_t grid2 = std::max<int64_t>(1, std::min<int64_t>({(int64_t)nbig[1], gather_block_grid(false),
                                                                            ((int64_t)1 << 27) / cap2}));
             if (c->big_tmp.grow(grid2 * 2 * cap2)) return STORMGPU_ENOMEM;
             launch_gather_block(rd, ix, sp.I, c->huge_list.p, nbig[1], go, c->big_tmp.p, (int)cap2, grid2,
-                                c->counters.p + 15, c->huge_list.p + n, c->huge_h.p + n, c->big_count.p + 1, c->seeds,
-                                st);
+                                c->counters.p + 15, c->huge_list.p + n, c->huge_h.p + n, c->big_count.p + 1, nullptr,
+                                nullptr, false, c->seeds, st);
             launches++;
           }
         }
@@ -533,9 +547,9 @@ static int map_device_once(stormgpu_ctx* c, const stormgpu_reads* reads, stormgp
   cudaEventElapsedTime(&tt, c->ev[6], c->ev[7]);
   S.ms_gather = tg; S.ms_filter = tf; S.ms_align = ta; S.ms_replay = tr; S.ms_total = tt;
   S.kernels = launches;
-  if (n > 0) {
-    c->dens_cand = (double)max_cand / (double)n;
-    c->dens_pass = (double)max_pass / (double)n;
+  if (n > 0 && wsum > 0) {
+    c->dens_cand = (double)max_cand / wsum;
+    c->dens_pass = (double)max_pass / wsum;
   }
   return 0;
 }
@@ -555,13 +569,14 @@ static int map_range(stormgpu_ctx* c, const stormgpu_reads* reads, stormgpu_resu
   return sg::map_device_impl(c, &r, &o);
 }
 
-// Maps the batch as k consecutive pieces of (nearly) equal size, the stats summed.
-static int map_pieces(stormgpu_ctx* c, const stormgpu_reads* reads, stormgpu_results* out, int64_t k) {
-  const int64_t n = reads->n;
+// Maps the batch as consecutive pieces [cuts[q], cuts[q + 1]), the stats summed.
+static int map_cuts(stormgpu_ctx* c, const stormgpu_reads* reads, stormgpu_results* out,
+                    const std::vector<int64_t>& cuts) {
   stormgpu_stats acc;
   memset(&acc, 0, sizeof(acc));
-  for (int64_t q = 0; q < k; ++q) {
-    if (const int e = map_range(c, reads, out, n * q / k, n * (q + 1) / k)) return e;
+  for (size_t q = 0; q + 1 < cuts.size(); ++q) {
+    if (cuts[q + 1] <= cuts[q]) continue;
+    if (const int e = map_range(c, reads, out, cuts[q], cuts[q + 1])) return e;
     add_stats(acc, c->stats);
   }
   acc.ms_index = c->stats.ms_index;
@@ -569,14 +584,36 @@ static int map_pieces(stormgpu_ctx* c, const stormgpu_reads* reads, stormgpu_res
   return 0;
 }
 
+// k consecutive pieces of (nearly) equal size
+static int map_pieces(stormgpu_ctx* c, const stormgpu_reads* reads, stormgpu_results* out, int64_t k) {
+  std::vector<int64_t> cuts;
+  for (int64_t q = 0; q <= k; ++q) cuts.push_back(reads->n * q / k);
+  return map_cuts(c, reads, out, cuts);
+}
+
 int sg::map_device_impl(stormgpu_ctx* c, const stormgpu_reads* reads, stormgpu_results* out) {
-  {  // at the last call's density the batch would be cut after its gather: cut it now
+  if (reads->n > 1 && (c->dens_cand > 0 || c->dens_pass > 0)) {
+    // at the last call's density per unit of work weight the batch would be cut after its
+    // gather: cut it now, into pieces of equal weight (a batch's reads need not be mixed: a file
+    // of several lengths often lists them one length after the other).  0.8: the pieces still
+    // differ in repeat content; one that overflows is cut after its gather.
     const int64_t n = reads->n;
-    // 0.7: the pieces of one batch differ in density (read lengths, repeats), and a piece that
-    // still overflows is cut after its gather
-    const double need = std::max(c->dens_cand * (double)n / (0.7 * (double)kMaxCandidatesPerPass),
-                                 c->dens_pass * (double)n / (0.7 * (double)kMaxPassingPerPass));
-    if (n > 1 && need > 1.0) return map_pieces(c, reads, out, std::min<int64_t>(n, (int64_t)std::ceil(need)));
+    std::vector<int16_t> hl(n);
+    SG_CUDA(cudaMemcpyAsync(hl.data(), reads->lengths, sizeof(int16_t) * n, cudaMemcpyDeviceToHost, c->st));
+    SG_CUDA(cudaStreamSynchronize(c->st));
+    std::vector<double> cum(n + 1, 0.0);
+    for (int64_t r = 0; r < n; ++r) cum[r + 1] = cum[r] + read_weight(hl[r]);
+    const double W = cum[n];
+    const double need = std::max(c->dens_cand * W / (0.8 * (double)kMaxCandidatesPerPass),
+                                 c->dens_pass * W / (0.8 * (double)kMaxPassingPerPass));
+    if (need > 1.0) {
+      const int64_t k = std::min<int64_t>(n, (int64_t)std::ceil(need));
+      std::vector<int64_t> cuts(1, 0);
+      for (int64_t q = 1; q < k; ++q)
+        cuts.push_back(std::lower_bound(cum.begin(), cum.end(), W * (double)q / (double)k) - cum.begin());
+      cuts.push_back(n);
+      return map_cuts(c, reads, out, cuts);
+    }
   }
   WorkBudget* saved = g_work_budget;
   g_work_budget = &c->work;
