@@ -554,108 +554,108 @@ __global__ void __launch_bounds__(kBT) gather_block_kernel(ReadsDev rd, IndexVie
     // the rest of the read, compiled twice: slices in shared memory (a read with few positions)
     // or in the block's global slices, each with plain shared or global memory operations
     auto per_read = [&](auto in_shared) {
-    constexpr bool SMALL = decltype(in_shared)::value;
-    int32_t* const A = SMALL ? dsm : Ag;
-    int32_t* const B = SMALL ? dsm + kSmallCap : Bg;
-    // gather: every (seed, read position) item's CSR range, placed by a block scan; the range
-    // of the values is taken on the way
-    int32_t vmin = 0x7fffffff, vmax = (int32_t)0x80000000;
-    auto put = [&](int k, int32_t v) {
-      vmin = min(vmin, v);
-      vmax = max(vmax, v);
-      A[k] = v;
-    };
-    for (int si = 0; si < gs.n; ++si) {
-      const int np = seed_npos(gs.s[si], L);
-      const int32_t* first = ix.first[si];
-      const int32_t* mp = ix.map[si];
-      for (int t0 = 0; t0 < np; t0 += kBT) {
-        int a, c, rp;
-        item_lookup(first, gs.s[si], t0 + threadIdx.x, srd, L, a, c, rp);
-        const int incl = warp_incl_scan(c);
-        if (lane == 31) wtot[w] = incl;
-        __syncthreads();
-        int before = 0, tot = 0;
-        for (int q = 0; q < kBT / 32; ++q) {
-          if (q < w) before += wtot[q];
-          tot += wtot[q];
+      constexpr bool SMALL = decltype(in_shared)::value;
+      int32_t* const A = SMALL ? dsm : Ag;
+      int32_t* const B = SMALL ? dsm + kSmallCap : Bg;
+      // gather: every (seed, read position) item's CSR range, placed by a block scan; the range
+      // of the values is taken on the way
+      int32_t vmin = 0x7fffffff, vmax = (int32_t)0x80000000;
+      auto put = [&](int k, int32_t v) {
+        vmin = min(vmin, v);
+        vmax = max(vmax, v);
+        A[k] = v;
+      };
+      for (int si = 0; si < gs.n; ++si) {
+        const int np = seed_npos(gs.s[si], L);
+        const int32_t* first = ix.first[si];
+        const int32_t* mp = ix.map[si];
+        for (int t0 = 0; t0 < np; t0 += kBT) {
+          int a, c, rp;
+          item_lookup(first, gs.s[si], t0 + threadIdx.x, srd, L, a, c, rp);
+          const int incl = warp_incl_scan(c);
+          if (lane == 31) wtot[w] = incl;
+          __syncthreads();
+          int before = 0, tot = 0;
+          for (int q = 0; q < kBT / 32; ++q) {
+            if (q < w) before += wtot[q];
+            tot += wtot[q];
+          }
+          const int dst = s_H + before + incl - c;
+          if (c <= 8) {
+            for (int u = 0; u < c; ++u) put(dst + u, __ldg(mp + a + u) - rp);
+          }
+          unsigned bm = __ballot_sync(0xffffffffu, c > 8);  // long lists: the warp copies each
+          while (bm) {
+            const int j = __ffs(bm) - 1;
+            bm &= bm - 1;
+            const int aj = __shfl_sync(0xffffffffu, a, j), cj = __shfl_sync(0xffffffffu, c, j);
+            const int dj = __shfl_sync(0xffffffffu, dst, j), rj = __shfl_sync(0xffffffffu, rp, j);
+            for (int u = lane; u < cj; u += 32) put(dj + u, __ldg(mp + aj + u) - rj);
+          }
+          __syncthreads();
+          if (threadIdx.x == 0) s_H += tot;
+          __syncthreads();
         }
-        const int dst = s_H + before + incl - c;
-        if (c <= 8) {
-          for (int u = 0; u < c; ++u) put(dst + u, __ldg(mp + a + u) - rp);
+      }
+      // range
+      vmin = __reduce_min_sync(0xffffffffu, vmin);
+      vmax = __reduce_max_sync(0xffffffffu, vmax);
+      if (lane == 0) {
+        atomicMin(&s_min, vmin);
+        atomicMax(&s_max, vmax);
+      }
+      __syncthreads();
+      vmin = s_min;
+      const uint32_t range = (uint32_t)s_max - (uint32_t)vmin;
+      int nb = 1;
+      while (nb < kMaxBuckets && nb * 8 < H) nb <<= 1;
+      int shift = 0;
+      while ((range >> shift) >= (uint32_t)nb) ++shift;
+      for (int b = threadIdx.x; b < nb; b += kBT) cnt[b] = 0;
+      __syncthreads();
+      for (int i = threadIdx.x; i < H; i += kBT) atomicAdd(&cnt[((uint32_t)A[i] - (uint32_t)vmin) >> shift], 1);
+      __syncthreads();
+      block_excl_scan(cnt, nb, wtot);
+      for (int i = threadIdx.x; i < H; i += kBT) {
+        const int32_t v = A[i];
+        B[atomicAdd(&cnt[((uint32_t)v - (uint32_t)vmin) >> shift], 1)] = v;
+      }
+      __syncthreads();  // cnt[b] is now the end of bucket b
+      for (int b = threadIdx.x; b < nb; b += kBT) {
+        const int s0 = b ? cnt[b - 1] : 0, e = cnt[b];
+        int u = 0;
+        for (int x = s0; x < e; ++x) {  // insertion into the sorted distinct prefix B[s0, s0 + u)
+          const int32_t t = B[x];
+          int y = u - 1;
+          while (y >= 0 && B[s0 + y] > t) --y;
+          if (y >= 0 && B[s0 + y] == t) continue;
+          for (int z = u - 1; z > y; --z) B[s0 + z + 1] = B[s0 + z];
+          B[s0 + y + 1] = t;
+          ++u;
         }
-        unsigned bm = __ballot_sync(0xffffffffu, c > 8);  // long lists: the warp copies each
-        while (bm) {
-          const int j = __ffs(bm) - 1;
-          bm &= bm - 1;
-          const int aj = __shfl_sync(0xffffffffu, a, j), cj = __shfl_sync(0xffffffffu, c, j);
-          const int dj = __shfl_sync(0xffffffffu, dst, j), rj = __shfl_sync(0xffffffffu, rp, j);
-          for (int u = lane; u < cj; u += 32) put(dj + u, __ldg(mp + aj + u) - rj);
+        uoff[b] = u;
+      }
+      __syncthreads();
+      const int U = block_excl_scan(uoff, nb, wtot);
+      for (int b = threadIdx.x; b < nb; b += kBT) {
+        const int s0 = b ? cnt[b - 1] : 0, o = uoff[b];
+        const int u = (b + 1 < nb ? uoff[b + 1] : U) - o;
+        for (int k = 0; k < u; ++k) A[o + k] = B[s0 + k];
+      }
+      __syncthreads();
+      const int drop = A[0] <= -I ? 1 : 0;  // the first diagonal must exceed -I (run.c:617, :648)
+      const int Uo = U - drop;
+      if (threadIdx.x == 0) s_base = Uo ? atomicAdd(&go.counters[7], (unsigned long long)Uo) : 0ull;
+      __syncthreads();
+      const unsigned long long base = s_base;
+      if ((int64_t)(base + Uo) > go.cap) {
+        if (threadIdx.x == 0) atomicExch(&go.counters[8], 1ull);
+      } else {
+        for (int k = threadIdx.x; k < Uo; k += kBT) {
+          go.fr[base + k] = r;
+          go.fd[base + k] = A[k + drop];
         }
-        __syncthreads();
-        if (threadIdx.x == 0) s_H += tot;
-        __syncthreads();
       }
-    }
-    // range
-    vmin = __reduce_min_sync(0xffffffffu, vmin);
-    vmax = __reduce_max_sync(0xffffffffu, vmax);
-    if (lane == 0) {
-      atomicMin(&s_min, vmin);
-      atomicMax(&s_max, vmax);
-    }
-    __syncthreads();
-    vmin = s_min;
-    const uint32_t range = (uint32_t)s_max - (uint32_t)vmin;
-    int nb = 1;
-    while (nb < kMaxBuckets && nb * 8 < H) nb <<= 1;
-    int shift = 0;
-    while ((range >> shift) >= (uint32_t)nb) ++shift;
-    for (int b = threadIdx.x; b < nb; b += kBT) cnt[b] = 0;
-    __syncthreads();
-    for (int i = threadIdx.x; i < H; i += kBT) atomicAdd(&cnt[((uint32_t)A[i] - (uint32_t)vmin) >> shift], 1);
-    __syncthreads();
-    block_excl_scan(cnt, nb, wtot);
-    for (int i = threadIdx.x; i < H; i += kBT) {
-      const int32_t v = A[i];
-      B[atomicAdd(&cnt[((uint32_t)v - (uint32_t)vmin) >> shift], 1)] = v;
-    }
-    __syncthreads();  // cnt[b] is now the end of bucket b
-    for (int b = threadIdx.x; b < nb; b += kBT) {
-      const int s0 = b ? cnt[b - 1] : 0, e = cnt[b];
-      int u = 0;
-      for (int x = s0; x < e; ++x) {  // insertion into the sorted distinct prefix B[s0, s0 + u)
-        const int32_t t = B[x];
-        int y = u - 1;
-        while (y >= 0 && B[s0 + y] > t) --y;
-        if (y >= 0 && B[s0 + y] == t) continue;
-        for (int z = u - 1; z > y; --z) B[s0 + z + 1] = B[s0 + z];
-        B[s0 + y + 1] = t;
-        ++u;
-      }
-      uoff[b] = u;
-    }
-    __syncthreads();
-    const int U = block_excl_scan(uoff, nb, wtot);
-    for (int b = threadIdx.x; b < nb; b += kBT) {
-      const int s0 = b ? cnt[b - 1] : 0, o = uoff[b];
-      const int u = (b + 1 < nb ? uoff[b + 1] : U) - o;
-      for (int k = 0; k < u; ++k) A[o + k] = B[s0 + k];
-    }
-    __syncthreads();
-    const int drop = A[0] <= -I ? 1 : 0;  // the first diagonal must exceed -I (run.c:617, :648)
-    const int Uo = U - drop;
-    if (threadIdx.x == 0) s_base = Uo ? atomicAdd(&go.counters[7], (unsigned long long)Uo) : 0ull;
-    __syncthreads();
-    const unsigned long long base = s_base;
-    if ((int64_t)(base + Uo) > go.cap) {
-      if (threadIdx.x == 0) atomicExch(&go.counters[8], 1ull);
-    } else {
-      for (int k = threadIdx.x; k < Uo; k += kBT) {
-        go.fr[base + k] = r;
-        go.fd[base + k] = A[k + drop];
-      }
-    }
     };
     if constexpr (SMEM) per_read(std::true_type{});
     else per_read(std::false_type{});
