@@ -4,8 +4,9 @@
 // index.c:212-241).
 //
 // Build = seed keys of every indexed position (kernel) -> stable LSD radix sort of (key, pos)
-// -> per-key runs of the sorted list (start, count) -> repeat filter (exact integer moments; the host turns them into the
-// largest admissible count) -> two scans -> compaction into the CSR.  HBM-streaming work.
+// -> per-key runs of the sorted list (start, count) -> repeat filter (exact integer moments;
+// the host turns them into the largest admissible count) -> a scan of the kept counts ->
+// compaction into the CSR.  HBM-streaming work.
 #include <cmath>
 #include <vector>
 
