@@ -28,6 +28,31 @@ static int oracle_map(void *user, const stormgpu_params *p, const char *seeds, c
   return rc;
 }
 
+/* the same in pieces, each piece's results handed to chunk() before the next maps (the front
+ * end's pipelined SAM output, exercised on the CPU) */
+static int oracle_map_chunked(void *user, const stormgpu_params *p, const char *seeds, const sh_refs *refs,
+                              const sh_reads *reads, stormgpu_results *out, int64_t piece, storm_chunk_fn chunk,
+                              void *chunk_user, char *err, int errlen) {
+  if (piece <= 0 || piece >= reads->n) piece = reads->n > 0 ? reads->n : 1;
+  for (int64_t first = 0; first < reads->n; first += piece) {
+    const int64_t n = reads->n - first < piece ? reads->n - first : piece;
+    sh_reads pr = *reads;
+    pr.n = n;
+    pr.codes += first * reads->code_stride;
+    if (pr.levels) pr.levels += first * reads->level_stride;
+    pr.lengths += first;
+    if (pr.first_level) pr.first_level += first;
+    stormgpu_results po = *out;
+    po.hits += 4 * first;
+    po.tb += 4 * first * out->tb_stride;
+    po.mapped += first;
+    const int rc = oracle_map(user, p, seeds, refs, &pr, &po, err, errlen);
+    if (rc) return rc;
+    chunk(chunk_user, first, n);
+  }
+  return 0;
+}
+
 /* greedy placement, restated: reads in read order, kept iff their rank-0 alignment exists (and
  * leads rank 1 by the -u threshold), then a stable insertion into (sequence, start) order
  * (genome_map.c:187-214, printed position-major by genome_map.c:551-796) */
@@ -53,6 +78,6 @@ static int oracle_place_greedy(void *user, const sh_refs *refs, const stormgpu_r
 }
 
 int main(int argc, char **argv) {
-  storm_mapper m = {"oracle", oracle_map, oracle_place_greedy, NULL, NULL};
+  storm_mapper m = {"oracle", oracle_map, oracle_place_greedy, NULL, NULL, NULL, oracle_map_chunked};
   return storm_cli_main(argc, argv, STORM_COLOUR, &m);
 }

@@ -84,6 +84,68 @@ static void *prep_job_run(void *arg) {
   return NULL;
 }
 
+/* SAM records written by a second thread, piece after piece in read order, while the next
+ * piece maps */
+enum { SAM_PIPE_SLOTS = 64 };
+typedef struct sam_pipe {
+  pthread_mutex_t mu;
+  pthread_cond_t cv;
+  int64_t first[SAM_PIPE_SLOTS], count[SAM_PIPE_SLOTS];
+  int head, tail, done, rc;
+  char msg[512];
+  FILE *f;
+  const sh_sam_opts *so;
+  const sh_refs *refs;
+  const sh_reads *reads;
+  const stormgpu_results *res;
+} sam_pipe;
+
+static void *sam_pipe_run(void *arg) {
+  sam_pipe *q = (sam_pipe *)arg;
+  for (;;) {
+    pthread_mutex_lock(&q->mu);
+    while (q->head == q->tail && !q->done) pthread_cond_wait(&q->cv, &q->mu);
+    if (q->head == q->tail) {
+      pthread_mutex_unlock(&q->mu);
+      return NULL;
+    }
+    const int64_t first = q->first[q->head % SAM_PIPE_SLOTS], count = q->count[q->head % SAM_PIPE_SLOTS];
+    pthread_mutex_unlock(&q->mu);
+    if (q->rc == 0) {
+      q->rc = sh_write_sam(q->f, q->so, q->refs, q->reads, q->res, first, count, first == 0);
+      if (q->rc) snprintf(q->msg, sizeof(q->msg), "%s", sh_last_error());
+    }
+    pthread_mutex_lock(&q->mu);
+    q->head++;
+    pthread_cond_broadcast(&q->cv);
+    pthread_mutex_unlock(&q->mu);
+  }
+}
+
+/* storm_chunk_fn: queue the piece's records (waits while every slot is taken) */
+static void sam_pipe_push(void *arg, int64_t first, int64_t count) {
+  sam_pipe *q = (sam_pipe *)arg;
+  pthread_mutex_lock(&q->mu);
+  while (q->tail - q->head >= SAM_PIPE_SLOTS) pthread_cond_wait(&q->cv, &q->mu);
+  q->first[q->tail % SAM_PIPE_SLOTS] = first;
+  q->count[q->tail % SAM_PIPE_SLOTS] = count;
+  q->tail++;
+  pthread_cond_broadcast(&q->cv);
+  pthread_mutex_unlock(&q->mu);
+}
+
+static void sam_pipe_finish(sam_pipe *q, pthread_t th) {
+  pthread_mutex_lock(&q->mu);
+  q->done = 1;
+  pthread_cond_broadcast(&q->cv);
+  pthread_mutex_unlock(&q->mu);
+  pthread_join(th, NULL);
+}
+
+/* reads mapped in this many pieces when the SAM output is written beside the mapping */
+enum { SAM_PIPE_PIECES = 4 };
+#define SAM_PIPE_MIN_READS 200000
+
 /* seed.c:140-179: one seed per line, '%' lines ignored, trailing blanks removed, ';' added */
 static char *seeds_from_file(const char *path) {
   FILE *f = fopen(path, "r");
@@ -296,10 +358,40 @@ int storm_cli_main(int argc, char **argv, int colour, const storm_mapper *mapper
     err("Not enough memory for the results of %ld reads.", (long)reads.n);
     exit(1);
   }
+  sh_sam_opts so;
+  memset(&so, 0, sizeof(so));
+  so.colour = colour; so.max_rank = map_unordered; so.print_all = print_all;
+  so.uniqueness = uniqueness; so.uniqueness_threshold = uniq_thr; so.min_score = min_score;
+  so.delta_m = delta_m; so.quality_base = quality_base; so.argc = argc; so.argv = argv;
+  static char obuf[1 << 22];
+  if (map_unordered && output) setvbuf(output, obuf, _IOFBF, sizeof(obuf));
+
+  /* with -M and a SAM file, a large read set maps in pieces and each piece's records are
+   * written by a second thread while the next piece maps */
+  int64_t pipe_min = SAM_PIPE_MIN_READS;  /* STORM_PIPE_MIN_READS lowers it (tests of small inputs) */
+  if (getenv("STORM_PIPE_MIN_READS")) pipe_min = atoll(getenv("STORM_PIPE_MIN_READS"));
+  const int pipelined = map_unordered && output && mapper->map_chunked && reads.n >= pipe_min && reads.n >= 2;
+  sam_pipe pipe;
+  pthread_t pipe_th;
+  if (pipelined) {
+    memset(&pipe, 0, sizeof(pipe));
+    pthread_mutex_init(&pipe.mu, NULL);
+    pthread_cond_init(&pipe.cv, NULL);
+    pipe.f = output; pipe.so = &so; pipe.refs = &refs; pipe.reads = &reads; pipe.res = &res;
+    if (pthread_create(&pipe_th, NULL, sam_pipe_run, &pipe) != 0) {
+      err("Could not start the SAM output thread.");
+      exit(1);
+    }
+  }
   char emsg[512] = {0};
   const double t_map = now_s();
-  int rc = mapper->map(mapper->user, &p, seeds, &refs, &reads, &res, emsg, sizeof(emsg));
-  msg(2, "Times: index build and mapping %.3f s.\n", now_s() - t_map);
+  int rc = pipelined ? mapper->map_chunked(mapper->user, &p, seeds, &refs, &reads, &res,
+                                           (reads.n + SAM_PIPE_PIECES - 1) / SAM_PIPE_PIECES, sam_pipe_push,
+                                           &pipe, emsg, sizeof(emsg))
+                     : mapper->map(mapper->user, &p, seeds, &refs, &reads, &res, emsg, sizeof(emsg));
+  msg(2, "Times: index build and mapping %.3f s%s.\n", now_s() - t_map,
+      pipelined ? " (SAM output of each piece beside the next)" : "");
+  if (rc != 0 && pipelined) sam_pipe_finish(&pipe, pipe_th);
   if (rc == STORMGPU_EINVAL && strstr(emsg, "seed")) {
     err("The seed pattern is invalid: \"%s\".\nExpected: {0,1}+ or {-,#}+ with at least one '1'/'#' (seed separator ';').", seeds);
     exit(-1);
@@ -313,22 +405,21 @@ int storm_cli_main(int argc, char **argv, int colour, const storm_mapper *mapper
   msg(1, "\nAligned %ld of %ld reads (%5.2f%%) in %ld seconds.\n", (long)mapped, (long)reads.n,
       reads.n ? mapped * 100.0 / reads.n : 0.0, (long)(time(NULL) - t0));
 
-  sh_sam_opts so;
-  memset(&so, 0, sizeof(so));
-  so.colour = colour; so.max_rank = map_unordered; so.print_all = print_all;
-  so.uniqueness = uniqueness; so.uniqueness_threshold = uniq_thr; so.min_score = min_score;
-  so.delta_m = delta_m; so.quality_base = quality_base; so.argc = argc; so.argv = argv;
   if (map_unordered) {
     if (output) {
-      static char obuf[1 << 22];
-      setvbuf(output, obuf, _IOFBF, sizeof(obuf));
       const double t_sam = now_s();
-      if (sh_write_sam(output, &so, &refs, &reads, &res, 0, reads.n, 1) != 0) {
+      if (pipelined) {
+        sam_pipe_finish(&pipe, pipe_th);
+        if (pipe.rc != 0) {
+          err("%s", pipe.msg);
+          exit(1);
+        }
+      } else if (sh_write_sam(output, &so, &refs, &reads, &res, 0, reads.n, 1) != 0) {
         err("%s", sh_last_error());
         exit(1);
       }
       fflush(output);
-      msg(2, "Times: SAM output %.3f s.\n", now_s() - t_sam);
+      msg(2, "Times: SAM output %.3f s%s.\n", now_s() - t_sam, pipelined ? " after the mapping" : "");
     } else {
       err("No file name provided for SAM output.");
     }

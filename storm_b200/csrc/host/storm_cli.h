@@ -12,6 +12,9 @@
 extern "C" {
 #endif
 
+/* called by a chunked map once the results of reads [first, first + count) are in `out` */
+typedef void (*storm_chunk_fn)(void *chunk_user, int64_t first, int64_t count);
+
 typedef struct storm_mapper {
   const char *name;
   /* fill `out` (already allocated for reads->n reads) for all reads against all sequences;
@@ -29,6 +32,12 @@ typedef struct storm_mapper {
    * device set-up that needs only the parameters and the seeds (map must still work, and report
    * the error, if it failed) */
   void (*prepare)(void *user, const stormgpu_params *p, const char *seeds);
+  /* may be NULL; else the same as map, in consecutive pieces of about `piece` reads, calling
+   * chunk() after each piece's results are in `out` and before the next piece maps (the
+   * command line writes a piece's SAM records while the next one maps) */
+  int (*map_chunked)(void *user, const stormgpu_params *p, const char *seeds, const sh_refs *refs,
+                     const sh_reads *reads, stormgpu_results *out, int64_t piece, storm_chunk_fn chunk,
+                     void *chunk_user, char *err, int errlen);
 } storm_mapper;
 
 int storm_cli_main(int argc, char **argv, int colour, const storm_mapper *mapper);

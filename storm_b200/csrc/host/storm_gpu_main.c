@@ -18,8 +18,24 @@ static void gpu_prepare(void *user, const stormgpu_params *p, const char *seeds)
   if (stormgpu_open(p, seeds, &gs->ctx) != 0) gs->ctx = NULL;  /* gpu_map opens again and reports */
 }
 
-static int gpu_map(void *user, const stormgpu_params *p, const char *seeds, const sh_refs *refs,
-                   const sh_reads *reads, stormgpu_results *out, char *err, int errlen) {
+/* reads [first, first + n) of v, and their part of the results */
+static void piece_views(const stormgpu_reads *v, const stormgpu_results *out, int64_t first, int64_t n,
+                        stormgpu_reads *pv, stormgpu_results *po) {
+  *pv = *v;
+  *po = *out;
+  pv->n = n;
+  pv->codes += first * v->code_stride;
+  if (pv->levels) pv->levels += first * v->level_stride;
+  pv->lengths += first;
+  if (pv->first_levels) pv->first_levels += first;
+  po->hits += 4 * first;
+  po->tb += 4 * first * out->tb_stride;
+  po->mapped += first;
+}
+
+static int gpu_map_chunked(void *user, const stormgpu_params *p, const char *seeds, const sh_refs *refs,
+                           const sh_reads *reads, stormgpu_results *out, int64_t piece, storm_chunk_fn chunk,
+                           void *chunk_user, char *err, int errlen) {
   gpu_state *gs = (gpu_state *)user;
   stormgpu_ctx *ctx = gs->ctx;
   gs->ctx = NULL;
@@ -34,15 +50,29 @@ static int gpu_map(void *user, const stormgpu_params *p, const char *seeds, cons
   if (rc) goto fail;
   stormgpu_reads v;
   sh_reads_view(reads, &v);
-  rc = stormgpu_map(ctx, &v, out);
-  if (rc) goto fail;
+  if (piece <= 0 || piece >= reads->n) piece = reads->n;
+  for (int64_t first = 0; first < reads->n || first == 0; first += piece) {
+    const int64_t n = reads->n - first < piece ? reads->n - first : piece;
+    stormgpu_reads pv;
+    stormgpu_results po;
+    piece_views(&v, out, first, n, &pv, &po);
+    rc = stormgpu_map(ctx, &pv, &po);
+    if (rc) goto fail;
+    if (chunk) chunk(chunk_user, first, n);
+    if (reads->n == 0) break;
+  }
   gs->ctx = ctx;
   return 0;
 fail:
   snprintf(err, (size_t)errlen, "%s", stormgpu_last_error());
-  if (rc == STORMGPU_EINVAL && strstr(err, "seed") == NULL && strstr(err, "invalid") != NULL) {}
   if (ctx) stormgpu_close(ctx);
   return rc;
+}
+
+/* the whole read set in one call (the greedy placement reads the context's device results) */
+static int gpu_map(void *user, const stormgpu_params *p, const char *seeds, const sh_refs *refs,
+                   const sh_reads *reads, stormgpu_results *out, char *err, int errlen) {
+  return gpu_map_chunked(user, p, seeds, refs, reads, out, 0, NULL, NULL, err, errlen);
 }
 
 static int gpu_place_greedy(void *user, const sh_refs *refs, const stormgpu_results *res, int64_t n,
@@ -66,6 +96,6 @@ static void gpu_finish(void *user) {
 
 int main(int argc, char **argv) {
   gpu_state gs = {NULL};
-  storm_mapper m = {"cuda", gpu_map, gpu_place_greedy, gpu_finish, &gs, gpu_prepare};
+  storm_mapper m = {"cuda", gpu_map, gpu_place_greedy, gpu_finish, &gs, gpu_prepare, gpu_map_chunked};
   return storm_cli_main(argc, argv, STORM_COLOUR, &m);
 }

@@ -228,3 +228,28 @@ def test_csfasta_reads(tmp_path, with_qual):
     args = ["-M", "2", "-z", "90", "-t", "100", "-i", "5"] + (["-q", "reads.qual"] if with_qual else [])
     lines = run_pair(str(tmp_path), 1, args, reads="reads.csfasta")
     assert _mapped(lines) > 500
+
+
+@pytest.mark.parametrize("colour,args", [
+    (0, ["-M", "4", "-A", "-z", "90", "-t", "95"]),
+    (1, ["-M", "2", "-i", "7", "-z", "105", "-t", "110"]),
+])
+def test_pipelined_sam_output_is_the_same(nuc_data, col_data, colour, args):
+    """The front end maps a large read set in pieces and writes each piece's SAM records from a
+    second thread while the next maps (STORM_PIPE_MIN_READS lowers the size at which it does so):
+    the SAM and -O files are those of the one-piece run, byte for byte."""
+    _build()
+    d = col_data if colour else nuc_data
+    outs = {}
+    for tag, env_extra in (("whole", {}), ("pieces", {"STORM_PIPE_MIN_READS": "2"})):
+        env = dict(os.environ, MALLOC_PERTURB_="255", **env_extra)
+        cmd = [ORACLE_BIN[colour], "-g", "ref.fa", "-r", "reads.fq", "-o", tag + ".sam", "-O", tag + ".un.fq",
+               "-v", "0"] + args
+        p = subprocess.run(cmd, cwd=d, env=env, capture_output=True, timeout=600)
+        assert p.returncode == 0, p.stderr[-2000:]
+        with open(os.path.join(d, tag + ".sam"), "rb") as f:
+            sam = [l for l in f.read().split(b"\n") if not l.startswith(b"@PG")]
+        with open(os.path.join(d, tag + ".un.fq"), "rb") as f:
+            outs[tag] = (sam, f.read())
+    assert _mapped(outs["whole"][0]) > 0
+    assert outs["pieces"] == outs["whole"]
