@@ -85,7 +85,8 @@ struct stormgpu_ctx {
   sg::DevBuf<stormgpu_hit> hits;
   sg::DevBuf<uint8_t> tb, mapped;
   // pass buffers
-  sg::DevBuf<int32_t> pstart, pcount, p_read, p_diag, big_list, small_list, big_count, huge_list, huge_h;
+  sg::DevBuf<int32_t> pstart, pcount, p_read, p_diag, big_list, big_h, small_list, small_h, big_count, huge_list,
+      huge_h;
   sg::DevBuf<int64_t> scan_tmp64, foff;
   sg::DevBuf<int32_t> fr, fd;
   sg::DevBuf<uint8_t> flag;       // pass byte per candidate

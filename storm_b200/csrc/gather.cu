@@ -347,9 +347,9 @@ __global__ void __launch_bounds__(kGWarps * 32, 8) gather_fused_kernel(ReadsDev 
     const uint8_t* read = rs;
     const int T = so[nseeds];
     int H = 0;
-    // a read with more positions than the warp holds stops here and goes to the block kernel,
-    // which looks it up again (its lookups and positions are counted there)
-    for (int r0 = 0; r0 < T && H <= cap; r0 += 32 * kItems) {
+    // a read with more positions than the warp holds is only counted from there on and goes to
+    // the block kernel with its count (its lookups and positions are counted there)
+    for (int r0 = 0; r0 < T; r0 += 32 * kItems) {
       // every lane looks up its items (all key-table loads in flight together) ...
       int a[kItems], cnt[kItems], rp[kItems], sid[kItems];
 #pragma unroll
@@ -371,7 +371,7 @@ __global__ void __launch_bounds__(kGWarps * 32, 8) gather_fused_kernel(ReadsDev 
 #pragma unroll
       for (int m = 1; m < kItems; ++m) dst[m] = dst[m - 1] + cnt[m - 1];
       H += __shfl_sync(0xffffffffu, incl, 31);
-      if (H > cap) break;  // uniform over the warp
+      if (H > cap) continue;  // uniform over the warp: counting only
 #pragma unroll
       for (int m = 0; m < kItems; ++m) {
         if (cnt[m] <= 8) {
@@ -400,7 +400,17 @@ __global__ void __launch_bounds__(kGWarps * 32, 8) gather_fused_kernel(ReadsDev 
       }
     }
     if (H > cap) {
-      if (lane == 0) go.big_list[atomicAdd(go.big_count, 1)] = (int32_t)r;
+      if (lane == 0) {
+        if (H <= kSmallGatherCap) {
+          const int k = atomicAdd(go.big_count + 2, 1);
+          go.small_list[k] = (int32_t)r;
+          go.small_h[k] = H;
+        } else {
+          const int k = atomicAdd(go.big_count, 1);
+          go.big_list[k] = (int32_t)r;
+          go.big_h[k] = H;
+        }
+      }
       __syncwarp();
       continue;
     }
@@ -467,16 +477,15 @@ __device__ __forceinline__ int block_excl_scan(int32_t* a, int n, int* wtot) {
 }
 
 // SMEM: the slices in dynamic shared memory (every read of the list has at most kSmallCap
-// positions).  Without it a launch keeps its shared memory small (the L1 cache shares that
-// storage, and the global slices of reads with many positions live off it); when small_list
-// is given it hands its reads of at most kSmallCap positions on to a SMEM launch there.
+// positions).  Without it a launch keeps its shared memory small: the L1 cache shares that
+// storage, and the global slices of reads with many positions live off it.
 template <bool SMEM>
 __global__ void __launch_bounds__(kBT) gather_block_kernel(ReadsDev rd, IndexView ix, int I, const int32_t* __restrict__ list,
+                                                           const int32_t* __restrict__ list_h,
                                                            const int32_t* __restrict__ list_count, int64_t nlist,
                                                            GatherOut go, int32_t* __restrict__ scratch, int cap,
                                                            unsigned long long* cursor, int32_t* huge_list, int32_t* huge_h,
-                                                           int32_t* huge_count, int32_t* small_list,
-                                                           int32_t* small_count, const __grid_constant__ SeedSet gs) {
+                                                           int32_t* huge_count, const __grid_constant__ SeedSet gs) {
   __shared__ int32_t cnt[kMaxBuckets];   // per bucket: count, start, then end
   __shared__ int32_t uoff[kMaxBuckets];  // per bucket: distinct values, then their offset
   __shared__ int wtot[kBT / 32];
@@ -494,7 +503,7 @@ __global__ void __launch_bounds__(kBT) gather_block_kernel(ReadsDev rd, IndexVie
     if (threadIdx.x == 0) {
       const unsigned long long k = atomicAdd(cursor, 1ull);
       s_read = (int64_t)k < n ? list[k] : -1;
-      s_H = 0;
+      s_H = (int64_t)k < n ? list_h[k] : 0;
       s_min = 0x7fffffff;
       s_max = (int32_t)0x80000000;
     }
@@ -508,25 +517,10 @@ __global__ void __launch_bounds__(kBT) gather_block_kernel(ReadsDev rd, IndexVie
       for (int b = threadIdx.x; b < kReadBytes; b += kBT) srd[b] = b < nbytes ? src[b] : 0;
     }
     __syncthreads();
-    // the read's positions first counted (two key-table loads per item against one load per
-    // position), so that they go straight to shared memory when few, else to the global slice,
-    // and a read above `cap` loads none of them here
+    // the read's position count came with it (the warp gather counted it), so a read above
+    // `cap` loads none of its positions here
     int T = 0;
-    {
-      int part = 0;
-      for (int si = 0; si < gs.n; ++si) {
-        const int np = seed_npos(gs.s[si], L);
-        T += np;
-        for (int t = threadIdx.x; t < np; t += kBT) {
-          int a, c, rp;
-          item_lookup(ix.first[si], gs.s[si], t, srd, L, a, c, rp);
-          part += c;
-        }
-      }
-      part = __reduce_add_sync(0xffffffffu, part);
-      if (lane == 0 && part) atomicAdd(&s_H, part);
-      __syncthreads();
-    }
+    for (int si = 0; si < gs.n; ++si) T += seed_npos(gs.s[si], L);
     const int H = s_H;
     if (H > cap) {
       if (threadIdx.x == 0) {
@@ -534,11 +528,6 @@ __global__ void __launch_bounds__(kBT) gather_block_kernel(ReadsDev rd, IndexVie
         huge_list[k] = r;
         huge_h[k] = H;
       }
-      __syncthreads();
-      continue;
-    }
-    if (!SMEM && small_list && H <= kSmallCap) {
-      if (threadIdx.x == 0) small_list[atomicAdd(small_count, 1)] = r;
       __syncthreads();
       continue;
     }
@@ -686,19 +675,18 @@ int64_t gather_block_grid(bool smem) {
   return resident_grid(gather_block_kernel<true>, kBT, kBlockGatherSmem);
 }
 
-void launch_gather_block(const ReadsDev& rd, const IndexView& ix, int I, const int32_t* list, int64_t nlist,
-                         const GatherOut& go, int32_t* scratch, int cap, int64_t grid, unsigned long long* cursor,
-                         int32_t* huge_list, int32_t* huge_h, int32_t* huge_count, int32_t* small_list,
-                         int32_t* small_count, bool smem, const SeedSet& seeds, cudaStream_t st) {
+void launch_gather_block(const ReadsDev& rd, const IndexView& ix, int I, const int32_t* list, const int32_t* list_h,
+                         int64_t nlist, const GatherOut& go, int32_t* scratch, int cap, int64_t grid,
+                         unsigned long long* cursor, int32_t* huge_list, int32_t* huge_h, int32_t* huge_count,
+                         bool smem, const SeedSet& seeds, cudaStream_t st) {
   if (nlist <= 0 || grid <= 0) return;
   if (smem) {
     set_smem_attribute_once(reinterpret_cast<const void*>(gather_block_kernel<true>), (int)kBlockGatherSmem);
     gather_block_kernel<true><<<(unsigned)grid, kBT, kBlockGatherSmem, st>>>(
-        rd, ix, I, list, nullptr, nlist, go, scratch, cap, cursor, huge_list, huge_h, huge_count, nullptr, nullptr, seeds);
+        rd, ix, I, list, list_h, nullptr, nlist, go, scratch, cap, cursor, huge_list, huge_h, huge_count, seeds);
   } else {
-    gather_block_kernel<false><<<(unsigned)grid, kBT, 0, st>>>(rd, ix, I, list, nullptr, nlist, go, scratch, cap, cursor,
-                                                               huge_list, huge_h, huge_count, small_list, small_count,
-                                                               seeds);
+    gather_block_kernel<false><<<(unsigned)grid, kBT, 0, st>>>(rd, ix, I, list, list_h, nullptr, nlist, go, scratch,
+                                                               cap, cursor, huge_list, huge_h, huge_count, seeds);
   }
 }
 

@@ -341,8 +341,8 @@ static int map_device_once(stormgpu_ctx* c, const stormgpu_reads* reads, stormgp
     rev.levels = reads->levels ? c->rlevels.p : nullptr;
   }
   if (c->pstart.grow(n) || c->pcount.grow(n) || c->scan_tmp64.grow(scan_tmp_elems(n) + 8) ||
-      c->big_list.grow(n) || c->small_list.grow(n) || c->huge_list.grow(2 * n) || c->huge_h.grow(2 * n) ||
-      c->big_count.grow(3) ||
+      c->big_list.grow(n) || c->big_h.grow(n) || c->small_list.grow(n) || c->small_h.grow(n) ||
+      c->huge_list.grow(2 * n) || c->huge_h.grow(2 * n) || c->big_count.grow(3) ||
       c->counters.grow(32) || c->fr.grow(std::max<int64_t>(n * 64, 1 << 20)) ||
       c->fd.grow(std::max<int64_t>(n * 64, 1 << 20)))
     return STORMGPU_ENOMEM;
@@ -369,31 +369,32 @@ static int map_device_once(stormgpu_ctx* c, const stormgpu_reads* reads, stormgp
         SG_CUDA(cudaMemsetAsync(c->big_count.p, 0, sizeof(int32_t) * 3, st));
         GatherOut go;
         go.fr = c->fr.p; go.fd = c->fd.p; go.cap = c->fr.cap; go.counters = c->counters.p;
-        go.big_list = c->big_list.p; go.big_count = c->big_count.p;
+        go.big_list = c->big_list.p; go.big_h = c->big_h.p; go.small_list = c->small_list.p;
+        go.small_h = c->small_h.p; go.big_count = c->big_count.p;
         go.cursor = c->counters.p + 12;  // zeroed just above
         go.reads_per_steal = c->tune.gather_reads_per_steal;
         go.warp_cap = c->tune.gather_warp_cap;
         launch_gather_fused(rd, ix, sp.I, go, c->seeds, st);
         launches++;
-        int32_t nbig[3] = {0, 0, 0};  // handed to the block gather, above its slice, with few positions
-        SG_CUDA(cudaMemcpyAsync(nbig, c->big_count.p, sizeof(int32_t) * 2, cudaMemcpyDeviceToHost, st));
+        int32_t nbig[3] = {0, 0, 0};  // handed to the block gather with many positions, above its slice, with few
+        SG_CUDA(cudaMemcpyAsync(nbig, c->big_count.p, sizeof(nbig), cudaMemcpyDeviceToHost, st));
         SG_CUDA(cudaStreamSynchronize(st));
-        if (nbig[0] > 0) {  // reads with more positions than a warp holds: a block each
+        if (nbig[2] > 0) {  // reads with few positions: sorted in shared memory
+          const int64_t grid_s = std::min<int64_t>(nbig[2], gather_block_grid(true));
+          launch_gather_block(rd, ix, sp.I, c->small_list.p, c->small_h.p, nbig[2], go, c->big_tmp.p, kBlockGatherCap,
+                              grid_s, c->counters.p + 9, c->huge_list.p, c->huge_h.p, c->big_count.p + 1, true,
+                              c->seeds, st);
+          launches++;
+        }
+        if (nbig[0] > 0) {  // reads with many positions: a block each, slices in global memory
           const int64_t grid = std::min<int64_t>(nbig[0], gather_block_grid(false));
           if (c->big_tmp.grow(grid * 2 * (int64_t)kBlockGatherCap)) return STORMGPU_ENOMEM;
-          launch_gather_block(rd, ix, sp.I, c->big_list.p, nbig[0], go, c->big_tmp.p, kBlockGatherCap, grid,
-                              c->counters.p + 14, c->huge_list.p, c->huge_h.p, c->big_count.p + 1, c->small_list.p,
-                              c->big_count.p + 2, false, c->seeds, st);
+          launch_gather_block(rd, ix, sp.I, c->big_list.p, c->big_h.p, nbig[0], go, c->big_tmp.p, kBlockGatherCap,
+                              grid, c->counters.p + 14, c->huge_list.p, c->huge_h.p, c->big_count.p + 1, false,
+                              c->seeds, st);
           launches++;
-          SG_CUDA(cudaMemcpyAsync(nbig, c->big_count.p, sizeof(nbig), cudaMemcpyDeviceToHost, st));
+          SG_CUDA(cudaMemcpyAsync(nbig + 1, c->big_count.p + 1, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
           SG_CUDA(cudaStreamSynchronize(st));
-          if (nbig[2] > 0) {  // the ones with few positions: sorted in shared memory
-            const int64_t grid_s = std::min<int64_t>(nbig[2], gather_block_grid(true));
-            launch_gather_block(rd, ix, sp.I, c->small_list.p, nbig[2], go, c->big_tmp.p, kBlockGatherCap, grid_s,
-                                c->counters.p + 9, c->huge_list.p, c->huge_h.p, c->big_count.p + 1, nullptr, nullptr,
-                                true, c->seeds, st);
-            launches++;
-          }
           if (nbig[1] > 0) {  // beyond kBlockGatherCap: the same with a slice of the largest read's size
             std::vector<int32_t> hh(nbig[1]);
             SG_CUDA(cudaMemcpyAsync(hh.data(), c->huge_h.p, sizeof(int32_t) * nbig[1], cudaMemcpyDeviceToHost, st));
@@ -405,9 +406,9 @@ static int map_device_once(stormgpu_ctx* c, const stormgpu_reads* reads, stormgp
             const int64_t grid2 = std::max<int64_t>(1, std::min<int64_t>({(int64_t)nbig[1], gather_block_grid(false),
                                                                            ((int64_t)1 << 27) / cap2}));
             if (c->big_tmp.grow(grid2 * 2 * cap2)) return STORMGPU_ENOMEM;
-            launch_gather_block(rd, ix, sp.I, c->huge_list.p, nbig[1], go, c->big_tmp.p, (int)cap2, grid2,
-                                c->counters.p + 15, c->huge_list.p + n, c->huge_h.p + n, c->big_count.p + 1, nullptr,
-                                nullptr, false, c->seeds, st);
+            launch_gather_block(rd, ix, sp.I, c->huge_list.p, c->huge_h.p, nbig[1], go, c->big_tmp.p, (int)cap2,
+                                grid2, c->counters.p + 15, c->huge_list.p + n, c->huge_h.p + n, c->big_count.p + 1,
+                                false, c->seeds, st);
             launches++;
           }
         }
