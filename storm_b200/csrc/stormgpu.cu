@@ -610,8 +610,11 @@ int sg::map_device_impl(stormgpu_ctx* c, const stormgpu_reads* reads, stormgpu_r
     if (need > 1.0) {
       const int64_t k = std::min<int64_t>(n, (int64_t)std::ceil(need));
       std::vector<int64_t> cuts(1, 0);
-      for (int64_t q = 1; q < k; ++q)
-        cuts.push_back(std::lower_bound(cum.begin(), cum.end(), W * (double)q / (double)k) - cum.begin());
+      for (int64_t q = 1; q < k; ++q) {  // strictly increasing, every piece smaller than the batch
+        int64_t cut = std::lower_bound(cum.begin(), cum.end(), W * (double)q / (double)k) - cum.begin();
+        cut = std::min<int64_t>(std::max<int64_t>(cut, cuts.back() + 1), n - (k - q));
+        cuts.push_back(cut);
+      }
       cuts.push_back(n);
       return map_cuts(c, reads, out, cuts);
     }
