@@ -233,7 +233,9 @@ int stormgpu_get_tuning(stormgpu_ctx *ctx, stormgpu_tuning *out);
 /* Set them; STORMGPU_EINVAL (nothing changed) if one is outside its range. */
 int stormgpu_set_tuning(stormgpu_ctx *ctx, const stormgpu_tuning *t);
 /* Autotuner: maps the reads (or `sample` of them, spread evenly over the batch, when
- * 0 < sample < n) once per candidate value of each parameter,
+ * 0 < sample < n; a sample whose mapping takes under 50 ms is grown, up to the whole batch,
+ * so that the stage times are not decided by fixed launch costs) once per candidate value of
+ * each parameter,
  * stage by stage, times the stage it affects with CUDA events, and keeps the fastest value of
  * each (the result is in the context and, when `out` is not null, in *out).  The reads are
  * on the host, as for stormgpu_map.  Requires stormgpu_build_index.  Afterwards the context's

@@ -54,40 +54,62 @@ extern "C" int stormgpu_autotune(stormgpu_ctx* c, const stormgpu_reads* reads, i
                                  stormgpu_tuning* out) {
   if (!c || !reads || reads->n < 0) { sg_set_error("null argument"); return STORMGPU_EINVAL; }
   if (!c->indexed) { sg_set_error("stormgpu_build_index must be called before stormgpu_autotune"); return STORMGPU_ESTATE; }
-  // the sample: reads spread evenly over the batch (a batch sorted by length keeps its mix)
-  stormgpu_reads r = *reads;
+  // the sample: reads spread evenly over the batch (a batch sorted by length keeps its mix),
+  // grown until one mapping of it takes kMinSampleMs: on a sample whose stages take a fraction of
+  // a millisecond the fixed costs of the launches decide, and the pick can be the worst setting
+  // for the batch (the colour workload's 2M reads, on an 8000-read sample: the largest hit bucket,
+  // gather 40 ms, where the smallest gives 26 ms)
+  constexpr double kMinSampleMs = 50.0;
+  stormgpu_reads r;
   std::vector<uint8_t> sc, sl, sf;
   std::vector<int16_t> slen;
-  if (sample > 0 && r.n > sample) {
-    const int64_t m = sample;
-    sc.resize((size_t)(m * r.code_stride));
-    if (r.levels) sl.resize((size_t)(m * r.level_stride));
-    if (r.first_levels) sf.resize((size_t)m);
-    slen.resize((size_t)m);
-    for (int64_t k = 0; k < m; ++k) {
-      const int64_t j = k * reads->n / m;
-      memcpy(sc.data() + k * r.code_stride, reads->codes + j * r.code_stride, (size_t)r.code_stride);
-      if (r.levels) memcpy(sl.data() + k * r.level_stride, reads->levels + j * r.level_stride, (size_t)r.level_stride);
-      if (r.first_levels) sf[(size_t)k] = reads->first_levels[j];
-      slen[(size_t)k] = reads->lengths[j];
+  std::vector<stormgpu_hit> hits;
+  std::vector<uint8_t> tb, mapped;
+  stormgpu_results res;
+  auto make_sample = [&](int64_t m) {
+    r = *reads;
+    if (m > 0 && r.n > m) {
+      sc.assign((size_t)(m * r.code_stride), 0);
+      sl.assign(r.levels ? (size_t)(m * r.level_stride) : 0, 0);
+      sf.assign(r.first_levels ? (size_t)m : 0, 0);
+      slen.assign((size_t)m, 0);
+      for (int64_t k = 0; k < m; ++k) {
+        const int64_t j = k * reads->n / m;
+        memcpy(sc.data() + k * r.code_stride, reads->codes + j * r.code_stride, (size_t)r.code_stride);
+        if (r.levels) memcpy(sl.data() + k * r.level_stride, reads->levels + j * r.level_stride, (size_t)r.level_stride);
+        if (r.first_levels) sf[(size_t)k] = reads->first_levels[j];
+        slen[(size_t)k] = reads->lengths[j];
+      }
+      r.n = m;
+      r.codes = sc.data();
+      r.levels = r.levels ? sl.data() : nullptr;
+      r.first_levels = r.first_levels ? sf.data() : nullptr;
+      r.lengths = slen.data();
     }
-    r.n = m;
-    r.codes = sc.data();
-    r.levels = r.levels ? sl.data() : nullptr;
-    r.first_levels = r.first_levels ? sf.data() : nullptr;
-    r.lengths = slen.data();
-  }
+    int maxL = 0;
+    for (int64_t k = 0; k < r.n; ++k) maxL = std::max<int>(maxL, r.lengths[k]);
+    const int64_t tbs = ((maxL + c->p.allowed_indels + 1) / 2 + 7) & ~7LL;
+    hits.assign((size_t)std::max<int64_t>(r.n * 4, 1), stormgpu_hit{});
+    tb.assign((size_t)std::max<int64_t>(r.n * 4 * tbs, 1), 0);
+    mapped.assign((size_t)std::max<int64_t>(r.n, 1), 0);
+    res = stormgpu_results{hits.data(), tb.data(), tbs, mapped.data()};
+  };
+  int64_t m = sample > 0 ? sample : reads->n;
+  make_sample(m);
   if (r.n == 0) {  // nothing to time: the parameters stay as they are
     if (out) *out = c->tune;
     return 0;
   }
-  int maxL = 0;
-  for (int64_t k = 0; k < r.n; ++k) maxL = std::max<int>(maxL, r.lengths[k]);
-  const int64_t tbs = ((maxL + c->p.allowed_indels + 1) / 2 + 7) & ~7LL;
-  std::vector<stormgpu_hit> hits((size_t)std::max<int64_t>(r.n * 4, 1));
-  std::vector<uint8_t> tb((size_t)std::max<int64_t>(r.n * 4 * tbs, 1)), mapped((size_t)std::max<int64_t>(r.n, 1));
-  stormgpu_results res{hits.data(), tb.data(), tbs, mapped.data()};
   const stormgpu_stats saved = c->stats;
+  for (int grow = 0; grow < 8 && r.n < reads->n; ++grow) {
+    for (int k = 0; k < 2; ++k)  // the first run of a larger sample may grow the buffers
+      if (const int rc = stormgpu_map(c, &r, &res)) { c->stats = saved; return rc; }
+    const double ms = c->stats.ms_total;
+    if (ms >= kMinSampleMs) break;
+    const double f = ms > 0 ? std::min(16.0, 1.2 * kMinSampleMs / ms) : 16.0;
+    m = std::min<int64_t>(reads->n, std::max<int64_t>(m + 1, (int64_t)((double)m * f)));
+    make_sample(m);
+  }
 
   // stage time of one setting: best of two runs after a warm-up (which also sizes the buffers)
   auto time_of = [&](const stormgpu_tuning& t, double stormgpu_stats::*stage, double* ms) -> int {
