@@ -206,6 +206,9 @@ typedef struct stormgpu_stats {
   double  ms_index, ms_gather, ms_filter, ms_align, ms_replay, ms_total;
   int64_t passes;            /* strand passes run (one filter launch each; a batch cut into pieces
                                 runs one per piece, sequence and strand) */
+  int64_t graph_passes;      /* of them, passes that ran inside a CUDA graph (every pass of a call
+                                captured as one graph and launched once, no host read between
+                                its launches) */
 } stormgpu_stats;
 int stormgpu_get_stats(stormgpu_ctx *ctx, stormgpu_stats *out);
 
@@ -228,6 +231,12 @@ typedef struct stormgpu_tuning {
                                      ranks; a later round's alignment stops as soon as it cannot
                                      reach the read's running threshold.  1: one round */
 } stormgpu_tuning;
+/* CUDA graphs (default on, unless the environment sets STORMGPU_GRAPHS=0 when the context
+ * opens): from the second mapping call of a context on, all strand passes of a call are
+ * captured as one graph, with every list sized from the densest pass seen so far (+25 %), and
+ * launched once; a call whose lists outgrow those sizes is run again as separate launches with
+ * the host reading each list size (the results are the same either way).  0 turns them off. */
+int stormgpu_set_graphs(stormgpu_ctx *ctx, int enable);
 /* The context's parameters (defaults 768, 4, 8, 32, 0, 4). */
 int stormgpu_get_tuning(stormgpu_ctx *ctx, stormgpu_tuning *out);
 /* Set them; STORMGPU_EINVAL (nothing changed) if one is outside its range. */

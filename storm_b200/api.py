@@ -52,7 +52,7 @@ class Stats(C.Structure):
                                          "hit_positions", "filter_cells", "align_cells", "kernels",
                                          "filter_band_cells")] + \
                [(n, C.c_double) for n in ("ms_index", "ms_gather", "ms_filter", "ms_align",
-                                          "ms_replay", "ms_total")] + [("passes", C.c_int64)]
+                                          "ms_replay", "ms_total")] + [("passes", C.c_int64), ("graph_passes", C.c_int64)]
 
 
 class Tuning(C.Structure):
@@ -91,6 +91,7 @@ def lib():
         L.stormgpu_get_stats.argtypes = [C.c_void_p, C.POINTER(Stats)]
         L.stormgpu_get_tuning.argtypes = [C.c_void_p, C.POINTER(Tuning)]
         L.stormgpu_set_tuning.argtypes = [C.c_void_p, C.POINTER(Tuning)]
+        L.stormgpu_set_graphs.argtypes = [C.c_void_p, C.c_int]
         L.stormgpu_autotune.argtypes = [C.c_void_p, C.POINTER(Reads), C.c_int64, C.POINTER(Tuning)]
         L.stormgpu_server_set_tuning.argtypes = [C.c_void_p, C.POINTER(Tuning)]
         L.stormgpu_sw_filter.argtypes = [C.c_int, C.c_int, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
@@ -224,6 +225,10 @@ class Mapper:
         for k, v in kw.items():
             setattr(t, k, int(v))
         _check(lib().stormgpu_set_tuning(self._ctx, C.byref(t)))
+
+    def set_graphs(self, enable: bool):
+        """CUDA graphs for the strand passes (on by default; the results are the same)."""
+        _check(lib().stormgpu_set_graphs(self._ctx, 1 if enable else 0))
 
     def autotune(self, batch: ReadBatch, sample: int = 200000) -> dict:
         """Pick the launch parameters by timing them on (up to `sample` of) the batch."""

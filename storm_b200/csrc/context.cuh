@@ -108,6 +108,18 @@ struct stormgpu_ctx {
   // call: a batch that would exceed a pass's bounds at that density is cut up front instead of
   // after its gather
   double dens_cand = 0, dens_pass = 0;
+  // CUDA graph of the strand passes: on unless turned off (stormgpu_set_graphs, STORMGPU_GRAPHS=0)
+  // or broken (a capture or instantiation that failed turns it off for the context); the
+  // executable graph of the last call, updated in place by the next call of the same shape; its
+  // stage events; its device state (list sizes, status, sums of the counters)
+  bool graphs = true;
+  bool graph_broken = false;
+  cudaGraphExec_t gexec = nullptr;
+  std::vector<cudaEvent_t> gev;
+  sg::DevBuf<unsigned long long> gstate;
+  // slice size (index positions) of the graph's launch for reads with the most positions: the
+  // largest the host-synced passes needed so far
+  int64_t huge_cap = 1 << 17;
   // genome_map placement
   sg::DevBuf<uint32_t> gm_k0, gm_v0, gm_k1, gm_v1, gm_tmp, gm_base;
 };

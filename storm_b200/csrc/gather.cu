@@ -676,16 +676,16 @@ int64_t gather_block_grid(bool smem) {
 }
 
 void launch_gather_block(const ReadsDev& rd, const IndexView& ix, int I, const int32_t* list, const int32_t* list_h,
-                         int64_t nlist, const GatherOut& go, int32_t* scratch, int cap, int64_t grid,
-                         unsigned long long* cursor, int32_t* huge_list, int32_t* huge_h, int32_t* huge_count,
-                         bool smem, const SeedSet& seeds, cudaStream_t st) {
+                         int64_t nlist, const int32_t* nlist_dev, const GatherOut& go, int32_t* scratch, int cap,
+                         int64_t grid, unsigned long long* cursor, int32_t* huge_list, int32_t* huge_h,
+                         int32_t* huge_count, bool smem, const SeedSet& seeds, cudaStream_t st) {
   if (nlist <= 0 || grid <= 0) return;
   if (smem) {
     set_smem_attribute_once(reinterpret_cast<const void*>(gather_block_kernel<true>), (int)kBlockGatherSmem);
     gather_block_kernel<true><<<(unsigned)grid, kBT, kBlockGatherSmem, st>>>(
-        rd, ix, I, list, list_h, nullptr, nlist, go, scratch, cap, cursor, huge_list, huge_h, huge_count, seeds);
+        rd, ix, I, list, list_h, nlist_dev, nlist, go, scratch, cap, cursor, huge_list, huge_h, huge_count, seeds);
   } else {
-    gather_block_kernel<false><<<(unsigned)grid, kBT, 0, st>>>(rd, ix, I, list, list_h, nullptr, nlist, go, scratch,
+    gather_block_kernel<false><<<(unsigned)grid, kBT, 0, st>>>(rd, ix, I, list, list_h, nlist_dev, nlist, go, scratch,
                                                                cap, cursor, huge_list, huge_h, huge_count, seeds);
   }
 }

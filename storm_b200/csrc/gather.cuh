@@ -31,16 +31,17 @@ constexpr int kBlockGatherCap = 65536;
 // different seed families can run concurrently on different streams.
 void launch_gather_fused(const ReadsDev& rd, const IndexView& ix, int I, const GatherOut& go, const SeedSet& seeds,
                          cudaStream_t st);
-// The nlist reads of `list` with their position counts `list_h`, a persistent grid of `grid`
-// blocks (at most gather_block_grid(smem) useful) taking reads from the zeroed `cursor`; scratch
-// holds 2 * cap words per block.  Reads with more than `cap` positions are appended to
-// (huge_list, huge_h).  smem: the slices in shared memory, for lists whose reads have at most
-// kSmallGatherCap positions.
+// The nlist reads of `list` with their position counts `list_h` (with nlist_dev, which may be
+// null, the count is read from there when the kernel starts and nlist is only nonzero), a
+// persistent grid of `grid` blocks (at most gather_block_grid(smem) useful) taking reads from the
+// zeroed `cursor`; scratch holds 2 * cap words per block.  Reads with more than `cap` positions
+// are appended to (huge_list, huge_h), counted in huge_count.  smem: the slices in shared memory,
+// for lists whose reads have at most kSmallGatherCap positions.
 constexpr int kSmallGatherCap = 4096;
 void launch_gather_block(const ReadsDev& rd, const IndexView& ix, int I, const int32_t* list, const int32_t* list_h,
-                         int64_t nlist, const GatherOut& go, int32_t* scratch, int cap, int64_t grid,
-                         unsigned long long* cursor, int32_t* huge_list, int32_t* huge_h, int32_t* huge_count,
-                         bool smem, const SeedSet& seeds, cudaStream_t st);
+                         int64_t nlist, const int32_t* nlist_dev, const GatherOut& go, int32_t* scratch, int cap,
+                         int64_t grid, unsigned long long* cursor, int32_t* huge_list, int32_t* huge_h,
+                         int32_t* huge_count, bool smem, const SeedSet& seeds, cudaStream_t st);
 int64_t gather_block_grid(bool smem);
 
 }  // namespace sg

@@ -673,8 +673,10 @@ __device__ __forceinline__ int round_of_rank(int rank, int rounds) {
 }
 
 // per round: slots whose rank falls in it (one atomic per warp and round)
-__global__ void round_count_kernel(int64_t npass, int rounds, const int32_t* __restrict__ p_read,
-                                   const int32_t* __restrict__ pstart, int64_t* __restrict__ count) {
+__global__ void round_count_kernel(int64_t npass, const int64_t* __restrict__ npass_dev, int rounds,
+                                   const int32_t* __restrict__ p_read, const int32_t* __restrict__ pstart,
+                                   int64_t* __restrict__ count) {
+  if (npass_dev) npass = *npass_dev;
   const int lane = threadIdx.x & 31;
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
   for (int64_t base = (int64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < npass; base += stride) {
@@ -688,9 +690,11 @@ __global__ void round_count_kernel(int64_t npass, int rounds, const int32_t* __r
 }
 
 // the lists: a warp's slots of one round go out together, in slot order
-__global__ void round_scatter_kernel(int64_t npass, int rounds, const int32_t* __restrict__ p_read,
-                                     const int32_t* __restrict__ pstart, const int64_t* __restrict__ count,
-                                     unsigned long long* __restrict__ cursors, int32_t* __restrict__ slots) {
+__global__ void round_scatter_kernel(int64_t npass, const int64_t* __restrict__ npass_dev, int rounds,
+                                     const int32_t* __restrict__ p_read, const int32_t* __restrict__ pstart,
+                                     const int64_t* __restrict__ count, unsigned long long* __restrict__ cursors,
+                                     int32_t* __restrict__ slots) {
+  if (npass_dev) npass = *npass_dev;
   const int lane = threadIdx.x & 31;
   int64_t start[kMaxAlignRounds];
   int64_t acc = 0;
@@ -713,14 +717,15 @@ __global__ void round_scatter_kernel(int64_t npass, int rounds, const int32_t* _
   }
 }
 
-void launch_round_lists(int64_t npass, int rounds, const int32_t* p_read, const int32_t* pstart, int64_t* round_count,
-                        unsigned long long* cursors, int32_t* round_slots, cudaStream_t st) {
+void launch_round_lists(int64_t npass, const int64_t* npass_dev, int rounds, const int32_t* p_read,
+                        const int32_t* pstart, int64_t* round_count, unsigned long long* cursors, int32_t* round_slots,
+                        cudaStream_t st) {
   if (npass <= 0) return;
   int64_t blocks = (npass + 255) / 256;
   if (blocks > 148 * 16) blocks = 148 * 16;
-  round_count_kernel<<<(unsigned)blocks, 256, 0, st>>>(npass, rounds, p_read, pstart, round_count);
-  round_scatter_kernel<<<(unsigned)blocks, 256, 0, st>>>(npass, rounds, p_read, pstart, round_count, cursors,
-                                                         round_slots);
+  round_count_kernel<<<(unsigned)blocks, 256, 0, st>>>(npass, npass_dev, rounds, p_read, pstart, round_count);
+  round_scatter_kernel<<<(unsigned)blocks, 256, 0, st>>>(npass, npass_dev, rounds, p_read, pstart, round_count,
+                                                         cursors, round_slots);
 }
 
 }  // namespace sg

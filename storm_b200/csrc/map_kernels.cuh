@@ -101,9 +101,11 @@ void launch_replay(int64_t n, const ScoreParams& sp, int ref_id, int sense, Pass
                    stormgpu_hit* hits, uint8_t* tb, int64_t tbs, uint8_t* mapped, cudaStream_t st);
 // The slots of every round of a pass, in slot order within a warp's run: counts into
 // round_count (zeroed by the caller), then the lists into round_slots.  `cursors` holds
-// `rounds` zeroed counters.
-void launch_round_lists(int64_t npass, int rounds, const int32_t* p_read, const int32_t* pstart, int64_t* round_count,
-                        unsigned long long* cursors, int32_t* round_slots, cudaStream_t st);
+// `rounds` zeroed counters.  With npass_dev (may be null) npass is an upper bound for the grid
+// and the slot count is read from there.
+void launch_round_lists(int64_t npass, const int64_t* npass_dev, int rounds, const int32_t* p_read,
+                        const int32_t* pstart, int64_t* round_count, unsigned long long* cursors, int32_t* round_slots,
+                        cudaStream_t st);
 // Replay of round pb.round (the ranks of that round), continuing from pb.thr.
 void launch_replay_round(int64_t n, const ScoreParams& sp, int ref_id, int sense, PassBuffers& pb, int rounds,
                          stormgpu_hit* hits, uint8_t* tb, int64_t tbs, uint8_t* mapped, cudaStream_t st);

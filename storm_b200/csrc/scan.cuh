@@ -92,6 +92,11 @@ inline int64_t scan_tmp_elems(int64_t n) {
   return t + 1;
 }
 
+// kernel launches of one exclusive_scan of n elements
+inline int scan_launches(int64_t n) {
+  return n <= 0 ? 0 : n <= kScanTile ? 1 : 2 + scan_launches((n + kScanTile - 1) / kScanTile);
+}
+
 template <typename Tin, typename Tout>
 void exclusive_scan(const Tin* in, Tout* out, int64_t n, Tout* total, Tout* tmp, cudaStream_t st) {
   if (n <= 0) {

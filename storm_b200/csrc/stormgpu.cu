@@ -169,7 +169,14 @@ extern "C" int stormgpu_open(const stormgpu_params* params, const char* seeds, s
   }
   for (auto& e : c->ev) cudaEventCreate(&e);
   for (auto& e : c->rev) cudaEventCreate(&e);
+  if (const char* g = getenv("STORMGPU_GRAPHS")) c->graphs = atoi(g) != 0;
   *out = c;
+  return 0;
+}
+
+extern "C" int stormgpu_set_graphs(stormgpu_ctx* c, int enable) {
+  if (!c) { sg_set_error("null argument"); return STORMGPU_EINVAL; }
+  c->graphs = enable != 0;
   return 0;
 }
 
@@ -188,7 +195,10 @@ extern "C" void stormgpu_close(stormgpu_ctx* c) {
   c->first_levels.release(); c->lengths.release(); c->hits.release(); c->tb.release();
   c->mapped.release();
   c->pstart.release(); c->pcount.release(); c->p_read.release(); c->p_diag.release();
-  c->big_list.release(); c->big_count.release(); c->huge_list.release(); c->huge_h.release();
+  c->big_list.release(); c->big_h.release(); c->small_list.release(); c->small_h.release();
+  c->big_count.release(); c->huge_list.release(); c->huge_h.release(); c->gstate.release();
+  if (c->gexec) cudaGraphExecDestroy(c->gexec);
+  for (auto& e : c->gev) cudaEventDestroy(e);
   c->scan_tmp64.release();
   c->a_score.release(); c->a_bound.release(); c->a_tblen.release(); c->big_tmp.release();
   c->a_pos.release(); c->a_tb.release(); c->scratch.release(); c->counters.release();
@@ -275,7 +285,7 @@ static void add_stats(stormgpu_stats& S, const stormgpu_stats& s) {
   S.seed_lookups += s.seed_lookups; S.hit_positions += s.hit_positions; S.filter_cells += s.filter_cells;
   S.align_cells += s.align_cells; S.kernels += s.kernels; S.filter_band_cells += s.filter_band_cells;
   S.ms_gather += s.ms_gather; S.ms_filter += s.ms_filter; S.ms_align += s.ms_align; S.passes += s.passes;
-  S.ms_replay += s.ms_replay; S.ms_total += s.ms_total;
+  S.ms_replay += s.ms_replay; S.ms_total += s.ms_total; S.graph_passes += s.graph_passes;
 }
 
 // sort keys of the length order: key = read length, value = read index
@@ -289,6 +299,331 @@ static __global__ void length_keys_kernel(const int16_t* __restrict__ lengths, i
 
 // Work weight of a read: its seed positions, about L - 15 (candidates grow with them).
 static inline double read_weight(int L) { return L > 16 ? (double)(L - 15) : 1.0; }
+
+// ------------------------------------------------------------------------------ graph passes
+//
+// Every strand pass of a call as one CUDA graph: the lists are sized up front (from the densest
+// pass of the last call, +25 %), every launch takes its list size from device memory, and a
+// one-thread gate after the gather and after the filter writes the size the next stages take,
+// or 0 with a status when a list would not fit (or the batch must be cut): the passes from there
+// on then do nothing, and the host, reading the status once after the graph, maps the call
+// again with the host-synced passes.
+
+constexpr int kGraphRetry = 2;
+
+// words of the graph's device state (c->gstate)
+enum : int {
+  kGsCand = 0,    // candidates the filter of the current pass takes (0: skipped)
+  kGsPass,        // passing candidates the alignment of the current pass takes (0: skipped)
+  kGsStatus,      // 1: a list outgrew its capacity, 2: the batch must be cut, 4: too many passing
+  kGsLookups,     // sums over the passes of the stage counters
+  kGsPositions,
+  kGsCandidates,
+  kGsCells,
+  kGsBand,
+  kGsAlignCells,
+  kGsPassed,
+  kGsMaxCand,     // densest pass
+  kGsMaxPass,
+  kGsWords = 16
+};
+
+static __global__ void gate_gather_kernel(const unsigned long long* __restrict__ counters,
+                                          const int32_t* __restrict__ big_count, int64_t cand_cap, int64_t cand_max,
+                                          unsigned long long* __restrict__ gs) {
+  const unsigned long long u = counters[7];
+  unsigned long long s = gs[kGsStatus];
+  // candidate list overflow, a read above the slices of the last gather launch, or a full list
+  if (counters[8] || big_count[3] > 0 || u > (unsigned long long)cand_cap) s |= 1;
+  if (u > (unsigned long long)cand_max) s |= 2;
+  gs[kGsStatus] = s;
+  gs[kGsCand] = s ? 0 : u;
+  gs[kGsLookups] += counters[3];
+  gs[kGsPositions] += counters[4];
+  if (u > gs[kGsMaxCand]) gs[kGsMaxCand] = u;
+}
+
+static __global__ void gate_filter_kernel(const int64_t* __restrict__ total, int64_t pass_cap, int64_t pass_max,
+                                          int64_t nreads, unsigned long long* __restrict__ gs) {
+  const int64_t p = *total;
+  unsigned long long s = gs[kGsStatus];
+  if (p > pass_cap) s |= 4;
+  if (p > pass_max && nreads > 1) s |= 2;
+  gs[kGsStatus] = s;
+  gs[kGsPass] = s ? 0 : (unsigned long long)p;
+  if (!s) gs[kGsPassed] += (unsigned long long)p;
+  if ((unsigned long long)p > gs[kGsMaxPass]) gs[kGsMaxPass] = (unsigned long long)p;
+}
+
+static __global__ void pass_sums_kernel(const unsigned long long* __restrict__ counters,
+                                        unsigned long long* __restrict__ gs) {
+  gs[kGsCandidates] += counters[5];
+  gs[kGsCells] += counters[2];
+  gs[kGsBand] += counters[6];
+  gs[kGsAlignCells] += counters[13];
+}
+
+// What the passes of one call share (set up by map_device_once before them).
+struct PassSetup {
+  ScoreParams sp;
+  ReadsDev fwd, rev;
+  int64_t n;
+  int maxL, minL;
+  double wsum;
+  int wpr;          // scratch words per row of an alignment
+  int64_t tbs;      // traceback bytes per passing candidate
+  stormgpu_results* out;
+};
+
+// The lists a graph call needs (false: they could not be allocated, and the call runs without a
+// graph).
+static bool graph_buffers(stormgpu_ctx* c, const PassSetup& P, int64_t* cand_cap, int64_t* pass_cap,
+                          int64_t* grid_h) {
+  const int64_t n = P.n;
+  const int64_t want_cand = (int64_t)(c->dens_cand * P.wsum * 1.25) + 65536;
+  const int64_t want_pass = (int64_t)(c->dens_pass * P.wsum * 1.25) + 4096;
+  const int64_t grid_b = gather_block_grid(false);
+  *grid_h = std::max<int64_t>(1, std::min<int64_t>(grid_b, ((int64_t)1 << 25) / c->huge_cap));
+  const int rounds = std::max(1, std::min<int>(c->tune.align_rounds, kMaxAlignRounds));
+  if (c->fr.grow(want_cand) || c->fd.grow(want_cand) || c->big_count.grow(4) || c->gstate.grow(kGsWords) ||
+      c->big_tmp.grow(std::max(grid_b * 2 * (int64_t)kBlockGatherCap, *grid_h * 2 * c->huge_cap)) ||
+      c->rexp.grow(n * rexp_stride(P.maxL)))
+    return false;
+  *cand_cap = std::min(c->fr.cap, c->fd.cap);
+  const int64_t nw = (*cand_cap + 31) / 32;
+  if (c->flag.grow(nw * 32) || c->flagw.grow(nw) || c->foff.grow(nw + 1) ||
+      c->scan_tmp64.grow(scan_tmp_elems(std::max<int64_t>(nw, n)) + 8) || c->p_read.grow(want_pass) ||
+      c->p_diag.grow(want_pass) || c->a_score.grow(want_pass) || c->a_bound.grow(want_pass) ||
+      c->a_tblen.grow(want_pass) || c->a_pos.grow(want_pass * 4) || c->a_tb.grow(want_pass * P.tbs))
+    return false;
+  *pass_cap = std::min({c->p_read.cap, c->p_diag.cap, c->a_score.cap, c->a_bound.cap, c->a_tblen.cap,
+                        c->a_pos.cap / 4, c->a_tb.cap / P.tbs});
+  if (c->scratch.grow(align_workers(*pass_cap, P.sp) * (int64_t)P.maxL * P.wpr)) return false;
+  if (rounds > 1 && (c->thr.grow(n) || c->round_slots.grow(*pass_cap) || c->rounds.grow(16))) return false;
+  return true;
+}
+
+// The launches of every pass on c's stream, each list size read from the device (captured into
+// the graph; nothing here waits for the device).  E: the stage events, per_pass per pass.
+static int enqueue_graph_passes(stormgpu_ctx* c, const PassSetup& P, int64_t cand_cap, int64_t pass_cap,
+                                int64_t grid_h, int per_pass, int64_t& launches) {
+  cudaStream_t st = c->st;
+  const ScoreParams& sp = P.sp;
+  const int64_t n = P.n;
+  unsigned long long* gs = c->gstate.p;
+  const int64_t nw = (cand_cap + 31) / 32;
+  const int rounds = std::max(1, std::min<int>(c->tune.align_rounds, kMaxAlignRounds));
+  const int64_t rstride = rexp_stride(P.maxL);
+  const int64_t grid_s = gather_block_grid(true), grid_b = gather_block_grid(false);
+  auto rec = [&](cudaEvent_t e) { return cudaEventRecordWithFlags(e, st, cudaEventRecordExternal); };
+  SG_CUDA(cudaMemsetAsync(gs, 0, sizeof(unsigned long long) * kGsWords, st));
+  int pi = 0;
+  for (size_t ref_id = 0; ref_id < c->refs.size(); ++ref_id) {
+    RefSeq& R = c->refs[ref_id];
+    IndexView ix;
+    memset(&ix, 0, sizeof(ix));
+    for (int si = 0; si < c->seeds.n; ++si) { ix.first[si] = R.idx[si].first; ix.map[si] = R.idx[si].map; }
+    for (int strand = 0; strand < 2; ++strand) {
+      if (!(c->p.senses & (1 << strand))) continue;
+      const ReadsDev& rd = strand ? P.rev : P.fwd;
+      cudaEvent_t* E = c->gev.data() + (size_t)pi * per_pass;
+      ++pi;
+      SG_CUDA(rec(E[0]));
+      // hit gather: the warp kernel, then the block kernels over the lists it filled, then the
+      // reads above the block kernel's slices (reads above this launch's slices end the graph
+      // call: the host-synced passes size their slices to fit)
+      SG_CUDA(cudaMemsetAsync(c->counters.p, 0, sizeof(unsigned long long) * 32, st));
+      SG_CUDA(cudaMemsetAsync(c->big_count.p, 0, sizeof(int32_t) * 4, st));
+      GatherOut go;
+      go.fr = c->fr.p; go.fd = c->fd.p; go.cap = cand_cap; go.counters = c->counters.p;
+      go.big_list = c->big_list.p; go.big_h = c->big_h.p; go.small_list = c->small_list.p;
+      go.small_h = c->small_h.p; go.big_count = c->big_count.p;
+      go.cursor = c->counters.p + 12;
+      go.reads_per_steal = c->tune.gather_reads_per_steal;
+      go.warp_cap = c->tune.gather_warp_cap;
+      launch_gather_fused(rd, ix, sp.I, go, c->seeds, st);
+      launch_gather_block(rd, ix, sp.I, c->small_list.p, c->small_h.p, n, c->big_count.p + 2, go, c->big_tmp.p,
+                          kBlockGatherCap, grid_s, c->counters.p + 9, c->huge_list.p, c->huge_h.p, c->big_count.p + 1,
+                          true, c->seeds, st);
+      launch_gather_block(rd, ix, sp.I, c->big_list.p, c->big_h.p, n, c->big_count.p + 0, go, c->big_tmp.p,
+                          kBlockGatherCap, grid_b, c->counters.p + 14, c->huge_list.p, c->huge_h.p,
+                          c->big_count.p + 1, false, c->seeds, st);
+      launch_gather_block(rd, ix, sp.I, c->huge_list.p, c->huge_h.p, n, c->big_count.p + 1, go, c->big_tmp.p,
+                          (int)c->huge_cap, grid_h, c->counters.p + 15, c->huge_list.p + n, c->huge_h.p + n,
+                          c->big_count.p + 3, false, c->seeds, st);
+      gate_gather_kernel<<<1, 1, 0, st>>>(c->counters.p, c->big_count.p, cand_cap, kMaxCandidatesPerPass, gs);
+      launches += 5;
+      SG_CUDA(rec(E[1]));
+      // filter over the gate's candidate count
+      FilterJob job;
+      memset(&job, 0, sizeof(job));
+      if (c->tune.filter_cursor) job.cursor = c->counters.p + 10;
+      job.rows = c->tune.filter_rows;
+      job.n = cand_cap; job.n_dev = gs + kGsCand;
+      job.fr = c->fr.p; job.fd = c->fd.p; job.flag = c->flag.p; job.codes = rd.codes;
+      job.cstride = rd.cstride; job.lengths = rd.lengths; job.genome = R.d_codes; job.W = sp.W; job.Is = sp.Is;
+      job.fm = sp.fm; job.fx = sp.fx; job.fo = sp.fo; job.fe = sp.fe; job.fthr = sp.fthr;
+      job.counters = c->counters.p;
+      launch_expand_reads(rd, c->rexp.p, rstride, st);
+      job.gexp = R.d_gexp; job.rexp = c->rexp.p; job.rstride = rstride; job.min_len = P.minL;
+      launch_filter_flat_job(job, sp, filter_dpx_ok(sp, P.maxL), st);
+      launches += 2;
+      SG_CUDA(rec(E[2]));
+      // passing candidates, in order, over the whole capacity (the words past the count are zero)
+      launch_pack_flags(cand_cap, gs + kGsCand, c->flag.p, c->flagw.p, st);
+      exclusive_scan<PassWord, int64_t>(reinterpret_cast<const PassWord*>(c->flagw.p), c->foff.p, nw, c->foff.p + nw,
+                                        c->scan_tmp64.p, st);
+      gate_filter_kernel<<<1, 1, 0, st>>>(c->foff.p + nw, pass_cap, kMaxPassingPerPass, n, gs);
+      launches += 2 + scan_launches(nw);
+      const int64_t* np = reinterpret_cast<const int64_t*>(gs + kGsPass);
+      PassBuffers pb;
+      memset(&pb, 0, sizeof(pb));
+      pb.pstart = c->pstart.p; pb.pcount = c->pcount.p;
+      pb.counters = c->counters.p;
+      SG_CUDA(cudaMemsetAsync(c->pcount.p, 0, sizeof(int32_t) * n, st));
+      pb.p_read = c->p_read.p; pb.p_diag = c->p_diag.p; pb.p_cap = pass_cap;
+      launch_compact(nw, c->flagw.p, c->foff.p, c->fr.p, c->fd.p, c->p_read.p, c->p_diag.p, pass_cap, st);
+      launch_slot_bounds(pass_cap, np, c->p_read.p, c->pstart.p, c->pcount.p, st);
+      launches += 3;
+      pb.a_score = c->a_score.p; pb.a_bound = c->a_bound.p; pb.a_tblen = c->a_tblen.p;
+      pb.a_pos = c->a_pos.p; pb.a_tb = c->a_tb.p; pb.tbs = P.tbs;
+      pb.cursor = c->counters.p + 11;
+      pb.npass_dev = np;
+      pb.steal = c->tune.align_steal;
+      pb.a_scratch = c->scratch.p;
+      pb.cells = c->counters.p + 13;
+      if (rounds == 1) {
+        launch_align(rd, sp, R.d_codes, R.d_mask, 0, pass_cap, pb, st);
+        launches++;
+        SG_CUDA(rec(E[3]));
+        launch_replay(n, sp, (int)ref_id, strand ? -1 : 1, pb, P.out->hits, P.out->tb, P.out->tb_stride,
+                      P.out->mapped, st);
+        launches++;
+      } else {
+        SG_CUDA(cudaMemsetAsync(c->rounds.p, 0, sizeof(int64_t) * 16, st));
+        launch_round_lists(pass_cap, np, rounds, c->p_read.p, c->pstart.p, c->rounds.p,
+                           reinterpret_cast<unsigned long long*>(c->rounds.p + 8), c->round_slots.p, st);
+        launches += 2;
+        pb.round_slots = c->round_slots.p;
+        pb.round_count = c->rounds.p;
+        pb.thr = c->thr.p;
+        SG_CUDA(rec(E[5]));
+        for (int k = 0; k < rounds; ++k) {
+          pb.round = k;
+          pb.cursor = c->counters.p + 16 + k;
+          launch_align(rd, sp, R.d_codes, R.d_mask, 0, pass_cap, pb, st);
+          SG_CUDA(rec(E[6 + 2 * k]));
+          launch_replay_round(n, sp, (int)ref_id, strand ? -1 : 1, pb, rounds, P.out->hits, P.out->tb,
+                              P.out->tb_stride, P.out->mapped, st);
+          SG_CUDA(rec(E[7 + 2 * k]));
+          launches += 2;
+        }
+        SG_CUDA(rec(E[3]));
+      }
+      pass_sums_kernel<<<1, 1, 0, st>>>(c->counters.p, gs);
+      launches++;
+      SG_CUDA(rec(E[4]));
+    }
+  }
+  return 0;
+}
+
+// Every pass of the call as one graph.  0: done (results in P.out, stats in c->stats);
+// kGraphRetry: the results are not usable (a list did not fit, or graphs do not work here) and
+// the call must run the host-synced passes; else an error code.
+static int map_passes_graph(stormgpu_ctx* c, const PassSetup& P, int64_t launches) {
+  cudaStream_t st = c->st;
+  int64_t cand_cap = 0, pass_cap = 0, grid_h = 0;
+  if (!graph_buffers(c, P, &cand_cap, &pass_cap, &grid_h)) {
+    cudaGetLastError();
+    c->work.over = false;  // the host-synced passes allocate what they need, no more
+    return kGraphRetry;
+  }
+  const int rounds = std::max(1, std::min<int>(c->tune.align_rounds, kMaxAlignRounds));
+  const int per_pass = 5 + (rounds > 1 ? 1 + 2 * rounds : 0);
+  int npasses = 0;
+  for (size_t r = 0; r < c->refs.size(); ++r)
+    for (int strand = 0; strand < 2; ++strand) npasses += (c->p.senses >> strand) & 1;
+  while (c->gev.size() < (size_t)npasses * per_pass) {
+    cudaEvent_t e;
+    SG_CUDA(cudaEventCreate(&e));
+    c->gev.push_back(e);
+  }
+  // capture (nothing runs), then update the last call's executable graph in place when the
+  // shape is the same, else instantiate anew
+  cudaGraph_t g = nullptr;
+  auto broken = [&]() {
+    cudaGetLastError();
+    if (g) cudaGraphDestroy(g);
+    c->graph_broken = true;
+    return kGraphRetry;
+  };
+  if (cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed) != cudaSuccess) return broken();
+  const int erc = enqueue_graph_passes(c, P, cand_cap, pass_cap, grid_h, per_pass, launches);
+  const cudaError_t ece = cudaStreamEndCapture(st, &g);
+  if (erc || ece != cudaSuccess || !g) return broken();
+  bool ready = false;
+  if (c->gexec) {
+    cudaGraphExecUpdateResultInfo info;
+    ready = cudaGraphExecUpdate(c->gexec, g, &info) == cudaSuccess;
+    if (!ready) {
+      cudaGetLastError();
+      cudaGraphExecDestroy(c->gexec);
+      c->gexec = nullptr;
+    }
+  }
+  if (!ready && cudaGraphInstantiate(&c->gexec, g, 0) != cudaSuccess) {
+    c->gexec = nullptr;
+    return broken();
+  }
+  cudaGraphDestroy(g);
+  g = nullptr;
+  unsigned long long h[kGsWords];
+  SG_CUDA(cudaEventRecord(c->ev[6], st));
+  SG_CUDA(cudaGraphLaunch(c->gexec, st));
+  SG_CUDA(cudaEventRecord(c->ev[7], st));
+  SG_CUDA(cudaMemcpyAsync(h, c->gstate.p, sizeof(h), cudaMemcpyDeviceToHost, st));
+  SG_CUDA(cudaStreamSynchronize(st));
+  SG_CUDA(cudaGetLastError());
+  if (h[kGsStatus]) return kGraphRetry;
+  stormgpu_stats& S = c->stats;
+  S.candidates = (int64_t)h[kGsCandidates];
+  S.filter_cells = (int64_t)h[kGsCells];
+  S.filter_band_cells = (int64_t)h[kGsBand];
+  S.seed_lookups = (int64_t)h[kGsLookups];
+  S.hit_positions = (int64_t)h[kGsPositions];
+  S.filter_passed = (int64_t)h[kGsPassed];
+  S.aligned = (int64_t)h[kGsPassed];
+  S.align_cells = (int64_t)h[kGsAlignCells];
+  S.passes = npasses;
+  S.graph_passes = npasses;
+  // stage times from the graph's events (as the host-synced passes split them)
+  float tg = 0, tf = 0, ta = 0, tr = 0, tt = 0;
+  for (int pi = 0; pi < npasses; ++pi) {
+    const cudaEvent_t* E = c->gev.data() + (size_t)pi * per_pass;
+    float a = 0, b = 0, d = 0, e = 0;
+    cudaEventElapsedTime(&a, E[0], E[1]);
+    cudaEventElapsedTime(&b, E[1], E[2]);
+    cudaEventElapsedTime(&d, E[2], E[3]);
+    cudaEventElapsedTime(&e, E[3], E[4]);
+    for (int k = 0; rounds > 1 && k < rounds; ++k) {
+      float x = 0;
+      cudaEventElapsedTime(&x, E[6 + 2 * k], E[7 + 2 * k]);
+      d -= x;
+      e += x;
+    }
+    tg += a; tf += b; ta += d; tr += e;
+  }
+  cudaEventElapsedTime(&tt, c->ev[6], c->ev[7]);
+  cudaGetLastError();
+  S.ms_gather = tg; S.ms_filter = tf; S.ms_align = ta; S.ms_replay = tr; S.ms_total = tt;
+  S.kernels = launches;
+  if (P.wsum > 0) {
+    c->dens_cand = (double)h[kGsMaxCand] / P.wsum;
+    c->dens_pass = (double)h[kGsMaxPass] / P.wsum;
+  }
+  return 0;
+}
 
 static int map_device_once(stormgpu_ctx* c, const stormgpu_reads* reads, stormgpu_results* out) {
   if (!c->indexed) { sg_set_error("stormgpu_build_index must be called before mapping"); return STORMGPU_ESTATE; }
@@ -349,6 +684,15 @@ static int map_device_once(stormgpu_ctx* c, const stormgpu_reads* reads, stormgp
   const int BW = 2 * sp.I + 1;
   const int wpr = (2 * BW + 31) / 32 + (sp.colour ? (BW + 31) / 32 : 0);
   const int64_t tbs = ((maxL + sp.I + 1) / 2 + 7) & ~7LL;
+  if (c->graphs && !c->graph_broken && c->dens_cand > 0 && c->huge_cap <= ((int64_t)1 << 22)) {
+    const PassSetup P{sp, fwd, rev, n, maxL, minL, wsum, wpr, tbs, out};
+    const int g = map_passes_graph(c, P, launches);
+    if (g != kGraphRetry) return g;
+    // a list outgrew its capacity: the passes again, each sized by the host (the graph's
+    // replays may have updated the results of its first passes)
+    launch_init_results(n, out->hits, out->mapped, out->tb, out->tb_stride, st);
+    launches++;
+  }
   float tg = 0, tf = 0, ta = 0, tr = 0;
   int64_t max_cand = 0, max_pass = 0;  // densest strand pass of this call
   SG_CUDA(cudaEventRecord(c->ev[6], st));
@@ -381,7 +725,7 @@ static int map_device_once(stormgpu_ctx* c, const stormgpu_reads* reads, stormgp
         SG_CUDA(cudaStreamSynchronize(st));
         if (nbig[2] > 0) {  // reads with few positions: sorted in shared memory
           const int64_t grid_s = std::min<int64_t>(nbig[2], gather_block_grid(true));
-          launch_gather_block(rd, ix, sp.I, c->small_list.p, c->small_h.p, nbig[2], go, c->big_tmp.p, kBlockGatherCap,
+          launch_gather_block(rd, ix, sp.I, c->small_list.p, c->small_h.p, nbig[2], nullptr, go, c->big_tmp.p, kBlockGatherCap,
                               grid_s, c->counters.p + 9, c->huge_list.p, c->huge_h.p, c->big_count.p + 1, true,
                               c->seeds, st);
           launches++;
@@ -389,7 +733,7 @@ static int map_device_once(stormgpu_ctx* c, const stormgpu_reads* reads, stormgp
         if (nbig[0] > 0) {  // reads with many positions: a block each, slices in global memory
           const int64_t grid = std::min<int64_t>(nbig[0], gather_block_grid(false));
           if (c->big_tmp.grow(grid * 2 * (int64_t)kBlockGatherCap)) return STORMGPU_ENOMEM;
-          launch_gather_block(rd, ix, sp.I, c->big_list.p, c->big_h.p, nbig[0], go, c->big_tmp.p, kBlockGatherCap,
+          launch_gather_block(rd, ix, sp.I, c->big_list.p, c->big_h.p, nbig[0], nullptr, go, c->big_tmp.p, kBlockGatherCap,
                               grid, c->counters.p + 14, c->huge_list.p, c->huge_h.p, c->big_count.p + 1, false,
                               c->seeds, st);
           launches++;
@@ -402,11 +746,12 @@ static int map_device_once(stormgpu_ctx* c, const stormgpu_reads* reads, stormgp
             int64_t cap2 = kBlockGatherCap;
             for (int k = 0; k < nbig[1]; ++k) while (cap2 < hh[k]) cap2 <<= 1;
             if (cap2 > (int64_t)1 << 30) { sg_set_error("a read has %lld index positions", (long long)cap2); return STORMGPU_EINVAL; }
+            c->huge_cap = std::max<int64_t>(c->huge_cap, cap2);
             // at most 1 GiB of slices
             const int64_t grid2 = std::max<int64_t>(1, std::min<int64_t>({(int64_t)nbig[1], gather_block_grid(false),
                                                                            ((int64_t)1 << 27) / cap2}));
             if (c->big_tmp.grow(grid2 * 2 * cap2)) return STORMGPU_ENOMEM;
-            launch_gather_block(rd, ix, sp.I, c->huge_list.p, c->huge_h.p, nbig[1], go, c->big_tmp.p, (int)cap2,
+            launch_gather_block(rd, ix, sp.I, c->huge_list.p, c->huge_h.p, nbig[1], nullptr, go, c->big_tmp.p, (int)cap2,
                                 grid2, c->counters.p + 15, c->huge_list.p + n, c->huge_h.p + n, c->big_count.p + 1,
                                 false, c->seeds, st);
             launches++;
@@ -444,7 +789,8 @@ static int map_device_once(stormgpu_ctx* c, const stormgpu_reads* reads, stormgp
       launches += 2;
       S.passes++;
       SG_CUDA(cudaEventRecord(c->ev[2], st));
-      launch_pack_flags(utot, c->flag.p, c->flagw.p, st);
+      launch_pack_flags(utot, nullptr, c->flag.p, c->flagw.p, st);
+      launches += (utot > 0 ? 1 : 0) + scan_launches(nwords);
       exclusive_scan<PassWord, int64_t>(reinterpret_cast<const PassWord*>(c->flagw.p), c->foff.p, nwords,
                                         c->foff.p + nwords, c->scan_tmp64.p, st);
       unsigned long long cnt[8];
@@ -472,8 +818,8 @@ static int map_device_once(stormgpu_ctx* c, const stormgpu_reads* reads, stormgp
             c->a_tblen.grow(npass) || c->a_pos.grow(npass * 4) || c->a_tb.grow(npass * tbs))
           return STORMGPU_ENOMEM;
         pb.p_read = c->p_read.p; pb.p_diag = c->p_diag.p; pb.p_cap = c->p_read.cap;
-        launch_compact(nwords, c->flagw.p, c->foff.p, c->fr.p, c->fd.p, c->p_read.p, c->p_diag.p, st);
-        launch_slot_bounds(npass, c->p_read.p, c->pstart.p, c->pcount.p, st);
+        launch_compact(nwords, c->flagw.p, c->foff.p, c->fr.p, c->fd.p, c->p_read.p, c->p_diag.p, c->p_read.cap, st);
+        launch_slot_bounds(npass, nullptr, c->p_read.p, c->pstart.p, c->pcount.p, st);
         launches += 3;
         pb.a_score = c->a_score.p; pb.a_bound = c->a_bound.p; pb.a_tblen = c->a_tblen.p;
         pb.a_pos = c->a_pos.p; pb.a_tb = c->a_tb.p; pb.tbs = tbs;
@@ -492,7 +838,7 @@ static int map_device_once(stormgpu_ctx* c, const stormgpu_reads* reads, stormgp
           // before left, then replayed
           if (c->thr.grow(n) || c->round_slots.grow(npass) || c->rounds.grow(16)) return STORMGPU_ENOMEM;
           SG_CUDA(cudaMemsetAsync(c->rounds.p, 0, sizeof(int64_t) * 16, st));
-          launch_round_lists(npass, rounds, c->p_read.p, c->pstart.p, c->rounds.p,
+          launch_round_lists(npass, nullptr, rounds, c->p_read.p, c->pstart.p, c->rounds.p,
                              reinterpret_cast<unsigned long long*>(c->rounds.p + 8), c->round_slots.p, st);
           launches += 2;
           pb.round_slots = c->round_slots.p;

@@ -229,12 +229,19 @@ void launch_filter_flat_job(const FilterJob& job, const ScoreParams& sp, bool dp
 
 // ------------------------------------------------------------------ compaction of passing candidates
 
-// pass bytes -> pass bits, one word per 32 candidates (the scan then runs over words)
-__global__ void pack_flags_kernel(int64_t n, const uint8_t* __restrict__ flag, uint32_t* __restrict__ words) {
-  const int64_t nw = (n + 31) / 32;
+// pass bytes -> pass bits, one word per 32 candidates (the scan then runs over words); the
+// words of [n_dev, ncap) (all of them from n_dev on, when it is given) are zero
+__global__ void pack_flags_kernel(int64_t ncap, const unsigned long long* __restrict__ n_dev,
+                                  const uint8_t* __restrict__ flag, uint32_t* __restrict__ words) {
+  const int64_t nw = (ncap + 31) / 32;
+  const int64_t n = n_dev ? min(ncap, (int64_t)*n_dev) : ncap;
   for (int64_t w = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; w < nw; w += (int64_t)gridDim.x * blockDim.x) {
     uint32_t bits = 0;
     const int64_t t0 = w * 32;
+    if (t0 >= n) {
+      words[w] = 0;
+      continue;
+    }
     if (t0 + 32 <= n) {
       const uint4* p = reinterpret_cast<const uint4*>(flag + t0);  // flag is 16-byte aligned, t0 a multiple of 32
       const uint4 q0 = p[0], q1 = p[1];
@@ -250,22 +257,24 @@ __global__ void pack_flags_kernel(int64_t n, const uint8_t* __restrict__ flag, u
   }
 }
 
-void launch_pack_flags(int64_t n, const uint8_t* flag, uint32_t* words, cudaStream_t st) {
-  if (n <= 0) return;
-  int64_t blocks = ((n + 31) / 32 + 255) / 256;
+void launch_pack_flags(int64_t ncap, const unsigned long long* n_dev, const uint8_t* flag, uint32_t* words,
+                       cudaStream_t st) {
+  if (ncap <= 0) return;
+  int64_t blocks = ((ncap + 31) / 32 + 255) / 256;
   if (blocks > 148 * 32) blocks = 148 * 32;
-  pack_flags_kernel<<<(unsigned)blocks, 256, 0, st>>>(n, flag, words);
+  pack_flags_kernel<<<(unsigned)blocks, 256, 0, st>>>(ncap, n_dev, flag, words);
 }
 
 // passing candidates, in order, into (p_read, p_diag): one thread per word of pass bits
+// (slots from pcap on are not written)
 __global__ void compact_kernel(int64_t nwords, const uint32_t* __restrict__ flag, const int64_t* __restrict__ woff,
                                const int32_t* __restrict__ fr, const int32_t* __restrict__ fd,
-                               int32_t* __restrict__ p_read, int32_t* __restrict__ p_diag) {
+                               int32_t* __restrict__ p_read, int32_t* __restrict__ p_diag, int64_t pcap) {
   for (int64_t w = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; w < nwords; w += (int64_t)gridDim.x * blockDim.x) {
     uint32_t m = flag[w];
     if (!m) continue;
     int64_t o = woff[w];
-    while (m) {
+    while (m && o < pcap) {
       const int64_t t = w * 32 + (__ffs(m) - 1);
       p_read[o] = fr[t];
       p_diag[o] = fd[t];
@@ -275,16 +284,20 @@ __global__ void compact_kernel(int64_t nwords, const uint32_t* __restrict__ flag
   }
 }
 
-__global__ void slot_bounds_kernel(int64_t npass, const int32_t* __restrict__ p_read, int32_t* __restrict__ pstart,
+__global__ void slot_bounds_kernel(int64_t npass, const int64_t* __restrict__ npass_dev,
+                                   const int32_t* __restrict__ p_read, int32_t* __restrict__ pstart,
                                    int32_t* __restrict__ pcount) {
+  if (npass_dev) npass = *npass_dev;
   for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < npass; s += (int64_t)gridDim.x * blockDim.x) {
     const int r = p_read[s];
     if (s == 0 || p_read[s - 1] != r) pstart[r] = (int32_t)s;
   }
 }
 
-__global__ void slot_count_kernel(int64_t npass, const int32_t* __restrict__ p_read, const int32_t* __restrict__ pstart,
+__global__ void slot_count_kernel(int64_t npass, const int64_t* __restrict__ npass_dev,
+                                  const int32_t* __restrict__ p_read, const int32_t* __restrict__ pstart,
                                   int32_t* __restrict__ pcount) {
+  if (npass_dev) npass = *npass_dev;
   for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < npass; s += (int64_t)gridDim.x * blockDim.x) {
     const int r = p_read[s];
     if (s == npass - 1 || p_read[s + 1] != r) pcount[r] = (int32_t)(s - pstart[r] + 1);
@@ -292,19 +305,20 @@ __global__ void slot_count_kernel(int64_t npass, const int32_t* __restrict__ p_r
 }
 
 void launch_compact(int64_t nwords, const uint32_t* flag, const int64_t* woff, const int32_t* fr, const int32_t* fd,
-                    int32_t* p_read, int32_t* p_diag, cudaStream_t st) {
+                    int32_t* p_read, int32_t* p_diag, int64_t pcap, cudaStream_t st) {
   if (nwords <= 0) return;
   int64_t blocks = (nwords + 255) / 256;
   if (blocks > 148 * 32) blocks = 148 * 32;
-  compact_kernel<<<(unsigned)blocks, 256, 0, st>>>(nwords, flag, woff, fr, fd, p_read, p_diag);
+  compact_kernel<<<(unsigned)blocks, 256, 0, st>>>(nwords, flag, woff, fr, fd, p_read, p_diag, pcap);
 }
 
-void launch_slot_bounds(int64_t npass, const int32_t* p_read, int32_t* pstart, int32_t* pcount, cudaStream_t st) {
+void launch_slot_bounds(int64_t npass, const int64_t* npass_dev, const int32_t* p_read, int32_t* pstart,
+                        int32_t* pcount, cudaStream_t st) {
   if (npass <= 0) return;
   int64_t blocks = (npass + 255) / 256;
   if (blocks > 148 * 32) blocks = 148 * 32;
-  slot_bounds_kernel<<<(unsigned)blocks, 256, 0, st>>>(npass, p_read, pstart, pcount);
-  slot_count_kernel<<<(unsigned)blocks, 256, 0, st>>>(npass, p_read, pstart, pcount);
+  slot_bounds_kernel<<<(unsigned)blocks, 256, 0, st>>>(npass, npass_dev, p_read, pstart, pcount);
+  slot_count_kernel<<<(unsigned)blocks, 256, 0, st>>>(npass, npass_dev, p_read, pstart, pcount);
 }
 
 }  // namespace sg

@@ -37,8 +37,10 @@ void launch_expand_reads(const ReadsDev& rd, uint8_t* rexp, int64_t rstride, cud
 
 bool filter_dpx_ok(const ScoreParams& sp, int max_len);
 void launch_filter_flat_job(const FilterJob& job, const ScoreParams& sp, bool dpx, cudaStream_t st);
-// pass bytes of n candidates -> words of 32 pass bits (bit t & 31 of word t >> 5)
-void launch_pack_flags(int64_t n, const uint8_t* flag, uint32_t* words, cudaStream_t st);
+// pass bytes of the ncap candidates -> words of 32 pass bits (bit t & 31 of word t >> 5); with
+// n_dev (may be null) only the first *n_dev candidates count, the words after them are zero
+void launch_pack_flags(int64_t ncap, const unsigned long long* n_dev, const uint8_t* flag, uint32_t* words,
+                       cudaStream_t st);
 // A word of pass bits, counted as its number of passing candidates when scanned.
 struct PassWord {
   uint32_t bits;
@@ -50,9 +52,13 @@ struct PassWord {
 #endif
   }
 };
-// passing candidates, in order: word w's set bits go to woff[w], woff[w] + 1, ...
+// passing candidates, in order: word w's set bits go to woff[w], woff[w] + 1, ... (those below
+// pcap: the capacity of p_read / p_diag)
 void launch_compact(int64_t nwords, const uint32_t* flag, const int64_t* woff, const int32_t* fr, const int32_t* fd,
-                    int32_t* p_read, int32_t* p_diag, cudaStream_t st);
-void launch_slot_bounds(int64_t npass, const int32_t* p_read, int32_t* pstart, int32_t* pcount, cudaStream_t st);
+                    int32_t* p_read, int32_t* p_diag, int64_t pcap, cudaStream_t st);
+// pstart / pcount of every read with passing candidates; npass is the slot count, or with
+// npass_dev (may be null) an upper bound for the grid and the count is read from there
+void launch_slot_bounds(int64_t npass, const int64_t* npass_dev, const int32_t* p_read, int32_t* pstart,
+                        int32_t* pcount, cudaStream_t st);
 
 }  // namespace sg

@@ -297,6 +297,111 @@ def test_map_results_do_not_depend_on_the_launch_tuning():
     m.close()
 
 
+def _same_results(got, base):
+    assert np.array_equal(got.mapped, base.mapped)
+    assert got.hits.tobytes() == base.hits.tobytes()
+    assert got.tb.tobytes() == base.tb.tobytes()
+
+
+def _stage_sums(st):
+    return {k: st[k] for k in ("candidates", "filter_passed", "aligned", "seed_lookups", "hit_positions",
+                               "filter_cells", "filter_band_cells", "align_cells", "passes")}
+
+
+def test_graph_passes_give_the_host_synced_results():
+    """From a context's second mapping call on, every strand pass of a call runs inside one CUDA
+    graph, its lists sized from the densest pass seen so far and every launch taking its list
+    size from device memory.  Results and stage counters must be those of the passes run as
+    separate launches with the host reading each size, for one alignment round and for several."""
+    from storm_b200 import synth
+    genome = synth.make_genome([80000], 61, gc=0.42, repeat_frac=0.4)
+    seqs, quals = synth.simulate_nucleotide_reads(genome, 2500, [35, 75, 150], 63)
+    codes, levels, lengths = _reads_arrays(seqs, quals)
+    prm = api.params(indels=15, min_score=100, min_score_filter=95)
+    batch = api.ReadBatch(codes, lengths, levels)
+    tbs = ((150 + 15 + 1) // 2 + 7) & ~7
+
+    def mapper(graphs):
+        m = api.Mapper(prm, "##-##-###-###;###--#-#--#--####")
+        for _, s in genome:
+            cp = ffi.pack2(s, PADB)
+            mk = ffi.pack2(np.zeros(len(s), np.uint8), PADB, fill=0x55)
+            m.add_reference(cp[PADB:], mk[PADB:], len(s))
+        m.build_index()
+        m.set_graphs(graphs)
+        return m
+
+    plain, g = mapper(False), mapper(True)
+    for rounds in (4, 1, 3):
+        plain.set_tuning(align_rounds=rounds)
+        g.set_tuning(align_rounds=rounds)
+        base = plain.map(batch, tbs)
+        sb = plain.stats()
+        assert sb["graph_passes"] == 0 and sb["passes"] == 2
+        for _ in range(2):
+            got = g.map(batch, tbs)
+            sg = g.stats()
+            _same_results(got, base)
+            assert _stage_sums(sg) == _stage_sums(sb)
+        assert sg["graph_passes"] == sg["passes"] == 2, sg
+        assert sg["ms_filter"] > 0 and sg["ms_gather"] > 0 and sg["ms_total"] > 0, sg
+    plain.close()
+    g.close()
+    assert base.mapped.sum() > len(seqs) // 4
+
+
+def test_graph_call_whose_lists_outgrow_their_sizes_runs_again():
+    """A graph call sizes its lists from the last call: after reads from unique sequence, reads of
+    a 600-copy tandem repeat (a 150-bp read gathers about 200,000 index positions on its strand,
+    and has hundreds of candidates and passing candidates) outgrow the passing-candidate list and
+    the slices of the gather for reads with the most positions.  That call must run again as
+    separate launches and give the results of a context without graphs; the next call of the
+    same batch then fits its graph."""
+    from storm_b200 import synth
+    rng = np.random.default_rng(91)
+    unit = synth.random_bases(rng, 1000, 0.45)
+    flank = synth.random_bases(rng, 40000, 0.45)
+    g_ = np.concatenate([flank] + [_mutate(rng, unit, 0.02) for _ in range(600)] +
+                        [synth.random_bases(rng, 20000, 0.45)])
+    seqs, quals = synth.simulate_nucleotide_reads([("chr1", g_[20000:])], 400, [50, 150], 92)
+    codes, levels, lengths = _reads_arrays(seqs, quals)
+    useq, uqual = synth.simulate_nucleotide_reads([("flank", flank)], 300, [150], 93)
+    ucodes, ulevels, ulengths = _reads_arrays(useq, uqual)
+    prm = api.params(indels=15, min_score=100, min_score_filter=100)
+    tbs = ((150 + 15 + 1) // 2 + 7) & ~7
+    batch = api.ReadBatch(codes, lengths, levels)
+    unique = api.ReadBatch(ucodes, ulengths, ulevels)
+
+    def mapper(graphs):
+        m = api.Mapper(prm, "##-##-###-###;###--#-#--#--####;####--#--#---#---###")
+        cp = ffi.pack2(g_, PADB)
+        mk = ffi.pack2(np.zeros(len(g_), np.uint8), PADB, fill=0x55)
+        m.add_reference(cp[PADB:], mk[PADB:], len(g_))
+        m.build_index()
+        m.set_graphs(graphs)
+        return m
+
+    plain, g = mapper(False), mapper(True)
+    ubase = plain.map(unique, tbs)
+    base = plain.map(batch, tbs)
+    sb = plain.stats()
+    assert sb["hit_positions"] / len(seqs) > 50000, sb
+    assert sb["candidates"] > 100000 and sb["filter_passed"] > 20000, sb
+    _same_results(g.map(unique, tbs), ubase)
+    assert g.stats()["graph_passes"] == 0  # no density yet: separate launches
+    _same_results(g.map(unique, tbs), ubase)
+    assert g.stats()["graph_passes"] == 2
+    _same_results(g.map(batch, tbs), base)  # outgrows the sizes of the unique reads
+    st = g.stats()
+    assert st["graph_passes"] == 0 and _stage_sums(st) == _stage_sums(sb), st
+    _same_results(g.map(batch, tbs), base)
+    st = g.stats()
+    assert st["graph_passes"] == 2 and _stage_sums(st) == _stage_sums(sb), st
+    plain.close()
+    g.close()
+    assert base.mapped.sum() > len(seqs) // 2
+
+
 def test_large_host_batch_gives_the_small_batch_results():
     """A host-buffer batch of a million reads (3,000 distinct reads repeated): every read's
     result must be the one it gets in a batch of its own 3,000."""
