@@ -508,6 +508,7 @@ def mixed_arm(a, w):
                 "tuning": tuning, "tuning_s": round(tune_s, 2),
                 "mapped_fraction": mapped_total / max(1, reads_total),
                 "gpu_launches": int(sum(s["kernels"] for s in stats)),
+                "cuda_graph": {"passes": int(agg["passes"]), "graph_passes": int(agg["graph_passes"])},
                 "roofline": roof, "stages": stages, "clocks": clocks, "e2e": e2e, "cpu_baseline": cpu,
                 "parity_vs_reference": parity, "batching": batching,
                 "counts_per_step": {k: int(agg[k] / len(stats)) for k in
@@ -718,6 +719,8 @@ def whole_set_arm(a, w):
             "vs_baseline": None, "dtype": "u8/int16/int32", "data": "synthetic",
             "config": dict(headline_config(a, w), step="index build (all seeds) + map every read, both strands"),
             "tuning": tuning, "gpu_launches": int(sum(s["kernels"] for s in stats)),
+            "cuda_graph": {"passes": int(sum(s["passes"] for s in stats)),
+                           "graph_passes": int(sum(s["graph_passes"] for s in stats))},
             "roofline": {"kernel": dom, **{k: per[dom][k] for k in ("bound", "achieved", "peak", "unit", "frac")},
                          "traffic": None},
             "stages": stages, "clocks": clocks,

@@ -108,6 +108,10 @@ struct stormgpu_ctx {
   // call: a batch that would exceed a pass's bounds at that density is cut up front instead of
   // after its gather
   double dens_cand = 0, dens_pass = 0;
+  // the same densities for the list sizes of a graph call: the larger of the last call's and
+  // 0.9 x the value before it, so that calls of different densities in turn (one read length
+  // after another) do not outgrow their lists each time
+  double gdens_cand = 0, gdens_pass = 0;
   // CUDA graph of the strand passes: on unless turned off (stormgpu_set_graphs, STORMGPU_GRAPHS=0)
   // or broken (a capture or instantiation that failed turns it off for the context); the
   // executable graph of the last call, updated in place by the next call of the same shape; its

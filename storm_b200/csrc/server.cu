@@ -93,7 +93,7 @@ struct Slot {
   stormgpu_ctx* ws = nullptr;
   // candidates and passing candidates per unit of work weight of the densest pass of the last
   // batch, per chain step (each step's seeds have their own): the sizes of a step's graph
-  double dens[16][2] = {};
+  double dens[16][4] = {};
   uint8_t* staging = nullptr;  // pinned host memory
   int64_t staging_cap = 0;
   std::thread th;
@@ -273,11 +273,10 @@ int run_chain(stormgpu_server* s, Slot* sl, Request* q, std::string& err) {
                      fl ? cv.first_levels[cur] : nullptr};
     stormgpu_results o{cv.hits, cv.tb, tbs, cv.mapped};
     const int ks = std::min(k, 15);
-    ws->dens_cand = sl->dens[ks][0];
-    ws->dens_pass = sl->dens[ks][1];
+    double* dk = sl->dens[ks];
+    ws->dens_cand = dk[0]; ws->dens_pass = dk[1]; ws->gdens_cand = dk[2]; ws->gdens_pass = dk[3];
     if (const int rc = map_device_impl(ws, &r, &o)) return fail(rc);
-    sl->dens[ks][0] = ws->dens_cand;
-    sl->dens[ks][1] = ws->dens_pass;
+    dk[0] = ws->dens_cand; dk[1] = ws->dens_pass; dk[2] = ws->gdens_cand; dk[3] = ws->gdens_pass;
     chain_scatter_kernel<<<grid_for(m), 256, 0, st>>>(m, cv.ids[cur], cv.hits, cv.tb, cv.mapped, tbs, k,
                                                       cv.hits_all, cv.tb_all, cv.mapped_all,
                                                       cv.step_all, cv.unmapped);

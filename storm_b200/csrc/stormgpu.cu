@@ -363,6 +363,13 @@ static __global__ void pass_sums_kernel(const unsigned long long* __restrict__ c
   gs[kGsAlignCells] += counters[13];
 }
 
+static void set_densities(stormgpu_ctx* c, double cand, double pass) {
+  c->dens_cand = cand;
+  c->dens_pass = pass;
+  c->gdens_cand = std::max(cand, 0.9 * c->gdens_cand);
+  c->gdens_pass = std::max(pass, 0.9 * c->gdens_pass);
+}
+
 // What the passes of one call share (set up by map_device_once before them).
 struct PassSetup {
   ScoreParams sp;
@@ -380,8 +387,8 @@ struct PassSetup {
 static bool graph_buffers(stormgpu_ctx* c, const PassSetup& P, int64_t* cand_cap, int64_t* pass_cap,
                           int64_t* grid_h) {
   const int64_t n = P.n;
-  const int64_t want_cand = (int64_t)(c->dens_cand * P.wsum * 1.25) + 65536;
-  const int64_t want_pass = (int64_t)(c->dens_pass * P.wsum * 1.25) + 4096;
+  const int64_t want_cand = (int64_t)(c->gdens_cand * P.wsum * 1.25) + 65536;
+  const int64_t want_pass = (int64_t)(c->gdens_pass * P.wsum * 1.25) + 4096;
   const int64_t grid_b = gather_block_grid(false);
   *grid_h = std::max<int64_t>(1, std::min<int64_t>(grid_b, ((int64_t)1 << 25) / c->huge_cap));
   const int rounds = std::max(1, std::min<int>(c->tune.align_rounds, kMaxAlignRounds));
@@ -618,10 +625,7 @@ static int map_passes_graph(stormgpu_ctx* c, const PassSetup& P, int64_t launche
   cudaGetLastError();
   S.ms_gather = tg; S.ms_filter = tf; S.ms_align = ta; S.ms_replay = tr; S.ms_total = tt;
   S.kernels = launches;
-  if (P.wsum > 0) {
-    c->dens_cand = (double)h[kGsMaxCand] / P.wsum;
-    c->dens_pass = (double)h[kGsMaxPass] / P.wsum;
-  }
+  if (P.wsum > 0) set_densities(c, (double)h[kGsMaxCand] / P.wsum, (double)h[kGsMaxPass] / P.wsum);
   return 0;
 }
 
@@ -684,7 +688,7 @@ static int map_device_once(stormgpu_ctx* c, const stormgpu_reads* reads, stormgp
   const int BW = 2 * sp.I + 1;
   const int wpr = (2 * BW + 31) / 32 + (sp.colour ? (BW + 31) / 32 : 0);
   const int64_t tbs = ((maxL + sp.I + 1) / 2 + 7) & ~7LL;
-  if (c->graphs && !c->graph_broken && c->dens_cand > 0 && c->huge_cap <= ((int64_t)1 << 22)) {
+  if (c->graphs && !c->graph_broken && c->gdens_cand > 0 && c->huge_cap <= ((int64_t)1 << 22)) {
     const PassSetup P{sp, fwd, rev, n, maxL, minL, wsum, wpr, tbs, out};
     const int g = map_passes_graph(c, P, launches);
     if (g != kGraphRetry) return g;
@@ -894,10 +898,7 @@ static int map_device_once(stormgpu_ctx* c, const stormgpu_reads* reads, stormgp
   cudaEventElapsedTime(&tt, c->ev[6], c->ev[7]);
   S.ms_gather = tg; S.ms_filter = tf; S.ms_align = ta; S.ms_replay = tr; S.ms_total = tt;
   S.kernels = launches;
-  if (n > 0 && wsum > 0) {
-    c->dens_cand = (double)max_cand / wsum;
-    c->dens_pass = (double)max_pass / wsum;
-  }
+  if (n > 0 && wsum > 0) set_densities(c, (double)max_cand / wsum, (double)max_pass / wsum);
   return 0;
 }
 
