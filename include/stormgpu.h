@@ -190,6 +190,20 @@ void stormgpu_server_close(stormgpu_server *s);
 int stormgpu_genome_map_greedy(stormgpu_ctx *ctx, int32_t uniqueness_threshold, int32_t *order,
                                int64_t *n_placed);
 
+/* Contextual placement of the mapping without -M and without -G (the default; genome_map.c:
+ * 233-531, order of genome_map.c:551-796): the mapped reads in descending (unsigned) order of
+ * their rank-0 score, ties in read order, each placed at the first of its ranks with the highest
+ * score adjusted to the consensus of the reads placed before it (genome_map.c:366-424) -- when
+ * uniqueness is set (-u), only if the adjusted rank-0 score leads the adjusted rank-1 score by
+ * more than uniqueness_threshold -- whose counters it then updates.  Output in (sequence,
+ * start) order, reads of one position in placement order: read[i] and the placed rank rank[i]
+ * for i < *n_placed (read and rank hold n int32 on the host).  Works on the results of the last
+ * stormgpu_map call on ctx, which stay on the device.
+ * Replaces: genome_map__build_contextual (genome_map.c:432-531) and the position-major walk of
+ * genome_map__generate_SAM_output (genome_map.c:551-796). */
+int stormgpu_genome_map_contextual(stormgpu_ctx *ctx, int32_t uniqueness, int32_t uniqueness_threshold,
+                                   int32_t *read, int32_t *rank, int64_t *n_placed);
+
 /* Statistics of the last stormgpu_map* call. */
 typedef struct stormgpu_stats {
   int64_t candidates;        /* diagonals produced by the hit gather */

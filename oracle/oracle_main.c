@@ -78,6 +78,6 @@ static int oracle_place_greedy(void *user, const sh_refs *refs, const stormgpu_r
 }
 
 int main(int argc, char **argv) {
-  storm_mapper m = {"oracle", oracle_map, oracle_place_greedy, NULL, NULL, NULL, oracle_map_chunked};
+  storm_mapper m = {"oracle", oracle_map, oracle_place_greedy, NULL, NULL, NULL, oracle_map_chunked, NULL};
   return storm_cli_main(argc, argv, STORM_COLOUR, &m);
 }

@@ -92,6 +92,9 @@ def lib():
         L.stormgpu_get_tuning.argtypes = [C.c_void_p, C.POINTER(Tuning)]
         L.stormgpu_set_tuning.argtypes = [C.c_void_p, C.POINTER(Tuning)]
         L.stormgpu_set_graphs.argtypes = [C.c_void_p, C.c_int]
+        L.stormgpu_genome_map_greedy.argtypes = [C.c_void_p, C.c_int32, C.c_void_p, C.POINTER(C.c_int64)]
+        L.stormgpu_genome_map_contextual.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p,
+                                                     C.POINTER(C.c_int64)]
         L.stormgpu_autotune.argtypes = [C.c_void_p, C.POINTER(Reads), C.c_int64, C.POINTER(Tuning)]
         L.stormgpu_server_set_tuning.argtypes = [C.c_void_p, C.POINTER(Tuning)]
         L.stormgpu_sw_filter.argtypes = [C.c_int, C.c_int, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
@@ -225,6 +228,20 @@ class Mapper:
         for k, v in kw.items():
             setattr(t, k, int(v))
         _check(lib().stormgpu_set_tuning(self._ctx, C.byref(t)))
+
+    def genome_map(self, n: int, greedy: bool = False, uniqueness_threshold: int | None = None):
+        """Placement of the last `map` call's n reads without -M (genome_map.c): the placed reads
+        in position order and the rank each is placed at (greedy: always rank 0)."""
+        read = np.zeros(max(n, 1), np.int32)
+        rank = np.zeros(max(n, 1), np.int32)
+        npl = C.c_int64(0)
+        thr = 0 if uniqueness_threshold is None else int(uniqueness_threshold)
+        if greedy:
+            _check(lib().stormgpu_genome_map_greedy(self._ctx, thr, read.ctypes.data, C.byref(npl)))
+        else:
+            _check(lib().stormgpu_genome_map_contextual(self._ctx, 0 if uniqueness_threshold is None else 1, thr,
+                                                        read.ctypes.data, rank.ctypes.data, C.byref(npl)))
+        return read[:npl.value], rank[:npl.value]
 
     def set_graphs(self, enable: bool):
         """CUDA graphs for the strand passes (on by default; the results are the same)."""

@@ -13,7 +13,7 @@ LIB_DIR = os.path.join(PKG, "lib")
 BIN_DIR = os.path.join(PKG, "bin")
 LIB = os.path.join(LIB_DIR, "libstormgpu.so")
 HOST_LIB = os.path.join(LIB_DIR, "libstormhost.so")
-CU_SOURCES = ["stormgpu.cu", "index_build.cu", "map_kernels.cu", "sw_filter.cu", "gather.cu", "intpeak.cu", "align_noalloc.cu", "server.cu", "genome_map.cu", "autotune.cu"]
+CU_SOURCES = ["stormgpu.cu", "index_build.cu", "map_kernels.cu", "sw_filter.cu", "gather.cu", "intpeak.cu", "align_noalloc.cu", "server.cu", "genome_map.cu", "genome_map_ctx.cu", "autotune.cu"]
 HOST_SOURCES = ["host/storm_host.c", "host/storm_cli.c", "host/storm_gpu_main.c"]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
               "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr"]

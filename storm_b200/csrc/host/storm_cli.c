@@ -432,6 +432,7 @@ int storm_cli_main(int argc, char **argv, int colour, const storm_mapper *mapper
       exit(1);
     }
     int64_t npl = 0;
+    const double t_place = now_s();
     if (map_greedy) {
       if (!mapper->place_greedy ||
           mapper->place_greedy(mapper->user, &refs, &res, reads.n, uniqueness ? uniq_thr : 0, pl, &npl, emsg,
@@ -439,10 +440,17 @@ int storm_cli_main(int argc, char **argv, int colour, const storm_mapper *mapper
         err("Mapping failed (%s): %s", mapper->name, emsg);
         exit(2);
       }
+    } else if (mapper->place_contextual) {
+      if (mapper->place_contextual(mapper->user, &refs, &res, reads.n, uniqueness, uniq_thr, pl, &npl, emsg,
+                                   sizeof(emsg)) != 0) {
+        err("Mapping failed (%s): %s", mapper->name, emsg);
+        exit(2);
+      }
     } else {
       sh_genome_map_contextual(&refs, &res, reads.n, colour, allowed_indels, match, mismatch, uniqueness, uniq_thr,
                                pl, &npl);
     }
+    msg(2, "Times: placement of %ld reads %.3f s.\n", (long)npl, now_s() - t_place);
     if (output) {
       static char obuf2[1 << 22];
       setvbuf(output, obuf2, _IOFBF, sizeof(obuf2));

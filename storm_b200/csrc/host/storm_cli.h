@@ -38,6 +38,10 @@ typedef struct storm_mapper {
   int (*map_chunked)(void *user, const stormgpu_params *p, const char *seeds, const sh_refs *refs,
                      const sh_reads *reads, stormgpu_results *out, int64_t piece, storm_chunk_fn chunk,
                      void *chunk_user, char *err, int errlen);
+  /* may be NULL (then the host's sh_genome_map_contextual); else the contextual placement
+   * (no -M, no -G) of the results of the last map call, as sh_genome_map_contextual */
+  int (*place_contextual)(void *user, const sh_refs *refs, const stormgpu_results *res, int64_t n, int uniqueness,
+                          int uniqueness_threshold, sh_placement *out, int64_t *n_out, char *err, int errlen);
 } storm_mapper;
 
 int storm_cli_main(int argc, char **argv, int colour, const storm_mapper *mapper);

@@ -88,6 +88,22 @@ static int gpu_place_greedy(void *user, const sh_refs *refs, const stormgpu_resu
   return rc;
 }
 
+static int gpu_place_contextual(void *user, const sh_refs *refs, const stormgpu_results *res, int64_t n,
+                                int uniqueness, int uniqueness_threshold, sh_placement *out, int64_t *n_out,
+                                char *err, int errlen) {
+  (void)refs; (void)res;
+  gpu_state *gs = (gpu_state *)user;
+  int32_t *rd = malloc(sizeof(int32_t) * (size_t)(n ? n : 1)), *rk = malloc(sizeof(int32_t) * (size_t)(n ? n : 1));
+  int rc = rd && rk ? stormgpu_genome_map_contextual(gs->ctx, uniqueness, uniqueness_threshold, rd, rk, n_out)
+                    : STORMGPU_ENOMEM;
+  if (rc) snprintf(err, (size_t)errlen, "%s", rd && rk ? stormgpu_last_error() : "host allocation failed");
+  else
+    for (int64_t i = 0; i < *n_out; ++i) out[i] = (sh_placement){rd[i], rk[i]};
+  free(rd);
+  free(rk);
+  return rc;
+}
+
 static void gpu_finish(void *user) {
   gpu_state *gs = (gpu_state *)user;
   if (gs->ctx) stormgpu_close(gs->ctx);
@@ -96,6 +112,7 @@ static void gpu_finish(void *user) {
 
 int main(int argc, char **argv) {
   gpu_state gs = {NULL};
-  storm_mapper m = {"cuda", gpu_map, gpu_place_greedy, gpu_finish, &gs, gpu_prepare, gpu_map_chunked};
+  storm_mapper m = {"cuda", gpu_map, gpu_place_greedy, gpu_finish, &gs, gpu_prepare, gpu_map_chunked,
+                    gpu_place_contextual};
   return storm_cli_main(argc, argv, STORM_COLOUR, &m);
 }

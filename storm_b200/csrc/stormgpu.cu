@@ -1046,6 +1046,7 @@ extern "C" int stormgpu_map(stormgpu_ctx* c, const stormgpu_reads* reads, stormg
   int rc = map_device_impl(c, &dr, &dres);
   if (rc) return rc;
   c->last_n = n;
+  c->last_tbs = out->tb_stride;
   if (n > 0) {
     SG_CUDA(cudaMemcpyAsync(out->hits, c->hits.p, sizeof(stormgpu_hit) * n * 4, cudaMemcpyDeviceToHost, st));
     SG_CUDA(cudaMemcpyAsync(out->tb, c->tb.p, n * 4 * out->tb_stride, cudaMemcpyDeviceToHost, st));

@@ -46,11 +46,32 @@ def _without_m(args):
 
 @pytest.mark.skipif(not ffi.ref_available(), reason="oracle/_ref not built")
 @pytest.mark.parametrize("cfg,scale,extra", [(0, 0.2, []), (0, 0.2, ["-G"]), (0, 0.05, ["-G", "-u", "5", "-i", "7"]),
-                                             (1, 0.02, []), (1, 0.02, ["-G"])])
+                                             (0, 0.05, ["-u", "5", "-i", "7"]), (1, 0.02, []), (1, 0.05, ["-u", "3"]),
+                                             (1, 0.02, ["-G"])])
 def test_gpu_cli_genome_map_matches_reference(cfg, scale, extra, tmp_path):
-    """Without -M: the per-position map (greedy placement sorted on the GPU, contextual placement
-    on the mapped records), SAM written position-major."""
+    """Without -M: the per-position map (greedy placement by a device sort, contextual placement
+    in device waves), SAM written position-major."""
     _live(cfg, scale, extra, tmp_path, strip_m=True)
+
+
+@pytest.mark.skipif(not ffi.ref_available(), reason="oracle/_ref not built")
+def test_gpu_cli_contextual_placement_of_piled_reads(tmp_path):
+    """Reads piled on repeated and overlapping positions (40 kbp, half of it repeats, 4,000 reads
+    with indels): the contextual rescoring against the consensus decides between copies, and the
+    device waves run long chains of reads that share positions."""
+    genome = synth.make_genome([40000], 12, 0.45, 0.5)
+    synth.write_fasta(str(tmp_path / "ref.fa"), genome)
+    seqs, quals = synth.simulate_nucleotide_reads(genome, 4000, 50, 13, synth.ReadModel(indel_rate=0.01, indel_max=2))
+    synth.write_fastq(str(tmp_path / "reads.fq"), seqs, quals)
+    outs = {}
+    for tag, exe in (("ref", os.path.join(ffi.REF_DIR, "storm-nucleotide")), ("gpu", _exe("nucleotide"))):
+        p = subprocess.run([exe, "-g", "ref.fa", "-r", "reads.fq", "-o", tag + ".sam", "-v", "0", "-i", "5", "-z", "90",
+                            "-t", "95"], cwd=str(tmp_path), env=dict(os.environ, MALLOC_PERTURB_="255"),
+                           capture_output=True, timeout=600)
+        assert p.returncode == 0, p.stderr[-3000:]
+        outs[tag] = [l for l in (tmp_path / (tag + ".sam")).read_bytes().split(b"\n") if not l.startswith(b"@PG")]
+    assert outs["gpu"] == outs["ref"]
+    assert sum(1 for l in outs["gpu"] if l and not l.startswith(b"@")) > 1000
 
 
 def _live(cfg, scale, extra, tmp_path, strip_m=False):
