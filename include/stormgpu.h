@@ -223,6 +223,8 @@ typedef struct stormgpu_stats {
   int64_t graph_passes;      /* of them, passes that ran inside a CUDA graph (every pass of a call
                                 captured as one graph and launched once, no host read between
                                 its launches) */
+  int64_t placement_waves;   /* waves of the last stormgpu_genome_map_contextual call on the
+                                context (reads placed together in one wave share no position) */
 } stormgpu_stats;
 int stormgpu_get_stats(stormgpu_ctx *ctx, stormgpu_stats *out);
 

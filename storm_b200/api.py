@@ -52,7 +52,8 @@ class Stats(C.Structure):
                                          "hit_positions", "filter_cells", "align_cells", "kernels",
                                          "filter_band_cells")] + \
                [(n, C.c_double) for n in ("ms_index", "ms_gather", "ms_filter", "ms_align",
-                                          "ms_replay", "ms_total")] + [("passes", C.c_int64), ("graph_passes", C.c_int64)]
+                                          "ms_replay", "ms_total")] + [("passes", C.c_int64), ("graph_passes", C.c_int64),
+                                                                 ("placement_waves", C.c_int64)]
 
 
 class Tuning(C.Structure):

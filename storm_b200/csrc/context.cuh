@@ -104,7 +104,6 @@ struct stormgpu_ctx {
   cudaEvent_t rev[2 * 6 + 1];  // alignment rounds: before the first, after each round's alignment and replay
   int64_t last_n = -1;  // reads of the last stormgpu_map call (its results stay in hits / mapped)
   int64_t last_tbs = 0;  // its traceback stride
-  int64_t gm_waves = 0;  // waves of the last contextual placement
   sg::WorkBudget work;  // working memory of the mapping buffers; work.limit 0 = no limit
   // candidates and passing candidates per read of the densest strand pass of the last mapping
   // call: a batch that would exceed a pass's bounds at that density is cut up front instead of

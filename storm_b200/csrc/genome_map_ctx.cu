@@ -230,9 +230,16 @@ __global__ void ctx_mark_kernel(int64_t nm, CtxMap M, uint32_t* __restrict__ bit
   }
 }
 
+// Waves run back to back without the host: wave w takes the list `pending` of counts[cur]
+// reads and appends the reads it leaves to the other list, counted in counts[cur ^ 1] (zeroed by
+// its first kernel); counts[2] counts the waves that had pending reads.
+
 // every position of every span of the pending reads: the earliest rank
-__global__ void ctx_rank_kernel(int64_t np, const uint32_t* __restrict__ pending, CtxMap M) {
+__global__ void ctx_rank_kernel(unsigned long long* __restrict__ counts, int cur, const uint32_t* __restrict__ pending,
+                                CtxMap M) {
   const int lane = threadIdx.x & 31;
+  const int64_t np = (int64_t)counts[cur];
+  if (blockIdx.x == 0 && threadIdx.x == 0) counts[cur ^ 1] = 0;
   for (int64_t q = warp_id(); q < np; q += warp_count()) {
     const uint32_t j = pending[q];
     const int64_t r = M.order[j];
@@ -246,9 +253,11 @@ __global__ void ctx_rank_kernel(int64_t np, const uint32_t* __restrict__ pending
 }
 
 // the pending reads that are earliest on every position they read: placed now
-__global__ void ctx_place_kernel(int64_t np, const uint32_t* __restrict__ pending, CtxMap M, int uniqueness,
+__global__ void ctx_place_kernel(const unsigned long long* __restrict__ counts, int cur,
+                                 const uint32_t* __restrict__ pending, CtxMap M, int uniqueness,
                                  int uniqueness_threshold, int32_t* __restrict__ placed) {
   const int lane = threadIdx.x & 31;
+  const int64_t np = (int64_t)counts[cur];
   for (int64_t q = warp_id(); q < np; q += warp_count()) {
     const uint32_t j = pending[q];
     const int64_t r = M.order[j];
@@ -279,10 +288,12 @@ __global__ void ctx_place_kernel(int64_t np, const uint32_t* __restrict__ pendin
 }
 
 // the spans of this wave's pending reads back to no rank; the reads still pending to `next`
-__global__ void ctx_reset_kernel(int64_t np, const uint32_t* __restrict__ pending, CtxMap M,
-                                 const int32_t* __restrict__ placed, uint32_t* __restrict__ next,
-                                 unsigned long long* __restrict__ next_count) {
+__global__ void ctx_reset_kernel(unsigned long long* __restrict__ counts, int cur, const uint32_t* __restrict__ pending,
+                                 CtxMap M, const int32_t* __restrict__ placed, uint32_t* __restrict__ next) {
   const int lane = threadIdx.x & 31;
+  const int64_t np = (int64_t)counts[cur];
+  unsigned long long* next_count = counts + (cur ^ 1);
+  if (blockIdx.x == 0 && threadIdx.x == 0 && np > 0) counts[2]++;
   for (int64_t q = warp_id(); q < np; q += warp_count()) {
     const uint32_t j = pending[q];
     const int64_t r = M.order[j];
@@ -437,7 +448,7 @@ extern "C" int stormgpu_genome_map_contextual(stormgpu_ctx* c, int32_t uniquenes
   M.minrank = S.get<uint32_t>(cov);
   int32_t* placed = S.get<int32_t>(nm);
   uint32_t *pend0 = S.get<uint32_t>(nm), *pend1 = S.get<uint32_t>(nm);
-  unsigned long long* cnt = S.get<unsigned long long>(2);
+  unsigned long long* cnt = S.get<unsigned long long>(3);
   if (!M.created || !M.aligned || !M.inserted || !M.minrank || !placed || !pend0 || !pend1 || !cnt) return nomem();
   SG_CUDA(cudaMemsetAsync(M.created, 0, (size_t)cov, st));
   SG_CUDA(cudaMemsetAsync(M.aligned, 0, sizeof(uint32_t) * cov, st));
@@ -445,27 +456,33 @@ extern "C" int stormgpu_genome_map_contextual(stormgpu_ctx* c, int32_t uniquenes
   SG_CUDA(cudaMemsetAsync(M.minrank, 0xff, sizeof(uint32_t) * cov, st));
   SG_CUDA(cudaMemsetAsync(placed, 0xfe, sizeof(int32_t) * nm, st));  // kPending in every rank
   rank_iota_kernel<<<grid_for(nm, 256), 256, 0, st>>>(nm, pend0);  // every rank pending
-  int64_t np = nm, waves = 0;
-  uint32_t *cur = pend0, *nxt = pend1;
-  while (np > 0) {
-    const unsigned g = grid_for(np * 32, 256);
-    ctx_rank_kernel<<<g, 256, 0, st>>>(np, cur, M);
-    ctx_place_kernel<<<g, 256, 0, st>>>(np, cur, M, uniqueness, uniqueness_threshold, placed);
-    SG_CUDA(cudaMemsetAsync(cnt, 0, sizeof(unsigned long long), st));
-    ctx_reset_kernel<<<g, 256, 0, st>>>(np, cur, M, placed, nxt, cnt);
-    unsigned long long left = 0;
-    SG_CUDA(cudaMemcpyAsync(&left, cnt, sizeof(left), cudaMemcpyDeviceToHost, st));
+  // waves in groups of kGroup between two reads of the pending count (a wave with none pending
+  // costs three near-empty launches)
+  constexpr int kGroup = 16;
+  const unsigned long long init[3] = {(unsigned long long)nm, 0, 0};
+  SG_CUDA(cudaMemcpyAsync(cnt, init, sizeof(init), cudaMemcpyHostToDevice, st));
+  const unsigned g = grid_for(nm * 32, 256);
+  uint32_t* lists[2] = {pend0, pend1};
+  int cur = 0;
+  unsigned long long h[3] = {(unsigned long long)nm, 0, 0};
+  static_assert(kGroup % 2 == 0, "a group ends on the list it started from");
+  for (;;) {
+    for (int k = 0; k < kGroup; ++k, cur ^= 1) {
+      ctx_rank_kernel<<<g, 256, 0, st>>>(cnt, cur, lists[cur], M);
+      ctx_place_kernel<<<g, 256, 0, st>>>(cnt, cur, lists[cur], M, uniqueness, uniqueness_threshold, placed);
+      ctx_reset_kernel<<<g, 256, 0, st>>>(cnt, cur, lists[cur], M, placed, lists[cur ^ 1]);
+    }
+    const unsigned long long before = h[cur];
+    SG_CUDA(cudaMemcpyAsync(h, cnt, sizeof(h), cudaMemcpyDeviceToHost, st));
     SG_CUDA(cudaStreamSynchronize(st));
     SG_CUDA(cudaGetLastError());
-    if ((int64_t)left >= np) {  // cannot happen: the earliest pending rank is always placed
-      sg_set_error("stormgpu_genome_map_contextual: a wave placed no read");
+    if (h[cur] == 0) break;
+    if (h[cur] >= before) {  // cannot happen: the earliest pending rank is always placed
+      sg_set_error("stormgpu_genome_map_contextual: %d waves placed no read", kGroup);
       return STORMGPU_ECUDA;
     }
-    np = (int64_t)left;
-    std::swap(cur, nxt);
-    ++waves;
   }
-  c->gm_waves = waves;
+  c->stats.placement_waves = (int64_t)h[2];
   // the placed reads by start position, ties in placement order (genome_map.c:551-796)
   SG_CUDA(cudaMemsetAsync(cnt, 0, sizeof(unsigned long long), st));
   ctx_out_keys_kernel<<<grid_for(nm, 256), 256, 0, st>>>(nm, M, placed, k0, pend0, cnt);

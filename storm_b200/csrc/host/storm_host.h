@@ -109,8 +109,8 @@ typedef struct sh_placement {
  * (a stable sort on the unsigned value, as the reference's radix sort); every alignment of the
  * read rescored against the consensus of the reads placed so far (6-bit counters per code that
  * wrap, genome_map.c:37-48), the best placed and the consensus updated along its traceback.
- * out holds n entries; *n_out receives the number placed.  Inherently sequential: it runs
- * here, on the GPU's top-4 records. */
+ * out holds n entries; *n_out receives the number placed.  The restatement the oracle front end
+ * places with (the CUDA command line places on the device, stormgpu_genome_map_contextual). */
 int sh_genome_map_contextual(const sh_refs *refs, const stormgpu_results *res, int64_t n, int colour, int indels,
                              int match, int mismatch, int uniqueness, int uniqueness_threshold,
                              sh_placement *out, int64_t *n_out);
