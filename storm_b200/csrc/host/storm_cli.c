@@ -454,8 +454,13 @@ int storm_cli_main(int argc, char **argv, int colour, const storm_mapper *mapper
     if (output) {
       static char obuf2[1 << 22];
       setvbuf(output, obuf2, _IOFBF, sizeof(obuf2));
-      sh_write_genome_map_sam(output, &so, &refs, &reads, &res, pl, npl);
+      const double t_sam = now_s();
+      if (sh_write_genome_map_sam(output, &so, &refs, &reads, &res, pl, npl) != 0) {
+        err("%s", sh_last_error());
+        exit(1);
+      }
       fflush(output);
+      msg(2, "Times: SAM output %.3f s.\n", now_s() - t_sam);
     } else {
       err("No file name provided for SAM output.");
     }

@@ -1261,6 +1261,69 @@ void sh_sort_placements(const stormgpu_results *res, sh_placement *pl, int64_t n
   free(k);
 }
 
+/* the records of placements [first, first + count) (genome_map.c:551-796): each line formatted
+ * in a buffer (the fields of the reference's fprintf) and written at once.  In colour space the
+ * reference's running reference symbol (the first base transformed by every colour before the
+ * start; placements come in (sequence, position) order) is the symbol at the start.  Returns 0,
+ * or STORMGPU_ENOMEM when a line buffer cannot be allocated. */
+static int write_placement_records(FILE *f, const sh_sam_opts *o, const sh_refs *refs, const sh_reads *reads,
+                                   const stormgpu_results *res, const sh_placement *pl, int64_t first,
+                                   int64_t count, uint8_t *const *chk) {
+  const int colour = o->colour;
+  char cigar[4 * STORMGPU_MAX_READ_LEN + 64], seq[2 * STORMGPU_MAX_READ_LEN + 8];
+  size_t lcap = 4096;
+  char *line = malloc(lcap);
+  if (!line) return STORMGPU_ENOMEM;
+  for (int64_t i = first; i < first + count; ++i) {
+    const int64_t r = pl[i].read;
+    const int k = pl[i].rank;
+    const stormgpu_hit *h = &res->hits[r * 4];
+    const int ref = h[k].ref_id;
+    const int64_t start = h[k].ref_start;
+    const int sym = colour ? symbol_at(refs, chk, ref, start) : 0;
+    const int rev = (h[k].sense & 2) != 0;
+    const int mapq = sh_mapq(k, h[0].score, h[1].score, h[k].score, o->min_score, o->delta_m);
+    const int ed = sh_traceback_to_cigar(res->tb + (size_t)(r * 4 + k) * (size_t)res->tb_stride, h[k].tb_len,
+                                         refs->codes[ref], start, colour, sym, cigar, seq);
+    const char *rname = refs->names[ref] ? refs->names[ref] : "*";
+    const int L = reads->lengths[r];
+    const size_t need = strlen(reads->names[r]) + strlen(rname) + strlen(cigar) + strlen(seq) + (size_t)L + 160;
+    if (need > lcap) {
+      char *grown = realloc(line, 2 * need);
+      if (!grown) { free(line); return STORMGPU_ENOMEM; }
+      line = grown;
+      lcap = 2 * need;
+    }
+    char *p = line;
+    p = put_str(p, reads->names[r]); *p++ = '\t';
+    p = put_long(p, rev ? 0x10 : 0); *p++ = '\t';
+    p = put_str(p, rname); *p++ = '\t';
+    p = put_long(p, (long)(start + 1)); *p++ = '\t';
+    p = put_long(p, mapq); *p++ = '\t';
+    p = put_str(p, cigar);
+    p = put_str(p, "\t*\t0\t0\t");
+    p = put_str(p, seq); *p++ = '\t';
+    if (reads->levels) {
+      const uint8_t *lv = reads->levels + r * reads->level_stride;
+      if (rev) {
+        for (int q = L - 1; q >= 0; --q) { int c = o->quality_base + LEVEL_UB[get2(lv, q)]; *p++ = (char)(c < 126 ? c : 126); }
+        if (colour) { int c = o->quality_base + LEVEL_UB[reads->first_level[r]]; *p++ = (char)(c < 126 ? c : 126); }
+      } else {
+        if (colour) { int c = o->quality_base + LEVEL_UB[reads->first_level[r]]; *p++ = (char)(c < 126 ? c : 126); }
+        for (int q = 0; q < L; ++q) { int c = o->quality_base + LEVEL_UB[get2(lv, q)]; *p++ = (char)(c < 126 ? c : 126); }
+      }
+    } else {
+      *p++ = '*';
+    }
+    p = put_str(p, "\tAS:i:"); p = put_long(p, h[k].score);
+    p = put_str(p, "\tNM:i:"); p = put_long(p, ed);
+    *p++ = '\n';
+    fwrite(line, 1, (size_t)(p - line), f);
+  }
+  free(line);
+  return 0;
+}
+
 int sh_write_genome_map_sam(FILE *f, const sh_sam_opts *o, const sh_refs *refs, const sh_reads *reads,
                             const stormgpu_results *res, const sh_placement *pl, int64_t n_pl) {
   const int colour = o->colour;
@@ -1272,44 +1335,42 @@ int sh_write_genome_map_sam(FILE *f, const sh_sam_opts *o, const sh_refs *refs, 
   fprintf(f, "@PG\tID:%s\tVN:%s\tCL:\"", "SToRM", "0.0101");
   for (int i = 0; i < o->argc; ++i) fprintf(f, "%s ", o->argv[i]);
   fprintf(f, "\"\n");
-  char cigar[4 * STORMGPU_MAX_READ_LEN + 64], seq[2 * STORMGPU_MAX_READ_LEN + 8];
-  char *qbuf = malloc((size_t)reads->max_len + 8);
-  int cur_ref = -1, sym = 0;
-  int64_t cur_pos = 0;
-  for (int64_t i = 0; i < n_pl; ++i) {
-    const int64_t r = pl[i].read;
-    const int k = pl[i].rank;
-    const stormgpu_hit *h = &res->hits[r * 4];
-    const int ref = h[k].ref_id;
-    const int64_t start = h[k].ref_start;
-    if (colour) {  /* the reference's running ref_symbol: first base transformed by every colour before */
-      if (ref != cur_ref) { cur_ref = ref; cur_pos = 0; sym = refs->first_base[ref]; }
-      for (; cur_pos < start && cur_pos < refs->sizes[ref]; ++cur_pos) sym ^= get2(refs->codes[ref], cur_pos);
+  /* records formatted in chunks, several chunks at once, written in placement order */
+  uint8_t **chk = colour ? symbol_checkpoints(refs) : NULL;
+  int nthreads = 1;
+#ifdef _OPENMP
+  nthreads = omp_get_max_threads();
+#endif
+  int64_t CH = n_pl / (4 * (int64_t)nthreads);
+  CH = CH < 256 ? 256 : CH > 16384 ? 16384 : CH;
+  const int64_t per_round = CH * nthreads * 2;
+  char **bufs = calloc((size_t)nthreads * 2, sizeof(char *));
+  size_t *lens = calloc((size_t)nthreads * 2, sizeof(size_t));
+  int nomem = !bufs || !lens || (colour && !chk);
+  for (int64_t lo = 0; !nomem && lo < n_pl; lo += per_round) {
+    const int64_t hi = lo + per_round < n_pl ? lo + per_round : n_pl;
+    const int nchunks = (int)((hi - lo + CH - 1) / CH);
+#pragma omp parallel for schedule(dynamic, 1) reduction(|| : nomem)
+    for (int c = 0; c < nchunks; ++c) {
+      const int64_t a = lo + (int64_t)c * CH, e = a + CH < hi ? a + CH : hi;
+      FILE *m = open_memstream(&bufs[c], &lens[c]);
+      if (!m) { nomem = 1; continue; }
+      if (write_placement_records(m, o, refs, reads, res, pl, a, e - a, chk)) nomem = 1;
+      fclose(m);
     }
-    const int rev = (h[k].sense & 2) != 0;
-    const int mapq = sh_mapq(k, h[0].score, h[1].score, h[k].score, o->min_score, o->delta_m);
-    const int ed = sh_traceback_to_cigar(res->tb + (size_t)(r * 4 + k) * (size_t)res->tb_stride, h[k].tb_len,
-                                         refs->codes[ref], start, colour, sym & 3, cigar, seq);
-    fprintf(f, "%s\t%d\t%s\t%ld\t%d\t%s\t*\t0\t0\t%s\t", reads->names[r], rev ? 0x10 : 0,
-            refs->names[ref] ? refs->names[ref] : "*", (long)(start + 1), mapq, cigar, seq);
-    const int L = reads->lengths[r];
-    if (reads->levels) {
-      const uint8_t *lv = reads->levels + r * reads->level_stride;
-      int qi = 0;
-      if (rev) {
-        for (int q = L - 1; q >= 0; --q) { int c = o->quality_base + LEVEL_UB[get2(lv, q)]; qbuf[qi++] = (char)(c < 126 ? c : 126); }
-        if (colour) { int c = o->quality_base + LEVEL_UB[reads->first_level[r]]; qbuf[qi++] = (char)(c < 126 ? c : 126); }
-      } else {
-        if (colour) { int c = o->quality_base + LEVEL_UB[reads->first_level[r]]; qbuf[qi++] = (char)(c < 126 ? c : 126); }
-        for (int q = 0; q < L; ++q) { int c = o->quality_base + LEVEL_UB[get2(lv, q)]; qbuf[qi++] = (char)(c < 126 ? c : 126); }
-      }
-      fwrite(qbuf, 1, (size_t)qi, f);
-    } else {
-      fputc('*', f);
+    for (int c = 0; c < nchunks; ++c) {
+      if (!nomem) fwrite(bufs[c], 1, lens[c], f);
+      free(bufs[c]);
+      bufs[c] = NULL;
     }
-    fprintf(f, "\tAS:i:%d\tNM:i:%d\n", h[k].score, ed);
   }
-  free(qbuf);
+  free(bufs);
+  free(lens);
+  if (chk) {
+    for (int s = 0; s < refs->n; ++s) free(chk[s]);
+    free(chk);
+  }
+  if (nomem) return fail(STORMGPU_ENOMEM, "Out of memory while writing the SAM output.");
   return 0;
 }
 
