@@ -323,6 +323,7 @@ int storm_cli_main(int argc, char **argv, int colour, const storm_mapper *mapper
   const int reads_rc = sh_load_reads(reads_file, qual_file, colour, quality_base, 1, &reads);
   char reads_msg[512];
   snprintf(reads_msg, sizeof(reads_msg), "%s", sh_last_error());
+  const int reads_final = reads_rc != 0 && sh_last_error_final();
   const double t_reads = now_s();
   const int sort_rc = reads_rc == 0 ? sh_sort_reads(&reads) : 0;
   if (sort_rc != 0) snprintf(reads_msg, sizeof(reads_msg), "%s", sh_last_error());
@@ -332,6 +333,7 @@ int storm_cli_main(int argc, char **argv, int colour, const storm_mapper *mapper
   if (reads_rc != 0 || sort_rc != 0) {
     err("%s", reads_msg);
     if (reads_rc == STORMGPU_ENOMEM || sort_rc == STORMGPU_ENOMEM) exit(1);  /* SAFE_FAILURE__ALLOC, util.h:70-80 */
+    if (reads_final) exit(-1);  /* RETURN_INPUT_ERR from inside the loader */
     err("Reads could not be loaded. Exiting.");
     exit(-1);
   }

@@ -16,13 +16,23 @@
 #include <string.h>
 
 static __thread char g_err[512];  /* per thread: loads may run in parallel threads */
+static __thread int g_err_final;   /* g_err is the reference's whole message before it exits */
 const char *sh_last_error(void) { return g_err; }
+int sh_last_error_final(void) { return g_err_final; }
 static int fail(int code, const char *fmt, ...) {
   va_list ap;
   va_start(ap, fmt);
   vsnprintf(g_err, sizeof(g_err), fmt, ap);
   va_end(ap);
+  g_err_final = 0;
   return code;
+}
+/* "seams corrupt" at a line of a read file: the reference reports it and exits in the loader
+ * (reads_data.c:429-432) */
+static int fail_corrupt_line(int lineno) {
+  snprintf(g_err, sizeof(g_err), "\nReads file seams corrupt at line %d. Exiting.\n", lineno);
+  g_err_final = 1;
+  return STORMGPU_EINVAL;
 }
 
 /* Quality levels (read_quality.h:83-91, read_quality.c:189-195) */
@@ -370,6 +380,13 @@ static int fill_one(sh_reads *out, const char *buf, const rawread *r, int64_t i,
     /* colour: level of colour k is the quality of file colour k+1 (compress shift 1); the
      * last one reads one past the parsed qualities, which is 0 (read_quality.c:31-41) */
     for (int k = 0; k < L; ++k) put2(lv, k, quality_level(colour ? (k + 1 < L ? qv[k + 1] : 0) : qv[k]));
+  } else if (any_qual) {
+    /* a record without its quality line (the file's last, cut short): the reference keeps a NULL
+     * quality for it (reads_data.c:479), aligned at level 3 (alignment.c:157-160) */
+    uint8_t *lv = out->levels + i * out->level_stride;
+    for (int k = 0; k < L; ++k) put2(lv, k, 3);
+    out->first_level[i] = 3;
+    out->no_quality[i] = 1;
   }
   return 0;
 }
@@ -407,6 +424,12 @@ static int fill_reads(sh_reads *out, char *buf, rawread *rr, int64_t n, int colo
   if (!out->codes || (any_qual && !out->levels) || !out->lengths || !out->tags || !out->names || !out->first_base ||
       !out->first_level || !out->file_index)
     return fail(STORMGPU_ENOMEM, "Not enough memory for %ld reads.", (long)n);
+  if (any_qual) {
+    int64_t missing = 0;
+    for (int64_t i = 0; i < n; ++i) missing += !rr[i].has_qual;
+    if (missing && !(out->no_quality = calloc((size_t)n, 1)))
+      return fail(STORMGPU_ENOMEM, "Not enough memory for %ld reads.", (long)n);
+  }
   for (int64_t i = 0; i < n; ++i) buf[rr[i].name_off + (size_t)rr[i].name_len] = 0;
   /* reads are independent: filled in parallel; the first failing read (in file order) is filled
    * again alone to report its message, as a sequential pass would */
@@ -469,7 +492,7 @@ static int load_fastq(const char *path, int colour, int quality_base, int allow_
     size_t l2 = ll;
     while (l2 > 0 && (line[l2 - 1] == '\r' || line[l2 - 1] == '\n')) l2--;
     if (state == 0) {
-      if (ll == 0 || line[0] != '@') { free(rr); free(buf); free(title); return fail(STORMGPU_EINVAL, "Reads file seams corrupt at line %d.", lineno + 1); }
+      if (ll == 0 || line[0] != '@') { free(rr); free(buf); free(title); return fail_corrupt_line(lineno + 1); }
       if (n == cap && grow_raw(&rr, &cap)) { free(rr); free(buf); free(title); return fail(STORMGPU_ENOMEM, "Not enough memory to read %s.", path); }
       rr[n].name_off = (size_t)(line - buf) + 1;
       rr[n].name_len = header_name_len(line, l2);
@@ -477,14 +500,14 @@ static int load_fastq(const char *path, int colour, int quality_base, int allow_
       rr[n].qual_len = 0;
       state = 1;
     } else if (state == 1) {
-      if (ll == 0) { free(rr); free(buf); free(title); return fail(STORMGPU_EINVAL, "Reads file seams corrupt at line %d.", lineno + 1); }
+      if (ll == 0) { free(rr); free(buf); free(title); return fail_corrupt_line(lineno + 1); }
       rr[n].seq_off = (size_t)(line - buf);
       rr[n].seq_len = (int)strcspn(line, "\r\n");
       if ((size_t)rr[n].seq_len > ll) rr[n].seq_len = (int)ll;
       n++;
       state = 2;
     } else if (state == 2) {
-      if (ll == 0 || line[0] != '+') { free(rr); free(buf); free(title); return fail(STORMGPU_EINVAL, "Reads file seams corrupt at line %d.", lineno + 1); }
+      if (ll == 0 || line[0] != '+') { free(rr); free(buf); free(title); return fail_corrupt_line(lineno + 1); }
       state = 3;
     } else {
       rr[n - 1].qual_off = (size_t)(line - buf);
@@ -651,7 +674,7 @@ int sh_load_reads(const char *path, const char *qual_path, int colour, int quali
 void sh_free_reads(sh_reads *r) {
   free(r->arena);
   free(r->names); free(r->codes); free(r->levels); free(r->lengths); free(r->tags);
-  free(r->first_base); free(r->first_level); free(r->file_index); free(r->db_name);
+  free(r->first_base); free(r->first_level); free(r->file_index); free(r->db_name); free(r->no_quality);
   memset(r, 0, sizeof(*r));
 }
 
@@ -710,10 +733,12 @@ int sh_sort_reads(sh_reads *r) {
   uint64_t *tags = malloc(sizeof(uint64_t) * (size_t)n);
   char **names = malloc(sizeof(char *) * (size_t)n);
   uint8_t *fb = malloc((size_t)n), *fl = malloc((size_t)n);
+  uint8_t *nq = r->no_quality ? malloc((size_t)n) : NULL;
   int64_t *fi = malloc(sizeof(int64_t) * (size_t)n);
-  if (!k || !t || !cnt || !codes || (r->levels && !levels) || !lengths || !tags || !names || !fb || !fl || !fi) {
+  if (!k || !t || !cnt || !codes || (r->levels && !levels) || !lengths || !tags || !names || !fb || !fl || !fi ||
+      (r->no_quality && !nq)) {
     free(k); free(t); free(cnt); free(codes); free(levels); free(lengths); free(tags); free(names);
-    free(fb); free(fl); free(fi);
+    free(fb); free(fl); free(fi); free(nq);
     return fail(STORMGPU_ENOMEM, "Not enough memory to sort %ld reads.", (long)n);
   }
   uint64_t vt = 0;
@@ -739,11 +764,12 @@ int sh_sort_reads(sh_reads *r) {
     if (levels) memcpy(levels + i * r->level_stride, r->levels + s * r->level_stride, (size_t)r->level_stride);
     lengths[i] = r->lengths[s]; tags[i] = r->tags[s]; names[i] = r->names[s];
     fb[i] = r->first_base[s]; fl[i] = r->first_level[s]; fi[i] = r->file_index[s];
+    if (nq) nq[i] = r->no_quality[s];
   }
   free(r->codes); free(r->levels); free(r->lengths); free(r->tags); free(r->names);
-  free(r->first_base); free(r->first_level); free(r->file_index);
+  free(r->first_base); free(r->first_level); free(r->file_index); free(r->no_quality);
   r->codes = codes; r->levels = levels; r->lengths = lengths; r->tags = tags; r->names = names;
-  r->first_base = fb; r->first_level = fl; r->file_index = fi;
+  r->first_base = fb; r->first_level = fl; r->file_index = fi; r->no_quality = nq;
   free(k); free(t); free(cnt);
   return 0;
 }
@@ -853,6 +879,12 @@ int sh_mapq(int rank, int score0, int score1, int score_rank, int min_score, int
   return mapq;
 }
 
+/* whether read r's record had qualities (the reference writes "*", or the maximal quality in
+ * the unmapped FASTQ, for a read whose quality is NULL) */
+static inline int has_quality(const sh_reads *reads, int64_t r) {
+  return reads->levels && !(reads->no_quality && reads->no_quality[r]);
+}
+
 /* base of sequence s at position pos in colour space, from its first base and colours */
 
 typedef struct colour_cursor { int seq; int64_t pos; int base; } colour_cursor;
@@ -954,7 +986,7 @@ static int write_sam_records(FILE *f, const sh_sam_opts *o, const sh_refs *refs,
         p = put_str(p, cigar);
         p = put_str(p, "\t*\t0\t0\t");
         p = put_str(p, seq); *p++ = '\t';
-        if (reads->levels) {
+        if (has_quality(reads, r)) {
           const uint8_t *lv = reads->levels + r * reads->level_stride;
           if (rev) {
             for (int q = L - 1; q >= 0; --q) { int c = o->quality_base + LEVEL_UB[get2(lv, q)]; *p++ = (char)(c < 126 ? c : 126); }
@@ -982,7 +1014,7 @@ static int write_sam_records(FILE *f, const sh_sam_opts *o, const sh_refs *refs,
         for (int q = 0; q < L; ++q) qbuf[q] = B[get2(cd, q)];
         fwrite(qbuf, 1, (size_t)L, f);
         fputc('\t', f);
-        if (reads->levels) {
+        if (has_quality(reads, r)) {
           const uint8_t *lv = reads->levels + r * reads->level_stride;
           for (int q = 0; q < L; ++q) { int c = o->quality_base + LEVEL_UB[get2(lv, q)]; qbuf[q] = (char)(c < 126 ? c : 126); }
           fwrite(qbuf, 1, (size_t)L, f);
@@ -1303,7 +1335,7 @@ static int write_placement_records(FILE *f, const sh_sam_opts *o, const sh_refs 
     p = put_str(p, cigar);
     p = put_str(p, "\t*\t0\t0\t");
     p = put_str(p, seq); *p++ = '\t';
-    if (reads->levels) {
+    if (has_quality(reads, r)) {
       const uint8_t *lv = reads->levels + r * reads->level_stride;
       if (rev) {
         for (int q = L - 1; q >= 0; --q) { int c = o->quality_base + LEVEL_UB[get2(lv, q)]; *p++ = (char)(c < 126 ? c : 126); }
@@ -1389,7 +1421,7 @@ int sh_write_unmapped_fastq(FILE *f, const sh_sam_opts *o, const sh_reads *reads
       for (int k = 0; k < L; ++k) fputc(CL[get2(cd, k)], f);
     }
     fprintf(f, "\n+%s\n", reads->names[r]);
-    if (reads->levels) {
+    if (has_quality(reads, r)) {
       const uint8_t *lv = reads->levels + r * reads->level_stride;
       if (o->colour) { int c = o->quality_base + LEVEL_UB[reads->first_level[r]]; fputc(c < 126 ? c : 126, f); }
       for (int q = 0; q < L; ++q) { int c = o->quality_base + LEVEL_UB[get2(lv, q)]; fputc(c < 126 ? c : 126, f); }

@@ -53,10 +53,16 @@ typedef struct sh_reads {
   uint8_t  *first_level;   /* colour: level of the first colour's quality */
   int64_t  *file_index;    /* original position in the file */
   char     *arena;         /* the names[] strings live here (one allocation) */
+  uint8_t  *no_quality;    /* per read: 1 when its record has no quality line while others have
+                              one (its levels are then all 3 and its QUAL is written as the
+                              reference writes a NULL quality); NULL when there is no such read */
 } sh_reads;
 
 /* Status: 0 ok, negative on error (message in sh_last_error()). */
 const char *sh_last_error(void);
+/* 1 when the last error's message is the reference's whole message for a failure it reports
+ * and exits on (print it alone), 0 when the caller adds its own line as the reference does */
+int sh_last_error_final(void);
 
 int  sh_load_reference(const char *path, int colour, int ignore_lowercase, sh_refs *out);
 void sh_free_reference(sh_refs *r);

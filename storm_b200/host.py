@@ -26,7 +26,7 @@ class ShReads(C.Structure):
                 ("codes", C.c_void_p), ("code_stride", C.c_int64), ("levels", C.c_void_p),
                 ("level_stride", C.c_int64), ("lengths", C.c_void_p), ("tags", C.c_void_p),
                 ("first_base", C.c_void_p), ("first_level", C.c_void_p), ("file_index", C.c_void_p),
-                ("arena", C.c_void_p)]
+                ("arena", C.c_void_p), ("no_quality", C.c_void_p)]
 
 
 _h = None

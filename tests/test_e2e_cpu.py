@@ -253,3 +253,66 @@ def test_pipelined_sam_output_is_the_same(nuc_data, col_data, colour, args):
             outs[tag] = (sam, f.read())
     assert _mapped(outs["whole"][0]) > 0
     assert outs["pieces"] == outs["whole"]
+
+
+def _fastq_text(seqs, quals, names=None):
+    out = []
+    for k, (s, q) in enumerate(zip(seqs, quals)):
+        out.append(b"@" + (names[k] if names else b"r%d extra words" % k) + b"\n")
+        out.append(synth.BASES[s].tobytes() + b"\n+\n" + bytes(int(v) + 33 for v in q) + b"\n")
+    return b"".join(out)
+
+
+@pytest.mark.parametrize("colour,case", [(0, "header_without_at"), (0, "missing_plus"), (0, "empty_sequence"),
+                                         (0, "crlf"), (0, "title_comments"), (0, "last_record_without_quality"),
+                                         (0, "last_record_without_quality_unmapped"),
+                                         (0, "blank_line_between_records"), (1, "last_record_without_quality"),
+                                         (1, "last_record_without_quality_unmapped"), (1, "missing_plus")])
+def test_fastq_layouts_and_errors_like_reference(tmp_path, colour, case):
+    """FASTQ read files of unusual layout, valid or not (reads_data.c:351-566): the exit code, the
+    error message, and for a valid file the SAM and unmapped FASTQ must be the reference's (a
+    record cut short before its quality line keeps a NULL quality there)."""
+    genome = synth.make_genome([20000], 23)
+    synth.write_fasta(str(tmp_path / "ref.fa"), genome)
+    if colour:
+        pr, cols, q = synth.simulate_colour_reads(genome, 400, 49, 24)
+        synth.write_colour_fastq(str(tmp_path / "col.fq"), pr, cols, q)
+        text = (tmp_path / "col.fq").read_bytes()
+    else:
+        seqs, quals = synth.simulate_nucleotide_reads(genome, 400, 50, 24)
+        text = _fastq_text(seqs, quals)
+    recs = text.split(b"\n")  # 4 lines per record
+    if case == "last_record_without_quality_unmapped":  # a read that maps nowhere, then cut short
+        rnd = np.random.default_rng(25).integers(0, 4, size=len(recs[-4]))
+        recs[-4] = (recs[-4][:1] + bytes(b"0123"[v] for v in rnd[1:])) if colour else bytes(b"ACGT"[v] for v in rnd)
+        case = "last_record_without_quality"
+    if case == "header_without_at":
+        recs[4 * 37] = recs[4 * 37][1:]
+    elif case == "missing_plus":
+        del recs[4 * 51 + 2]
+    elif case == "empty_sequence":
+        recs[4 * 12 + 1] = b""
+    elif case == "crlf":
+        recs = [l + b"\r" if l else l for l in recs]
+    elif case == "title_comments":
+        recs = [b"# Title: layout test", b"# a comment"] + recs
+    elif case == "last_record_without_quality":
+        recs = recs[:-2]
+    elif case == "blank_line_between_records":
+        recs.insert(4 * 20, b"")
+    (tmp_path / "reads.fq").write_bytes(b"\n".join(recs))
+    _build()
+    res = {}
+    for name, exe in (("ref", REF_BIN[colour]), ("new", ORACLE_BIN[colour])):
+        p = subprocess.run([exe, "-g", "ref.fa", "-r", "reads.fq", "-o", name + ".sam", "-O", name + ".fq", "-v", "0",
+                            "-M", "1", "-z", "90", "-t", "95"] + (["-i", "7"] if colour else []), cwd=str(tmp_path),
+                           env=dict(os.environ, MALLOC_PERTURB_="255"), capture_output=True, timeout=600)
+        res[name] = p
+    assert res["new"].returncode == res["ref"].returncode, (res["ref"].stderr[-500:], res["new"].stderr[-500:])
+    if res["ref"].returncode != 0:
+        assert res["new"].stderr == res["ref"].stderr
+        return
+    for ext in (".sam", ".fq"):
+        a = [l for l in (tmp_path / ("ref" + ext)).read_bytes().split(b"\n") if not l.startswith(b"@PG")]
+        b = [l for l in (tmp_path / ("new" + ext)).read_bytes().split(b"\n") if not l.startswith(b"@PG")]
+        assert a == b, _first_diff(a, b)
