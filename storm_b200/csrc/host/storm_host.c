@@ -11,6 +11,7 @@
 #include <math.h>
 #include <stdio.h>
 #include <sys/stat.h>
+#include <unistd.h>
 #include <stdarg.h>
 #include <stdlib.h>
 #include <string.h>
@@ -60,6 +61,29 @@ static char *slurp(const char *path, size_t *len, int *oom) {
   if (fstat(fileno(f), &st) == 0 && S_ISREG(st.st_mode) && st.st_size > 0) cap = (size_t)st.st_size + 1;
   char *buf = malloc(cap + 1);
   if (!buf) { fclose(f); *oom = 1; return NULL; }
+  if (cap > ((size_t)64 << 20)) {
+    /* a large regular file: the threads read equal ranges of it (the copy out of the page cache
+     * and the buffer's first touch in parallel); the file's end is then confirmed as below */
+    const size_t size = cap - 1;
+    int nt = 1, bad = 0;
+#ifdef _OPENMP
+    nt = omp_get_max_threads();
+#endif
+    if (nt > 64) nt = 64;
+    const int fd = fileno(f);
+#pragma omp parallel for schedule(static) num_threads(nt) reduction(|| : bad)
+    for (int t = 0; t < nt; ++t) {
+      size_t lo = size * (size_t)t / (size_t)nt;
+      const size_t hi = size * (size_t)(t + 1) / (size_t)nt;
+      while (lo < hi) {
+        const ssize_t got = pread(fd, buf + lo, hi - lo, (off_t)lo);
+        if (got <= 0) { bad = 1; break; }
+        lo += (size_t)got;
+      }
+    }
+    if (!bad && fseeko(f, (off_t)size, SEEK_SET) == 0) n = size;  /* else read it all again below */
+    else rewind(f);
+  }
   for (;;) {
     if (n == cap) {
       char *grown = realloc(buf, 2 * cap + 1);
@@ -455,6 +479,50 @@ static int fill_reads(sh_reads *out, char *buf, rawread *rr, int64_t n, int colo
   return 0;
 }
 
+/* The start of every line of buf[from, len), as next_line walks them (a line after each '\n'
+ * that is not the buffer's last byte), found by the threads over equal byte ranges.  Returns 0,
+ * or 1 when memory runs out. */
+static int line_starts(const char *buf, size_t len, size_t from, size_t **out, int64_t *n_out) {
+  *out = NULL;
+  *n_out = 0;
+  if (from >= len) return 0;
+  int nt = 1;
+#ifdef _OPENMP
+  nt = omp_get_max_threads();
+#endif
+  if (len - from < ((size_t)1 << 20)) nt = 1;
+  if (nt > 256) nt = 256;
+  int64_t cnt[257] = {0};
+  /* '\n' at p, with p + 1 < len, in thread t's range [lo, hi) */
+#define SH_RANGE(t, lo, hi)                                                   \
+  const size_t lo = from + (len - from) * (size_t)(t) / (size_t)nt;          \
+  const size_t hi = from + (len - from) * (size_t)((t) + 1) / (size_t)nt;
+#pragma omp parallel for schedule(static) num_threads(nt)
+  for (int t = 0; t < nt; ++t) {
+    SH_RANGE(t, lo, hi)
+    int64_t c = 0;
+    for (const char *p = buf + lo, *e = buf + hi; (p = memchr(p, '\n', (size_t)(e - p))) != NULL; ++p)
+      if ((size_t)(p - buf) + 1 < len) c++;
+    cnt[t + 1] = c;
+  }
+  for (int t = 0; t < nt; ++t) cnt[t + 1] += cnt[t];
+  const int64_t n = 1 + cnt[nt];
+  size_t *ls = malloc(sizeof(size_t) * (size_t)n);
+  if (!ls) return 1;
+  ls[0] = from;
+#pragma omp parallel for schedule(static) num_threads(nt)
+  for (int t = 0; t < nt; ++t) {
+    SH_RANGE(t, lo, hi)
+    int64_t k = 1 + cnt[t];
+    for (const char *p = buf + lo, *e = buf + hi; (p = memchr(p, '\n', (size_t)(e - p))) != NULL; ++p)
+      if ((size_t)(p - buf) + 1 < len) ls[k++] = (size_t)(p - buf) + 1;
+  }
+#undef SH_RANGE
+  *out = ls;
+  *n_out = n;
+  return 0;
+}
+
 static int load_fastq(const char *path, int colour, int quality_base, int allow_mixed, sh_reads *out) {
   size_t len;
   int oom;
@@ -482,41 +550,57 @@ static int load_fastq(const char *path, int colour, int quality_base, int allow_
     if (ll > 0 && line[0] == '#') { lineno++; continue; }
     break;
   }
-  pos = rec_start;
-  int64_t cap = 1 << 16, n = 0;
+  /* the lines from rec_start: their starts found in parallel, then the record structure in one
+   * pass over them (the reference's line types and its error line numbers), then each record's
+   * name and sequence lengths in parallel */
+  size_t *ls = NULL;
+  int64_t nl = 0;
+  if (line_starts(buf, len, rec_start, &ls, &nl)) { free(buf); free(title); return fail(STORMGPU_ENOMEM, "Not enough memory to read %s.", path); }
+  int64_t cap = nl / 4 + 2, n = 0;
   rawread *rr = malloc(sizeof(rawread) * (size_t)cap);
-  if (!rr) { free(buf); free(title); return fail(STORMGPU_ENOMEM, "Not enough memory to read %s.", path); }
+  if (!rr) { free(ls); free(buf); free(title); return fail(STORMGPU_ENOMEM, "Not enough memory to read %s.", path); }
   int any_qual = 0;
   int state = 0; /* 0 header, 1 seq, 2 plus, 3 qual */
-  while (next_line(buf, len, &pos, &line, &ll)) {
+  const size_t last_end = len > 0 && buf[len - 1] == '\n' ? len - 1 : len;
+  for (int64_t i = 0; i < nl; ++i) {
+    line = buf + ls[i];
+    ll = (i + 1 < nl ? ls[i + 1] - 1 : last_end) - ls[i];  /* without '\n' */
     size_t l2 = ll;
-    while (l2 > 0 && (line[l2 - 1] == '\r' || line[l2 - 1] == '\n')) l2--;
+    while (l2 > 0 && line[l2 - 1] == '\r') l2--;
     if (state == 0) {
-      if (ll == 0 || line[0] != '@') { free(rr); free(buf); free(title); return fail_corrupt_line(lineno + 1); }
-      if (n == cap && grow_raw(&rr, &cap)) { free(rr); free(buf); free(title); return fail(STORMGPU_ENOMEM, "Not enough memory to read %s.", path); }
-      rr[n].name_off = (size_t)(line - buf) + 1;
-      rr[n].name_len = header_name_len(line, l2);
+      if (ll == 0 || line[0] != '@') { free(ls); free(rr); free(buf); free(title); return fail_corrupt_line(lineno + 1); }
+      if (n == cap && grow_raw(&rr, &cap)) { free(ls); free(rr); free(buf); free(title); return fail(STORMGPU_ENOMEM, "Not enough memory to read %s.", path); }
+      rr[n].name_off = ls[i] + 1;
+      rr[n].name_len = (int)(l2 < INT32_MAX ? l2 : INT32_MAX);  /* the header's length for now */
       rr[n].has_qual = 0;
       rr[n].qual_len = 0;
       state = 1;
     } else if (state == 1) {
-      if (ll == 0) { free(rr); free(buf); free(title); return fail_corrupt_line(lineno + 1); }
-      rr[n].seq_off = (size_t)(line - buf);
-      rr[n].seq_len = (int)strcspn(line, "\r\n");
-      if ((size_t)rr[n].seq_len > ll) rr[n].seq_len = (int)ll;
+      if (ll == 0) { free(ls); free(rr); free(buf); free(title); return fail_corrupt_line(lineno + 1); }
+      rr[n].seq_off = ls[i];
+      rr[n].seq_len = (int)(ll < INT32_MAX ? ll : INT32_MAX);  /* the line's length for now */
       n++;
       state = 2;
     } else if (state == 2) {
-      if (ll == 0 || line[0] != '+') { free(rr); free(buf); free(title); return fail_corrupt_line(lineno + 1); }
+      if (ll == 0 || line[0] != '+') { free(ls); free(rr); free(buf); free(title); return fail_corrupt_line(lineno + 1); }
       state = 3;
     } else {
-      rr[n - 1].qual_off = (size_t)(line - buf);
+      rr[n - 1].qual_off = ls[i];
       rr[n - 1].qual_len = (int)l2;
       rr[n - 1].has_qual = 1;
       any_qual = 1;
       state = 0;
     }
     lineno++;
+  }
+  free(ls);
+  /* the name: after the '@', up to the first char outside '!'..'~' or '@' (at most 255); the
+   * sequence: up to the first '\r' (or the line's end) */
+#pragma omp parallel for schedule(static)
+  for (int64_t i = 0; i < n; ++i) {
+    rr[i].name_len = header_name_len(buf + rr[i].name_off - 1, (size_t)rr[i].name_len);
+    const size_t sl = strcspn(buf + rr[i].seq_off, "\r\n");
+    if (sl < (size_t)rr[i].seq_len) rr[i].seq_len = (int)sl;
   }
   if (n == 0) { free(rr); free(buf); free(title); return fail(STORMGPU_EINVAL, "Reads could not be loaded."); }
   int rc = fill_reads(out, buf, rr, n, colour, quality_base, allow_mixed, any_qual);
