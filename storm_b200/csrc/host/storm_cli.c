@@ -469,7 +469,10 @@ int storm_cli_main(int argc, char **argv, int colour, const storm_mapper *mapper
     free(pl);
   }
   if (mapper->finish) mapper->finish(mapper->user);
-  if (unmapped) sh_write_unmapped_fastq(unmapped, &so, &reads, &res);
+  if (unmapped && sh_write_unmapped_fastq(unmapped, &so, &reads, &res) != 0) {
+    err("%s", sh_last_error());
+    exit(1);
+  }
   if (output && output != stdout) fclose(output);
   if (unmapped) fclose(unmapped);
   free(res.hits); free(res.tb); free(res.mapped);

@@ -1490,32 +1490,89 @@ int sh_write_genome_map_sam(FILE *f, const sh_sam_opts *o, const sh_refs *refs, 
   return 0;
 }
 
-int sh_write_unmapped_fastq(FILE *f, const sh_sam_opts *o, const sh_reads *reads,
-                            const stormgpu_results *res) {
+/* the unmapped reads among [first, first + count), each record formatted in a buffer and written
+ * at once.  Returns 0, or STORMGPU_ENOMEM when the buffer cannot be allocated. */
+static int write_unmapped_records(FILE *f, const sh_sam_opts *o, const sh_reads *reads,
+                                  const stormgpu_results *res, int64_t first, int64_t count) {
   static const char B[4] = {'A', 'C', 'G', 'T'}, CL[4] = {'0', '1', '2', '3'};
-  for (int64_t r = 0; r < reads->n; ++r) {
+  size_t lcap = 4096;
+  char *line = malloc(lcap);
+  if (!line) return STORMGPU_ENOMEM;
+  for (int64_t r = first; r < first + count; ++r) {
     if (res->mapped[r]) continue;
-    int L = reads->lengths[r];
-    fprintf(f, "@%s\n", reads->names[r]);
+    const int L = reads->lengths[r];
+    const size_t need = 2 * strlen(reads->names[r]) + 2 * (size_t)L + 16;
+    if (need > lcap) {
+      char *grown = realloc(line, 2 * need);
+      if (!grown) { free(line); return STORMGPU_ENOMEM; }
+      line = grown;
+      lcap = 2 * need;
+    }
+    char *p = line;
+    *p++ = '@';
+    p = put_str(p, reads->names[r]);
+    *p++ = '\n';
     const uint8_t *cd = reads->codes + r * reads->code_stride;
     if (!o->colour) {
-      for (int k = 0; k < L; ++k) fputc(B[get2(cd, k)], f);
+      for (int k = 0; k < L; ++k) *p++ = B[get2(cd, k)];
     } else {
-      fputc(B[reads->first_base[r] & 3], f);
-      for (int k = 0; k < L; ++k) fputc(CL[get2(cd, k)], f);
+      *p++ = B[reads->first_base[r] & 3];
+      for (int k = 0; k < L; ++k) *p++ = CL[get2(cd, k)];
     }
-    fprintf(f, "\n+%s\n", reads->names[r]);
+    *p++ = '\n';
+    *p++ = '+';
+    p = put_str(p, reads->names[r]);
+    *p++ = '\n';
     if (has_quality(reads, r)) {
       const uint8_t *lv = reads->levels + r * reads->level_stride;
-      if (o->colour) { int c = o->quality_base + LEVEL_UB[reads->first_level[r]]; fputc(c < 126 ? c : 126, f); }
-      for (int q = 0; q < L; ++q) { int c = o->quality_base + LEVEL_UB[get2(lv, q)]; fputc(c < 126 ? c : 126, f); }
+      if (o->colour) { int c = o->quality_base + LEVEL_UB[reads->first_level[r]]; *p++ = (char)(c < 126 ? c : 126); }
+      for (int q = 0; q < L; ++q) { int c = o->quality_base + LEVEL_UB[get2(lv, q)]; *p++ = (char)(c < 126 ? c : 126); }
     } else {
-      int c = o->quality_base + 93;
-      if (o->colour) fputc(c < 126 ? c : 126, f);
-      for (int q = 0; q < L; ++q) fputc(c < 126 ? c : 126, f);
+      const int c = o->quality_base + 93;  /* MAX_READ_QUALITY for a NULL quality (hit_map.c:565-571) */
+      if (o->colour) *p++ = (char)(c < 126 ? c : 126);
+      for (int q = 0; q < L; ++q) *p++ = (char)(c < 126 ? c : 126);
     }
-    fputc('\n', f);
+    *p++ = '\n';
+    fwrite(line, 1, (size_t)(p - line), f);
   }
+  free(line);
+  return 0;
+}
+
+/* hit_map.c:514-579: records formatted in chunks, several chunks at once, written in read order */
+int sh_write_unmapped_fastq(FILE *f, const sh_sam_opts *o, const sh_reads *reads,
+                            const stormgpu_results *res) {
+  const int64_t count = reads->n;
+  int nthreads = 1;
+#ifdef _OPENMP
+  nthreads = omp_get_max_threads();
+#endif
+  int64_t CH = count / (4 * (int64_t)nthreads);
+  CH = CH < 1024 ? 1024 : CH > 65536 ? 65536 : CH;
+  const int64_t per_round = CH * nthreads * 2;
+  char **bufs = calloc((size_t)nthreads * 2, sizeof(char *));
+  size_t *lens = calloc((size_t)nthreads * 2, sizeof(size_t));
+  int nomem = !bufs || !lens;
+  for (int64_t lo = 0; !nomem && lo < count; lo += per_round) {
+    const int64_t hi = lo + per_round < count ? lo + per_round : count;
+    const int nchunks = (int)((hi - lo + CH - 1) / CH);
+#pragma omp parallel for schedule(dynamic, 1) reduction(|| : nomem)
+    for (int c = 0; c < nchunks; ++c) {
+      const int64_t a = lo + (int64_t)c * CH, e = a + CH < hi ? a + CH : hi;
+      FILE *m = open_memstream(&bufs[c], &lens[c]);
+      if (!m) { nomem = 1; continue; }
+      if (write_unmapped_records(m, o, reads, res, a, e - a)) nomem = 1;
+      fclose(m);
+    }
+    for (int c = 0; c < nchunks; ++c) {
+      if (!nomem) fwrite(bufs[c], 1, lens[c], f);
+      free(bufs[c]);
+      bufs[c] = NULL;
+    }
+  }
+  free(bufs);
+  free(lens);
+  if (nomem) return fail(STORMGPU_ENOMEM, "Out of memory while writing the unmapped reads.");
   return 0;
 }
 
