@@ -145,9 +145,10 @@ int sh_load_reference(const char *path, int colour, int ignore_lowercase, sh_ref
   char *buf = slurp(path, &len, &oom);
   if (!buf) return read_failed(oom, path, "reference sequence");
   /* count chunks: lines starting with '>' (reference_data.c:210-220) */
-  int nseq = 0;
-  for (size_t i = 0; i < len; ++i)
-    if ((i == 0 || buf[i - 1] == '\n') && buf[i] == '>') nseq++;
+  int nseq = len > 0 && buf[0] == '>';
+#pragma omp parallel for schedule(static) reduction(+ : nseq) if (len > ((size_t)64 << 20))
+  for (int64_t i = 1; i < (int64_t)len; ++i)
+    if (buf[i] == '>' && buf[i - 1] == '\n') nseq++;
   int headerless = nseq == 0;
   if (headerless) nseq = 1;
   out->names = calloc((size_t)nseq, sizeof(char *));
@@ -184,15 +185,12 @@ int sh_load_reference(const char *path, int colour, int ignore_lowercase, sh_ref
       if (out->names[s][0] == '=' || out->names[s][0] == '*') out->names[s][0] = '-';
       p = (e < len) ? e + 1 : e;
     }
-    /* measure */
-    size_t q = p;
+    /* measure: the symbols up to the next '>' that are not spaces */
+    const char *hq = memchr(buf + p, '>', len - p);
+    const size_t q = hq ? (size_t)(hq - buf) : len;
     int64_t size = 0;
-    while (q < len) {
-      const int k = cls[(unsigned char)buf[q]];
-      if (k == REF_HEADER) break;
-      q++;
-      size += k != REF_SPACE;
-    }
+#pragma omp parallel for schedule(static) reduction(+ : size) if (q - p > ((size_t)64 << 20))
+    for (int64_t u = (int64_t)p; u < (int64_t)q; ++u) size += cls[(unsigned char)buf[u]] != REF_SPACE;
     if (size == 0) break; /* reference_data.c:67-70, load_reference_db:241-246 */
     int64_t nbytes = (size + 3) / 4 + 1;
     int64_t tot = nbytes + 2 * SH_PAD_BYTES;
