@@ -44,6 +44,11 @@ static inline int quality_level(int q) {
   return i;
 }
 
+/* inputs at least this large take the threaded paths of the loaders (a file read by ranges,
+ * line starts and sequence measures by threads, a reference sequence filled by threads) */
+static size_t g_parallel_min = (size_t)64 << 20;
+void sh_set_parallel_min_bytes(size_t bytes) { g_parallel_min = bytes; }
+
 static inline void put2(uint8_t *p, int64_t i, int v) {
   p[i >> 2] = (uint8_t)(p[i >> 2] | ((v & 3) << ((i & 3) << 1)));
 }
@@ -61,7 +66,7 @@ static char *slurp(const char *path, size_t *len, int *oom) {
   if (fstat(fileno(f), &st) == 0 && S_ISREG(st.st_mode) && st.st_size > 0) cap = (size_t)st.st_size + 1;
   char *buf = malloc(cap + 1);
   if (!buf) { fclose(f); *oom = 1; return NULL; }
-  if (cap > ((size_t)64 << 20)) {
+  if (cap > g_parallel_min && cap > 1) {
     /* a large regular file: the threads read equal ranges of it (the copy out of the page cache
      * and the buffer's first touch in parallel); the file's end is then confirmed as below */
     const size_t size = cap - 1;
@@ -120,11 +125,144 @@ static int grow_regions(int32_t **rs, int32_t **re, int32_t *cap) {
   return 0;
 }
 
+enum { REF_SPACE = 4, REF_HEADER = 5, REF_OTHER = 6 };
+
+/* One reference sequence, the symbols of buf[p, q) (size of them not spaces), filled by threads
+ * exactly as the one-pass loop of sh_load_reference fills it: every byte range counts its
+ * symbols, masked symbols and last base first; the masked symbols' rand() & 3 codes are drawn
+ * in order beforehand (nucleotide); the ranges then write their codes (whole bytes directly, the
+ * bytes shared with a neighbour by atomic OR) and their masked runs, which are joined in order.
+ * Symbol j is output position j, or j - 1 in colour space, where the first symbol only gives the
+ * first base.  Returns 0, or 1 when memory runs out. */
+typedef struct ref_range {
+  size_t lo, hi;
+  int64_t nsym, noth, nseg, sym0, oth0, seg0;
+  int last, carry;  /* last base code of the range (-1: none); the code before the range */
+} ref_range;
+
+static int fill_sequence_threads(const char *buf, size_t p, size_t q, const uint8_t cls[256], int colour,
+                                 int64_t size, uint8_t *cd, uint8_t *mk, uint8_t *first_base, int32_t **rs,
+                                 int32_t **re, int32_t *rcap, int32_t *nr) {
+  int nc = 1;
+#ifdef _OPENMP
+  nc = omp_get_max_threads();
+#endif
+  nc = nc < 1 ? 1 : nc > 256 ? 256 : nc;
+  ref_range *rg = calloc((size_t)nc, sizeof(ref_range));
+  if (!rg) return 1;
+  for (int c = 0; c < nc; ++c) {
+    rg[c].lo = p + (q - p) * (size_t)c / (size_t)nc;
+    rg[c].hi = p + (q - p) * (size_t)(c + 1) / (size_t)nc;
+  }
+#pragma omp parallel for schedule(static) num_threads(nc)
+  for (int c = 0; c < nc; ++c) {
+    int64_t ns = 0, no = 0, nseg = 0;
+    int last = -1, in_run = 0;
+    for (size_t u = rg[c].lo; u < rg[c].hi; ++u) {
+      const int k = cls[(unsigned char)buf[u]];
+      if (k == REF_SPACE) continue;
+      ns++;
+      if (k == REF_OTHER) { no++; nseg += !in_run; in_run = 1; }
+      else { last = k; in_run = 0; }
+    }
+    rg[c].nsym = ns; rg[c].noth = no; rg[c].nseg = nseg; rg[c].last = last;
+  }
+  int64_t sym = 0, oth = 0, seg = 0;
+  int carry = 0;
+  for (int c = 0; c < nc; ++c) {
+    rg[c].sym0 = sym; rg[c].oth0 = oth; rg[c].seg0 = seg; rg[c].carry = carry;
+    sym += rg[c].nsym; oth += rg[c].noth; seg += rg[c].nseg;
+    if (rg[c].last >= 0) carry = rg[c].last;
+  }
+  uint8_t *rnd = colour || oth == 0 ? NULL : malloc((size_t)oth);
+  int64_t *sj0 = malloc(sizeof(int64_t) * (size_t)(seg ? seg : 1)), *sj1 = malloc(sizeof(int64_t) * (size_t)(seg ? seg : 1));
+  if ((!colour && oth && !rnd) || !sj0 || !sj1) { free(rnd); free(sj0); free(sj1); free(rg); return 1; }
+  for (int64_t u = 0; rnd && u < oth; ++u) rnd[u] = (uint8_t)(rand() & 3);  /* in the loop's order */
+#pragma omp parallel for schedule(static) num_threads(nc)
+  for (int c = 0; c < nc; ++c) {
+    int64_t j = rg[c].sym0, o = rg[c].oth0, sg = rg[c].seg0;
+    int code_prev = rg[c].carry, in_run = 0;
+    /* the output positions of the range: [ilo, ihi) */
+    const int64_t ilo = colour ? (j > 0 ? j - 1 : 0) : j;
+    const int64_t ihi = colour ? (j + rg[c].nsym > 0 ? j + rg[c].nsym - 1 : 0) : j + rg[c].nsym;
+    int64_t cur = -1;
+    unsigned cacc = 0, macc = 0;
+#define SH_FLUSH()                                                                                 \
+    do {                                                                                           \
+      if (cur >= 0) {                                                                              \
+        if (4 * cur >= ilo && 4 * cur + 4 <= ihi) cd[cur] = (uint8_t)cacc;                        \
+        else if (cacc) __atomic_fetch_or(&cd[cur], (uint8_t)cacc, __ATOMIC_RELAXED);               \
+        if (macc) __atomic_fetch_or(&mk[cur], (uint8_t)macc, __ATOMIC_RELAXED);                    \
+      }                                                                                            \
+    } while (0)
+    for (size_t u = rg[c].lo; u < rg[c].hi; ++u) {
+      const int k = cls[(unsigned char)buf[u]];
+      if (k == REF_SPACE) continue;
+      const int64_t i = colour ? (j > 0 ? j - 1 : 0) : j;
+      if ((i >> 2) != cur) {
+        SH_FLUSH();
+        cur = i >> 2;
+        cacc = macc = 0;
+      }
+      int code;
+      if (k == REF_OTHER) {
+        code = colour ? code_prev : rnd[o++];
+        if (!in_run) { sj0[sg] = j; sj1[sg] = -1; sg++; in_run = 1; }
+        macc |= 1u << ((i & 3) << 1);
+      } else {
+        code = k;
+        if (in_run) { sj1[sg - 1] = j; in_run = 0; }
+      }
+      if (colour && j == 0) {
+        *first_base = (uint8_t)code;
+        code_prev = code;
+        j++;
+        continue;
+      }
+      cacc |= (unsigned)(colour ? code_prev ^ code : code) << ((i & 3) << 1);
+      code_prev = code;
+      j++;
+    }
+    SH_FLUSH();
+#undef SH_FLUSH
+  }
+  /* the masked runs in order, a run open at the end of a range joined with the next range's */
+  const int64_t total = sym;
+  int64_t open = -1;
+  int rc = 0;
+  for (int c = 0; c < nc && !rc; ++c) {
+    if (rg[c].nsym == 0) continue;
+    int64_t s0 = rg[c].seg0, s1 = rg[c].seg0 + rg[c].nseg;
+    int cont = open >= 0 && s0 < s1 && sj0[s0] == rg[c].sym0;
+    if (open >= 0 && !cont) {
+      const int64_t a = colour ? (open > 0 ? open - 1 : 0) : open, b = colour ? rg[c].sym0 - 1 : rg[c].sym0;
+      if (*nr == *rcap && grow_regions(rs, re, rcap)) { rc = 1; break; }
+      (*rs)[*nr] = (int32_t)a; (*re)[*nr] = (int32_t)b; (*nr)++;
+      open = -1;
+    }
+    for (int64_t g = s0; g < s1; ++g) {
+      const int64_t start = (g == s0 && cont) ? open : sj0[g];
+      open = -1;
+      if (sj1[g] < 0) { open = start; continue; }
+      const int64_t a = colour ? (start > 0 ? start - 1 : 0) : start, b = colour ? sj1[g] - 1 : sj1[g];
+      if (*nr == *rcap && grow_regions(rs, re, rcap)) { rc = 1; break; }
+      (*rs)[*nr] = (int32_t)a; (*re)[*nr] = (int32_t)b; (*nr)++;
+    }
+  }
+  if (!rc && open >= 0) {
+    const int64_t a = colour ? (open > 0 ? open - 1 : 0) : open, b = colour ? (total > 0 ? total - 1 : 0) : total;
+    if (*nr == *rcap && grow_regions(rs, re, rcap)) rc = 1;
+    else { (*rs)[*nr] = (int32_t)a; (*re)[*nr] = (int32_t)b; (*nr)++; }
+  }
+  (void)size;
+  free(rnd); free(sj0); free(sj1); free(rg);
+  return rc;
+}
+
 /* reference_data.c:14-190: one FASTA chunk per '>' header; whitespace skipped; letters
  * upper-cased unless -j; non-ACGT letters are masked and coded rand()&3 (nucleotide) or as
  * the previous base (colour); colour space stores the XOR of consecutive bases and keeps
  * the first base apart; masked regions are the maximal runs of masked codes. */
-enum { REF_SPACE = 4, REF_HEADER = 5, REF_OTHER = 6 };
 
 /* Class of each input byte: 0-3 the base (upper-cased first unless -j), REF_SPACE (isspace),
  * REF_HEADER ('>'), REF_OTHER (masked). */
@@ -146,7 +284,7 @@ int sh_load_reference(const char *path, int colour, int ignore_lowercase, sh_ref
   if (!buf) return read_failed(oom, path, "reference sequence");
   /* count chunks: lines starting with '>' (reference_data.c:210-220) */
   int nseq = len > 0 && buf[0] == '>';
-#pragma omp parallel for schedule(static) reduction(+ : nseq) if (len > ((size_t)64 << 20))
+#pragma omp parallel for schedule(static) reduction(+ : nseq) if (len > g_parallel_min)
   for (int64_t i = 1; i < (int64_t)len; ++i)
     if (buf[i] == '>' && buf[i - 1] == '\n') nseq++;
   int headerless = nseq == 0;
@@ -189,7 +327,7 @@ int sh_load_reference(const char *path, int colour, int ignore_lowercase, sh_ref
     const char *hq = memchr(buf + p, '>', len - p);
     const size_t q = hq ? (size_t)(hq - buf) : len;
     int64_t size = 0;
-#pragma omp parallel for schedule(static) reduction(+ : size) if (q - p > ((size_t)64 << 20))
+#pragma omp parallel for schedule(static) reduction(+ : size) if (q - p > g_parallel_min)
     for (int64_t u = (int64_t)p; u < (int64_t)q; ++u) size += cls[(unsigned char)buf[u]] != REF_SPACE;
     if (size == 0) break; /* reference_data.c:67-70, load_reference_db:241-246 */
     int64_t nbytes = (size + 3) / 4 + 1;
@@ -208,6 +346,16 @@ int sh_load_reference(const char *path, int colour, int ignore_lowercase, sh_ref
     int64_t i = 0, mstart = -1;
     int code_prev = 0, have_first = 0;
     unsigned cacc = 0; /* the codes of the byte being filled */
+    if (q - p > g_parallel_min) {
+      if (fill_sequence_threads(buf, p, q, cls, colour, size, cd, mk, &out->first_base[s], &rs, &re, &rcap, &nr)) {
+        free(ca); free(ma); free(rs); free(re); free(buf);
+        out->n = s + 1;
+        sh_free_reference(out);
+        return fail(STORMGPU_ENOMEM, "Not enough memory for the reference sequences.");
+      }
+      i = colour ? (size > 0 ? size - 1 : 0) : size;
+      p = q;
+    }
     while (p < len) {
       const int k = cls[(unsigned char)buf[p]];
       if (k == REF_HEADER) break;
@@ -242,7 +390,7 @@ int sh_load_reference(const char *path, int colour, int ignore_lowercase, sh_ref
       i++;
       code_prev = code;
     }
-    if (i & 3) cd[i >> 2] = (uint8_t)cacc;
+    if ((i & 3) && cacc) cd[i >> 2] = (uint8_t)cacc;
     if (mstart != -1) {
       if (nr == rcap && grow_regions(&rs, &re, &rcap)) {
         free(ca); free(ma); free(rs); free(re); free(buf);
@@ -488,7 +636,7 @@ static int line_starts(const char *buf, size_t len, size_t from, size_t **out, i
 #ifdef _OPENMP
   nt = omp_get_max_threads();
 #endif
-  if (len - from < ((size_t)1 << 20)) nt = 1;
+  if (len - from < g_parallel_min / 64) nt = 1;
   if (nt > 256) nt = 256;
   int64_t cnt[257] = {0};
   /* '\n' at p, with p + 1 < len, in thread t's range [lo, hi) */

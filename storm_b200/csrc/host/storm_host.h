@@ -60,6 +60,9 @@ typedef struct sh_reads {
 
 /* Status: 0 ok, negative on error (message in sh_last_error()). */
 const char *sh_last_error(void);
+/* Inputs of at least `bytes` take the loaders' threaded paths (default 64 MiB; the results do
+ * not depend on it). */
+void sh_set_parallel_min_bytes(size_t bytes);
 /* 1 when the last error's message is the reference's whole message for a failure it reports
  * and exits on (print it alone), 0 when the caller adds its own line as the reference does */
 int sh_last_error_final(void);

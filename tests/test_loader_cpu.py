@@ -41,3 +41,64 @@ def test_large_file_loads_like_its_halves(tmp_path, colour):
         assert np.array_equal(got, want), field
     assert np.array_equal(whole.lengths, np.concatenate([a.lengths, b.lengths]))
     assert np.array_equal(whole.first_levels, np.concatenate([a.first_levels, b.first_levels]))
+
+
+def _refs_snapshot(ref):
+    import ctypes as C
+    s = ref._s
+    out = []
+    for k in range(s.n):
+        size = int(s.sizes[k])
+        nb = (size + 3) // 4 + 4
+        rs = C.cast(s.rs[k], C.POINTER(C.c_int32))
+        re_ = C.cast(s.re[k], C.POINTER(C.c_int32))
+        regions = [(rs[r], re_[r]) for r in range(int(s.nreg[k]))]
+        out.append((s.names[k], size, C.string_at(s.codes[k], nb), C.string_at(s.masks[k], nb), regions,
+                    int(s.first_base[k])))
+    return out
+
+
+def _random_fasta(rng, nseq):
+    parts = []
+    for k in range(nseq):
+        n = int(rng.integers(1, 40000)) if k else int(rng.integers(20000, 60000))
+        seq = np.frombuffer(b"ACGTacgt", np.uint8)[rng.integers(0, 8, size=n)].copy()
+        for _ in range(int(rng.integers(0, 12))):  # masked runs: N, other letters, at either end too
+            a = int(rng.integers(0, n))
+            b = min(n, a + int(rng.integers(1, 3000)))
+            seq[a:b] = np.frombuffer(b"NNNNRYn-", np.uint8)[rng.integers(0, 8, size=b - a)]
+        if rng.random() < 0.3:
+            seq[0] = ord("N")
+        text = bytearray()
+        u = 0
+        while u < n:
+            w = int(rng.integers(1, 120))
+            text += seq[u:u + w].tobytes()
+            u += w
+            text += b"\r\n" if rng.random() < 0.1 else b" \t\n" if rng.random() < 0.05 else b"\n"
+        parts.append(b">seq%d some text\n" % k + bytes(text))
+    return b"".join(parts)
+
+
+@pytest.mark.parametrize("colour,ignore_lowercase,seed", [(0, 0, 1), (0, 1, 2), (1, 0, 3), (1, 1, 4), (0, 0, 5)])
+def test_reference_filled_by_threads_like_one_pass(tmp_path, colour, ignore_lowercase, seed):
+    """A reference FASTA loaded with the threaded paths forced on every sequence (read by ranges,
+    headers and sizes counted by threads, codes, masks and masked runs filled by threads, the
+    masked symbols' rand() codes drawn in order) gives what the one-pass loader gives."""
+    import ctypes as C
+    libc = C.CDLL(None)
+    L = host.hostlib()
+    L.sh_set_parallel_min_bytes.argtypes = [C.c_size_t]
+    rng = np.random.default_rng(seed)
+    (tmp_path / "ref.fa").write_bytes(_random_fasta(rng, 5))
+    try:
+        libc.srand(1)
+        one = _refs_snapshot(host.Reference(str(tmp_path / "ref.fa"), colour, ignore_lowercase))
+        L.sh_set_parallel_min_bytes(1)
+        libc.srand(1)
+        threads = _refs_snapshot(host.Reference(str(tmp_path / "ref.fa"), colour, ignore_lowercase))
+    finally:
+        L.sh_set_parallel_min_bytes(64 << 20)
+    assert len(one) == 5 and sum(len(r[4]) for r in one) > 5
+    for a, b in zip(one, threads):
+        assert a == b
