@@ -102,3 +102,44 @@ def test_reference_filled_by_threads_like_one_pass(tmp_path, colour, ignore_lowe
     assert len(one) == 5 and sum(len(r[4]) for r in one) > 5
     for a, b in zip(one, threads):
         assert a == b
+
+
+@pytest.mark.parametrize("layout", ["plain", "crlf", "comments", "cut_short", "corrupt"])
+def test_reads_loaded_by_threads_like_one_pass(tmp_path, layout):
+    """A FASTQ file loaded with the threaded paths forced (read by ranges, line starts found by
+    threads) gives the one-pass loader's reads, or its error message and line number."""
+    import ctypes as C
+    L = host.hostlib()
+    L.sh_set_parallel_min_bytes.argtypes = [C.c_size_t]
+    genome = synth.make_genome([30000], 71)
+    seqs, quals = synth.simulate_nucleotide_reads(genome, 3000, [35, 50, 100], 72)
+    synth.write_fastq(str(tmp_path / "r.fq"), seqs, quals)
+    lines = (tmp_path / "r.fq").read_bytes().split(b"\n")
+    if layout == "crlf":
+        lines = [l + b"\r" if l else l for l in lines]
+    elif layout == "comments":
+        lines = [b"# Title: threads", b"# comment"] + lines
+    elif layout == "cut_short":
+        lines = lines[:-2]
+    elif layout == "corrupt":
+        lines[4 * 2345 + 2] = b"x"
+    (tmp_path / "r.fq").write_bytes(b"\n".join(lines))
+
+    def load():
+        try:
+            r = host.ReadSet(str(tmp_path / "r.fq"), 0, sort=True)
+        except Exception as e:  # the loader's message
+            return str(e)
+        return (r.n, r.codes.tobytes(), None if r.levels is None else r.levels.tobytes(), r.lengths.tobytes())
+
+    try:
+        one = load()
+        L.sh_set_parallel_min_bytes(1)
+        threads = load()
+    finally:
+        L.sh_set_parallel_min_bytes(64 << 20)
+    assert one == threads
+    if layout == "corrupt":
+        assert "line %d" % (4 * 2345 + 3) in one
+    else:
+        assert one[0] == 3000
