@@ -769,6 +769,82 @@ static int load_fastq(const char *path, int colour, int quality_base, int allow_
  * Quality lines are the quality file's lines that are neither comments nor headers, one per read
  * in order; a short line keeps the values of the previous read for the missing positions (the
  * reference parses into one buffer reused across reads, load_data.c:15-33). */
+/* The quality file of a FASTA / CSFASTA read set (reads_data.c:73-345): its lines that are
+ * neither empty, comments nor headers, one per read in order, each a list of integers split on
+ * spaces; a short line keeps, for the positions it lacks, the values of the reads before it (the
+ * reference parses into one buffer kept across reads, load_data.c:15-33).  Lines are found and
+ * parsed by threads, the positions a short line lacks then taken from the latest read before it
+ * that had them, and the levels written by threads.  out->levels is allocated (zeroed).  Returns
+ * 0, or 1 when memory runs out. */
+static int parse_quality_lines(const char *qb, size_t qlen, int colour, sh_reads *out, int64_t n) {
+  if (!out->levels) return 1;
+  size_t *qls = NULL;
+  int64_t nql = 0;
+  if (line_starts(qb, qlen, 0, &qls, &nql)) return 1;
+  const size_t qend = qlen > 0 && qb[qlen - 1] == '\n' ? qlen - 1 : qlen;
+  int64_t *keep = malloc(sizeof(int64_t) * (size_t)(n ? n : 1));
+  if (!keep) { free(qls); return 1; }
+  int64_t nq = 0;
+  size_t maxll = 0;
+  for (int64_t t = 0; t < nql && nq < n; ++t) {
+    const char *line = qb + qls[t];
+    const size_t ll = (t + 1 < nql ? qls[t + 1] - 1 : qend) - qls[t];
+    if (ll == 0 || line[0] == '\r' || line[0] == '#' || line[0] == '>') continue;
+    keep[nq++] = t;
+    if (ll > maxll) maxll = ll;
+  }
+  const int need = out->max_len + (colour ? 1 : 0);
+  short *pv = malloc(sizeof(short) * (size_t)(nq ? nq : 1) * (size_t)(need ? need : 1));
+  int *pc = malloc(sizeof(int) * (size_t)(nq ? nq : 1));
+  int nomem = !pv || !pc;
+#pragma omp parallel reduction(|| : nomem)
+  {
+    char *tmp = nomem ? NULL : malloc(maxll + 1);
+    if (!tmp) nomem = 1;
+#pragma omp for schedule(static)
+    for (int64_t i = 0; i < nq; ++i) {
+      if (!tmp) continue;
+      const int64_t t = keep[i];
+      const size_t ll = (t + 1 < nql ? qls[t + 1] - 1 : qend) - qls[t];
+      memcpy(tmp, qb + qls[t], ll);
+      tmp[ll] = 0;
+      const int want = out->lengths[i] + (colour ? 1 : 0);
+      short *row = pv + (size_t)i * (size_t)need;
+      char *save = NULL, *tok = strtok_r(tmp, " ", &save);
+      int j = 0;
+      for (; j < want && tok; ++j, tok = strtok_r(NULL, " ", &save)) row[j] = (short)atoi(tok);
+      pc[i] = j;
+    }
+    free(tmp);
+  }
+  int64_t short_lines = 0;
+  for (int64_t i = 0; !nomem && i < nq; ++i) short_lines += pc[i] < out->lengths[i] + (colour ? 1 : 0);
+  if (!nomem && short_lines) {
+    /* the positions a short line lacks: the buffer's value then, the reads replayed in order */
+    short *qv = calloc((size_t)need + 1, sizeof(short));
+    if (!qv) nomem = 1;
+    for (int64_t i = 0; qv && i < nq; ++i) {
+      const int want = out->lengths[i] + (colour ? 1 : 0);
+      short *row = pv + (size_t)i * (size_t)need;
+      for (int j = pc[i]; j < want; ++j) row[j] = qv[j];
+      memcpy(qv, row, sizeof(short) * (size_t)pc[i]);
+    }
+    free(qv);
+  }
+  if (!nomem) {
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < nq; ++i) {
+      const int L = out->lengths[i];
+      const short *row = pv + (size_t)i * (size_t)need;
+      uint8_t *lv = out->levels + i * out->level_stride;
+      if (colour) out->first_level[i] = (uint8_t)quality_level(row[0]);
+      for (int k = 0; k < L; ++k) put2(lv, k, quality_level(row[k + (colour ? 1 : 0)]));
+    }
+  }
+  free(pv); free(pc); free(keep); free(qls);
+  return nomem;
+}
+
 static int load_fasta(const char *path, const char *qual_path, int colour, int allow_mixed, sh_reads *out) {
   size_t len;
   int oom;
@@ -854,30 +930,7 @@ static int load_fasta(const char *path, const char *qual_path, int colour, int a
     else {
       out->has_quality = 1;
       out->levels = calloc((size_t)n, (size_t)out->level_stride);
-      const int need = out->max_len + (colour ? 1 : 0);
-      short *qv = calloc((size_t)need + 1, sizeof(short));  /* kept across reads */
-      size_t qp = 0;
-      int64_t i = 0;
-      char *tmp = malloc(qlen + 1);
-      if (!out->levels || !qv || !tmp) {
-        rc = fail(STORMGPU_ENOMEM, "Not enough memory to read %s.", qual_path);
-        i = n;  /* nothing is parsed */
-      }
-      while (i < n && next_line(qb, qlen, &qp, &line, &ll)) {
-        if (ll == 0 || line[0] == '\r' || line[0] == '#' || line[0] == '>') continue;
-        memcpy(tmp, line, ll);
-        tmp[ll] = 0;
-        const int L = out->lengths[i];
-        const int want = L + (colour ? 1 : 0);
-        char *save = NULL, *tok = strtok_r(tmp, " ", &save);
-        for (int j = 0; j < want && tok; ++j, tok = strtok_r(NULL, " ", &save)) qv[j] = (short)atoi(tok);
-        uint8_t *lv = out->levels + i * out->level_stride;
-        if (colour) out->first_level[i] = (uint8_t)quality_level(qv[0]);
-        for (int k = 0; k < L; ++k) put2(lv, k, quality_level(qv[k + (colour ? 1 : 0)]));
-        i++;
-      }
-      free(tmp);
-      free(qv);
+      rc = parse_quality_lines(qb, qlen, colour, out, n) ? fail(STORMGPU_ENOMEM, "Not enough memory to read %s.", qual_path) : 0;
       free(qb);
     }
   }

@@ -208,7 +208,7 @@ def test_fasta_reads(tmp_path):
 @pytest.mark.parametrize("with_qual", [True, False])
 def test_csfasta_reads(tmp_path, with_qual):
     """Colour reads as CSFASTA (primer base + colours), with the qualities in a .qual file of
-    integers (-q): comments and headers there too, a negative value, and one short line."""
+    integers (-q): comments and headers there too, a negative value, and short lines."""
     genome = synth.make_genome([40000], 19)
     synth.write_fasta(str(tmp_path / "ref.fa"), genome)
     pr, cols, q = synth.simulate_colour_reads(genome, 1500, 50, 20)
@@ -224,6 +224,10 @@ def test_csfasta_reads(tmp_path, with_qual):
                 v[5] = -1
             if k == 77:
                 v = v[:30]  # short line: the rest keeps the previous read's values
+            if k % 7 in (5, 6):
+                v = v[:len(v) - 1 - k % 5]  # more short lines, two in a row
+            if k % 97 == 11:
+                v = v[:3]
             f.write(b">r%d_F3\n%s\n" % (k, b" ".join(b"%d" % x for x in v)))
     args = ["-M", "2", "-z", "90", "-t", "100", "-i", "5"] + (["-q", "reads.qual"] if with_qual else [])
     lines = run_pair(str(tmp_path), 1, args, reads="reads.csfasta")
